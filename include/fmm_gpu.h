@@ -1,0 +1,170 @@
+/* fmm_gpu.h — C ABI of the B200 FMM force evaluator (libfmmgpu.so).
+ *
+ * Drop-in boundary for the force pass of rezucch1/nbody-FMM.  The reference's
+ * interface is the C++ virtual
+ *     SystemUpdateMethod::update(const std::vector<Particle>&)
+ *         (src/system_updaters/system_update_method.hpp:24-31)
+ * implemented by FMM (src/system_updaters/FMM.cpp:9-12) and NaiveUpdate
+ * (src/system_updaters/naive_update.cpp:9-35), and called by
+ *     QuadratureMethod::integrate(SystemUpdateMethod*, std::vector<Particle>&, const double&)
+ *         (src/quadratures/quadrature_method.hpp:24).
+ * A reference-side adapter packs the particles into plain arrays and calls
+ * the entry points below (the adapter is shown in INTEGRATION.md and shipped
+ * as nbody-fmm_b200/cpp/gpu_fmm.hpp).
+ *
+ * Conventions:
+ *  - positions / velocities / accelerations are row-major n x dim FP64
+ *    (x0 y0 z0 x1 ...), masses n FP64; all host pointers are caller-owned;
+ *  - accelerations follow the reference: a_i = G * grad_i with
+ *      3D grad_i = -sum_j m_j (x_i - x_j) / |x_i - x_j|^3     (leaf.cpp:118-142)
+ *      2D grad_i = -sum_j m_j (x_i - x_j) / |x_i - x_j|^2     (leaf.cpp:81-95)
+ *    and Particle::compute_new_accelaration (particle.cpp:16-21) multiplying by G;
+ *  - optional potential output: G * phi, phi_i = sum_j m_j/|d| (3D),
+ *    -sum_j m_j log|d| (2D), so that grad = nabla phi;
+ *  - every call returns FMM_OK (0) or a negative FMM_ERR_* code; no C++
+ *    exception crosses the ABI; fmm_strerror() describes a code;
+ *  - one context per host thread; calls on a context are stream-ordered on
+ *    the context's stream (or the stream passed to the *_device calls).
+ */
+#ifndef FMM_GPU_H
+#define FMM_GPU_H
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FMM_API __attribute__((visibility("default")))
+#else
+#define FMM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  FMM_OK = 0,
+  FMM_ERR_INVALID_ARGUMENT = -1,
+  FMM_ERR_CUDA = -2,
+  FMM_ERR_OUT_OF_MEMORY = -3,
+  FMM_ERR_NONFINITE_INPUT = -4,   /* NaN/Inf position or mass */
+  FMM_ERR_NONFINITE_OUTPUT = -5,  /* e.g. coincident particles, as the reference divides by zero */
+  FMM_ERR_UNSUPPORTED = -6,
+  FMM_ERR_TIMEOUT = -7,
+  FMM_ERR_NO_DEVICE = -8,
+  FMM_ERR_INTERNAL = -9
+};
+
+/* M2L arithmetic. */
+enum {
+  FMM_M2L_FP32 = 0,  /* SIMT FP32 batched contraction (plain GPU FMM) */
+  FMM_M2L_TC = 1     /* tcgen05 tensor-core contraction, split precision */
+};
+
+/* Direct-sum softening forms. */
+enum {
+  FMM_SOFT_PLUMMER = 0,   /* r^2 -> r^2 + eps2 in every kernel */
+  FMM_SOFT_NAIVE_REF = 1  /* NaiveUpdate's form: 3D m d/((r^2+1e-4) r), 2D m d/(r^2+1e-4) (naive_update.cpp:19-30) */
+};
+
+/* Integrators (src/quadratures/). */
+enum {
+  FMM_INT_SYMPLECTIC_EULER = 0, /* SyplecticEuler::integrate, symplectic_euler.cpp:8-15 */
+  FMM_INT_RK4 = 1               /* classical RK4 (RungeKutta4, runge_kutta_4.cpp:10-93, intends this) */
+};
+
+typedef struct fmm_config {
+  int32_t dim;        /* 2 or 3 (Tensor::dim of the particles) */
+  int32_t p;          /* expansion order; the reference hard-codes L = 2 (tree.cpp:94) */
+  int32_t leaf_cap;   /* leaf threshold; the reference hard-codes 20 (tree.cpp:32) */
+  int32_t m2l_mode;   /* FMM_M2L_* */
+  double eps2;        /* softening added to r^2 in the near field (0: the reference FMM) */
+  double G;           /* gravitational constant; reference 6.6743e-11 (system_update_method.hpp:17) */
+  int32_t device;     /* CUDA device ordinal */
+  int32_t reserved[7];
+} fmm_config;
+
+typedef struct fmm_stats {
+  int32_t depth;            /* leaf depth of the last tree */
+  int32_t n_levels;
+  int64_t n_leaves;
+  int64_t n_cells;          /* all levels */
+  int64_t m2l_pairs;        /* interaction-list pairs evaluated by M2L */
+  int64_t p2p_pairs;        /* particle pairs evaluated directly */
+  double ms_tree;           /* device time of the tree build */
+  double ms_upward;         /* P2M + M2M */
+  double ms_m2l;
+  double ms_downward;       /* L2L + L2P */
+  double ms_p2p;
+  double ms_total;          /* whole force pass (device time) */
+  double reserved[6];
+} fmm_stats;
+
+typedef struct fmm_ctx fmm_ctx;
+
+FMM_API const char *fmm_strerror(int code);
+FMM_API const char *fmm_version(void);
+
+/* Defaults: dim 3, p 8, leaf_cap 64, FP32 M2L, eps2 0, G 1, device 0. */
+FMM_API int fmm_config_default(fmm_config *cfg);
+
+/* Creates a context (allocates device workspace lazily, grown on demand). */
+FMM_API int fmm_create(const fmm_config *cfg, fmm_ctx **out);
+FMM_API int fmm_destroy(fmm_ctx *ctx);
+
+/* One FMM force pass from host buffers: replaces FMM::update
+ * (FMM.cpp:9-12) — builds the tree (Tree::init_tree, tree.cpp:15-91) and runs
+ * P2M, M2M, M2L, L2L, L2P and P2P (tree.cpp:93-111).  acc: n x dim, pot
+ * nullable.  Synchronous. */
+FMM_API int fmm_evaluate(fmm_ctx *ctx, int64_t n, const double *pos, const double *mass, double *acc, double *pot);
+
+/* The same pass on device-resident buffers, ordered on `stream`
+ * (a cudaStream_t; NULL = the context's stream).  Returns after enqueueing
+ * the work; call fmm_synchronize() before reading the results or the status
+ * of the device-side checks. */
+FMM_API int fmm_evaluate_device(fmm_ctx *ctx, int64_t n, const double *d_pos, const double *d_mass, double *d_acc,
+                        double *d_pot, void *stream);
+FMM_API int fmm_synchronize(fmm_ctx *ctx);
+
+/* FP64 O(N^2) direct sum on the GPU for `ntargets` target indices (all if
+ * targets is NULL): replaces NaiveUpdate::update (naive_update.cpp:9-35)
+ * when soft_mode is FMM_SOFT_NAIVE_REF; otherwise the Plummer form with
+ * cfg.eps2.  Host buffers; acc is ntargets x dim. */
+FMM_API int fmm_direct(fmm_ctx *ctx, int64_t n, const double *pos, const double *mass, int64_t ntargets,
+               const int64_t *targets, int32_t soft_mode, double *acc, double *pot);
+FMM_API int fmm_direct_device(fmm_ctx *ctx, int64_t n, const double *d_pos, const double *d_mass, int64_t ntargets,
+                      const int64_t *d_targets, int32_t soft_mode, double *d_acc, double *d_pot, void *stream);
+
+/* Advances pos/vel (host, n x dim, in place) by `steps` steps of `method`
+ * with time step dt, the state staying on the device between steps:
+ * replaces QuadratureMethod::integrate with an FMM update method
+ * (symplectic_euler.cpp:8-15; runge_kutta_4.cpp:10-93).  acc_out (nullable)
+ * receives the acceleration of the last force evaluation. */
+FMM_API int fmm_integrate(fmm_ctx *ctx, int32_t method, double dt, int32_t steps, int64_t n, double *pos, double *vel,
+                  const double *mass, double *acc_out);
+
+/* Tree export, for bit-exact comparison with Tree::init_tree (tree.cpp:15-91).
+ * fmm_tree_build builds the tree of `pos` (host) and keeps it; the getters
+ * copy it out.  Leaves are in ascending key order, each leaf's particles in
+ * input order (tree.cpp:62-66); perm[start[i]..start[i+1]) are the indices
+ * of leaf i.  Level d keys are ascending. */
+FMM_API int fmm_tree_build(fmm_ctx *ctx, int64_t n, const double *pos);
+FMM_API int fmm_tree_depth(fmm_ctx *ctx, int32_t *depth);
+FMM_API int fmm_tree_level_size(fmm_ctx *ctx, int32_t level, int64_t *count);
+FMM_API int fmm_tree_level_keys(fmm_ctx *ctx, int32_t level, uint64_t *keys);
+FMM_API int fmm_tree_leaves(fmm_ctx *ctx, uint64_t *keys, int64_t *start, int64_t *perm);
+/* Neighbour (kind 0, |delta| <= 1, self excluded) or interaction (kind 1)
+ * list pairs of level d as (target key, source key): the lists of
+ * NodeI::compute_interaction_list (node_i.cpp:23-99).  With tkey == NULL
+ * only *count is set. */
+FMM_API int fmm_tree_pairs(fmm_ctx *ctx, int32_t level, int32_t kind, int64_t *count, uint64_t *tkey, uint64_t *skey);
+
+/* Statistics of the last force pass (per-phase device times, sizes). */
+FMM_API int fmm_last_stats(fmm_ctx *ctx, fmm_stats *out);
+
+/* Number of kernel launches the library issued since the context was
+ * created (all entry points). */
+FMM_API int64_t fmm_launch_count(fmm_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FMM_GPU_H */

@@ -1,0 +1,40 @@
+// Expansion passes (P2M, M2M, M2L, L2L, L2P) and the near field.
+#pragma once
+#include "tree.cuh"
+
+namespace fmm {
+
+// Operator tables in the layout the contraction kernels read: for each slot a
+// K x KP matrix stored input-major (entry [in][out]); KP = 32 * ceil(K/32),
+// padded with zeros.  Slots: M2L 343 relative offsets (7^3, index
+// (dx+3) + 7(dy+3) + 49(dz+3); |d| <= 1 rows are zero), then 8 M2M and 8 L2L
+// child slots.  2D: 49 offsets, 4 + 4 child slots.
+struct OpTables {
+  int dim = 3, p = 0, K = 0, KP = 0, KS = 0;
+  int n_m2l = 0, off_m2m = 0, off_l2l = 0, n_slots = 0;
+  DevBuf<float> tab;        // n_slots * K * KP
+  DevBuf<double> scratch;   // FP64 staging
+};
+
+struct ExpBuffers {
+  DevBuf<float> M, L;  // n_cells * KS each (indexed by absolute cell - cell0)
+  DevBuf<int> tlist;   // class-grouped target cells (levels >= 2)
+  DevBuf<uint64_t> ckey, ckey_alt;  // (level, class) sort keys of those cells
+  DevBuf<uint32_t> cval;
+  DevBuf<int4> batches;
+  DevBuf<uint32_t> cls_count;
+};
+
+// Per-pass parameters.
+struct PassGeom {
+  double lo[3], ext[3], emax;
+};
+
+int build_op_tables(OpTables &ops, int dim, int p, const PassGeom &g, cudaStream_t st, int64_t &launches);
+void upload_class_tables();
+
+int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, int p, double eps2, double G,
+                   const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, cudaStream_t st, fmm_stats &stats,
+                   cudaEvent_t *ev);
+
+}  // namespace fmm

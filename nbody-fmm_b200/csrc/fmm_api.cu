@@ -1,0 +1,420 @@
+// C ABI of libfmmgpu.so (declared in include/fmm_gpu.h).
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "direct.cuh"
+#include "expansions.cuh"
+#include "fmm_gpu.h"
+
+namespace fmm {
+static thread_local std::string g_cuda_err;
+void set_cuda_error(cudaError_t e, const char *what, const char *file, int line) {
+  char buf[512];
+  snprintf(buf, sizeof(buf), "%s (%s) at %s:%d", cudaGetErrorString(e), what, file, line);
+  g_cuda_err = buf;
+}
+const char *last_cuda_error_text() { return g_cuda_err.c_str(); }
+}  // namespace fmm
+
+using namespace fmm;
+
+struct fmm_ctx {
+  fmm_config cfg;
+  cudaStream_t stream = nullptr;
+  Workspace ws;
+  TreeState tree;
+  OpTables ops;
+  ExpBuffers eb;
+  DevBuf<double> d_pos, d_mass, d_acc, d_pot, d_vel, d_x0, d_v0, d_xs, d_vs, d_asum, d_vsum;
+  DevBuf<int64_t> d_targets;
+  fmm_stats stats;
+  cudaEvent_t ev[6] = {};
+  bool timing_pending = false;
+  bool have_tree = false;
+};
+
+static int check_cfg(const fmm_config *c) {
+  if (!c) return FMM_ERR_INVALID_ARGUMENT;
+  if (c->dim != 2 && c->dim != 3) return FMM_ERR_INVALID_ARGUMENT;
+  if (c->p < 0 || c->p > FMM_MAX_P) return FMM_ERR_INVALID_ARGUMENT;
+  if (c->dim == 3 && (c->p + 1) * (c->p + 1) > 192) return FMM_ERR_UNSUPPORTED;  // contraction register tile
+  if (c->leaf_cap < 1) return FMM_ERR_INVALID_ARGUMENT;
+  if (c->m2l_mode != FMM_M2L_FP32 && c->m2l_mode != FMM_M2L_TC) return FMM_ERR_INVALID_ARGUMENT;
+  if (!(c->eps2 >= 0.0)) return FMM_ERR_INVALID_ARGUMENT;
+  return FMM_OK;
+}
+
+extern "C" {
+
+const char *fmm_strerror(int code) {
+  switch (code) {
+    case FMM_OK: return "ok";
+    case FMM_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case FMM_ERR_CUDA: return fmm::last_cuda_error_text()[0] ? fmm::last_cuda_error_text() : "CUDA error";
+    case FMM_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case FMM_ERR_NONFINITE_INPUT: return "non-finite position or mass";
+    case FMM_ERR_NONFINITE_OUTPUT: return "non-finite acceleration (coincident particles?)";
+    case FMM_ERR_UNSUPPORTED: return "unsupported configuration";
+    case FMM_ERR_TIMEOUT: return "device wait timed out";
+    case FMM_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "internal error";
+  }
+}
+
+const char *fmm_version(void) { return "fmmgpu 0.1 (sm_100a)"; }
+
+int fmm_config_default(fmm_config *cfg) {
+  if (!cfg) return FMM_ERR_INVALID_ARGUMENT;
+  memset(cfg, 0, sizeof(*cfg));
+  cfg->dim = 3;
+  cfg->p = 8;
+  cfg->leaf_cap = 64;
+  cfg->m2l_mode = FMM_M2L_FP32;
+  cfg->eps2 = 0.0;
+  cfg->G = 1.0;
+  cfg->device = 0;
+  return FMM_OK;
+}
+
+int fmm_create(const fmm_config *cfg, fmm_ctx **out) {
+  if (!out) return FMM_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int rc = check_cfg(cfg);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return FMM_ERR_NO_DEVICE;
+  if (cfg->device < 0 || cfg->device >= ndev) return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaSetDevice(cfg->device));
+  fmm_ctx *c = new (std::nothrow) fmm_ctx();
+  if (!c) return FMM_ERR_OUT_OF_MEMORY;
+  c->cfg = *cfg;
+  memset(&c->stats, 0, sizeof(c->stats));
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return FMM_ERR_CUDA;
+  }
+  for (auto &e : c->ev) cudaEventCreate(&e);
+  if (!c->ws.init_small()) {
+    fmm_destroy(c);
+    return FMM_ERR_OUT_OF_MEMORY;
+  }
+  upload_class_tables();
+  *out = c;
+  return FMM_OK;
+}
+
+int fmm_destroy(fmm_ctx *c) {
+  if (!c) return FMM_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(c->cfg.device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->ws.release_all();
+  c->ops.tab.release();
+  c->ops.scratch.release();
+  c->eb.M.release();
+  c->eb.L.release();
+  c->eb.tlist.release();
+  c->eb.batches.release();
+  c->eb.cls_count.release();
+  c->eb.ckey.release();
+  c->eb.ckey_alt.release();
+  c->eb.cval.release();
+  for (auto *b : {&c->d_pos, &c->d_mass, &c->d_acc, &c->d_pot, &c->d_vel, &c->d_x0, &c->d_v0, &c->d_xs, &c->d_vs,
+                  &c->d_asum, &c->d_vsum})
+    b->release();
+  c->d_targets.release();
+  for (auto &e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return FMM_OK;
+}
+
+static int evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass, double *d_acc,
+                           double *d_pot, cudaStream_t st) {
+  const int dim = c->cfg.dim;
+  if (n < 0 || n > (int64_t)INT32_MAX) return FMM_ERR_INVALID_ARGUMENT;
+  if (n == 0) return FMM_OK;
+  if (!d_pos || !d_mass || !d_acc) return FMM_ERR_INVALID_ARGUMENT;
+  if (dim == 2) return FMM_ERR_UNSUPPORTED;
+  CUDA_TRY(cudaEventRecord(c->ev[0], st));
+  int rc = build_tree(c->ws, c->tree, d_pos, d_mass, n, dim, c->cfg.leaf_cap, st);
+  if (rc) return rc;
+  if (!c->ws.ok) return FMM_ERR_OUT_OF_MEMORY;
+  c->have_tree = true;
+  PassGeom g;
+  g.emax = 0;
+  for (int d = 0; d < 3; ++d) {
+    g.lo[d] = c->tree.lo[d];
+    g.ext[d] = d < dim ? c->tree.hi[d] - c->tree.lo[d] : 0.0;
+    g.emax = std::max(g.emax, g.ext[d]);
+  }
+  rc = build_op_tables(c->ops, dim, c->cfg.p, g, st, c->ws.launches);
+  if (rc) return rc;
+  memset(&c->stats, 0, sizeof(c->stats));
+  rc = run_fmm_passes(c->ws, c->tree, c->ops, c->eb, c->cfg.p, c->cfg.eps2, c->cfg.G, g, d_acc, d_pot,
+                      c->cfg.m2l_mode, st, c->stats, c->ev);
+  if (rc) return rc;
+  if (!c->ws.ok) return FMM_ERR_OUT_OF_MEMORY;
+  c->stats.depth = c->tree.depth;
+  c->stats.n_levels = c->tree.depth + 1;
+  c->stats.n_leaves = c->tree.level_count[c->tree.depth];
+  c->timing_pending = true;
+  return FMM_OK;
+}
+
+static int finish(fmm_ctx *c, cudaStream_t st) {
+  CUDA_TRY(cudaStreamSynchronize(st));
+  unsigned int herr = 0;
+  CUDA_TRY(cudaMemcpy(&herr, c->ws.dev_err, sizeof(herr), cudaMemcpyDeviceToHost));
+  if (c->timing_pending) {
+    float ms[5] = {0, 0, 0, 0, 0};
+    for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], c->ev[i], c->ev[i + 1]);
+    c->stats.ms_tree = ms[0];
+    c->stats.ms_upward = ms[1];
+    c->stats.ms_m2l = ms[2];
+    c->stats.ms_downward = ms[3];
+    c->stats.ms_p2p = ms[4];
+    float tot = 0;
+    cudaEventElapsedTime(&tot, c->ev[0], c->ev[5]);
+    c->stats.ms_total = tot;
+    c->timing_pending = false;
+  }
+  if (herr & FMM_DEV_ERR_NONFINITE_INPUT) return FMM_ERR_NONFINITE_INPUT;
+  if (herr & FMM_DEV_ERR_NONFINITE_OUTPUT) return FMM_ERR_NONFINITE_OUTPUT;
+  return FMM_OK;
+}
+
+int fmm_evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass, double *d_acc,
+                        double *d_pot, void *stream) {
+  if (!c) return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  return evaluate_device(c, n, d_pos, d_mass, d_acc, d_pot, st);
+}
+
+int fmm_synchronize(fmm_ctx *c) {
+  if (!c) return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  CUDA_TRY(cudaDeviceSynchronize());
+  return finish(c, c->stream);
+}
+
+static int upload(fmm_ctx *c, int64_t n, const double *pos, const double *mass) {
+  const int dim = c->cfg.dim;
+  if (!c->d_pos.reserve((size_t)n * dim) || !c->d_mass.reserve((size_t)n) || !c->d_acc.reserve((size_t)n * dim) ||
+      !c->d_pot.reserve((size_t)n))
+    return FMM_ERR_OUT_OF_MEMORY;
+  CUDA_TRY(cudaMemcpyAsync(c->d_pos.ptr, pos, sizeof(double) * n * dim, cudaMemcpyHostToDevice, c->stream));
+  if (mass) CUDA_TRY(cudaMemcpyAsync(c->d_mass.ptr, mass, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+  return FMM_OK;
+}
+
+int fmm_evaluate(fmm_ctx *c, int64_t n, const double *pos, const double *mass, double *acc, double *pot) {
+  if (!c || n < 0 || (n > 0 && (!pos || !mass || !acc))) return FMM_ERR_INVALID_ARGUMENT;
+  if (n == 0) return FMM_OK;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  int rc = upload(c, n, pos, mass);
+  if (rc) return rc;
+  rc = evaluate_device(c, n, c->d_pos.ptr, c->d_mass.ptr, c->d_acc.ptr, pot ? c->d_pot.ptr : nullptr, c->stream);
+  if (rc) return rc;
+  const int dim = c->cfg.dim;
+  CUDA_TRY(cudaMemcpyAsync(acc, c->d_acc.ptr, sizeof(double) * n * dim, cudaMemcpyDeviceToHost, c->stream));
+  if (pot) CUDA_TRY(cudaMemcpyAsync(pot, c->d_pot.ptr, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
+  return finish(c, c->stream);
+}
+
+int fmm_direct_device(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass, int64_t ntargets,
+                      const int64_t *d_targets, int32_t soft_mode, double *d_acc, double *d_pot, void *stream) {
+  if (!c || n < 0 || ntargets < 0) return FMM_ERR_INVALID_ARGUMENT;
+  if (soft_mode != FMM_SOFT_PLUMMER && soft_mode != FMM_SOFT_NAIVE_REF) return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  return direct_sum(d_pos, d_mass, n, d_targets, ntargets, c->cfg.dim, c->cfg.eps2, soft_mode, c->cfg.G, d_acc, d_pot,
+                    st, c->ws.launches);
+}
+
+int fmm_direct(fmm_ctx *c, int64_t n, const double *pos, const double *mass, int64_t ntargets,
+               const int64_t *targets, int32_t soft_mode, double *acc, double *pot) {
+  if (!c || n < 0 || (n > 0 && (!pos || !mass || !acc))) return FMM_ERR_INVALID_ARGUMENT;
+  if (n == 0) return FMM_OK;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  const int dim = c->cfg.dim;
+  int64_t nt = targets ? ntargets : n;
+  for (int64_t i = 0; targets && i < nt; ++i)
+    if (targets[i] < 0 || targets[i] >= n) return FMM_ERR_INVALID_ARGUMENT;
+  int rc = upload(c, n, pos, mass);
+  if (rc) return rc;
+  if (!c->d_acc.reserve((size_t)nt * dim) || !c->d_pot.reserve((size_t)nt)) return FMM_ERR_OUT_OF_MEMORY;
+  const int64_t *dt = nullptr;
+  if (targets) {
+    if (!c->d_targets.reserve((size_t)nt)) return FMM_ERR_OUT_OF_MEMORY;
+    CUDA_TRY(cudaMemcpyAsync(c->d_targets.ptr, targets, sizeof(int64_t) * nt, cudaMemcpyHostToDevice, c->stream));
+    dt = c->d_targets.ptr;
+  }
+  rc = direct_sum(c->d_pos.ptr, c->d_mass.ptr, n, dt, nt, dim, c->cfg.eps2, soft_mode, c->cfg.G, c->d_acc.ptr,
+                  pot ? c->d_pot.ptr : nullptr, c->stream, c->ws.launches);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(acc, c->d_acc.ptr, sizeof(double) * nt * dim, cudaMemcpyDeviceToHost, c->stream));
+  if (pot) CUDA_TRY(cudaMemcpyAsync(pot, c->d_pot.ptr, sizeof(double) * nt, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return FMM_OK;
+}
+
+int fmm_integrate(fmm_ctx *c, int32_t method, double dt, int32_t steps, int64_t n, double *pos, double *vel,
+                  const double *mass, double *acc_out) {
+  if (!c || n < 0 || steps < 0 || (n > 0 && (!pos || !vel || !mass))) return FMM_ERR_INVALID_ARGUMENT;
+  if (method != FMM_INT_SYMPLECTIC_EULER && method != FMM_INT_RK4) return FMM_ERR_INVALID_ARGUMENT;
+  if (n == 0 || steps == 0) return FMM_OK;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  const int dim = c->cfg.dim;
+  const int64_t nd = n * dim;
+  int rc = upload(c, n, pos, mass);
+  if (rc) return rc;
+  if (!c->d_vel.reserve(nd)) return FMM_ERR_OUT_OF_MEMORY;
+  CUDA_TRY(cudaMemcpyAsync(c->d_vel.ptr, vel, sizeof(double) * nd, cudaMemcpyHostToDevice, c->stream));
+  double *x = c->d_pos.ptr, *v = c->d_vel.ptr, *a = c->d_acc.ptr;
+  cudaStream_t st = c->stream;
+  for (int s = 0; s < steps; ++s) {
+    if (method == FMM_INT_SYMPLECTIC_EULER) {
+      rc = evaluate_device(c, n, x, c->d_mass.ptr, a, nullptr, st);
+      if (rc) return rc;
+      se_update(x, v, a, nd, dt, st, c->ws.launches);
+    } else {
+      if (!c->d_xs.reserve(nd) || !c->d_vs.reserve(nd) || !c->d_asum.reserve(nd) || !c->d_vsum.reserve(nd))
+        return FMM_ERR_OUT_OF_MEMORY;
+      double *xs = c->d_xs.ptr, *vs = c->d_vs.ptr;
+      rc = evaluate_device(c, n, x, c->d_mass.ptr, a, nullptr, st);
+      if (rc) return rc;
+      rk4_stage(x, v, a, xs, vs, c->d_asum.ptr, c->d_vsum.ptr, nd, 0.5 * dt, 1.0, 1, st, c->ws.launches);
+      rc = evaluate_device(c, n, xs, c->d_mass.ptr, a, nullptr, st);
+      if (rc) return rc;
+      rk4_stage(x, v, a, xs, vs, c->d_asum.ptr, c->d_vsum.ptr, nd, 0.5 * dt, 2.0, 0, st, c->ws.launches);
+      rc = evaluate_device(c, n, xs, c->d_mass.ptr, a, nullptr, st);
+      if (rc) return rc;
+      rk4_stage(x, v, a, xs, vs, c->d_asum.ptr, c->d_vsum.ptr, nd, dt, 2.0, 0, st, c->ws.launches);
+      rc = evaluate_device(c, n, xs, c->d_mass.ptr, a, nullptr, st);
+      if (rc) return rc;
+      rk4_final(x, v, a, vs, c->d_asum.ptr, c->d_vsum.ptr, nd, dt, st, c->ws.launches);
+    }
+    rc = finish(c, st);
+    if (rc) return rc;
+  }
+  CUDA_TRY(cudaMemcpyAsync(pos, x, sizeof(double) * nd, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaMemcpyAsync(vel, v, sizeof(double) * nd, cudaMemcpyDeviceToHost, st));
+  if (acc_out) CUDA_TRY(cudaMemcpyAsync(acc_out, a, sizeof(double) * nd, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return FMM_OK;
+}
+
+// ------------------------------------------------------------ tree export
+int fmm_tree_build(fmm_ctx *c, int64_t n, const double *pos) {
+  if (!c || n <= 0 || n > (int64_t)INT32_MAX || !pos) return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  std::vector<double> ones((size_t)n, 1.0);
+  int rc = upload(c, n, pos, ones.data());
+  if (rc) return rc;
+  rc = build_tree(c->ws, c->tree, c->d_pos.ptr, c->d_mass.ptr, n, c->cfg.dim, c->cfg.leaf_cap, c->stream);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->have_tree = true;
+  return FMM_OK;
+}
+
+int fmm_tree_depth(fmm_ctx *c, int32_t *depth) {
+  if (!c || !depth || !c->have_tree) return FMM_ERR_INVALID_ARGUMENT;
+  *depth = c->tree.depth;
+  return FMM_OK;
+}
+
+int fmm_tree_level_size(fmm_ctx *c, int32_t level, int64_t *count) {
+  if (!c || !count || !c->have_tree || level < 0 || level > c->tree.depth) return FMM_ERR_INVALID_ARGUMENT;
+  *count = c->tree.level_count[level];
+  return FMM_OK;
+}
+
+int fmm_tree_level_keys(fmm_ctx *c, int32_t level, uint64_t *keys) {
+  if (!c || !keys || !c->have_tree || level < 0 || level > c->tree.depth) return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  CUDA_TRY(cudaMemcpy(keys, c->ws.cell_key + c->tree.level_off[level], sizeof(uint64_t) * c->tree.level_count[level],
+                      cudaMemcpyDeviceToHost));
+  return FMM_OK;
+}
+
+int fmm_tree_leaves(fmm_ctx *c, uint64_t *keys, int64_t *start, int64_t *perm) {
+  if (!c || !keys || !start || !perm || !c->have_tree) return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  const int D = c->tree.depth, nl = c->tree.level_count[D];
+  CUDA_TRY(cudaMemcpy(keys, c->ws.cell_key + c->tree.level_off[D], sizeof(uint64_t) * nl, cudaMemcpyDeviceToHost));
+  std::vector<int> pb(nl);
+  CUDA_TRY(cudaMemcpy(pb.data(), c->ws.cell_pbeg + c->tree.level_off[D], sizeof(int) * nl, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < nl; ++i) start[i] = pb[i];
+  start[nl] = c->tree.n;
+  std::vector<uint32_t> pv(c->tree.n);
+  CUDA_TRY(cudaMemcpy(pv.data(), c->tree.d_perm, sizeof(uint32_t) * c->tree.n, cudaMemcpyDeviceToHost));
+  for (int64_t i = 0; i < c->tree.n; ++i) perm[i] = pv[i];
+  return FMM_OK;
+}
+
+int fmm_tree_pairs(fmm_ctx *c, int32_t level, int32_t kind, int64_t *count, uint64_t *tkey, uint64_t *skey) {
+  if (!c || !count || !c->have_tree || level < 0 || level > c->tree.depth || (kind != 0 && kind != 1))
+    return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  const TreeState &t = c->tree;
+  const int dim = t.dim, nc = 1 << dim, ns = dim == 3 ? 27 : 9;
+  const int lo = t.cell0, hi = t.level_off[t.depth] + t.level_count[t.depth];
+  const int m = hi - lo;
+  std::vector<uint64_t> key(m);
+  std::vector<int> par(m), chi((size_t)m * nc), col((size_t)m * ns);
+  CUDA_TRY(cudaMemcpy(key.data(), c->ws.cell_key + lo, sizeof(uint64_t) * m, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(par.data(), c->ws.cell_parent + lo, sizeof(int) * m, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(chi.data(), c->ws.cell_child + (size_t)lo * nc, sizeof(int) * m * nc, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(col.data(), c->ws.cell_coll + (size_t)lo * ns, sizeof(int) * m * ns, cudaMemcpyDeviceToHost));
+  int64_t k = 0;
+  const int b = t.level_off[level] - lo, e = b + t.level_count[level];
+  for (int i = b; i < e; ++i) {
+    if (kind == 0) {
+      for (int s = 0; s < ns; ++s) {
+        int q = col[(size_t)i * ns + s];
+        if (q < 0 || q - lo == i) continue;
+        if (tkey) {
+          tkey[k] = key[i];
+          skey[k] = key[q - lo];
+        }
+        ++k;
+      }
+    } else if (level > 0) {
+      int P = par[i] - lo;
+      for (int s = 0; s < ns; ++s) {
+        int Q = col[(size_t)P * ns + s];
+        if (Q < 0) continue;
+        for (int ch = 0; ch < nc; ++ch) {
+          int q = chi[(size_t)(Q - lo) * nc + ch];
+          if (q < 0) continue;
+          bool nb = false;
+          for (int s2 = 0; s2 < ns; ++s2) nb |= col[(size_t)i * ns + s2] == q;
+          if (nb) continue;
+          if (tkey) {
+            tkey[k] = key[i];
+            skey[k] = key[q - lo];
+          }
+          ++k;
+        }
+      }
+    }
+  }
+  *count = k;
+  return FMM_OK;
+}
+
+int fmm_last_stats(fmm_ctx *c, fmm_stats *out) {
+  if (!c || !out) return FMM_ERR_INVALID_ARGUMENT;
+  *out = c->stats;
+  return FMM_OK;
+}
+
+int64_t fmm_launch_count(fmm_ctx *c) { return c ? c->ws.launches : -1; }
+
+}  // extern "C"

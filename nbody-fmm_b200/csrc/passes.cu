@@ -1,0 +1,595 @@
+// The FMM passes after the tree build: P2M, M2M, M2L, L2L, L2P and P2P
+// (Tree::compute_accelerations, tree.cpp:93-111; Leaf::compute_acceleration,
+// leaf.cpp:55-148).
+//
+// Translations are dense contractions.  Cells of one level with the same
+// child index ("class": the parities of their coordinates) have the same
+// set of interaction-list offsets (node_i.cpp:39-43: delta in
+// [-2-c%2, 3-c%2] minus the neighbours), so a batch of 64 such target cells
+// accumulates, slot by slot, Y[64 x K] += X_slot[64 x K] * T_slot[K x K] where
+// X_slot gathers the source expansion of each target at that offset (zero if
+// the cell does not exist).  M2M (8 child slots) and L2L (1 parent slot) use
+// the same kernel.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "expansions.cuh"
+
+namespace fmm {
+
+// [dim == 3][class] -> list of (table offset index | colleague slot << 9 | child << 14)
+__constant__ int c_m2l_slots[2][8][189];
+__constant__ float c_rec1[FMM_MAX_P + 1][FMM_MAX_P + 1];  // (2l-1)/(l^2-m^2)
+__constant__ float c_rec2[FMM_MAX_P + 1][FMM_MAX_P + 1];  // 1/(l^2-m^2)
+
+void upload_class_tables() {
+  static bool done = false;
+  if (done) return;
+  done = true;
+  static int h[2][8][189] = {};
+  for (int dim = 2; dim <= 3; ++dim)
+  for (int c = 0; c < (1 << dim); ++c) {
+    int cb[3] = {c & 1, (c >> 1) & 1, (c >> 2) & 1};
+    int k = 0;
+    int lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = a < dim ? -2 - cb[a] : 0;
+      hi[a] = a < dim ? 3 - cb[a] : 0;
+    }
+    for (int dz = lo[2]; dz <= hi[2]; ++dz)
+      for (int dy = lo[1]; dy <= hi[1]; ++dy)
+        for (int dx = lo[0]; dx <= hi[0]; ++dx) {
+          if (dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1) continue;
+          int dd[3] = {dx, dy, dz}, del[3], ch[3];
+          for (int a = 0; a < 3; ++a) {
+            int v = dd[a] + cb[a];         // in [-2, 3]
+            del[a] = (v + 2) / 2 - 1;      // floor(v / 2)
+            ch[a] = v - 2 * del[a];
+          }
+          int ti = dim == 3 ? (dx + 3) + 7 * (dy + 3) + 49 * (dz + 3) : (dx + 3) + 7 * (dy + 3);
+          int cs = dim == 3 ? (del[0] + 1) + 3 * (del[1] + 1) + 9 * (del[2] + 1) : (del[0] + 1) + 3 * (del[1] + 1);
+          int chi = ch[0] + 2 * ch[1] + (dim == 3 ? 4 * ch[2] : 0);
+          h[dim - 2][c][k++] = ti | (cs << 9) | (chi << 14);
+        }
+  }
+  cudaMemcpyToSymbol(c_m2l_slots, h, sizeof(h));
+  float r1[FMM_MAX_P + 1][FMM_MAX_P + 1] = {}, r2[FMM_MAX_P + 1][FMM_MAX_P + 1] = {};
+  for (int l = 0; l <= FMM_MAX_P; ++l)
+    for (int m = 0; m < l; ++m) {
+      r1[l][m] = (float)((2.0 * l - 1.0) / (double)(l * l - m * m));
+      r2[l][m] = (float)(1.0 / (double)(l * l - m * m));
+    }
+  cudaMemcpyToSymbol(c_rec1, r1, sizeof(r1));
+  cudaMemcpyToSymbol(c_rec2, r2, sizeof(r2));
+}
+
+// ------------------------------------------------------------ cp.async
+__device__ inline void cp_async16(void *smem, const void *gmem, int src_bytes) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ inline void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ inline void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+enum { MODE_M2L = 0, MODE_M2M = 1, MODE_L2L = 2 };
+static constexpr int CT_TGT = 64;  // targets per batch
+static constexpr int CT_THREADS = 256;
+
+struct ContractArgs {
+  const int4 *batches;  // {first (list offset or cell), count, level, class}
+  const int *tlist;     // class-grouped target cells, or null (targets first + i)
+  const float *X;
+  float *Y;
+  const float *tab;
+  const int *cparent, *cchild, *ccoll;
+  int cell0, K, KS, KP, dim, mode, slot_base, level_stride;
+};
+
+// Resolves the source cell of target `tgt` for slot s; returns -1 if absent.
+__device__ inline int contract_source(const ContractArgs &a, int tgt, int s, int cls, int level, int &tslot) {
+  const int nc = 1 << a.dim, ns = a.dim == 3 ? 27 : 9;
+  if (a.mode == MODE_M2L) {
+    int e = c_m2l_slots[a.dim - 2][cls][s];
+    tslot = (e & 511) + level * a.level_stride;
+    int P = a.cparent[tgt];
+    int Q = a.ccoll[(int64_t)P * ns + ((e >> 9) & 31)];
+    if (Q < 0) return -1;
+    return a.cchild[(int64_t)Q * nc + ((e >> 14) & 7)];
+  } else if (a.mode == MODE_M2M) {
+    tslot = a.slot_base + s;
+    return a.cchild[(int64_t)tgt * nc + s];
+  } else {
+    tslot = a.slot_base + cls;
+    return a.cparent[tgt];
+  }
+}
+
+template <int J, int NS>
+__global__ void __launch_bounds__(CT_THREADS) k_contract(ContractArgs a) {
+  extern __shared__ __align__(16) float smem[];
+  const int K = a.K, KS = a.KS, KP = a.KP;
+  float *Ts = smem;                              // [NS][K][KP]
+  float *Xs = Ts + (size_t)NS * K * KP;          // [NS][CT_TGT][KS]
+  int *s_src = (int *)(Xs + (size_t)NS * CT_TGT * KS);  // [NS][CT_TGT]
+  int *s_tslot = s_src + NS * CT_TGT;            // [NS]
+  int *s_any = s_tslot + NS;                     // [NS]
+  __shared__ int s_tgt[CT_TGT];
+
+  const int4 b = a.batches[blockIdx.x];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int cnt = b.y, level = b.z, cls = b.w;
+  if (tid < CT_TGT) s_tgt[tid] = tid < cnt ? (a.tlist ? a.tlist[b.x + tid] : b.x + tid) : -1;
+  __syncthreads();
+  const int nslots = a.mode == MODE_M2L ? (a.dim == 3 ? 189 : 27) : (a.mode == MODE_M2M ? (1 << a.dim) : 1);
+
+  float acc[8][J];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < J; ++j) acc[i][j] = 0.f;
+
+  auto prefetch = [&](int s, int buf) {
+    int src = -1, ts = 0;
+    if (tid < CT_TGT) {
+      int tg = s_tgt[tid];
+      if (tg >= 0) src = contract_source(a, tg, s, cls, level, ts);
+      s_src[buf * CT_TGT + tid] = src;
+      if (tid == 0 || src >= 0) s_tslot[buf] = ts;  // same for all targets of the batch
+    }
+    int any = __syncthreads_or(src >= 0);
+    if (tid == 0) s_any[buf] = any;
+    if (any) {
+      const float *T = a.tab + (size_t)s_tslot[buf] * K * KP;
+      float *Td = Ts + (size_t)buf * K * KP;
+      const int nT = K * KP / 4;
+      for (int c = tid; c < nT; c += CT_THREADS) cp_async16(Td + 4 * c, T + 4 * c, 16);
+      float *Xd = Xs + (size_t)buf * CT_TGT * KS;
+      const int cpr = KS / 4;
+      for (int c = tid; c < CT_TGT * cpr; c += CT_THREADS) {
+        int r = c / cpr, q = c % cpr;
+        int sr = s_src[buf * CT_TGT + r];
+        const float *g = sr >= 0 ? a.X + (size_t)(sr - a.cell0) * KS + 4 * q : a.X;
+        cp_async16(Xd + (size_t)r * KS + 4 * q, g, sr >= 0 ? 16 : 0);
+      }
+    }
+    cp_async_commit();
+  };
+
+  if (NS == 2) prefetch(0, 0);
+  for (int s = 0; s < nslots; ++s) {
+    const int buf = NS == 2 ? (s & 1) : 0;
+    if (NS == 1) {
+      prefetch(s, 0);
+      cp_async_wait<0>();
+    } else {
+      if (s + 1 < nslots) {
+        prefetch(s + 1, (s + 1) & 1);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+    }
+    __syncthreads();
+    if (s_any[buf]) {
+      const float *Tb = Ts + (size_t)buf * K * KP;
+      const float *Xb = Xs + (size_t)buf * CT_TGT * KS + (size_t)(warp * 8) * KS;
+#pragma unroll 2
+      for (int k = 0; k < K; ++k) {
+        float bv[J];
+#pragma unroll
+        for (int j = 0; j < J; ++j) bv[j] = Tb[(size_t)k * KP + lane + 32 * j];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          float av = Xb[(size_t)i * KS + k];
+#pragma unroll
+          for (int j = 0; j < J; ++j) acc[i][j] = fmaf(av, bv[j], acc[i][j]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // write out
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    int tg = s_tgt[warp * 8 + i];
+    if (tg < 0) continue;
+    float *y = a.Y + (size_t)(tg - a.cell0) * KS;
+#pragma unroll
+    for (int j = 0; j < J; ++j) {
+      int o = lane + 32 * j;
+      if (o < K) {
+        if (a.mode == MODE_M2M) y[o] = acc[i][j];
+        else y[o] += acc[i][j];
+      }
+    }
+  }
+}
+
+template <int J>
+static void launch_contract_j(const ContractArgs &a, int nb, int stages, size_t sh, cudaStream_t st) {
+  if (stages == 2) k_contract<J, 2><<<nb, CT_THREADS, sh, st>>>(a);
+  else k_contract<J, 1><<<nb, CT_THREADS, sh, st>>>(a);
+}
+
+static size_t contract_smem(int K, int KS, int KP, int NS) {
+  return sizeof(float) * ((size_t)NS * K * KP + (size_t)NS * CT_TGT * KS) + sizeof(int) * (NS * CT_TGT + 2 * NS) + 16;
+}
+
+static int launch_contract(const ContractArgs &a, int nb, cudaStream_t st, int64_t &launches) {
+  if (nb <= 0) return FMM_OK;
+  int J = (a.K + 31) / 32;
+  int stages = contract_smem(a.K, a.KS, a.KP, 2) <= 200 * 1024 ? 2 : 1;
+  size_t sh = contract_smem(a.K, a.KS, a.KP, stages);
+  if (sh > 227 * 1024) return FMM_ERR_UNSUPPORTED;
+  static size_t attr_set[8][3] = {};
+  auto set_attr = [&](auto kern) { return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh); };
+  if (attr_set[J][stages] < sh) {
+    cudaError_t e = cudaSuccess;
+    switch (J) {
+      case 1: e = stages == 2 ? set_attr(k_contract<1, 2>) : set_attr(k_contract<1, 1>); break;
+      case 2: e = stages == 2 ? set_attr(k_contract<2, 2>) : set_attr(k_contract<2, 1>); break;
+      case 3: e = stages == 2 ? set_attr(k_contract<3, 2>) : set_attr(k_contract<3, 1>); break;
+      case 4: e = stages == 2 ? set_attr(k_contract<4, 2>) : set_attr(k_contract<4, 1>); break;
+      case 5: e = stages == 2 ? set_attr(k_contract<5, 2>) : set_attr(k_contract<5, 1>); break;
+      case 6: e = stages == 2 ? set_attr(k_contract<6, 2>) : set_attr(k_contract<6, 1>); break;
+      default: return FMM_ERR_UNSUPPORTED;
+    }
+    if (e != cudaSuccess) return FMM_ERR_CUDA;
+    attr_set[J][stages] = sh;
+  }
+  switch (J) {
+    case 1: launch_contract_j<1>(a, nb, stages, sh, st); break;
+    case 2: launch_contract_j<2>(a, nb, stages, sh, st); break;
+    case 3: launch_contract_j<3>(a, nb, stages, sh, st); break;
+    case 4: launch_contract_j<4>(a, nb, stages, sh, st); break;
+    case 5: launch_contract_j<5>(a, nb, stages, sh, st); break;
+    case 6: launch_contract_j<6>(a, nb, stages, sh, st); break;
+    default: return FMM_ERR_UNSUPPORTED;
+  }
+  launches += 1;
+  return FMM_OK;
+}
+
+// ------------------------------------------------------------------ P2M
+// One thread per particle (leaf order); each coefficient is summed over the
+// particles of a leaf by a segmented warp reduction, then added by the
+// segment's first lane.
+__device__ inline float seg_sum(float v, const bool *same) {
+#pragma unroll
+  for (int o = 1, k = 0; o < 32; o <<= 1, ++k) {
+    float t = __shfl_down_sync(0xffffffffu, v, o);
+    if (same[k]) v += t;
+  }
+  return v;
+}
+
+__global__ void k_p2m3d(const float4 *part, const int *leaf_of, int64_t n, int cell0, float inv_s, int p, int KS,
+                        float *M) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  bool valid = i < n;
+  float4 q = valid ? part[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  int seg = valid ? leaf_of[i] : -1 - lane;
+  bool same[5];
+#pragma unroll
+  for (int o = 1, k = 0; o < 32; o <<= 1, ++k) {
+    int so = __shfl_down_sync(0xffffffffu, seg, o);
+    same[k] = (lane + o < 32) && so == seg;
+  }
+  int sp = __shfl_up_sync(0xffffffffu, seg, 1);
+  bool head = valid && (lane == 0 || sp != seg);
+  float *Mrow = M + (size_t)(valid ? seg - cell0 : 0) * KS;
+  const float x = q.x * inv_s, y = q.y * inv_s, z = q.z * inv_s, r2 = x * x + y * y + z * z, w = q.w;
+  float dre = 1.f, dim_ = 0.f;
+  for (int m = 0; m <= p; ++m) {
+    if (m > 0) {
+      float h = -0.5f / m;
+      float nre = h * (x * dre - y * dim_), nim = h * (x * dim_ + y * dre);
+      dre = nre;
+      dim_ = nim;
+    }
+    float p1re = dre, p1im = dim_, p2re = 0.f, p2im = 0.f;
+    for (int l = m; l <= p; ++l) {
+      float cre, cim;
+      if (l == m) {
+        cre = dre;
+        cim = dim_;
+      } else {
+        float a1 = c_rec1[l][m] * z, a2 = c_rec2[l][m] * r2;
+        cre = a1 * p1re - a2 * p2re;
+        cim = a1 * p1im - a2 * p2im;
+        p2re = p1re;
+        p2im = p1im;
+        p1re = cre;
+        p1im = cim;
+      }
+      float vr = seg_sum(w * cre, same);
+      if (head) atomicAdd(Mrow + re_idx(l, m), vr);
+      if (m > 0) {
+        float vi = seg_sum(-w * cim, same);
+        if (head) atomicAdd(Mrow + im_idx(l, m), vi);
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ L2P
+__device__ inline float2 lget(const float *Lr, int n, int m) {
+  if (m > n) return make_float2(0.f, 0.f);
+  if (m >= 0) return make_float2(Lr[re_idx(n, m)], m ? Lr[im_idx(n, m)] : 0.f);
+  // m = -1: L_n^-1 = -conj(L_n^1)
+  return make_float2(-Lr[re_idx(n, 1)], Lr[im_idx(n, 1)]);
+}
+
+__global__ void k_l2p3d(const float4 *part, const int *leaf_of, int64_t n, int cell0, float inv_s, int p, int KS,
+                        const float *L, float4 *far) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 q = part[i];
+  const float *Lr = L + (size_t)(leaf_of[i] - cell0) * KS;
+  const float x = q.x * inv_s, y = q.y * inv_s, z = q.z * inv_s, r2 = x * x + y * y + z * z;
+  float gx = 0.f, gy = 0.f, gz = 0.f, ph = 0.f;
+  float dre = 1.f, dim_ = 0.f;
+  for (int m = 0; m <= p; ++m) {
+    if (m > 0) {
+      float h = -0.5f / m;
+      float nre = h * (x * dre - y * dim_), nim = h * (x * dim_ + y * dre);
+      dre = nre;
+      dim_ = nim;
+    }
+    const float wm = m ? 2.f : 1.f;
+    float p1re = dre, p1im = dim_, p2re = 0.f, p2im = 0.f;
+    for (int l = m; l <= p; ++l) {
+      float cre, cim;
+      if (l == m) {
+        cre = dre;
+        cim = dim_;
+      } else {
+        float a1 = c_rec1[l][m] * z, a2 = c_rec2[l][m] * r2;
+        cre = a1 * p1re - a2 * p2re;
+        cim = a1 * p1im - a2 * p2im;
+        p2re = p1re;
+        p2im = p1im;
+        p1re = cre;
+        p1im = cim;
+      }
+      float2 Lv = lget(Lr, l, m);
+      ph += wm * (Lv.x * cre - Lv.y * cim);
+      if (l < p) {
+        float2 A = lget(Lr, l + 1, m), Lm = lget(Lr, l + 1, m - 1), Lp = lget(Lr, l + 1, m + 1);
+        gz += wm * (A.x * cre - A.y * cim);
+        float axr = 0.5f * (Lm.x - Lp.x), axi = 0.5f * (Lm.y - Lp.y);
+        gx += wm * (axr * cre - axi * cim);
+        float sr = Lp.x + Lm.x, si = Lp.y + Lm.y;  // Re(-i S R / 2) = Im(S R) / 2
+        gy += wm * 0.5f * (sr * cim + si * cre);
+      }
+    }
+  }
+  far[i] = make_float4(gx * inv_s * inv_s, gy * inv_s * inv_s, gz * inv_s * inv_s, ph * inv_s);
+}
+
+// ------------------------------------------------------------------ P2P
+// One warp per target leaf; the leaf's particles are spread over the lanes
+// (several lanes per particle for small leaves, each taking a share of the
+// sources).  Sources are the leaf itself (j != i) and its existing
+// neighbours (leaf.cpp:118-142), in FP32 relative to the target leaf centre.
+__global__ void k_p2p3d(int leaf_first, int nleaves, const int *pbeg, const int *pend, const int *coll,
+                        const float4 *part, const float4 *far, const uint32_t *perm, float hx, float hy, float hz,
+                        float eps2, double G, double *acc, double *pot, unsigned int *err) {
+  const int lane = threadIdx.x & 31;
+  const int wl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (wl >= nleaves) return;
+  const int g = leaf_first + wl;
+  const int tb = pbeg[g], nt = pend[g] - tb;
+  const int tp = nt < 32 ? nt : 32;
+  int Gl = 1;
+  while (Gl * 2 * tp <= 32) Gl *= 2;
+  const int tpp = 32 / Gl;
+  const int *cl = coll + (int64_t)g * 27;
+  bool bad = false;
+  for (int t0 = 0; t0 < nt; t0 += tpp) {
+    const int ti = t0 + lane / Gl, sub = lane % Gl;
+    const bool act = ti < nt;
+    const int me_i = tb + (act ? ti : 0);
+    const float4 me = part[me_i];
+    float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
+    for (int s = 0; s < 27; ++s) {
+      const int S = cl[s];
+      if (S < 0) continue;
+      const float tx = me.x - (s % 3 - 1) * hx, ty = me.y - ((s / 3) % 3 - 1) * hy, tz = me.z - (s / 9 - 1) * hz;
+      const int se = pend[S];
+      for (int j = pbeg[S] + sub; j < se; j += Gl) {
+        if (j == me_i) continue;
+        const float4 q = part[j];
+        const float rx = tx - q.x, ry = ty - q.y, rz = tz - q.z;
+        const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2)));
+        const float inv = rsqrtf(r2);
+        const float mi = q.w * inv;
+        const float mi3 = mi * inv * inv;
+        ax = fmaf(-rx, mi3, ax);
+        ay = fmaf(-ry, mi3, ay);
+        az = fmaf(-rz, mi3, az);
+        ph += mi;
+      }
+    }
+    for (int o = 1; o < Gl; o <<= 1) {
+      ax += __shfl_xor_sync(0xffffffffu, ax, o);
+      ay += __shfl_xor_sync(0xffffffffu, ay, o);
+      az += __shfl_xor_sync(0xffffffffu, az, o);
+      ph += __shfl_xor_sync(0xffffffffu, ph, o);
+    }
+    if (act && sub == 0) {
+      const float4 f = far[me_i];
+      const uint32_t o = perm[me_i];
+      double vx = G * ((double)f.x + ax), vy = G * ((double)f.y + ay), vz = G * ((double)f.z + az);
+      acc[3 * (size_t)o] = vx;
+      acc[3 * (size_t)o + 1] = vy;
+      acc[3 * (size_t)o + 2] = vz;
+      if (pot) pot[o] = G * ((double)f.w + ph);
+      bad |= !(isfinite(vx) && isfinite(vy) && isfinite(vz));
+    }
+  }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(err, FMM_DEV_ERR_NONFINITE_OUTPUT);
+}
+
+// ------------------------------------------------------------------ lists
+__global__ void k_class_keys(const uint64_t *ckey, int first, int count, int level, int dim, uint64_t *keys,
+                             uint32_t *vals, int out_off) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  int g = first + i;
+  keys[out_off + i] = ((uint64_t)level << dim) | (ckey[g] & ((1u << dim) - 1));
+  vals[out_off + i] = (uint32_t)g;
+}
+
+__global__ void k_class_hist(const uint64_t *keys, int n, uint32_t *hist) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) atomicAdd(&hist[keys[i] & 255u], 1u);
+}
+
+// ------------------------------------------------------------ driver
+static inline float fmax3(float a, float b, float c) { return std::max(a, std::max(b, c)); }
+
+int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, int p, double eps2, double G,
+                   const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, cudaStream_t st, fmm_stats &stats,
+                   cudaEvent_t *ev) {
+  (void)m2l_mode;
+  const int dim = t.dim, D = t.depth, KS = ops.KS;
+  const int64_t n = t.n;
+  const int ncell = t.n_cells, cell0 = t.cell0;
+  const int TPB = 256;
+  if (!eb.M.reserve((size_t)ncell * KS) || !eb.L.reserve((size_t)ncell * KS)) return FMM_ERR_OUT_OF_MEMORY;
+  CUDA_TRY(cudaMemsetAsync(eb.M.ptr, 0, sizeof(float) * (size_t)ncell * KS, st));
+  CUDA_TRY(cudaMemsetAsync(eb.L.ptr, 0, sizeof(float) * (size_t)ncell * KS, st));
+  const double emax = g.emax > 0 ? g.emax : 1.0;
+  const double sD = std::ldexp(emax, -D);
+  const float inv_sD = (float)(1.0 / sD);
+
+  // class-grouped target lists of levels >= 2
+  std::vector<int4> hb;
+  std::vector<int> lvl_b0(D + 2, 0), lvl_b1(D + 2, 0);
+  int ntl = 0;
+  const int *tl = nullptr;
+  if (D >= 2) {
+    ntl = t.level_off[D] + t.level_count[D] - t.level_off[2];
+    if (!eb.tlist.reserve(ntl) || !eb.cls_count.reserve(256) || !eb.ckey.reserve(ntl) || !eb.ckey_alt.reserve(ntl) ||
+        !eb.cval.reserve(ntl))
+      return FMM_ERR_OUT_OF_MEMORY;
+    for (int d = 2; d <= D; ++d)
+      k_class_keys<<<cdiv(t.level_count[d], TPB), TPB, 0, st>>>(ws.cell_key, t.level_off[d], t.level_count[d], d, dim,
+                                                                eb.ckey.ptr, eb.cval.ptr, t.level_off[d] - t.level_off[2]);
+    ws.launches += D - 1;
+    uint64_t *kk = eb.ckey.ptr, *kk2 = eb.ckey_alt.ptr;
+    uint32_t *vv = eb.cval.ptr, *vv2 = (uint32_t *)eb.tlist.ptr;
+    radix_sort(ws, kk, vv, kk2, vv2, ntl, 8, st);  // sorted (keys, cells) end in (kk, vv)
+    tl = (const int *)vv;
+    CUDA_TRY(cudaMemsetAsync(eb.cls_count.ptr, 0, 256 * sizeof(uint32_t), st));
+    k_class_hist<<<cdiv(ntl, TPB), TPB, 0, st>>>(kk, ntl, eb.cls_count.ptr);
+    ws.launches += 1;
+    uint32_t hc[256];
+    CUDA_TRY(cudaMemcpyAsync(hc, eb.cls_count.ptr, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    int off = 0;
+    const int ncls = 1 << dim;
+    for (int d = 2; d <= D; ++d) {
+      lvl_b0[d] = (int)hb.size();
+      for (int c = 0; c < ncls; ++c) {
+        int cnt = (int)hc[(d << dim) | c];
+        for (int s = 0; s < cnt; s += CT_TGT) hb.push_back(make_int4(off + s, std::min(CT_TGT, cnt - s), d, c));
+        off += cnt;
+      }
+      lvl_b1[d] = (int)hb.size();
+    }
+  }
+  // M2M batches (levels D-1 .. 2, consecutive cells)
+  std::vector<int> m2m_b0(D + 1, 0), m2m_b1(D + 1, 0);
+  for (int d = D - 1; d >= 2; --d) {
+    m2m_b0[d] = (int)hb.size();
+    for (int s = 0; s < t.level_count[d]; s += CT_TGT)
+      hb.push_back(make_int4(t.level_off[d] + s, std::min(CT_TGT, t.level_count[d] - s), d, -1));
+    m2m_b1[d] = (int)hb.size();
+  }
+  if (!eb.batches.reserve(hb.size() + 1)) return FMM_ERR_OUT_OF_MEMORY;
+  if (!hb.empty())
+    CUDA_TRY(cudaMemcpyAsync(eb.batches.ptr, hb.data(), hb.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+
+  ContractArgs ca;
+  ca.batches = eb.batches.ptr;
+  ca.tlist = nullptr;
+  ca.tab = ops.tab.ptr;
+  ca.cparent = ws.cell_parent;
+  ca.cchild = ws.cell_child;
+  ca.ccoll = ws.cell_coll;
+  ca.cell0 = cell0;
+  ca.K = ops.K;
+  ca.KS = KS;
+  ca.KP = ops.KP;
+  ca.dim = dim;
+  ca.level_stride = dim == 2 ? 49 : 0;
+
+  if (ev) cudaEventRecord(ev[1], st);
+  // P2M
+  k_p2m3d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.M.ptr);
+  ws.launches += 1;
+  // M2M, bottom-up
+  for (int d = D - 1; d >= 2; --d) {
+    ca.mode = MODE_M2M;
+    ca.slot_base = ops.off_m2m;
+    ca.tlist = nullptr;
+    ca.X = eb.M.ptr;
+    ca.Y = eb.M.ptr;
+    ContractArgs c2 = ca;
+    c2.batches = eb.batches.ptr + m2m_b0[d];
+    int rc = launch_contract(c2, m2m_b1[d] - m2m_b0[d], st, ws.launches);
+    if (rc) return rc;
+  }
+  if (ev) cudaEventRecord(ev[2], st);
+  // M2L, all levels in one launch
+  if (D >= 2) {
+    ContractArgs c2 = ca;
+    c2.mode = MODE_M2L;
+    c2.slot_base = 0;
+    c2.tlist = tl;
+    c2.X = eb.M.ptr;
+    c2.Y = eb.L.ptr;
+    c2.batches = eb.batches.ptr + lvl_b0[2];
+    int rc = launch_contract(c2, lvl_b1[D] - lvl_b0[2], st, ws.launches);
+    if (rc) return rc;
+  }
+  if (ev) cudaEventRecord(ev[3], st);
+  // L2L, top-down
+  for (int d = 3; d <= D; ++d) {
+    ContractArgs c2 = ca;
+    c2.mode = MODE_L2L;
+    c2.slot_base = ops.off_l2l;
+    c2.tlist = tl;
+    c2.X = eb.L.ptr;
+    c2.Y = eb.L.ptr;
+    c2.batches = eb.batches.ptr + lvl_b0[d];
+    int rc = launch_contract(c2, lvl_b1[d] - lvl_b0[d], st, ws.launches);
+    if (rc) return rc;
+  }
+  // L2P
+  k_l2p3d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far);
+  ws.launches += 1;
+  if (ev) cudaEventRecord(ev[4], st);
+  // P2P + output
+  const double inv2D = std::ldexp(1.0, -D);
+  const float hx = (float)(g.ext[0] * inv2D), hy = (float)(g.ext[1] * inv2D), hz = (float)(g.ext[2] * inv2D);
+  const int nl = t.level_count[D];
+  k_p2p3d<<<cdiv((int64_t)nl * 32, TPB), TPB, 0, st>>>(t.level_off[D], nl, ws.cell_pbeg, ws.cell_pend, ws.cell_coll,
+                                                      ws.part, ws.far, t.d_perm, hx, hy, hz, (float)eps2, G, d_acc,
+                                                      d_pot, ws.dev_err);
+  ws.launches += 1;
+  if (ev) cudaEventRecord(ev[5], st);
+  stats.n_cells = ncell;
+  (void)fmax3;
+  CUDA_TRY(cudaGetLastError());
+  return FMM_OK;
+}
+
+}  // namespace fmm

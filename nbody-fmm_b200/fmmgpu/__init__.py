@@ -1,0 +1,237 @@
+"""Python binding of libfmmgpu.so (the C ABI in include/fmm_gpu.h).
+
+`Context` mirrors the reference's update-method interface for the force
+pass: `evaluate` is FMM::update (src/system_updaters/FMM.cpp:9-12) on plain
+arrays, `direct` is NaiveUpdate::update (naive_update.cpp:9-35) in FP64,
+`integrate` is QuadratureMethod::integrate (quadrature_method.hpp:24) with
+the state kept on the GPU, and `tree` exports Tree::init_tree's structure
+(tree.cpp:15-91).  Accelerations are G * grad exactly as
+Particle::compute_new_accelaration stores them (particle.cpp:16-21).
+
+The library must be built (`make -C nbody-fmm_b200`); there is no CPU
+fallback: importing works without it, but creating a Context raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libfmmgpu.so")
+
+FMM_OK = 0
+FMM_ERR_INVALID_ARGUMENT = -1
+FMM_ERR_CUDA = -2
+FMM_ERR_OUT_OF_MEMORY = -3
+FMM_ERR_NONFINITE_INPUT = -4
+FMM_ERR_NONFINITE_OUTPUT = -5
+FMM_ERR_UNSUPPORTED = -6
+FMM_ERR_TIMEOUT = -7
+FMM_ERR_NO_DEVICE = -8
+
+FMM_M2L_FP32 = 0
+FMM_M2L_TC = 1
+FMM_SOFT_PLUMMER = 0
+FMM_SOFT_NAIVE_REF = 1
+FMM_INT_SYMPLECTIC_EULER = 0
+FMM_INT_RK4 = 1
+
+# Every symbol include/fmm_gpu.h declares.
+EXPORTED = (
+    "fmm_strerror", "fmm_version", "fmm_config_default", "fmm_create", "fmm_destroy", "fmm_evaluate",
+    "fmm_evaluate_device", "fmm_synchronize", "fmm_direct", "fmm_direct_device", "fmm_integrate",
+    "fmm_tree_build", "fmm_tree_depth", "fmm_tree_level_size", "fmm_tree_level_keys", "fmm_tree_leaves",
+    "fmm_tree_pairs", "fmm_last_stats", "fmm_launch_count",
+)
+
+
+class FmmConfig(ctypes.Structure):
+    _fields_ = [
+        ("dim", ctypes.c_int32), ("p", ctypes.c_int32), ("leaf_cap", ctypes.c_int32), ("m2l_mode", ctypes.c_int32),
+        ("eps2", ctypes.c_double), ("G", ctypes.c_double), ("device", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 7),
+    ]
+
+
+class FmmStats(ctypes.Structure):
+    _fields_ = [
+        ("depth", ctypes.c_int32), ("n_levels", ctypes.c_int32), ("n_leaves", ctypes.c_int64),
+        ("n_cells", ctypes.c_int64), ("m2l_pairs", ctypes.c_int64), ("p2p_pairs", ctypes.c_int64),
+        ("ms_tree", ctypes.c_double), ("ms_upward", ctypes.c_double), ("ms_m2l", ctypes.c_double),
+        ("ms_downward", ctypes.c_double), ("ms_p2p", ctypes.c_double), ("ms_total", ctypes.c_double),
+        ("reserved", ctypes.c_double * 6),
+    ]
+
+
+class FmmError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{msg} (code {code})")
+        self.code = code
+
+
+_d = ctypes.POINTER(ctypes.c_double)
+_i64 = ctypes.POINTER(ctypes.c_int64)
+_u64 = ctypes.POINTER(ctypes.c_uint64)
+_vp = ctypes.c_void_p
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Loads libfmmgpu.so and declares its prototypes."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FmmError(FMM_ERR_NO_DEVICE, f"{path} is missing: build it with `make -C nbody-fmm_b200`")
+    L = ctypes.CDLL(path)
+    L.fmm_strerror.restype = ctypes.c_char_p
+    L.fmm_strerror.argtypes = [ctypes.c_int]
+    L.fmm_version.restype = ctypes.c_char_p
+    L.fmm_config_default.argtypes = [ctypes.POINTER(FmmConfig)]
+    L.fmm_create.argtypes = [ctypes.POINTER(FmmConfig), ctypes.POINTER(_vp)]
+    L.fmm_destroy.argtypes = [_vp]
+    L.fmm_evaluate.argtypes = [_vp, ctypes.c_int64, _d, _d, _d, _d]
+    L.fmm_evaluate_device.argtypes = [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp]
+    L.fmm_synchronize.argtypes = [_vp]
+    L.fmm_direct.argtypes = [_vp, ctypes.c_int64, _d, _d, ctypes.c_int64, _i64, ctypes.c_int32, _d, _d]
+    L.fmm_direct_device.argtypes = [_vp, ctypes.c_int64, _vp, _vp, ctypes.c_int64, _vp, ctypes.c_int32, _vp, _vp, _vp]
+    L.fmm_integrate.argtypes = [_vp, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int64, _d, _d, _d, _d]
+    L.fmm_tree_build.argtypes = [_vp, ctypes.c_int64, _d]
+    L.fmm_tree_depth.argtypes = [_vp, ctypes.POINTER(ctypes.c_int32)]
+    L.fmm_tree_level_size.argtypes = [_vp, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]
+    L.fmm_tree_level_keys.argtypes = [_vp, ctypes.c_int32, _u64]
+    L.fmm_tree_leaves.argtypes = [_vp, _u64, _i64, _i64]
+    L.fmm_tree_pairs.argtypes = [_vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64), _u64, _u64]
+    L.fmm_last_stats.argtypes = [_vp, ctypes.POINTER(FmmStats)]
+    L.fmm_launch_count.restype = ctypes.c_int64
+    L.fmm_launch_count.argtypes = [_vp]
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != FMM_OK:
+        raise FmmError(rc, _lib.fmm_strerror(rc).decode())
+
+
+def _p(a, t=_d):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+class Context:
+    """One FMM force evaluator on one GPU (fmm_create / fmm_destroy)."""
+
+    def __init__(self, dim=3, p=8, leaf_cap=64, m2l_mode=FMM_M2L_FP32, eps2=0.0, G=1.0, device=0):
+        L = load_library()
+        cfg = FmmConfig()
+        _check(L.fmm_config_default(ctypes.byref(cfg)))
+        cfg.dim, cfg.p, cfg.leaf_cap, cfg.m2l_mode = dim, p, leaf_cap, m2l_mode
+        cfg.eps2, cfg.G, cfg.device = eps2, G, device
+        h = _vp()
+        _check(L.fmm_create(ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self.dim = dim
+        self.cfg = cfg
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.fmm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _arrays(self, pos, mass):
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        mass = np.ascontiguousarray(mass, dtype=np.float64)
+        if pos.ndim != 2 or pos.shape[1] != self.dim or mass.shape != (pos.shape[0],):
+            raise FmmError(FMM_ERR_INVALID_ARGUMENT, "pos must be (n, dim) and mass (n,)")
+        return pos, mass
+
+    def evaluate(self, pos, mass, want_pot=False):
+        """One force pass (host buffers): returns acc (n, dim) [, pot (n,)]."""
+        pos, mass = self._arrays(pos, mass)
+        n = pos.shape[0]
+        acc = np.zeros((n, self.dim))
+        pot = np.zeros(n) if want_pot else None
+        _check(_lib.fmm_evaluate(self._h, n, _p(pos), _p(mass), _p(acc), _p(pot)))
+        return (acc, pot) if want_pot else acc
+
+    def evaluate_device(self, n, pos_ptr, mass_ptr, acc_ptr, pot_ptr=None, stream=None):
+        """One force pass on device pointers (ints), enqueued on `stream`."""
+        _check(_lib.fmm_evaluate_device(self._h, n, pos_ptr, mass_ptr, acc_ptr, pot_ptr, stream))
+
+    def synchronize(self):
+        _check(_lib.fmm_synchronize(self._h))
+
+    def direct(self, pos, mass, targets=None, soft_mode=FMM_SOFT_PLUMMER, want_pot=False):
+        """FP64 direct sum on the GPU (acc = G * grad) for `targets` (all if None)."""
+        pos, mass = self._arrays(pos, mass)
+        n = pos.shape[0]
+        t = None if targets is None else np.ascontiguousarray(targets, dtype=np.int64)
+        nt = n if t is None else len(t)
+        acc = np.zeros((nt, self.dim))
+        pot = np.zeros(nt) if want_pot else None
+        _check(_lib.fmm_direct(self._h, n, _p(pos), _p(mass), nt, _p(t, _i64), soft_mode, _p(acc), _p(pot)))
+        return (acc, pot) if want_pot else acc
+
+    def direct_device(self, n, pos_ptr, mass_ptr, ntargets, targets_ptr, acc_ptr, pot_ptr=None,
+                      soft_mode=FMM_SOFT_PLUMMER, stream=None):
+        _check(_lib.fmm_direct_device(self._h, n, pos_ptr, mass_ptr, ntargets, targets_ptr, soft_mode, acc_ptr,
+                                      pot_ptr, stream))
+
+    def integrate(self, method, dt, steps, pos, vel, mass):
+        """Advances (pos, vel) by `steps` steps; returns new pos, vel and the last acc."""
+        pos, mass = self._arrays(pos, mass)
+        pos = pos.copy()
+        vel = np.array(vel, dtype=np.float64, order="C", copy=True)
+        acc = np.zeros_like(pos)
+        _check(_lib.fmm_integrate(self._h, method, dt, steps, pos.shape[0], _p(pos), _p(vel), _p(mass), _p(acc)))
+        return pos, vel, acc
+
+    def tree(self, pos, with_pairs=True):
+        """Builds the tree of `pos` and returns it in the oracle's dict layout."""
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        n = pos.shape[0]
+        _check(_lib.fmm_tree_build(self._h, n, _p(pos)))
+        D = ctypes.c_int32()
+        _check(_lib.fmm_tree_depth(self._h, ctypes.byref(D)))
+        D = D.value
+        cnt = ctypes.c_int64()
+        _check(_lib.fmm_tree_level_size(self._h, D, ctypes.byref(cnt)))
+        nl = cnt.value
+        keys = np.zeros(nl, np.uint64)
+        start = np.zeros(nl + 1, np.int64)
+        perm = np.zeros(n, np.int64)
+        _check(_lib.fmm_tree_leaves(self._h, _p(keys, _u64), _p(start, _i64), _p(perm, _i64)))
+        levels, pairs = [], []
+        for d in range(D + 1):
+            _check(_lib.fmm_tree_level_size(self._h, d, ctypes.byref(cnt)))
+            k = np.zeros(cnt.value, np.uint64)
+            _check(_lib.fmm_tree_level_keys(self._h, d, _p(k, _u64)))
+            levels.append(k)
+            pl = []
+            if with_pairs:
+                for kind in (0, 1):
+                    c = ctypes.c_int64()
+                    _check(_lib.fmm_tree_pairs(self._h, d, kind, ctypes.byref(c), None, None))
+                    tk = np.zeros(max(c.value, 1), np.uint64)
+                    sk = np.zeros(max(c.value, 1), np.uint64)
+                    _check(_lib.fmm_tree_pairs(self._h, d, kind, ctypes.byref(c), _p(tk, _u64), _p(sk, _u64)))
+                    pl.append((tk[: c.value], sk[: c.value]))
+            pairs.append(pl)
+        return dict(depth=D, leaf_keys=keys, leaf_start=start, perm=perm, level_keys=levels, pairs=pairs)
+
+    def stats(self):
+        s = FmmStats()
+        _check(_lib.fmm_last_stats(self._h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in FmmStats._fields_ if k != "reserved"}
+
+    def launch_count(self):
+        return int(_lib.fmm_launch_count(self._h))
