@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Throughput of the FMM force pass on B200 (particles per second).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+A step is one force evaluation of the whole system: tree build (the
+reference's Tree::init_tree) and every FMM pass, exactly the work of the
+reference's FMM::update (src/system_updaters/FMM.cpp:9-12).  Workload: a 3D
+Plummer sphere of N = 2^20 particles (scale radius 1, truncated at 20, seed
+2, equal masses summing to 1), expansion order p = 8, leaf capacity 64,
+forces in FP32 from FP64 positions, G = 1.
+
+value: N * K / (sum of the K per-step device times), inputs resident in HBM,
+       timed with CUDA events on the launching stream; a 256 MiB buffer is
+       written between steps (outside the event pair) to flush L2.  With N
+       GPUs each rank runs its own replica (the single-system pass does not
+       shard), value sums the particles of all ranks over the slowest rank.
+e2e:   the same metric through the public C ABI with pinned host buffers
+       (fmm_evaluate: host-to-device copy of positions and masses, the pass,
+       device-to-host copy of accelerations), wall-clock per call.
+roofline: the dominant kernel (the M2L contraction) timed live with CUDA
+       events; algorithmic FLOPs = 2 K^2 per interaction-list pair contracted,
+       K = (p+1)^2.
+cpu_baseline: the reference itself (compiled from its sources into
+       oracle/_ref) timing FMM::update on a bounded Plummer sample, 1 thread.
+--impl reference: the reference's CPU FMM on all host cores (one process per
+       core, each a bounded sample of the same workload), rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "nbody-fmm_b200"))
+
+METRIC = "3D FMM particles/s at 1e-6 rel force err: learned+TC vs plain GPU FMM"
+UNIT = "particles/s"
+REF_SAMPLE_N = 2048          # particles per reference process per step
+BASELINE_SAMPLE_N = 4096     # single-thread CPU baseline sample (about 15 s)
+
+
+def workload_desc(n, p, leaf, m2l):
+    return {
+        "workload": f"3D Plummer sphere N={n} (a=1, r<=20, seed 2), p={p}, leaf capacity {leaf}, "
+                    f"one force evaluation (tree build + all FMM passes) per step",
+        "n": n, "p": p, "leaf_cap": leaf, "m2l": m2l, "positions": "f64", "forces": "f32",
+        "l2": "256 MiB buffer written between steps (outside the timed events)",
+        "parallelism": "replicas",
+    }
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", f"fmm_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+# ---------------------------------------------------------------- ours
+def run_ours(args, world, rank, local):
+    import torch
+
+    import fmmgpu
+    from fmmgpu import workloads
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    n, p, leaf = args.n, args.p, args.leaf
+    mode = fmmgpu.FMM_M2L_TC if args.m2l == "tc" else fmmgpu.FMM_M2L_FP32
+    pos, mass = workloads.plummer(n, seed=2)
+    d_pos = torch.from_numpy(pos).to(dev)
+    d_mass = torch.from_numpy(mass).to(dev)
+    d_acc = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    d_pot = torch.empty((n,), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    ctx = fmmgpu.Context(dim=3, p=p, leaf_cap=leaf, m2l_mode=mode, G=1.0, device=local)
+    # a stream of our own (torch's default stream has handle 0, which the C
+    # ABI reads as "the context's stream")
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    sp = stream.cuda_stream
+
+    def one(pot=False):
+        ctx.evaluate_device(n, d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(),
+                            d_pot.data_ptr() if pot else None, sp)
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        one()
+        ctx.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(dev)
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    l0 = ctx.launch_count()
+    barrier()
+    step_ms, m2l_ms, stats = [], [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        one()
+        e1.record(stream)
+        ctx.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        s = ctx.stats()
+        stats.append(s)
+        m2l_ms.append(s["ms_m2l"])
+    barrier()
+    launches = ctx.launch_count() - l0
+    clocks = sampler.stop()
+    total_ms = float(sum(step_ms))
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = n * args.steps * world / (total_ms / 1e3)
+
+    # accuracy on 4096 sampled targets against the FP64 direct sum (GPU)
+    rng = np.random.default_rng(7)
+    tg = np.sort(rng.choice(n, size=min(4096, n), replace=False)).astype(np.int64)
+    d_tg = torch.from_numpy(tg).to(dev)
+    r_acc = torch.empty((len(tg), 3), dtype=torch.float64, device=dev)
+    r_pot = torch.empty((len(tg),), dtype=torch.float64, device=dev)
+    one(pot=True)
+    ctx.synchronize()
+    ctx.direct_device(n, d_pos.data_ptr(), d_mass.data_ptr(), len(tg), d_tg.data_ptr(), r_acc.data_ptr(),
+                      r_pot.data_ptr(), stream=sp)
+    torch.cuda.synchronize(dev)
+    a = d_acc[d_tg].cpu().numpy()
+    ph = d_pot[d_tg].cpu().numpy()
+    ra, rp = r_acc.cpu().numpy(), r_pot.cpu().numpy()
+    err = {
+        "targets": len(tg), "vs": "FP64 direct sum on the GPU",
+        "force_rel_l2": float(np.linalg.norm(a - ra) / np.linalg.norm(ra)),
+        "force_max_rel": float((np.linalg.norm(a - ra, axis=1) / np.linalg.norm(ra, axis=1)).max()),
+        "pot_rel_l2": float(np.linalg.norm(ph - rp) / np.linalg.norm(rp)),
+        "pot_max_rel": float((np.abs(ph - rp) / np.abs(rp)).max()),
+    }
+
+    # end to end through the C ABI with pinned host buffers
+    h_pos = torch.from_numpy(pos).pin_memory()
+    h_mass = torch.from_numpy(mass).pin_memory()
+    h_acc = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    hp, hm, ha = h_pos.numpy(), h_mass.numpy(), h_acc.numpy()
+    ctx.evaluate(hp, hm, out=ha)
+    e2e_s = 0.0
+    for _ in range(max(3, args.steps // 2)):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        ctx.evaluate(hp, hm, out=ha)
+        e2e_s += time.perf_counter() - t0
+    e2e_steps = max(3, args.steps // 2)
+    e2e_val = n * e2e_steps * world / e2e_s
+    if world > 1:
+        t = torch.tensor([e2e_val / world], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MIN)
+        e2e_val = float(t.item()) * world
+
+    # roofline of the dominant kernel (M2L contraction, FP32 SIMT)
+    s_last = stats[-1]
+    K = (p + 1) ** 2
+    flops = 2.0 * K * K * s_last["m2l_pairs"]
+    m2l_s = statistics.mean(m2l_ms) / 1e3
+    pk = peaks()
+    sm_max = float(pk.get("sm_max_mhz", 1965.0))
+    fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
+    roof = {
+        "kernel": "k_contract (M2L, FP32 SIMT)", "bound": "fp32", "unit": "TFLOP/s",
+        "achieved": flops / m2l_s / 1e12 if m2l_s > 0 else None,
+        "peak": fp32_peak,
+        "peak_source": f"derived: 148 SM x 128 FP32 lanes x 2 x {sm_max:.0f} MHz (no FP32 figure in MEASURED_PEAKS.json)",
+        "traffic": None,
+        "flops_per_launch": flops, "m2l_pairs": int(s_last["m2l_pairs"]), "ms_per_launch": m2l_s * 1e3,
+    }
+    roof["frac"] = roof["achieved"] / roof["peak"] if roof["achieved"] else None
+    traffic = load_traffic()
+    if traffic:
+        roof["traffic"] = traffic
+
+    phases = {k: float(np.mean([s[k] for s in stats])) for k in
+              ("ms_tree", "ms_upward", "ms_m2l", "ms_downward", "ms_p2p", "ms_total")}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded Plummer sphere)", "impl": "fmmgpu",
+        "config": workload_desc(n, p, leaf, args.m2l),
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(n * 3 * 8 + n * 8),
+                "d2h_bytes_per_step": int(n * 3 * 8)},
+        "roofline": roof, "error": err, "phases_ms": phases,
+        "tree": {"depth": s_last["depth"], "leaves": s_last["n_leaves"], "cells": s_last["n_cells"],
+                 "p2p_pairs": s_last["p2p_pairs"]},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(p, leaf)
+    ctx.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def load_traffic():
+    """DRAM bytes per M2L launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "m2l_traffic.json")
+    try:
+        return json.load(open(path))
+    except Exception:
+        return None
+
+
+# ------------------------------------------------------------- reference
+def _ref_worker(args):
+    n, p, leaf, seed = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    sys.path.insert(0, os.path.join(ROOT, "nbody-fmm_b200"))
+    from oracle import RefLib
+    from fmmgpu import workloads
+
+    R = RefLib()
+    pos, m = workloads.plummer(n, seed=seed)
+    t0 = time.perf_counter()
+    R.fmm(pos, m, p, leaf)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(p, leaf):
+    """The reference FMM::update, single thread, on a bounded sample."""
+    try:
+        dt = _ref_worker((BASELINE_SAMPLE_N, p, leaf, 2))
+    except Exception as e:  # reference build missing
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"unavailable: {e}"}
+    return {"value": BASELINE_SAMPLE_N / dt, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"reference FMM::update (oracle/_ref, g++ -O2), Plummer N={BASELINE_SAMPLE_N} seed 2, "
+                      f"p={p}, leaf capacity {leaf}, 1 thread, {dt:.1f} s"}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    n, p, leaf = REF_SAMPLE_N, args.p, args.leaf
+    with ctx.Pool(cores) as pool:
+        for _ in range(args.warmup):
+            pool.map(_ref_worker, [(n, p, leaf, 2 + i) for i in range(cores)])
+        step_s = []
+        for _ in range(args.steps):
+            ts = pool.map(_ref_worker, [(n, p, leaf, 2 + i) for i in range(cores)])
+            step_s.append(max(ts))
+    total = sum(step_s)
+    value = n * cores * args.steps / total
+    sample = (f"reference FMM::update (oracle/_ref, g++ -O2) on {cores} processes x Plummer N={n} (seeds 2..), "
+              f"p={p}, leaf capacity {leaf}, one process per host core; step = slowest process")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Plummer sphere)", "impl": "reference",
+        "config": workload_desc(args.n, p, leaf, "reference"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--p", type=int, default=8)
+    ap.add_argument("--leaf", type=int, default=64)
+    ap.add_argument("--m2l", default="fp32", choices=["fp32", "tc"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 0)
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

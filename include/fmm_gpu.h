@@ -79,7 +79,10 @@ typedef struct fmm_config {
   double eps2;        /* softening added to r^2 in the near field (0: the reference FMM) */
   double G;           /* gravitational constant; reference 6.6743e-11 (system_update_method.hpp:17) */
   int32_t device;     /* CUDA device ordinal */
-  int32_t reserved[7];
+  int32_t direct_max; /* interaction-list pairs (target, source) with n_target * n_source <= direct_max
+                         are summed directly (exactly) instead of through M2L; 0 = every pair by M2L
+                         as in the reference; -1 = automatic */
+  int32_t reserved[6];
 } fmm_config;
 
 typedef struct fmm_stats {
@@ -103,7 +106,7 @@ typedef struct fmm_ctx fmm_ctx;
 FMM_API const char *fmm_strerror(int code);
 FMM_API const char *fmm_version(void);
 
-/* Defaults: dim 3, p 8, leaf_cap 64, FP32 M2L, eps2 0, G 1, device 0. */
+/* Defaults: dim 3, p 8, leaf_cap 64, FP32 M2L, eps2 0, G 1, device 0, direct_max -1. */
 FMM_API int fmm_config_default(fmm_config *cfg);
 
 /* Creates a context (allocates device workspace lazily, grown on demand). */

@@ -34,7 +34,7 @@ int build_op_tables(OpTables &ops, int dim, int p, const PassGeom &g, cudaStream
 void upload_class_tables();
 
 int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, int p, double eps2, double G,
-                   const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, cudaStream_t st, fmm_stats &stats,
-                   cudaEvent_t *ev);
+                   const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, int64_t direct_max, cudaStream_t st,
+                   fmm_stats &stats, cudaEvent_t *ev);
 
 }  // namespace fmm

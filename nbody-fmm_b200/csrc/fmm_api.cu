@@ -44,6 +44,7 @@ static int check_cfg(const fmm_config *c) {
   if (c->leaf_cap < 1) return FMM_ERR_INVALID_ARGUMENT;
   if (c->m2l_mode != FMM_M2L_FP32 && c->m2l_mode != FMM_M2L_TC) return FMM_ERR_INVALID_ARGUMENT;
   if (!(c->eps2 >= 0.0)) return FMM_ERR_INVALID_ARGUMENT;
+  if (c->direct_max < -1) return FMM_ERR_INVALID_ARGUMENT;
   return FMM_OK;
 }
 
@@ -76,6 +77,7 @@ int fmm_config_default(fmm_config *cfg) {
   cfg->eps2 = 0.0;
   cfg->G = 1.0;
   cfg->device = 0;
+  cfg->direct_max = -1;
   return FMM_OK;
 }
 
@@ -132,6 +134,17 @@ int fmm_destroy(fmm_ctx *c) {
   return FMM_OK;
 }
 
+// Cut-off of the direct far field: pairs with n_t * n_s <= threshold are
+// summed particle by particle.  Automatic: the product at which one pair of
+// M2L (2 K^2 flops, K = (p+1)^2 in 3D) costs as much as n_t * n_s direct
+// interactions (~20 flops each), scaled by the contraction's lower
+// efficiency.
+static int64_t direct_threshold(const fmm_config &c) {
+  if (c.direct_max >= 0) return c.direct_max;
+  int K = c.dim == 3 ? (c.p + 1) * (c.p + 1) : 2 * c.p + 1;
+  return std::max<int64_t>(8, (int64_t)(2.0 * K * K / 20.0 / 2.5));
+}
+
 static int evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass, double *d_acc,
                            double *d_pot, cudaStream_t st) {
   const int dim = c->cfg.dim;
@@ -155,7 +168,7 @@ static int evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const dou
   if (rc) return rc;
   memset(&c->stats, 0, sizeof(c->stats));
   rc = run_fmm_passes(c->ws, c->tree, c->ops, c->eb, c->cfg.p, c->cfg.eps2, c->cfg.G, g, d_acc, d_pot,
-                      c->cfg.m2l_mode, st, c->stats, c->ev);
+                      c->cfg.m2l_mode, direct_threshold(c->cfg), st, c->stats, c->ev);
   if (rc) return rc;
   if (!c->ws.ok) return FMM_ERR_OUT_OF_MEMORY;
   c->stats.depth = c->tree.depth;
@@ -170,6 +183,10 @@ static int finish(fmm_ctx *c, cudaStream_t st) {
   unsigned int herr = 0;
   CUDA_TRY(cudaMemcpy(&herr, c->ws.dev_err, sizeof(herr), cudaMemcpyDeviceToHost));
   if (c->timing_pending) {
+    unsigned long long cnt[2] = {0, 0};
+    CUDA_TRY(cudaMemcpy(cnt, c->ws.counters, sizeof(cnt), cudaMemcpyDeviceToHost));
+    c->stats.m2l_pairs = (int64_t)cnt[0];
+    c->stats.p2p_pairs = (int64_t)cnt[1];
     float ms[5] = {0, 0, 0, 0, 0};
     for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], c->ev[i], c->ev[i + 1]);
     c->stats.ms_tree = ms[0];

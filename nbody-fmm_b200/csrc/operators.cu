@@ -110,10 +110,12 @@ __global__ void k_build_ops3d(float *tab, int p, int K, int KP, int n_m2l, doubl
   bool zero = false;
   if (slot < n_m2l) {
     kind = 0;
+    // slot offset = source cell - target cell; M2L translates by
+    // rho = (c_target - c_source) / s
     int dx = slot % 7 - 3, dy = (slot / 7) % 7 - 3, dz = slot / 49 - 3;
-    r[0] = dx * ax;
-    r[1] = dy * ay;
-    r[2] = dz * az;
+    r[0] = -dx * ax;
+    r[1] = -dy * ay;
+    r[2] = -dz * az;
     if ((dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 && dz <= 1) ||
         r[0] * r[0] + r[1] * r[1] + r[2] * r[2] == 0.0)
       zero = true;
@@ -219,8 +221,8 @@ __global__ void k_build_ops2d(float *tab, int p, int K, int KP, int n_m2l, doubl
   bool zero = false;
   if (slot < n_m2l) {
     kind = 0;
-    int dx = slot % 7 - 3, dy = slot / 7 - 3;
-    z = {dx * ax, dy * ay};
+    int dx = slot % 7 - 3, dy = slot / 7 - 3;  // source - target
+    z = {-dx * ax, -dy * ay};
     if ((dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1) || (z.re == 0.0 && z.im == 0.0)) zero = true;
   } else {
     int s = slot - n_m2l;

@@ -85,8 +85,10 @@ struct ContractArgs {
   const float *X;
   float *Y;
   const float *tab;
-  const int *cparent, *cchild, *ccoll;
+  const int *cparent, *cchild, *ccoll, *cpbeg, *cpend;
+  long long direct_max;  // M2L skips pairs with n_t * n_s <= direct_max (summed directly instead)
   int cell0, K, KS, KP, dim, mode, slot_base, level_stride;
+  unsigned long long *pair_count;  // M2L: number of (target, source) pairs contracted
 };
 
 // Resolves the source cell of target `tgt` for slot s; returns -1 if absent.
@@ -98,7 +100,12 @@ __device__ inline int contract_source(const ContractArgs &a, int tgt, int s, int
     int P = a.cparent[tgt];
     int Q = a.ccoll[(int64_t)P * ns + ((e >> 9) & 31)];
     if (Q < 0) return -1;
-    return a.cchild[(int64_t)Q * nc + ((e >> 14) & 7)];
+    int src = a.cchild[(int64_t)Q * nc + ((e >> 14) & 7)];
+    if (src >= 0 && a.direct_max > 0) {
+      long long nt = a.cpend[tgt] - a.cpbeg[tgt], nsrc = a.cpend[src] - a.cpbeg[src];
+      if (nt * nsrc <= a.direct_max) return -1;  // evaluated by the direct far field
+    }
+    return src;
   } else if (a.mode == MODE_M2M) {
     tslot = a.slot_base + s;
     return a.cchild[(int64_t)tgt * nc + s];
@@ -126,6 +133,7 @@ __global__ void __launch_bounds__(CT_THREADS) k_contract(ContractArgs a) {
   __syncthreads();
   const int nslots = a.mode == MODE_M2L ? (a.dim == 3 ? 189 : 27) : (a.mode == MODE_M2M ? (1 << a.dim) : 1);
 
+  unsigned long long npairs = 0;
   float acc[8][J];
 #pragma unroll
   for (int i = 0; i < 8; ++i)
@@ -140,8 +148,11 @@ __global__ void __launch_bounds__(CT_THREADS) k_contract(ContractArgs a) {
       s_src[buf * CT_TGT + tid] = src;
       if (tid == 0 || src >= 0) s_tslot[buf] = ts;  // same for all targets of the batch
     }
-    int any = __syncthreads_or(src >= 0);
-    if (tid == 0) s_any[buf] = any;
+    int any = __syncthreads_count(src >= 0);
+    if (tid == 0) {
+      s_any[buf] = any;
+      npairs += any;
+    }
     if (any) {
       const float *T = a.tab + (size_t)s_tslot[buf] * K * KP;
       float *Td = Ts + (size_t)buf * K * KP;
@@ -192,6 +203,7 @@ __global__ void __launch_bounds__(CT_THREADS) k_contract(ContractArgs a) {
     }
     __syncthreads();
   }
+  if (tid == 0 && a.pair_count && a.mode == MODE_M2L) atomicAdd(a.pair_count, npairs);
   // write out
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
@@ -376,44 +388,167 @@ __global__ void k_l2p3d(const float4 *part, const int *leaf_of, int64_t n, int c
 // One warp per target leaf; the leaf's particles are spread over the lanes
 // (several lanes per particle for small leaves, each taking a share of the
 // sources).  Sources are the leaf itself (j != i) and its existing
-// neighbours (leaf.cpp:118-142), in FP32 relative to the target leaf centre.
-__global__ void k_p2p3d(int leaf_first, int nleaves, const int *pbeg, const int *pend, const int *coll,
-                        const float4 *part, const float4 *far, const uint32_t *perm, float hx, float hy, float hz,
-                        float eps2, double G, double *acc, double *pot, unsigned int *err) {
+// neighbours (leaf.cpp:118-142).
+//
+// Precision: x_i - x_j = (t_i - shift) - s_j with t_i, s_j the offsets from
+// the two leaf centres and shift = c_s - c_t an exact multiple of the leaf
+// size.  Offsets are hi + lo FP32 pairs, the shift is hi + lo from FP64, and
+// (t_hi - shift_hi) is formed error-free (TwoSum), so each difference is
+// rounded once, relative to itself, whatever the separation.
+__device__ inline void two_sum(float a, float b, float &s, float &e) {
+  s = a + b;
+  float bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+
+struct P2PArgs {
+  int leaf_first, nleaves, depth;
+  const int *pbeg, *pend, *coll, *parent, *child, *leaf_of;
+  const uint64_t *ckey;
+  const float4 *part, *part_lo, *far;
+  const uint32_t *perm;
+  double hx, hy, hz;
+  float eps2;
+  long long direct_max;
+  double G;
+  double *acc, *pot;
+  unsigned int *err;
+  unsigned long long *pair_count;
+};
+
+// Sums source particles [jb, je) onto this lane's target, target offset
+// (tx, ty, tz) already expressed in the sources' leaf frame (plain FP32:
+// used for well-separated cells, at least two cells apart).
+__device__ inline void p2p_far_range(const float4 *part, int jb, int je, int sub, int Gl, float tx, float ty, float tz,
+                                     float eps2, float &ax, float &ay, float &az, float &ph) {
+  for (int j = jb + sub; j < je; j += Gl) {
+    const float4 q = part[j];
+    const float rx = tx - q.x, ry = ty - q.y, rz = tz - q.z;
+    const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2)));
+    float inv = rsqrtf(r2);
+    inv = inv * fmaf(-0.5f * r2 * inv, inv, 1.5f);
+    const float mi = q.w * inv;
+    const float mi3 = mi * inv * inv;
+    ax = fmaf(-rx, mi3, ax);
+    ay = fmaf(-ry, mi3, ay);
+    az = fmaf(-rz, mi3, az);
+    ph += mi;
+  }
+}
+
+// One warp per target leaf; the leaf's particles are spread over the lanes
+// (several lanes per particle for small leaves, each taking a share of the
+// sources).  Sources:
+//  - near field: the leaf itself (j != i) and its existing neighbours
+//    (leaf.cpp:118-142);
+//  - direct far field: the cells of the interaction lists of the leaf and of
+//    its ancestors with n_target * n_source <= direct_max (the M2L pass skips
+//    exactly these pairs).  An ancestor with more than direct_max particles
+//    cannot have such a pair, which ends the walk up the tree.
+//
+// Near-field precision: x_i - x_j = (t_i - shift) - s_j with t_i, s_j the
+// offsets from the two leaf centres and shift = c_s - c_t an exact multiple
+// of the leaf size.  Offsets are hi + lo FP32 pairs, the shift is hi + lo
+// from FP64, and (t_hi - shift_hi) is formed error-free (TwoSum), so each
+// difference is rounded once, relative to itself, whatever the separation.
+__global__ void k_p2p3d(P2PArgs a) {
   const int lane = threadIdx.x & 31;
   const int wl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (wl >= nleaves) return;
-  const int g = leaf_first + wl;
-  const int tb = pbeg[g], nt = pend[g] - tb;
+  if (wl >= a.nleaves) return;
+  const int g = a.leaf_first + wl;
+  const int tb = a.pbeg[g], nt = a.pend[g] - tb;
   const int tp = nt < 32 ? nt : 32;
   int Gl = 1;
   while (Gl * 2 * tp <= 32) Gl *= 2;
   const int tpp = 32 / Gl;
-  const int *cl = coll + (int64_t)g * 27;
+  const int *cl = a.coll + (int64_t)g * 27;
+  uint32_t gx, gy, gz;
+  morton_decode(3, a.ckey[g], gx, gy, gz);
   bool bad = false;
+  long long npairs = 0;
   for (int t0 = 0; t0 < nt; t0 += tpp) {
     const int ti = t0 + lane / Gl, sub = lane % Gl;
     const bool act = ti < nt;
     const int me_i = tb + (act ? ti : 0);
-    const float4 me = part[me_i];
+    const float4 me = a.part[me_i], mel = a.part_lo[me_i];
     float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
     for (int s = 0; s < 27; ++s) {
       const int S = cl[s];
       if (S < 0) continue;
-      const float tx = me.x - (s % 3 - 1) * hx, ty = me.y - ((s / 3) % 3 - 1) * hy, tz = me.z - (s / 9 - 1) * hz;
-      const int se = pend[S];
-      for (int j = pbeg[S] + sub; j < se; j += Gl) {
+      // shift = c_s - c_t in hi + lo
+      const double sx = (s % 3 - 1) * a.hx, sy = ((s / 3) % 3 - 1) * a.hy, sz = (s / 9 - 1) * a.hz;
+      const float shx = (float)sx, shy = (float)sy, shz = (float)sz;
+      float tx, ty, tz, ex, ey, ez;
+      two_sum(me.x, -shx, tx, ex);
+      two_sum(me.y, -shy, ty, ey);
+      two_sum(me.z, -shz, tz, ez);
+      ex += mel.x - (float)(sx - (double)shx);
+      ey += mel.y - (float)(sy - (double)shy);
+      ez += mel.z - (float)(sz - (double)shz);
+      const int se = a.pend[S];
+      if (t0 == 0 && lane == 0) npairs += (long long)nt * (se - a.pbeg[S]) - (S == g ? nt : 0);
+      for (int j = a.pbeg[S] + sub; j < se; j += Gl) {
         if (j == me_i) continue;
-        const float4 q = part[j];
-        const float rx = tx - q.x, ry = ty - q.y, rz = tz - q.z;
-        const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2)));
-        const float inv = rsqrtf(r2);
+        const float4 q = a.part[j], ql = a.part_lo[j];
+        const float rx = (tx - q.x) + (ex - ql.x);
+        const float ry = (ty - q.y) + (ey - ql.y);
+        const float rz = (tz - q.z) + (ez - ql.z);
+        const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, a.eps2)));
+        float inv = rsqrtf(r2);
+        inv = inv * fmaf(-0.5f * r2 * inv, inv, 1.5f);  // one Newton step
         const float mi = q.w * inv;
         const float mi3 = mi * inv * inv;
         ax = fmaf(-rx, mi3, ax);
         ay = fmaf(-ry, mi3, ay);
         az = fmaf(-rz, mi3, az);
         ph += mi;
+      }
+    }
+    // direct far field, walking up from the leaf
+    if (a.direct_max > 0) {
+      int A = g;
+      for (int d = a.depth; d >= 2; --d) {
+        const long long nA = a.pend[A] - a.pbeg[A];
+        if (nA > a.direct_max) break;
+        const int P = a.parent[A];
+        const int cls = (int)(a.ckey[A] & 7u);
+        const int *pc = a.coll + (int64_t)P * 27;
+        for (int c0 = 0; c0 < 216; c0 += 32) {
+          const int cand = c0 + lane;
+          int q = -1;
+          if (cand < 216) {
+            const int dl = cand >> 3, k = cand & 7;
+            const int Q = pc[dl];
+            if (Q >= 0) {
+              q = a.child[(int64_t)Q * 8 + k];
+              if (q >= 0) {
+                const int ddx = 2 * (dl % 3 - 1) + (k & 1) - (cls & 1);
+                const int ddy = 2 * ((dl / 3) % 3 - 1) + ((k >> 1) & 1) - ((cls >> 1) & 1);
+                const int ddz = 2 * (dl / 9 - 1) + ((k >> 2) & 1) - ((cls >> 2) & 1);
+                const bool adj = ddx >= -1 && ddx <= 1 && ddy >= -1 && ddy <= 1 && ddz >= -1 && ddz <= 1;
+                if (adj || nA * (long long)(a.pend[q] - a.pbeg[q]) > a.direct_max) q = -1;
+              }
+            }
+          }
+          unsigned mask = __ballot_sync(0xffffffffu, q >= 0);
+          while (mask) {
+            const int b = __ffs(mask) - 1;
+            mask &= mask - 1;
+            const int S = __shfl_sync(0xffffffffu, q, b);
+            const int l0 = a.leaf_of[a.pbeg[S]], l1 = a.leaf_of[a.pend[S] - 1];
+            if (t0 == 0 && lane == 0) npairs += (long long)nt * (a.pend[S] - a.pbeg[S]);
+            for (int l = l0; l <= l1; ++l) {
+              uint32_t lx, ly, lz;
+              morton_decode(3, a.ckey[l], lx, ly, lz);
+              const float shx = (float)(((double)lx - (double)gx) * a.hx);
+              const float shy = (float)(((double)ly - (double)gy) * a.hy);
+              const float shz = (float)(((double)lz - (double)gz) * a.hz);
+              p2p_far_range(a.part, a.pbeg[l], a.pend[l], sub, Gl, me.x - shx, me.y - shy, me.z - shz, a.eps2, ax,
+                            ay, az, ph);
+            }
+          }
+        }
+        A = P;
       }
     }
     for (int o = 1; o < Gl; o <<= 1) {
@@ -423,17 +558,18 @@ __global__ void k_p2p3d(int leaf_first, int nleaves, const int *pbeg, const int 
       ph += __shfl_xor_sync(0xffffffffu, ph, o);
     }
     if (act && sub == 0) {
-      const float4 f = far[me_i];
-      const uint32_t o = perm[me_i];
-      double vx = G * ((double)f.x + ax), vy = G * ((double)f.y + ay), vz = G * ((double)f.z + az);
-      acc[3 * (size_t)o] = vx;
-      acc[3 * (size_t)o + 1] = vy;
-      acc[3 * (size_t)o + 2] = vz;
-      if (pot) pot[o] = G * ((double)f.w + ph);
+      const float4 f = a.far[me_i];
+      const uint32_t o = a.perm[me_i];
+      double vx = a.G * ((double)f.x + ax), vy = a.G * ((double)f.y + ay), vz = a.G * ((double)f.z + az);
+      a.acc[3 * (size_t)o] = vx;
+      a.acc[3 * (size_t)o + 1] = vy;
+      a.acc[3 * (size_t)o + 2] = vz;
+      if (a.pot) a.pot[o] = a.G * ((double)f.w + ph);
       bad |= !(isfinite(vx) && isfinite(vy) && isfinite(vz));
     }
   }
-  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(err, FMM_DEV_ERR_NONFINITE_OUTPUT);
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.err, FMM_DEV_ERR_NONFINITE_OUTPUT);
+  if (lane == 0 && a.pair_count) atomicAdd(a.pair_count, (unsigned long long)npairs);
 }
 
 // ------------------------------------------------------------------ lists
@@ -447,16 +583,21 @@ __global__ void k_class_keys(const uint64_t *ckey, int first, int count, int lev
 }
 
 __global__ void k_class_hist(const uint64_t *keys, int n, uint32_t *hist) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) atomicAdd(&hist[keys[i] & 255u], 1u);
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    atomicAdd(&h[keys[i] & 255u], 1u);
+  __syncthreads();
+  if (h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
 }
 
 // ------------------------------------------------------------ driver
 static inline float fmax3(float a, float b, float c) { return std::max(a, std::max(b, c)); }
 
 int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, int p, double eps2, double G,
-                   const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, cudaStream_t st, fmm_stats &stats,
-                   cudaEvent_t *ev) {
+                   const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, int64_t direct_max, cudaStream_t st,
+                   fmm_stats &stats, cudaEvent_t *ev) {
   (void)m2l_mode;
   const int dim = t.dim, D = t.depth, KS = ops.KS;
   const int64_t n = t.n;
@@ -488,7 +629,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, i
     radix_sort(ws, kk, vv, kk2, vv2, ntl, 8, st);  // sorted (keys, cells) end in (kk, vv)
     tl = (const int *)vv;
     CUDA_TRY(cudaMemsetAsync(eb.cls_count.ptr, 0, 256 * sizeof(uint32_t), st));
-    k_class_hist<<<cdiv(ntl, TPB), TPB, 0, st>>>(kk, ntl, eb.cls_count.ptr);
+    k_class_hist<<<std::min(cdiv(ntl, TPB), 148 * 4), TPB, 0, st>>>(kk, ntl, eb.cls_count.ptr);
     ws.launches += 1;
     uint32_t hc[256];
     CUDA_TRY(cudaMemcpyAsync(hc, eb.cls_count.ptr, sizeof(hc), cudaMemcpyDeviceToHost, st));
@@ -524,12 +665,17 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, i
   ca.cparent = ws.cell_parent;
   ca.cchild = ws.cell_child;
   ca.ccoll = ws.cell_coll;
+  ca.cpbeg = ws.cell_pbeg;
+  ca.cpend = ws.cell_pend;
+  ca.direct_max = direct_max;
   ca.cell0 = cell0;
   ca.K = ops.K;
   ca.KS = KS;
   ca.KP = ops.KP;
   ca.dim = dim;
   ca.level_stride = dim == 2 ? 49 : 0;
+  ca.pair_count = ws.counters;
+  CUDA_TRY(cudaMemsetAsync(ws.counters, 0, 2 * sizeof(unsigned long long), st));
 
   if (ev) cudaEventRecord(ev[1], st);
   // P2M
@@ -579,11 +725,32 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, i
   if (ev) cudaEventRecord(ev[4], st);
   // P2P + output
   const double inv2D = std::ldexp(1.0, -D);
-  const float hx = (float)(g.ext[0] * inv2D), hy = (float)(g.ext[1] * inv2D), hz = (float)(g.ext[2] * inv2D);
-  const int nl = t.level_count[D];
-  k_p2p3d<<<cdiv((int64_t)nl * 32, TPB), TPB, 0, st>>>(t.level_off[D], nl, ws.cell_pbeg, ws.cell_pend, ws.cell_coll,
-                                                      ws.part, ws.far, t.d_perm, hx, hy, hz, (float)eps2, G, d_acc,
-                                                      d_pot, ws.dev_err);
+  P2PArgs pa;
+  pa.leaf_first = t.level_off[D];
+  pa.nleaves = t.level_count[D];
+  pa.depth = D;
+  pa.pbeg = ws.cell_pbeg;
+  pa.pend = ws.cell_pend;
+  pa.coll = ws.cell_coll;
+  pa.parent = ws.cell_parent;
+  pa.child = ws.cell_child;
+  pa.leaf_of = ws.leaf_of;
+  pa.ckey = ws.cell_key;
+  pa.part = ws.part;
+  pa.part_lo = ws.part_lo;
+  pa.far = ws.far;
+  pa.perm = t.d_perm;
+  pa.hx = g.ext[0] * inv2D;
+  pa.hy = g.ext[1] * inv2D;
+  pa.hz = g.ext[2] * inv2D;
+  pa.eps2 = (float)eps2;
+  pa.direct_max = direct_max;
+  pa.G = G;
+  pa.acc = d_acc;
+  pa.pot = d_pot;
+  pa.err = ws.dev_err;
+  pa.pair_count = ws.counters + 1;
+  k_p2p3d<<<cdiv((int64_t)pa.nleaves * 32, TPB), TPB, 0, st>>>(pa);
   ws.launches += 1;
   if (ev) cudaEventRecord(ev[5], st);
   stats.n_cells = ncell;

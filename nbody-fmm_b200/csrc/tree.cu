@@ -371,24 +371,28 @@ __global__ void k_fill_i32(int *p, int64_t n, int v) {
   if (i < n) p[i] = v;
 }
 
-// Gathers particles into leaf order: FP32 offset from the leaf's geometric
-// centre and FP32 mass (float4), used by P2M, L2P and P2P.
+// Gathers particles into leaf order: the offset from the leaf's geometric
+// centre split into FP32 hi + lo parts (x - c = hi + lo to ~48 bits), and the
+// FP32 mass, used by P2M, L2P (hi only) and P2P (hi and lo).
 __global__ void k_gather_particles(const double *pos, const double *mass, const uint32_t *perm, const int *leaf_of,
                                    const uint64_t *ckey, int64_t n, int dim, int depth, const double *geom,
-                                   float4 *part) {
+                                   float4 *part, float4 *part_lo) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint32_t j = perm[i];
   uint32_t q[3];
   morton_decode(dim, ckey[leaf_of[i]], q[0], q[1], q[2]);
-  float r[3] = {0.f, 0.f, 0.f};
+  float r[3] = {0.f, 0.f, 0.f}, rl[3] = {0.f, 0.f, 0.f};
   const double inv = ldexp(1.0, -depth);
   for (int d = 0; d < dim; ++d) {
     double ext = geom[3 + d] - geom[d];
     double c = geom[d] + ((double)q[d] + 0.5) * (ext * inv);
-    r[d] = (float)(pos[(int64_t)j * dim + d] - c);
+    double v = pos[(int64_t)j * dim + d] - c;
+    r[d] = (float)v;
+    rl[d] = (float)(v - (double)r[d]);
   }
   part[i] = make_float4(r[0], r[1], r[2], (float)mass[j]);
+  part_lo[i] = make_float4(rl[0], rl[1], rl[2], 0.f);
 }
 
 // ------------------------------------------------------------ host driver
@@ -514,7 +518,8 @@ int build_tree(Workspace &ws, TreeState &t, const double *d_pos, const double *d
     ws.launches += 1;
   }
   // particles in leaf order
-  k_gather_particles<<<nbN, TPB, 0, st>>>(d_pos, d_mass, pv, ws.leaf_of, ws.cell_key, n, dim, D, ws.geom, ws.part);
+  k_gather_particles<<<nbN, TPB, 0, st>>>(d_pos, d_mass, pv, ws.leaf_of, ws.cell_key, n, dim, D, ws.geom, ws.part,
+                                             ws.part_lo);
   ws.launches += 1;
   CUDA_TRY(cudaGetLastError());
   return FMM_OK;

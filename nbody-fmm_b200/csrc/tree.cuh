@@ -51,7 +51,8 @@ struct Workspace {
   DevBuf<uint64_t> bkeyA, bkeyB, bkeyC;
   DevBuf<uint32_t> bvalA, bvalB, bvalC, bu32A, bu32B, bu32C;
   DevBuf<int> bleaf_of;
-  DevBuf<float4> bpart;      // leaf-relative FP32 offset + mass, leaf order
+  DevBuf<float4> bpart;      // leaf-relative FP32 offset (hi part) + mass, leaf order
+  DevBuf<float4> bpart_lo;   // low part of the offset
   DevBuf<float4> bfar;       // far-field gradient (xyz) and potential (w), leaf order
   // per cell
   DevBuf<uint64_t> bcell_key;
@@ -62,22 +63,25 @@ struct Workspace {
   DevBuf<double> bgeom;
   DevBuf<uint32_t> bscalars;
   DevBuf<unsigned int> berr;
+  DevBuf<unsigned long long> bcount;  // [0] M2L pairs, [1] P2P particle pairs
 
   uint64_t *keyA = nullptr, *keyB = nullptr, *keyC = nullptr;
   uint32_t *valA = nullptr, *valB = nullptr, *valC = nullptr, *u32A = nullptr, *u32B = nullptr, *u32C = nullptr;
   int *leaf_of = nullptr;
-  float4 *part = nullptr, *far = nullptr;
+  float4 *part = nullptr, *part_lo = nullptr, *far = nullptr;
   uint64_t *cell_key = nullptr;
   int *cell_pbeg = nullptr, *cell_pend = nullptr, *cell_parent = nullptr, *cell_child = nullptr, *cell_coll = nullptr;
   unsigned long long *box_u64 = nullptr;
   double *geom = nullptr;
   uint32_t *scalars = nullptr;
   unsigned int *dev_err = nullptr;
+  unsigned long long *counters = nullptr;
   int64_t launches = 0;
   bool ok = true;
 
   bool init_small() {
-    ok &= bbox.reserve(8) && bgeom.reserve(8) && bscalars.reserve(8) && berr.reserve(4);
+    ok &= bbox.reserve(8) && bgeom.reserve(8) && bscalars.reserve(8) && berr.reserve(4) && bcount.reserve(4);
+    counters = bcount.ptr;
     box_u64 = bbox.ptr;
     geom = bgeom.ptr;
     scalars = bscalars.ptr;
@@ -88,12 +92,13 @@ struct Workspace {
     size_t m = (size_t)(n > 0 ? n : 1);
     ok &= bkeyA.reserve(m) && bkeyB.reserve(m) && bkeyC.reserve(m) && bvalA.reserve(m) && bvalB.reserve(m) &&
           bvalC.reserve(m) && bu32A.reserve(m) && bu32B.reserve(m) && bu32C.reserve(m) && bleaf_of.reserve(m) &&
-          bpart.reserve(m) && bfar.reserve(m);
+          bpart.reserve(m) && bpart_lo.reserve(m) && bfar.reserve(m);
     keyA = bkeyA.ptr; keyB = bkeyB.ptr; keyC = bkeyC.ptr;
     valA = bvalA.ptr; valB = bvalB.ptr; valC = bvalC.ptr;
     u32A = bu32A.ptr; u32B = bu32B.ptr; u32C = bu32C.ptr;
     leaf_of = bleaf_of.ptr;
     part = bpart.ptr;
+    part_lo = bpart_lo.ptr;
     far = bfar.ptr;
     return ok;
   }
@@ -121,10 +126,10 @@ struct Workspace {
     bkeyA.release(); bkeyB.release(); bkeyC.release();
     bvalA.release(); bvalB.release(); bvalC.release();
     bu32A.release(); bu32B.release(); bu32C.release();
-    bleaf_of.release(); bpart.release(); bfar.release();
+    bleaf_of.release(); bpart.release(); bpart_lo.release(); bfar.release();
     bcell_key.release(); bcell_pbeg.release(); bcell_pend.release(); bcell_parent.release();
     bcell_child.release(); bcell_coll.release();
-    bscan.release(); bhist.release(); bbox.release(); bgeom.release(); bscalars.release(); berr.release();
+    bscan.release(); bhist.release(); bbox.release(); bgeom.release(); bscalars.release(); berr.release(); bcount.release();
   }
 };
 

@@ -49,7 +49,7 @@ class FmmConfig(ctypes.Structure):
     _fields_ = [
         ("dim", ctypes.c_int32), ("p", ctypes.c_int32), ("leaf_cap", ctypes.c_int32), ("m2l_mode", ctypes.c_int32),
         ("eps2", ctypes.c_double), ("G", ctypes.c_double), ("device", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 7),
+        ("direct_max", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6),
     ]
 
 
@@ -121,12 +121,12 @@ def _p(a, t=_d):
 class Context:
     """One FMM force evaluator on one GPU (fmm_create / fmm_destroy)."""
 
-    def __init__(self, dim=3, p=8, leaf_cap=64, m2l_mode=FMM_M2L_FP32, eps2=0.0, G=1.0, device=0):
+    def __init__(self, dim=3, p=8, leaf_cap=64, m2l_mode=FMM_M2L_FP32, eps2=0.0, G=1.0, device=0, direct_max=-1):
         L = load_library()
         cfg = FmmConfig()
         _check(L.fmm_config_default(ctypes.byref(cfg)))
         cfg.dim, cfg.p, cfg.leaf_cap, cfg.m2l_mode = dim, p, leaf_cap, m2l_mode
-        cfg.eps2, cfg.G, cfg.device = eps2, G, device
+        cfg.eps2, cfg.G, cfg.device, cfg.direct_max = eps2, G, device, direct_max
         h = _vp()
         _check(L.fmm_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
@@ -154,12 +154,15 @@ class Context:
             raise FmmError(FMM_ERR_INVALID_ARGUMENT, "pos must be (n, dim) and mass (n,)")
         return pos, mass
 
-    def evaluate(self, pos, mass, want_pot=False):
-        """One force pass (host buffers): returns acc (n, dim) [, pot (n,)]."""
+    def evaluate(self, pos, mass, want_pot=False, out=None, out_pot=None):
+        """One force pass (host buffers): returns acc (n, dim) [, pot (n,)].
+        `out` / `out_pot` may be preallocated (e.g. pinned) C-contiguous float64 arrays."""
         pos, mass = self._arrays(pos, mass)
         n = pos.shape[0]
-        acc = np.zeros((n, self.dim))
-        pot = np.zeros(n) if want_pot else None
+        acc = out if out is not None else np.zeros((n, self.dim))
+        if acc.shape != (n, self.dim) or acc.dtype != np.float64 or not acc.flags.c_contiguous:
+            raise FmmError(FMM_ERR_INVALID_ARGUMENT, "out must be a C-contiguous (n, dim) float64 array")
+        pot = (out_pot if out_pot is not None else np.zeros(n)) if want_pot else None
         _check(_lib.fmm_evaluate(self._h, n, _p(pos), _p(mass), _p(acc), _p(pot)))
         return (acc, pot) if want_pot else acc
 

@@ -551,8 +551,26 @@ static void l2l_2d(int p, const cplx *b, cplx z, cplx *out) {
 /* Tree::compute_accelerations, tree.cpp:93-111: P2M/M2M bottom-up, M2L over
  * every interaction list, L2L top-down, then per leaf L2P + P2P over the leaf
  * itself (j != i) and its neighbour leaves (leaf.cpp:55-148). */
+static void pair_kernel(int dim, const double *xi, const double *xj, double mj, double eps2, double *g, double *ph) {
+  double dd[3] = {0, 0, 0}, r2 = eps2;
+  for (int a = 0; a < dim; ++a) { dd[a] = xi[a] - xj[a]; r2 += dd[a] * dd[a]; }
+  if (dim == 3) {
+    double ir = 1.0 / sqrt(r2);
+    for (int a = 0; a < 3; ++a) g[a] -= mj * dd[a] * ir * ir * ir;
+    *ph += mj * ir;
+  } else {
+    for (int a = 0; a < 2; ++a) g[a] -= mj * dd[a] / r2;
+    *ph -= 0.5 * mj * log(r2);
+  }
+}
+
 int orc_fmm(int dim, int64_t n, const double *pos, const double *mass, unsigned p_, unsigned threshold,
             int centre_mode, double *grad, double *pot) {
+  return orc_fmm_ex(dim, n, pos, mass, p_, threshold, centre_mode, 0.0, 0, grad, pot);
+}
+
+int orc_fmm_ex(int dim, int64_t n, const double *pos, const double *mass, unsigned p_, unsigned threshold,
+               int centre_mode, double eps2, int64_t direct_max, double *grad, double *pot) {
   orc_tree *t = orc_tree_build(dim, n, pos, threshold);
   if (!t) return -1;
   int p = (int)p_, D = t->depth;
@@ -569,6 +587,17 @@ int orc_fmm(int dim, int64_t n, const double *pos, const double *mass, unsigned 
   }
   double ext[3];
   for (int a = 0; a < dim; ++a) ext[a] = t->hi[a] - t->lo[a];
+  /* particle range [pb, pe) of every cell in leaf order */
+  int64_t **pb = (int64_t **)calloc(D + 1, sizeof(int64_t *)), **pe = (int64_t **)calloc(D + 1, sizeof(int64_t *));
+  for (int d = D; d >= 0; --d) {
+    pb[d] = (int64_t *)malloc(sizeof(int64_t) * t->ncell[d]);
+    pe[d] = (int64_t *)malloc(sizeof(int64_t) * t->ncell[d]);
+    for (int64_t i = 0; i < t->ncell[d]; ++i) {
+      if (d == D) { pb[d][i] = t->leaf_start[i]; pe[d][i] = t->leaf_start[i + 1]; }
+      else { pb[d][i] = pb[d + 1][t->cbeg[d][i]]; pe[d][i] = pe[d + 1][t->cend[d][i] - 1]; }
+    }
+  }
+  double *fd = (double *)calloc((size_t)n * 4, sizeof(double)); /* direct far field: grad xyz + phi per input index */
   /* centres */
   for (int d = D; d >= 0; --d)
     for (int64_t i = 0; i < t->ncell[d]; ++i) {
@@ -618,11 +647,21 @@ int orc_fmm(int dim, int64_t n, const double *pos, const double *mass, unsigned 
         }
       }
     }
-  /* M2L */
+  /* M2L (or the direct far field for small pairs) */
   for (int d = 0; d <= D; ++d)
     for (int64_t i = 0; i < t->ncell[d]; ++i)
       for (int64_t k = t->il_off[d][i]; k < t->il_off[d][i + 1]; ++k) {
         int64_t s = t->il_idx[d][k];
+        if (direct_max > 0 && (pe[d][i] - pb[d][i]) * (pe[d][s] - pb[d][s]) <= direct_max) {
+          for (int64_t a = pb[d][i]; a < pe[d][i]; ++a) {
+            int64_t pi = t->perm[a];
+            for (int64_t b = pb[d][s]; b < pe[d][s]; ++b) {
+              int64_t pj = t->perm[b];
+              pair_kernel(dim, pos + pi * dim, pos + pj * dim, mass[pj], eps2, fd + 4 * pi, fd + 4 * pi + 3);
+            }
+          }
+          continue;
+        }
         double r[3] = {0, 0, 0};
         for (int a = 0; a < dim; ++a) r[a] = cen[d][3 * i + a] - cen[d][3 * s + a];
         if (dim == 3) m2l_3d(p, M[d] + (int64_t)K * s, r, Lx[d] + (int64_t)K * i, work);
@@ -665,24 +704,15 @@ int orc_fmm(int dim, int64_t n, const double *pos, const double *mass, unsigned 
         for (int64_t kk = t->leaf_start[src]; kk < t->leaf_start[src + 1]; ++kk) {
           int64_t pj = t->perm[kk];
           if (pj == pi) continue;
-          double dd[3] = {0, 0, 0}, r2 = 0;
-          for (int a = 0; a < dim; ++a) { dd[a] = pos[pi * dim + a] - pos[pj * dim + a]; r2 += dd[a] * dd[a]; }
-          if (dim == 3) {
-            double ir = 1.0 / sqrt(r2);
-            for (int a = 0; a < 3; ++a) g[a] -= mass[pj] * dd[a] * ir * ir * ir;
-            ph += mass[pj] * ir;
-          } else {
-            for (int a = 0; a < 2; ++a) g[a] -= mass[pj] * dd[a] / r2;
-            ph -= 0.5 * mass[pj] * log(r2);
-          }
+          pair_kernel(dim, pos + pi * dim, pos + pj * dim, mass[pj], eps2, g, &ph);
         }
       }
-      for (int a = 0; a < dim; ++a) grad[pi * dim + a] = g[a];
-      if (pot) pot[pi] = ph;
+      for (int a = 0; a < dim; ++a) grad[pi * dim + a] = g[a] + fd[4 * pi + a];
+      if (pot) pot[pi] = ph + fd[4 * pi + 3];
     }
   }
-  for (int d = 0; d <= D; ++d) { free(cen[d]); free(M[d]); free(Lx[d]); }
-  free(cen); free(M); free(Lx); free(work);
+  for (int d = 0; d <= D; ++d) { free(cen[d]); free(M[d]); free(Lx[d]); free(pb[d]); free(pe[d]); }
+  free(cen); free(M); free(Lx); free(work); free(pb); free(pe); free(fd);
   orc_tree_free(t);
   return 0;
 }

@@ -54,6 +54,12 @@ void orc_naive_ref(int dim, int64_t n, const double *pos, const double *mass, do
  * are not convergent); 2D follows multipole_set2D.cpp / local_set2D.cpp. */
 int orc_fmm(int dim, int64_t n, const double *pos, const double *mass, unsigned p, unsigned threshold,
             int centre_mode, double *grad, double *pot);
+/* The same with a near-field softening eps2 (r^2 -> r^2 + eps2 in P2P and
+ * in the direct far field) and a direct far field: interaction-list pairs
+ * with n_target * n_source <= direct_max are summed particle by particle
+ * instead of by M2L (0 = none, as the reference). */
+int orc_fmm_ex(int dim, int64_t n, const double *pos, const double *mass, unsigned p, unsigned threshold,
+               int centre_mode, double eps2, int64_t direct_max, double *grad, double *pot);
 
 /* Scaled solid harmonics used by the CUDA path, m >= 0 only, packed
  * idx(n,m) = n(n+1)/2 + m, complex as (re, im):

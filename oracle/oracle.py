@@ -55,6 +55,8 @@ class Oracle:
         L.orc_direct.argtypes = [ctypes.c_int, ctypes.c_int64, _d, _d, ctypes.c_double, ctypes.c_int64, _i64, _d, _d]
         L.orc_naive_ref.argtypes = [ctypes.c_int, ctypes.c_int64, _d, _d, _d]
         L.orc_fmm.argtypes = [ctypes.c_int, ctypes.c_int64, _d, _d, ctypes.c_uint, ctypes.c_uint, ctypes.c_int, _d, _d]
+        L.orc_fmm_ex.argtypes = [ctypes.c_int, ctypes.c_int64, _d, _d, ctypes.c_uint, ctypes.c_uint, ctypes.c_int,
+                                 ctypes.c_double, ctypes.c_int64, _d, _d]
         for f in ("orc_regular_scaled", "orc_irregular_scaled", "orc_regular_racah", "orc_irregular_racah"):
             getattr(L, f).argtypes = [ctypes.c_uint, _d, _d]
         L.orc_p2m_3d.argtypes = [ctypes.c_uint, ctypes.c_int64, _d, _d, _d, _d]
@@ -126,13 +128,16 @@ class Oracle:
         self.L.orc_naive_ref(dim, n, _p(pos, _d), _p(mass, _d), _p(g, _d))
         return g
 
-    def fmm(self, pos, mass, p, threshold, centre_mode=0, want_pot=False):
+    def fmm(self, pos, mass, p, threshold, centre_mode=0, want_pot=False, eps2=0.0, direct_max=0):
+        """FMM force pass (grad = acceleration / G).  direct_max > 0 sums
+        interaction pairs with n_t * n_s <= direct_max directly."""
         pos = _f64(pos)
         mass = _f64(mass)
         n, dim = pos.shape
         g = np.zeros((n, dim))
         pot = np.zeros(n) if want_pot else None
-        rc = self.L.orc_fmm(dim, n, _p(pos, _d), _p(mass, _d), p, threshold, centre_mode, _p(g, _d), _p(pot, _d))
+        rc = self.L.orc_fmm_ex(dim, n, _p(pos, _d), _p(mass, _d), p, threshold, centre_mode, eps2, direct_max,
+                               _p(g, _d), _p(pot, _d))
         if rc != 0:
             raise ValueError("orc_fmm failed")
         return (g, pot) if want_pot else g

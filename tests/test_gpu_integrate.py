@@ -10,11 +10,11 @@ from fmmgpu import workloads
 pytestmark = pytest.mark.gpu
 
 
-def cpu_se(oracle, x, v, m, dt, steps, eps2):
-    """SyplecticEuler::integrate (symplectic_euler.cpp:8-15) with FP64 direct forces."""
+def cpu_se(force, x, v, dt, steps):
+    """SyplecticEuler::integrate (symplectic_euler.cpp:8-15)."""
     x, v = x.copy(), v.copy()
     for _ in range(steps):
-        a = oracle.direct(x, m, eps2=eps2)
+        a = force(x)
         v = v + dt * a
         x = x + dt * v
     return x, v
@@ -38,11 +38,15 @@ def test_symplectic_euler_c1(oracle):
     x, m = workloads.uniform_cube(500, seed=1)
     v = np.zeros_like(x)
     eps2 = 1e-6
-    with fmmgpu.Context(dim=3, p=6, leaf_cap=16, G=1.0, eps2=eps2) as c:
+    with fmmgpu.Context(dim=3, p=6, leaf_cap=16, G=1.0, eps2=eps2, direct_max=0) as c:
         xg, vg, _ = c.integrate(fmmgpu.FMM_INT_SYMPLECTIC_EULER, 1e-3, 10, x, v, m)
-    xc, vc = cpu_se(oracle, x, v, m, 1e-3, 10, eps2)
-    assert np.abs(xg - xc).max() < 1e-7
-    assert np.abs(vg - vc).max() < 1e-5 * np.abs(vc).max()
+    # the same FMM (p, leaf capacity, softening) in FP64 on the CPU
+    xc, vc = cpu_se(lambda y: oracle.fmm(y, m, 6, 16, eps2=eps2), x, v, 1e-3, 10)
+    assert np.abs(xg - xc).max() < 1e-9
+    assert np.abs(vg - vc).max() < 1e-6 * np.abs(vc).max()
+    # and within the FMM's truncation error of the exact dynamics
+    xd, vd = cpu_se(lambda y: oracle.direct(y, m, eps2=eps2), x, v, 1e-3, 10)
+    assert np.abs(xg - xd).max() < 1e-6
 
 
 def test_rk4_plummer(oracle):
