@@ -18,11 +18,13 @@ struct OpTables {
 
 struct ExpBuffers {
   DevBuf<float> M, L;  // n_cells * KS each (indexed by absolute cell - cell0)
-  DevBuf<int> tlist;   // class-grouped target cells (levels >= 2)
-  DevBuf<uint64_t> ckey, ckey_alt;  // (level, class) sort keys of those cells
-  DevBuf<uint32_t> cval;
+  DevBuf<int> tlist;      // class-grouped cells of levels >= 2 (L2L targets)
+  DevBuf<int> tlist_m2l;  // the same restricted to cells with possible M2L pairs
+  DevBuf<uint64_t> ckey, ckey_alt, ckey_m2l;  // (level, class) sort keys of those cells
+  DevBuf<uint32_t> cval, cval2;
   DevBuf<int4> batches;
   DevBuf<uint32_t> cls_count;
+  DevBuf<float4> lvl_off;  // particle offsets from their level-d ancestor (direct far field)
 };
 
 // Per-pass parameters.
@@ -33,7 +35,8 @@ struct PassGeom {
 int build_op_tables(OpTables &ops, int dim, int p, const PassGeom &g, cudaStream_t st, int64_t &launches);
 void upload_class_tables();
 
-int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, int p, double eps2, double G,
+int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, const double *d_pos,
+                   const double *d_mass, int p, double eps2, double G,
                    const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, int64_t direct_max, cudaStream_t st,
                    fmm_stats &stats, cudaEvent_t *ev);
 

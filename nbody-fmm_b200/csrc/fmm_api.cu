@@ -123,6 +123,10 @@ int fmm_destroy(fmm_ctx *c) {
   c->eb.ckey.release();
   c->eb.ckey_alt.release();
   c->eb.cval.release();
+  c->eb.cval2.release();
+  c->eb.ckey_m2l.release();
+  c->eb.tlist_m2l.release();
+  c->eb.lvl_off.release();
   for (auto *b : {&c->d_pos, &c->d_mass, &c->d_acc, &c->d_pot, &c->d_vel, &c->d_x0, &c->d_v0, &c->d_xs, &c->d_vs,
                   &c->d_asum, &c->d_vsum})
     b->release();
@@ -167,7 +171,7 @@ static int evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const dou
   rc = build_op_tables(c->ops, dim, c->cfg.p, g, st, c->ws.launches);
   if (rc) return rc;
   memset(&c->stats, 0, sizeof(c->stats));
-  rc = run_fmm_passes(c->ws, c->tree, c->ops, c->eb, c->cfg.p, c->cfg.eps2, c->cfg.G, g, d_acc, d_pot,
+  rc = run_fmm_passes(c->ws, c->tree, c->ops, c->eb, d_pos, d_mass, c->cfg.p, c->cfg.eps2, c->cfg.G, g, d_acc, d_pot,
                       c->cfg.m2l_mode, direct_threshold(c->cfg), st, c->stats, c->ev);
   if (rc) return rc;
   if (!c->ws.ok) return FMM_ERR_OUT_OF_MEMORY;

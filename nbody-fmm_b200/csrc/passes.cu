@@ -385,16 +385,7 @@ __global__ void k_l2p3d(const float4 *part, const int *leaf_of, int64_t n, int c
 }
 
 // ------------------------------------------------------------------ P2P
-// One warp per target leaf; the leaf's particles are spread over the lanes
-// (several lanes per particle for small leaves, each taking a share of the
-// sources).  Sources are the leaf itself (j != i) and its existing
-// neighbours (leaf.cpp:118-142).
-//
-// Precision: x_i - x_j = (t_i - shift) - s_j with t_i, s_j the offsets from
-// the two leaf centres and shift = c_s - c_t an exact multiple of the leaf
-// size.  Offsets are hi + lo FP32 pairs, the shift is hi + lo from FP64, and
-// (t_hi - shift_hi) is formed error-free (TwoSum), so each difference is
-// rounded once, relative to itself, whatever the separation.
+// Error-free sum: s + e == a + b exactly (Knuth's TwoSum).
 __device__ inline void two_sum(float a, float b, float &s, float &e) {
   s = a + b;
   float bb = s - a;
@@ -416,35 +407,13 @@ struct P2PArgs {
   unsigned long long *pair_count;
 };
 
-// Sums source particles [jb, je) onto this lane's target, target offset
-// (tx, ty, tz) already expressed in the sources' leaf frame (plain FP32:
-// used for well-separated cells, at least two cells apart).
-__device__ inline void p2p_far_range(const float4 *part, int jb, int je, int sub, int Gl, float tx, float ty, float tz,
-                                     float eps2, float &ax, float &ay, float &az, float &ph) {
-  for (int j = jb + sub; j < je; j += Gl) {
-    const float4 q = part[j];
-    const float rx = tx - q.x, ry = ty - q.y, rz = tz - q.z;
-    const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2)));
-    float inv = rsqrtf(r2);
-    inv = inv * fmaf(-0.5f * r2 * inv, inv, 1.5f);
-    const float mi = q.w * inv;
-    const float mi3 = mi * inv * inv;
-    ax = fmaf(-rx, mi3, ax);
-    ay = fmaf(-ry, mi3, ay);
-    az = fmaf(-rz, mi3, az);
-    ph += mi;
-  }
-}
-
 // One warp per target leaf; the leaf's particles are spread over the lanes
 // (several lanes per particle for small leaves, each taking a share of the
 // sources).  Sources:
 //  - near field: the leaf itself (j != i) and its existing neighbours
 //    (leaf.cpp:118-142);
-//  - direct far field: the cells of the interaction lists of the leaf and of
-//    its ancestors with n_target * n_source <= direct_max (the M2L pass skips
-//    exactly these pairs).  An ancestor with more than direct_max particles
-//    cannot have such a pair, which ends the walk up the tree.
+// The direct far field (interaction-list pairs summed particle by particle)
+// has been added into `far` by k_direct_far before this kernel runs.
 //
 // Near-field precision: x_i - x_j = (t_i - shift) - s_j with t_i, s_j the
 // offsets from the two leaf centres and shift = c_s - c_t an exact multiple
@@ -462,8 +431,6 @@ __global__ void k_p2p3d(P2PArgs a) {
   while (Gl * 2 * tp <= 32) Gl *= 2;
   const int tpp = 32 / Gl;
   const int *cl = a.coll + (int64_t)g * 27;
-  uint32_t gx, gy, gz;
-  morton_decode(3, a.ckey[g], gx, gy, gz);
   bool bad = false;
   long long npairs = 0;
   for (int t0 = 0; t0 < nt; t0 += tpp) {
@@ -504,53 +471,6 @@ __global__ void k_p2p3d(P2PArgs a) {
         ph += mi;
       }
     }
-    // direct far field, walking up from the leaf
-    if (a.direct_max > 0) {
-      int A = g;
-      for (int d = a.depth; d >= 2; --d) {
-        const long long nA = a.pend[A] - a.pbeg[A];
-        if (nA > a.direct_max) break;
-        const int P = a.parent[A];
-        const int cls = (int)(a.ckey[A] & 7u);
-        const int *pc = a.coll + (int64_t)P * 27;
-        for (int c0 = 0; c0 < 216; c0 += 32) {
-          const int cand = c0 + lane;
-          int q = -1;
-          if (cand < 216) {
-            const int dl = cand >> 3, k = cand & 7;
-            const int Q = pc[dl];
-            if (Q >= 0) {
-              q = a.child[(int64_t)Q * 8 + k];
-              if (q >= 0) {
-                const int ddx = 2 * (dl % 3 - 1) + (k & 1) - (cls & 1);
-                const int ddy = 2 * ((dl / 3) % 3 - 1) + ((k >> 1) & 1) - ((cls >> 1) & 1);
-                const int ddz = 2 * (dl / 9 - 1) + ((k >> 2) & 1) - ((cls >> 2) & 1);
-                const bool adj = ddx >= -1 && ddx <= 1 && ddy >= -1 && ddy <= 1 && ddz >= -1 && ddz <= 1;
-                if (adj || nA * (long long)(a.pend[q] - a.pbeg[q]) > a.direct_max) q = -1;
-              }
-            }
-          }
-          unsigned mask = __ballot_sync(0xffffffffu, q >= 0);
-          while (mask) {
-            const int b = __ffs(mask) - 1;
-            mask &= mask - 1;
-            const int S = __shfl_sync(0xffffffffu, q, b);
-            const int l0 = a.leaf_of[a.pbeg[S]], l1 = a.leaf_of[a.pend[S] - 1];
-            if (t0 == 0 && lane == 0) npairs += (long long)nt * (a.pend[S] - a.pbeg[S]);
-            for (int l = l0; l <= l1; ++l) {
-              uint32_t lx, ly, lz;
-              morton_decode(3, a.ckey[l], lx, ly, lz);
-              const float shx = (float)(((double)lx - (double)gx) * a.hx);
-              const float shy = (float)(((double)ly - (double)gy) * a.hy);
-              const float shz = (float)(((double)lz - (double)gz) * a.hz);
-              p2p_far_range(a.part, a.pbeg[l], a.pend[l], sub, Gl, me.x - shx, me.y - shy, me.z - shz, a.eps2, ax,
-                            ay, az, ph);
-            }
-          }
-        }
-        A = P;
-      }
-    }
     for (int o = 1; o < Gl; o <<= 1) {
       ax += __shfl_xor_sync(0xffffffffu, ax, o);
       ay += __shfl_xor_sync(0xffffffffu, ay, o);
@@ -572,14 +492,210 @@ __global__ void k_p2p3d(P2PArgs a) {
   if (lane == 0 && a.pair_count) atomicAdd(a.pair_count, (unsigned long long)npairs);
 }
 
+// --------------------------------------------------------- direct far field
+// Offsets of every particle (leaf order) from the centre of its ancestor at
+// level d, FP32, with the mass: the frame in which pairs of level-d cells
+// are summed directly.
+__global__ void k_level_offsets(const double *pos, const double *mass, const uint32_t *perm, const int *leaf_of,
+                                const uint64_t *ckey, int64_t n, int depth, int d, double lox, double loy, double loz,
+                                double ex, double ey, double ez, float4 *out) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t qx, qy, qz;
+  morton_decode(3, ckey[leaf_of[i]], qx, qy, qz);
+  const int sh = depth - d;
+  const double inv = ldexp(1.0, -d);
+  const uint32_t j = perm[i];
+  double cx = lox + ((double)(qx >> sh) + 0.5) * (ex * inv);
+  double cy = loy + ((double)(qy >> sh) + 0.5) * (ey * inv);
+  double cz = loz + ((double)(qz >> sh) + 0.5) * (ez * inv);
+  out[i] = make_float4((float)(pos[3 * (size_t)j] - cx), (float)(pos[3 * (size_t)j + 1] - cy),
+                       (float)(pos[3 * (size_t)j + 2] - cz), (float)mass[j]);
+}
+
+struct DirectArgs {
+  int first, count, depth_d;  // cells of level d: [first, first + count)
+  const int *pbeg, *pend, *coll, *parent, *child;
+  const uint64_t *ckey;
+  const float4 *off;  // particle offsets from their level-d ancestor's centre
+  float hx, hy, hz;   // level-d cell size
+  float eps2;
+  long long direct_max;
+  float4 *far;
+  unsigned long long *pair_count;
+};
+
+__device__ inline void pair_acc(float rx, float ry, float rz, float w, float eps2, float &ax, float &ay, float &az,
+                                float &ph) {
+  const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2)));
+  float inv = rsqrtf(r2);
+  inv = inv * fmaf(-0.5f * r2 * inv, inv, 1.5f);
+  const float mi = w * inv;
+  const float mi3 = mi * inv * inv;
+  ax = fmaf(-rx, mi3, ax);
+  ay = fmaf(-ry, mi3, ay);
+  az = fmaf(-rz, mi3, az);
+  ph += mi;
+}
+
+// One warp per level-d target cell T with n_T <= direct_max: the sources are
+// the cells S of T's interaction list (node_i.cpp:39-43) with
+// n_T * n_S <= direct_max, exactly the pairs the M2L contraction skips.
+// Small T (NT <= 8 targets): every lane holds all targets and takes every
+// 32nd particle of the concatenated sources; larger T: lanes over targets.
+template <int NT>
+__device__ void direct_small(const DirectArgs &a, int tb, int nt, const int *s_src, const float *s_shift,
+                             const int *s_pref, int nsrc, int lane) {
+  float tx[NT], ty[NT], tz[NT], ax[NT], ay[NT], az[NT], ph[NT];
+#pragma unroll
+  for (int k = 0; k < NT; ++k) {
+    float4 t = a.off[tb + (k < nt ? k : 0)];
+    tx[k] = t.x;
+    ty[k] = t.y;
+    tz[k] = t.z;
+    ax[k] = ay[k] = az[k] = ph[k] = 0.f;
+  }
+  const int total = s_pref[nsrc];
+  int si = 0;
+  for (int f = lane; f < total; f += 32) {
+    while (f >= s_pref[si + 1]) ++si;
+    const int j = a.pbeg[s_src[si]] + (f - s_pref[si]);
+    const float4 q = a.off[j];
+    const float qx = q.x + s_shift[3 * si], qy = q.y + s_shift[3 * si + 1], qz = q.z + s_shift[3 * si + 2];
+#pragma unroll
+    for (int k = 0; k < NT; ++k) pair_acc(tx[k] - qx, ty[k] - qy, tz[k] - qz, q.w, a.eps2, ax[k], ay[k], az[k], ph[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < NT; ++k) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+      ax[k] += __shfl_xor_sync(0xffffffffu, ax[k], o);
+      ay[k] += __shfl_xor_sync(0xffffffffu, ay[k], o);
+      az[k] += __shfl_xor_sync(0xffffffffu, az[k], o);
+      ph[k] += __shfl_xor_sync(0xffffffffu, ph[k], o);
+    }
+    if (lane == k && k < nt) {
+      float4 f0 = a.far[tb + k];
+      a.far[tb + k] = make_float4(f0.x + ax[k], f0.y + ay[k], f0.z + az[k], f0.w + ph[k]);
+    }
+  }
+}
+
+__global__ void k_direct_far(DirectArgs a) {
+  __shared__ int s_src_all[8][189];
+  __shared__ float s_shift_all[8][3 * 189];
+  __shared__ int s_pref_all[8][190];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int wl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (wl >= a.count) return;
+  const int T = a.first + wl;
+  const int tb = a.pbeg[T], nt = a.pend[T] - tb;
+  if ((long long)nt > a.direct_max) return;
+  int *s_src = s_src_all[wib];
+  float *s_shift = s_shift_all[wib];
+  int *s_pref = s_pref_all[wib];
+  const int P = a.parent[T];
+  const int cls = (int)(a.ckey[T] & 7u);
+  const int *pc = a.coll + (int64_t)P * 27;
+  int nsrc = 0;
+  if (lane == 0) s_pref[0] = 0;
+  for (int c0 = 0; c0 < 216; c0 += 32) {
+    const int cand = c0 + lane;
+    int q = -1, ns = 0, ddx = 0, ddy = 0, ddz = 0;
+    if (cand < 216) {
+      const int dl = cand >> 3, k = cand & 7;
+      const int Q = pc[dl];
+      if (Q >= 0) {
+        q = a.child[(int64_t)Q * 8 + k];
+        if (q >= 0) {
+          ddx = 2 * (dl % 3 - 1) + (k & 1) - (cls & 1);
+          ddy = 2 * ((dl / 3) % 3 - 1) + ((k >> 1) & 1) - ((cls >> 1) & 1);
+          ddz = 2 * (dl / 9 - 1) + ((k >> 2) & 1) - ((cls >> 2) & 1);
+          const bool adj = ddx >= -1 && ddx <= 1 && ddy >= -1 && ddy <= 1 && ddz >= -1 && ddz <= 1;
+          ns = a.pend[q] - a.pbeg[q];
+          if (adj || (long long)nt * ns > a.direct_max) q = -1;
+        }
+      }
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, q >= 0);
+    const int pos = nsrc + __popc(mask & ((1u << lane) - 1u));
+    if (q >= 0) {
+      s_src[pos] = q;
+      s_shift[3 * pos] = ddx * a.hx;  // c_S - c_T
+      s_shift[3 * pos + 1] = ddy * a.hy;
+      s_shift[3 * pos + 2] = ddz * a.hz;
+      s_pref[pos + 1] = ns;  // counts, turned into a prefix sum below
+    }
+    nsrc += __popc(mask);
+  }
+  __syncwarp();
+  if (nsrc == 0) return;
+  if (lane == 0) {
+    int acc = 0;
+    for (int k = 1; k <= nsrc; ++k) {
+      acc += s_pref[k];
+      s_pref[k] = acc;
+    }
+    if (a.pair_count) atomicAdd(a.pair_count, (unsigned long long)((long long)nt * acc));
+  }
+  __syncwarp();
+  if (nt <= 1) direct_small<1>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
+  else if (nt <= 2) direct_small<2>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
+  else if (nt <= 4) direct_small<4>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
+  else if (nt <= 8) direct_small<8>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
+  else {
+    // lanes over targets; every lane walks all sources (warp-uniform loads)
+    for (int t0 = 0; t0 < nt; t0 += 32) {
+      const int ti = t0 + lane;
+      const float4 t = a.off[tb + (ti < nt ? ti : 0)];
+      float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
+      for (int si = 0; si < nsrc; ++si) {
+        const float tx = t.x - s_shift[3 * si], ty = t.y - s_shift[3 * si + 1], tz = t.z - s_shift[3 * si + 2];
+        const int jb = a.pbeg[s_src[si]], je = a.pend[s_src[si]];
+        for (int j = jb; j < je; ++j) {
+          const float4 q = a.off[j];
+          pair_acc(tx - q.x, ty - q.y, tz - q.z, q.w, a.eps2, ax, ay, az, ph);
+        }
+      }
+      if (ti < nt) {
+        float4 f0 = a.far[tb + ti];
+        a.far[tb + ti] = make_float4(f0.x + ax, f0.y + ay, f0.z + az, f0.w + ph);
+      }
+    }
+  }
+}
+
 // ------------------------------------------------------------------ lists
-__global__ void k_class_keys(const uint64_t *ckey, int first, int count, int level, int dim, uint64_t *keys,
-                             uint32_t *vals, int out_off) {
+// Sort keys (level, class) of the cells of one level: key_all for L2L (every
+// cell), key_m2l for M2L with 255 for cells that cannot have an M2L pair under
+// the direct-pair rule (every child S of the parent's colleagues has
+// n_T * n_S <= direct_max; adjacency is ignored, so the test only errs
+// towards keeping a cell).
+__global__ void k_class_keys(const uint64_t *ckey, const int *cpbeg, const int *cpend, const int *cparent,
+                             const int *ccoll, const int *cchild, long long direct_max, int first, int count, int level,
+                             int dim, uint64_t *keys_all, uint64_t *keys_m2l, uint32_t *vals, int out_off) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   int g = first + i;
-  keys[out_off + i] = ((uint64_t)level << dim) | (ckey[g] & ((1u << dim) - 1));
+  const uint64_t k = ((uint64_t)level << dim) | (ckey[g] & ((1u << dim) - 1));
+  keys_all[out_off + i] = k;
   vals[out_off + i] = (uint32_t)g;
+  bool m2l = true;
+  if (direct_max > 0) {
+    const int nc = 1 << dim, ns = dim == 3 ? 27 : 9;
+    const long long nt = cpend[g] - cpbeg[g];
+    const int *pc = ccoll + (int64_t)cparent[g] * ns;
+    m2l = false;
+    for (int s = 0; s < ns && !m2l; ++s) {
+      const int Q = pc[s];
+      if (Q < 0 || nt * (cpend[Q] - cpbeg[Q]) <= direct_max) continue;
+      for (int c = 0; c < nc && !m2l; ++c) {
+        const int q = cchild[(int64_t)Q * nc + c];
+        if (q >= 0 && nt * (cpend[q] - cpbeg[q]) > direct_max) m2l = true;
+      }
+    }
+  }
+  keys_m2l[out_off + i] = m2l ? k : 255u;
 }
 
 __global__ void k_class_hist(const uint64_t *keys, int n, uint32_t *hist) {
@@ -595,7 +711,8 @@ __global__ void k_class_hist(const uint64_t *keys, int n, uint32_t *hist) {
 // ------------------------------------------------------------ driver
 static inline float fmax3(float a, float b, float c) { return std::max(a, std::max(b, c)); }
 
-int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, int p, double eps2, double G,
+int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, const double *d_pos_g,
+                   const double *d_mass_g, int p, double eps2, double G,
                    const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, int64_t direct_max, cudaStream_t st,
                    fmm_stats &stats, cudaEvent_t *ev) {
   (void)m2l_mode;
@@ -610,40 +727,53 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, i
   const double sD = std::ldexp(emax, -D);
   const float inv_sD = (float)(1.0 / sD);
 
-  // class-grouped target lists of levels >= 2
+  // class-grouped target lists of levels >= 2: every cell (for L2L) and the
+  // cells with possible M2L pairs (for M2L)
   std::vector<int4> hb;
-  std::vector<int> lvl_b0(D + 2, 0), lvl_b1(D + 2, 0);
+  std::vector<int> lvl_b0(D + 2, 0), lvl_b1(D + 2, 0), m2l_b0(D + 2, 0), m2l_b1(D + 2, 0);
   int ntl = 0;
-  const int *tl = nullptr;
+  const int *tl = nullptr, *tl_m2l = nullptr;
   if (D >= 2) {
     ntl = t.level_off[D] + t.level_count[D] - t.level_off[2];
-    if (!eb.tlist.reserve(ntl) || !eb.cls_count.reserve(256) || !eb.ckey.reserve(ntl) || !eb.ckey_alt.reserve(ntl) ||
-        !eb.cval.reserve(ntl))
+    if (!eb.tlist.reserve(ntl) || !eb.tlist_m2l.reserve(ntl) || !eb.cls_count.reserve(512) ||
+        !eb.ckey.reserve(ntl) || !eb.ckey_alt.reserve(ntl) || !eb.ckey_m2l.reserve(ntl) || !eb.cval.reserve(ntl) ||
+        !eb.cval2.reserve(ntl))
       return FMM_ERR_OUT_OF_MEMORY;
     for (int d = 2; d <= D; ++d)
-      k_class_keys<<<cdiv(t.level_count[d], TPB), TPB, 0, st>>>(ws.cell_key, t.level_off[d], t.level_count[d], d, dim,
-                                                                eb.ckey.ptr, eb.cval.ptr, t.level_off[d] - t.level_off[2]);
+      k_class_keys<<<cdiv(t.level_count[d], TPB), TPB, 0, st>>>(
+          ws.cell_key, ws.cell_pbeg, ws.cell_pend, ws.cell_parent, ws.cell_coll, ws.cell_child, direct_max,
+          t.level_off[d], t.level_count[d], d, dim, eb.ckey.ptr, eb.ckey_m2l.ptr, eb.cval.ptr,
+          t.level_off[d] - t.level_off[2]);
     ws.launches += D - 1;
+    CUDA_TRY(cudaMemcpyAsync(eb.cval2.ptr, eb.cval.ptr, sizeof(uint32_t) * ntl, cudaMemcpyDeviceToDevice, st));
     uint64_t *kk = eb.ckey.ptr, *kk2 = eb.ckey_alt.ptr;
     uint32_t *vv = eb.cval.ptr, *vv2 = (uint32_t *)eb.tlist.ptr;
     radix_sort(ws, kk, vv, kk2, vv2, ntl, 8, st);  // sorted (keys, cells) end in (kk, vv)
     tl = (const int *)vv;
-    CUDA_TRY(cudaMemsetAsync(eb.cls_count.ptr, 0, 256 * sizeof(uint32_t), st));
+    CUDA_TRY(cudaMemsetAsync(eb.cls_count.ptr, 0, 512 * sizeof(uint32_t), st));
     k_class_hist<<<std::min(cdiv(ntl, TPB), 148 * 4), TPB, 0, st>>>(kk, ntl, eb.cls_count.ptr);
-    ws.launches += 1;
-    uint32_t hc[256];
+    uint64_t *mk = eb.ckey_m2l.ptr, *mk2 = (kk == eb.ckey.ptr) ? eb.ckey_alt.ptr : eb.ckey.ptr;
+    uint32_t *mv = eb.cval2.ptr, *mv2 = (uint32_t *)eb.tlist_m2l.ptr;
+    radix_sort(ws, mk, mv, mk2, mv2, ntl, 8, st);
+    tl_m2l = (const int *)mv;
+    k_class_hist<<<std::min(cdiv(ntl, TPB), 148 * 4), TPB, 0, st>>>(mk, ntl, eb.cls_count.ptr + 256);
+    ws.launches += 2;
+    uint32_t hc[512];
     CUDA_TRY(cudaMemcpyAsync(hc, eb.cls_count.ptr, sizeof(hc), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
-    int off = 0;
     const int ncls = 1 << dim;
-    for (int d = 2; d <= D; ++d) {
-      lvl_b0[d] = (int)hb.size();
-      for (int c = 0; c < ncls; ++c) {
-        int cnt = (int)hc[(d << dim) | c];
-        for (int s = 0; s < cnt; s += CT_TGT) hb.push_back(make_int4(off + s, std::min(CT_TGT, cnt - s), d, c));
-        off += cnt;
+    for (int pass = 0; pass < 2; ++pass) {
+      const uint32_t *h = hc + 256 * pass;
+      int off = 0;
+      for (int d = 2; d <= D; ++d) {
+        (pass ? m2l_b0 : lvl_b0)[d] = (int)hb.size();
+        for (int c = 0; c < ncls; ++c) {
+          int cnt = (int)h[(d << dim) | c];
+          for (int s0 = 0; s0 < cnt; s0 += CT_TGT) hb.push_back(make_int4(off + s0, std::min(CT_TGT, cnt - s0), d, c));
+          off += cnt;
+        }
+        (pass ? m2l_b1 : lvl_b1)[d] = (int)hb.size();
       }
-      lvl_b1[d] = (int)hb.size();
     }
   }
   // M2M batches (levels D-1 .. 2, consecutive cells)
@@ -699,11 +829,11 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, i
     ContractArgs c2 = ca;
     c2.mode = MODE_M2L;
     c2.slot_base = 0;
-    c2.tlist = tl;
+    c2.tlist = tl_m2l;
     c2.X = eb.M.ptr;
     c2.Y = eb.L.ptr;
-    c2.batches = eb.batches.ptr + lvl_b0[2];
-    int rc = launch_contract(c2, lvl_b1[D] - lvl_b0[2], st, ws.launches);
+    c2.batches = eb.batches.ptr + m2l_b0[2];
+    int rc = launch_contract(c2, m2l_b1[D] - m2l_b0[2], st, ws.launches);
     if (rc) return rc;
   }
   if (ev) cudaEventRecord(ev[3], st);
@@ -723,6 +853,41 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, i
   k_l2p3d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far);
   ws.launches += 1;
   if (ev) cudaEventRecord(ev[4], st);
+  // direct far field, level by level (levels >= 2 have interaction lists)
+  if (direct_max > 0 && D >= 2) {
+    if (!eb.lvl_off.reserve((size_t)n)) return FMM_ERR_OUT_OF_MEMORY;
+    DirectArgs da;
+    da.pbeg = ws.cell_pbeg;
+    da.pend = ws.cell_pend;
+    da.coll = ws.cell_coll;
+    da.parent = ws.cell_parent;
+    da.child = ws.cell_child;
+    da.ckey = ws.cell_key;
+    da.eps2 = (float)eps2;
+    da.direct_max = direct_max;
+    da.far = ws.far;
+    da.pair_count = ws.counters + 1;
+    for (int d = D; d >= 2; --d) {
+      const double invd = std::ldexp(1.0, -d);
+      if (d == D) {
+        da.off = ws.part;
+      } else {
+        k_level_offsets<<<cdiv(n, TPB), TPB, 0, st>>>(d_pos_g, d_mass_g, t.d_perm, ws.leaf_of, ws.cell_key, n, D, d,
+                                                      g.lo[0], g.lo[1], g.lo[2], g.ext[0], g.ext[1], g.ext[2],
+                                                      eb.lvl_off.ptr);
+        ws.launches += 1;
+        da.off = eb.lvl_off.ptr;
+      }
+      da.first = t.level_off[d];
+      da.count = t.level_count[d];
+      da.depth_d = d;
+      da.hx = (float)(g.ext[0] * invd);
+      da.hy = (float)(g.ext[1] * invd);
+      da.hz = (float)(g.ext[2] * invd);
+      k_direct_far<<<cdiv((int64_t)da.count * 32, TPB), TPB, 0, st>>>(da);
+      ws.launches += 1;
+    }
+  }
   // P2P + output
   const double inv2D = std::ldexp(1.0, -D);
   P2PArgs pa;

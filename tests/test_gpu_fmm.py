@@ -144,7 +144,7 @@ def test_fmm_near_field_matches_reference():
     """p = 0: the far field's gradient vanishes and what remains is the
     reference's near-field sum (leaf.cpp:118-142), checked on its fixture."""
     z = golden("ref_near3d.npz")
-    with fmmgpu.Context(dim=3, p=0, leaf_cap=int(z["T"]), G=1.0) as c:
+    with fmmgpu.Context(dim=3, p=0, leaf_cap=int(z["T"]), G=1.0, direct_max=0) as c:
         a = c.evaluate(z["pos"], z["mass"])
     assert rel_l2(a, z["grad"]) < 1e-6
 
