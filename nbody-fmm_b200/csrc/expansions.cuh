@@ -24,7 +24,8 @@ struct ExpBuffers {
   DevBuf<uint32_t> cval, cval2;
   DevBuf<int4> batches;
   DevBuf<uint32_t> cls_count;
-  DevBuf<float4> lvl_off;  // particle offsets from their level-d ancestor (direct far field)
+  DevBuf<float4> lvl_off;
+  DevBuf<int> m2l_src, m2l_list, m2l_nslots;  // per M2L batch: resolved sources and present slots  // particle offsets from their level-d ancestor (direct far field)
 };
 
 // Per-pass parameters.

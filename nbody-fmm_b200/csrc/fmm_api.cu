@@ -127,6 +127,9 @@ int fmm_destroy(fmm_ctx *c) {
   c->eb.ckey_m2l.release();
   c->eb.tlist_m2l.release();
   c->eb.lvl_off.release();
+  c->eb.m2l_src.release();
+  c->eb.m2l_list.release();
+  c->eb.m2l_nslots.release();
   for (auto *b : {&c->d_pos, &c->d_mass, &c->d_acc, &c->d_pot, &c->d_vel, &c->d_x0, &c->d_v0, &c->d_xs, &c->d_vs,
                   &c->d_asum, &c->d_vsum})
     b->release();

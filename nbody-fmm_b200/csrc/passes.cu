@@ -87,6 +87,9 @@ struct ContractArgs {
   const float *tab;
   const int *cparent, *cchild, *ccoll, *cpbeg, *cpend;
   long long direct_max;  // M2L skips pairs with n_t * n_s <= direct_max (summed directly instead)
+  const int *src_tab;    // M2L: [batch][slot][CT_TGT] source cells resolved ahead (or null)
+  const int *slot_list;  // M2L: [batch][slot index] present slots, nslots_tab[batch] of them
+  const int *nslots_tab;
   int cell0, K, KS, KP, dim, mode, slot_base, level_stride;
   unsigned long long *pair_count;  // M2L: number of (target, source) pairs contracted
 };
@@ -131,7 +134,8 @@ __global__ void __launch_bounds__(CT_THREADS) k_contract(ContractArgs a) {
   const int cnt = b.y, level = b.z, cls = b.w;
   if (tid < CT_TGT) s_tgt[tid] = tid < cnt ? (a.tlist ? a.tlist[b.x + tid] : b.x + tid) : -1;
   __syncthreads();
-  const int nslots = a.mode == MODE_M2L ? (a.dim == 3 ? 189 : 27) : (a.mode == MODE_M2M ? (1 << a.dim) : 1);
+  const int nslots = a.mode == MODE_M2L ? (a.src_tab ? a.nslots_tab[blockIdx.x] : (a.dim == 3 ? 189 : 27))
+                                        : (a.mode == MODE_M2M ? (1 << a.dim) : 1);
 
   unsigned long long npairs = 0;
   float acc[8][J];
@@ -140,11 +144,20 @@ __global__ void __launch_bounds__(CT_THREADS) k_contract(ContractArgs a) {
 #pragma unroll
     for (int j = 0; j < J; ++j) acc[i][j] = 0.f;
 
+  const bool tabled = a.mode == MODE_M2L && a.src_tab;
+  const size_t tab_base = (size_t)blockIdx.x * 189;
   auto prefetch = [&](int s, int buf) {
     int src = -1, ts = 0;
     if (tid < CT_TGT) {
       int tg = s_tgt[tid];
-      if (tg >= 0) src = contract_source(a, tg, s, cls, level, ts);
+      if (tabled) {
+        const int slot = a.slot_list[tab_base + s];
+        const int e = c_m2l_slots[a.dim - 2][cls][slot];
+        ts = (e & 511) + level * a.level_stride;
+        src = a.src_tab[(tab_base + slot) * CT_TGT + tid];
+      } else if (tg >= 0) {
+        src = contract_source(a, tg, s, cls, level, ts);
+      }
       s_src[buf * CT_TGT + tid] = src;
       if (tid == 0 || src >= 0) s_tslot[buf] = ts;  // same for all targets of the batch
     }
@@ -264,6 +277,41 @@ static int launch_contract(const ContractArgs &a, int nb, cudaStream_t st, int64
   }
   launches += 1;
   return FMM_OK;
+}
+
+// Resolves the source cell of every (slot, target) of each M2L batch ahead of
+// the contraction (the lookups are chains of dependent loads, cheap when
+// thousands are in flight) and lists, per batch, the slots with at least one
+// source.  One block per batch.
+__global__ void k_m2l_sources(ContractArgs a, int *src_tab, int *slot_list, int *nslots_tab) {
+  __shared__ int s_flag[189];
+  __shared__ int s_tgt[CT_TGT];
+  const int4 b = a.batches[blockIdx.x];
+  const int tid = threadIdx.x;
+  const int nsl = a.dim == 3 ? 189 : 27;
+  if (tid < CT_TGT) s_tgt[tid] = tid < b.y ? a.tlist[b.x + tid] : -1;
+  for (int i = tid; i < 189; i += blockDim.x) s_flag[i] = 0;
+  __syncthreads();
+  const size_t base = (size_t)blockIdx.x * 189;
+  for (int e = tid; e < nsl * CT_TGT; e += blockDim.x) {
+    const int slot = e / CT_TGT, t = e % CT_TGT;
+    int src = -1, ts;
+    if (s_tgt[t] >= 0) src = contract_source(a, s_tgt[t], slot, b.w, b.z, ts);
+    src_tab[(base + slot) * CT_TGT + t] = src;
+    if (src >= 0) s_flag[slot] = 1;
+  }
+  __syncthreads();
+  if (tid < 32) {
+    int n = 0;
+    for (int c0 = 0; c0 < nsl; c0 += 32) {
+      const int sl = c0 + tid;
+      const bool f = sl < nsl && s_flag[sl];
+      const unsigned m = __ballot_sync(0xffffffffu, f);
+      if (f) slot_list[base + n + __popc(m & ((1u << tid) - 1u))] = sl;
+      n += __popc(m);
+    }
+    if (tid == 0) nslots_tab[blockIdx.x] = n;
+  }
 }
 
 // ------------------------------------------------------------------ P2M
@@ -581,7 +629,7 @@ __device__ void direct_small(const DirectArgs &a, int tb, int nt, const int *s_s
   }
 }
 
-__global__ void k_direct_far(DirectArgs a) {
+__global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   __shared__ int s_src_all[8][189];
   __shared__ float s_shift_all[8][3 * 189];
   __shared__ int s_pref_all[8][190];
@@ -599,24 +647,27 @@ __global__ void k_direct_far(DirectArgs a) {
   const int *pc = a.coll + (int64_t)P * 27;
   int nsrc = 0;
   if (lane == 0) s_pref[0] = 0;
-  for (int c0 = 0; c0 < 216; c0 += 32) {
-    const int cand = c0 + lane;
-    int q = -1, ns = 0, ddx = 0, ddy = 0, ddz = 0;
-    if (cand < 216) {
-      const int dl = cand >> 3, k = cand & 7;
-      const int Q = pc[dl];
-      if (Q >= 0) {
-        q = a.child[(int64_t)Q * 8 + k];
-        if (q >= 0) {
-          ddx = 2 * (dl % 3 - 1) + (k & 1) - (cls & 1);
-          ddy = 2 * ((dl / 3) % 3 - 1) + ((k >> 1) & 1) - ((cls >> 1) & 1);
-          ddz = 2 * (dl / 9 - 1) + ((k >> 2) & 1) - ((cls >> 2) & 1);
-          const bool adj = ddx >= -1 && ddx <= 1 && ddy >= -1 && ddy <= 1 && ddz >= -1 && ddz <= 1;
-          ns = a.pend[q] - a.pbeg[q];
-          if (adj || (long long)nt * ns > a.direct_max) q = -1;
-        }
-      }
-    }
+  // all candidate loads in flight at once: colleague, child, then counts
+  const int Qlane = lane < 27 ? pc[lane] : -1;
+  int qv[7], nsv[7];
+#pragma unroll
+  for (int r = 0; r < 7; ++r) {
+    const int cand = r * 32 + lane;
+    const int Q = __shfl_sync(0xffffffffu, Qlane, (cand >> 3) < 27 ? (cand >> 3) : 0);
+    qv[r] = (cand < 216 && Q >= 0) ? a.child[(int64_t)Q * 8 + (cand & 7)] : -1;
+  }
+#pragma unroll
+  for (int r = 0; r < 7; ++r) nsv[r] = qv[r] >= 0 ? a.pend[qv[r]] - a.pbeg[qv[r]] : 0;
+#pragma unroll
+  for (int r = 0; r < 7; ++r) {
+    const int cand = r * 32 + lane;
+    const int dl = cand >> 3, k = cand & 7;
+    int q = qv[r];
+    const int ddx = 2 * (dl % 3 - 1) + (k & 1) - (cls & 1);
+    const int ddy = 2 * ((dl / 3) % 3 - 1) + ((k >> 1) & 1) - ((cls >> 1) & 1);
+    const int ddz = 2 * (dl / 9 - 1) + ((k >> 2) & 1) - ((cls >> 2) & 1);
+    const bool adj = ddx >= -1 && ddx <= 1 && ddy >= -1 && ddy <= 1 && ddz >= -1 && ddz <= 1;
+    if (q >= 0 && (adj || (long long)nt * nsv[r] > a.direct_max)) q = -1;
     const unsigned mask = __ballot_sync(0xffffffffu, q >= 0);
     const int pos = nsrc + __popc(mask & ((1u << lane) - 1u));
     if (q >= 0) {
@@ -624,7 +675,7 @@ __global__ void k_direct_far(DirectArgs a) {
       s_shift[3 * pos] = ddx * a.hx;  // c_S - c_T
       s_shift[3 * pos + 1] = ddy * a.hy;
       s_shift[3 * pos + 2] = ddz * a.hz;
-      s_pref[pos + 1] = ns;  // counts, turned into a prefix sum below
+      s_pref[pos + 1] = nsv[r];  // counts, turned into a prefix sum below
     }
     nsrc += __popc(mask);
   }
@@ -798,6 +849,9 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   ca.cpbeg = ws.cell_pbeg;
   ca.cpend = ws.cell_pend;
   ca.direct_max = direct_max;
+  ca.src_tab = nullptr;
+  ca.slot_list = nullptr;
+  ca.nslots_tab = nullptr;
   ca.cell0 = cell0;
   ca.K = ops.K;
   ca.KS = KS;
@@ -833,7 +887,18 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     c2.X = eb.M.ptr;
     c2.Y = eb.L.ptr;
     c2.batches = eb.batches.ptr + m2l_b0[2];
-    int rc = launch_contract(c2, m2l_b1[D] - m2l_b0[2], st, ws.launches);
+    const int nbm = m2l_b1[D] - m2l_b0[2];
+    if (!eb.m2l_src.reserve((size_t)nbm * 189 * CT_TGT) || !eb.m2l_list.reserve((size_t)nbm * 189) ||
+        !eb.m2l_nslots.reserve(nbm))
+      return FMM_ERR_OUT_OF_MEMORY;
+    if (nbm > 0) {
+      k_m2l_sources<<<nbm, 256, 0, st>>>(c2, eb.m2l_src.ptr, eb.m2l_list.ptr, eb.m2l_nslots.ptr);
+      ws.launches += 1;
+    }
+    c2.src_tab = eb.m2l_src.ptr;
+    c2.slot_list = eb.m2l_list.ptr;
+    c2.nslots_tab = eb.m2l_nslots.ptr;
+    int rc = launch_contract(c2, nbm, st, ws.launches);
     if (rc) return rc;
   }
   if (ev) cudaEventRecord(ev[3], st);

@@ -330,31 +330,31 @@ __global__ void k_make_parents(uint64_t *ckey, int *cpbeg, int *cpend, int *cpar
 }
 
 // Colleagues (|delta| <= 1 on every axis, same level, self included) of the
-// cells of one level, from the parent's colleagues' children.
+// cells of one level.  With c = 2P + b per axis (b the cell's child bit),
+// the neighbour at offset delta is child ((b + delta) mod 2) of the parent's
+// colleague at offset floor((b + delta) / 2), so each of the 3^dim slots is
+// two dependent loads and no key decoding.
 __global__ void k_colleagues(const uint64_t *ckey, const int *cparent, const int *cchild, int *ccoll, int base,
                              int count, int dim) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= count) return;
   c += base;
   const int nc = 1 << dim, ns = dim == 3 ? 27 : 9;
+  const int b = (int)(ckey[c] & (uint64_t)(nc - 1));
+  const int *pc = ccoll + (int64_t)cparent[c] * ns;
   int *out = ccoll + (int64_t)c * ns;
-  for (int s = 0; s < ns; ++s) out[s] = -1;
-  uint32_t x, y, z;
-  morton_decode(dim, ckey[c], x, y, z);
-  const int P = cparent[c];
-  const int *pc = ccoll + (int64_t)P * ns;
   for (int s = 0; s < ns; ++s) {
-    int Q = pc[s];
-    if (Q < 0) continue;
-    for (int k = 0; k < nc; ++k) {
-      int q = cchild[(int64_t)Q * nc + k];
-      if (q < 0) continue;
-      uint32_t qx, qy, qz;
-      morton_decode(dim, ckey[q], qx, qy, qz);
-      int dx = (int)qx - (int)x, dy = (int)qy - (int)y, dz = (int)qz - (int)z;
-      if (dx < -1 || dx > 1 || dy < -1 || dy > 1 || dz < -1 || dz > 1) continue;
-      out[(dx + 1) + 3 * (dy + 1) + (dim == 3 ? 9 * (dz + 1) : 0)] = q;
+    int pslot = 0, child = 0, mul = 1;
+    for (int a = 0; a < dim; ++a) {
+      const int delta = (s / mul) % 3 - 1;
+      const int v = ((b >> a) & 1) + delta;  // in [-1, 2]
+      const int e = (v + 2) / 2 - 1;        // floor(v / 2)
+      pslot += (e + 1) * mul;
+      child |= (v - 2 * e) << a;
+      mul *= 3;
     }
+    const int Q = pc[pslot];
+    out[s] = Q >= 0 ? cchild[(int64_t)Q * nc + child] : -1;
   }
 }
 
