@@ -50,7 +50,8 @@ enum {
   FMM_ERR_UNSUPPORTED = -6,
   FMM_ERR_TIMEOUT = -7,
   FMM_ERR_NO_DEVICE = -8,
-  FMM_ERR_INTERNAL = -9
+  FMM_ERR_INTERNAL = -9,
+  FMM_ERR_TOO_LARGE = -10         /* request larger than fmm_direct_noalloc's fixed scratch */
 };
 
 /* M2L arithmetic. */
@@ -159,6 +160,27 @@ FMM_API int fmm_tree_leaves(fmm_ctx *ctx, uint64_t *keys, int64_t *start, int64_
  * NodeI::compute_interaction_list (node_i.cpp:23-99).  With tkey == NULL
  * only *count is set. */
 FMM_API int fmm_tree_pairs(fmm_ctx *ctx, int32_t level, int32_t kind, int64_t *count, uint64_t *tkey, uint64_t *skey);
+
+/* FP64 direct sum that allocates no device memory and needs no context.
+ * It has no counterpart in the reference (whose NaiveUpdate allocates
+ * freely on the host).  It is for callers that cannot call cudaMalloc when
+ * they need forces: codes whose own pool owns all device memory, callers
+ * under a fixed memory budget, and threads that must not block on the
+ * device the way cudaMalloc/cudaFree can.  Inputs and outputs are the
+ * caller's device buffers (layouts as in fmm_direct_device; targets, if
+ * given, must lie in [0, n)); it runs on the current device, ordered on
+ * `stream` (NULL = the legacy default stream), and returns after enqueueing.
+ * Its only scratch is a fixed array of FMM_NOALLOC_MAX_TARGETS partial sums
+ * (8 MiB) that every GPU loading this library holds until the process
+ * exits; requests with more than FMM_NOALLOC_MAX_TARGETS targets return
+ * FMM_ERR_TOO_LARGE.  The first call on a device looks up that array's
+ * device address (cudaGetSymbolAddress), so make it before any stream
+ * capture.  All calls on a device share the array: calls that overlap on
+ * the GPU (e.g. on two streams at once) race and give wrong results. */
+#define FMM_NOALLOC_MAX_TARGETS 262144
+FMM_API int fmm_direct_noalloc(int32_t dim, int64_t n, const double *d_pos, const double *d_mass, int64_t ntargets,
+                               const int64_t *d_targets, int32_t soft_mode, double eps2, double G, double *d_acc,
+                               double *d_pot, void *stream);
 
 /* Statistics of the last force pass (per-phase device times, sizes). */
 FMM_API int fmm_last_stats(fmm_ctx *ctx, fmm_stats *out);

@@ -61,6 +61,7 @@ const char *fmm_strerror(int code) {
     case FMM_ERR_UNSUPPORTED: return "unsupported configuration";
     case FMM_ERR_TIMEOUT: return "device wait timed out";
     case FMM_ERR_NO_DEVICE: return "no CUDA device";
+    case FMM_ERR_TOO_LARGE: return "more targets than fmm_direct_noalloc's fixed scratch holds (FMM_NOALLOC_MAX_TARGETS)";
     default: return "internal error";
   }
 }

@@ -28,6 +28,8 @@ FMM_ERR_NONFINITE_OUTPUT = -5
 FMM_ERR_UNSUPPORTED = -6
 FMM_ERR_TIMEOUT = -7
 FMM_ERR_NO_DEVICE = -8
+FMM_ERR_TOO_LARGE = -10
+FMM_NOALLOC_MAX_TARGETS = 262144
 
 FMM_M2L_FP32 = 0
 FMM_M2L_TC = 1
@@ -41,7 +43,7 @@ EXPORTED = (
     "fmm_strerror", "fmm_version", "fmm_config_default", "fmm_create", "fmm_destroy", "fmm_evaluate",
     "fmm_evaluate_device", "fmm_synchronize", "fmm_direct", "fmm_direct_device", "fmm_integrate",
     "fmm_tree_build", "fmm_tree_depth", "fmm_tree_level_size", "fmm_tree_level_keys", "fmm_tree_leaves",
-    "fmm_tree_pairs", "fmm_last_stats", "fmm_launch_count",
+    "fmm_tree_pairs", "fmm_last_stats", "fmm_launch_count", "fmm_direct_noalloc",
 )
 
 
@@ -105,6 +107,8 @@ def load_library(path=LIB_PATH):
     L.fmm_last_stats.argtypes = [_vp, ctypes.POINTER(FmmStats)]
     L.fmm_launch_count.restype = ctypes.c_int64
     L.fmm_launch_count.argtypes = [_vp]
+    L.fmm_direct_noalloc.argtypes = [ctypes.c_int32, ctypes.c_int64, _vp, _vp, ctypes.c_int64, _vp, ctypes.c_int32,
+                                     ctypes.c_double, ctypes.c_double, _vp, _vp, _vp]
     _lib = L
     return L
 
@@ -116,6 +120,18 @@ def _check(rc):
 
 def _p(a, t=_d):
     return None if a is None else a.ctypes.data_as(t)
+
+
+def direct_noalloc(dim, n, pos_ptr, mass_ptr, acc_ptr, pot_ptr=None, ntargets=0, targets_ptr=None,
+                   soft_mode=FMM_SOFT_PLUMMER, eps2=0.0, G=1.0, stream=None):
+    """FP64 direct sum on the current GPU into caller-owned device buffers,
+    without any device allocation and without a Context (fmm_direct_noalloc).
+    For callers that cannot allocate device memory when they need forces; at
+    most FMM_NOALLOC_MAX_TARGETS targets; concurrent calls on one GPU race
+    on the library's fixed scratch.  Enqueued on `stream` (an int handle)."""
+    L = load_library()
+    _check(L.fmm_direct_noalloc(dim, n, pos_ptr, mass_ptr, ntargets, targets_ptr, soft_mode, eps2, G, acc_ptr,
+                                pot_ptr, stream))
 
 
 class Context:
