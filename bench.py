@@ -279,12 +279,16 @@ def run_ours(args, world, rank, local):
 
 
 def load_traffic():
-    """DRAM bytes per M2L launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "m2l_traffic.json")
+    """DRAM bytes per M2L launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    from the committed ncu summary of that kernel, if present."""
+    path = os.path.join(ROOT, "profiles", "k_contract_m2l_plummer_2p20_p8.md")
     try:
-        return json.load(open(path))
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":")[1])
     except Exception:
-        return None
+        pass
+    return None
 
 
 # ------------------------------------------------------------- reference
