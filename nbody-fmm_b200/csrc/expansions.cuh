@@ -33,7 +33,7 @@ struct PassGeom {
   double lo[3], ext[3], emax;
 };
 
-int build_op_tables(OpTables &ops, int dim, int p, const PassGeom &g, cudaStream_t st, int64_t &launches);
+int build_op_tables(OpTables &ops, int dim, int p, int depth, const PassGeom &g, cudaStream_t st, int64_t &launches);
 void upload_class_tables();
 
 int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, const double *d_pos,

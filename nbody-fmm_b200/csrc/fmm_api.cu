@@ -159,7 +159,6 @@ static int evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const dou
   if (n < 0 || n > (int64_t)INT32_MAX) return FMM_ERR_INVALID_ARGUMENT;
   if (n == 0) return FMM_OK;
   if (!d_pos || !d_mass || !d_acc) return FMM_ERR_INVALID_ARGUMENT;
-  if (dim == 2) return FMM_ERR_UNSUPPORTED;
   CUDA_TRY(cudaEventRecord(c->ev[0], st));
   int rc = build_tree(c->ws, c->tree, d_pos, d_mass, n, dim, c->cfg.leaf_cap, st);
   if (rc) return rc;
@@ -172,7 +171,7 @@ static int evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const dou
     g.ext[d] = d < dim ? c->tree.hi[d] - c->tree.lo[d] : 0.0;
     g.emax = std::max(g.emax, g.ext[d]);
   }
-  rc = build_op_tables(c->ops, dim, c->cfg.p, g, st, c->ws.launches);
+  rc = build_op_tables(c->ops, dim, c->cfg.p, c->tree.depth, g, st, c->ws.launches);
   if (rc) return rc;
   memset(&c->stats, 0, sizeof(c->stats));
   rc = run_fmm_passes(c->ws, c->tree, c->ops, c->eb, d_pos, d_mass, c->cfg.p, c->cfg.eps2, c->cfg.G, g, d_acc, d_pot,

@@ -214,14 +214,19 @@ __device__ inline cd op2_coef(int kind, cd z, int n, int k) {
   }
 }
 
-__global__ void k_build_ops2d(float *tab, int p, int K, int KP, int n_m2l, double ax, double ay) {
+// 2D M2L tables are per level: the physical offset is s_d * rho, and
+// a_0 log(s_d rho) adds a_0 log(s_d) to b_0 (log_s0 = log s_0, s_d = s_0 2^-d).
+__global__ void k_build_ops2d(float *tab, int p, int K, int KP, int n_m2l, double ax, double ay, double log_s0) {
   const int slot = blockIdx.x;
   int kind;
   cd z;
   bool zero = false;
+  double log_s = 0.0;
   if (slot < n_m2l) {
     kind = 0;
-    int dx = slot % 7 - 3, dy = slot / 7 - 3;  // source - target
+    const int lev = slot / 49, off = slot % 49;
+    log_s = log_s0 - lev * 0.69314718055994530942;
+    int dx = off % 7 - 3, dy = off / 7 - 3;  // source - target
     z = {-dx * ax, -dy * ay};
     if ((dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1) || (z.re == 0.0 && z.im == 0.0)) zero = true;
   } else {
@@ -239,6 +244,7 @@ __global__ void k_build_ops2d(float *tab, int p, int K, int KP, int n_m2l, doubl
       dec2(out, n, po);
       dec2(in, k, pi);
       cd C = op2_coef(kind, z, n, k);
+      if (kind == 0 && n == 0 && k == 0) C.re += log_s;
       // x_k = a + i b: out += C a  (pi = 0),  out += C i b (pi = 1)
       if (pi == 0) val = po ? C.im : C.re;
       else val = po ? C.re : -C.im;
@@ -247,7 +253,7 @@ __global__ void k_build_ops2d(float *tab, int p, int K, int KP, int n_m2l, doubl
   }
 }
 
-int build_op_tables(OpTables &ops, int dim, int p, const PassGeom &g, cudaStream_t st, int64_t &launches) {
+int build_op_tables(OpTables &ops, int dim, int p, int depth, const PassGeom &g, cudaStream_t st, int64_t &launches) {
   int K = dim == 3 ? (p + 1) * (p + 1) : 2 * p + 1;
   int KP = 32 * ((K + 31) / 32);
   int KS = (K + 3) & ~3;
@@ -256,7 +262,7 @@ int build_op_tables(OpTables &ops, int dim, int p, const PassGeom &g, cudaStream
   ops.K = K;
   ops.KP = KP;
   ops.KS = KS;
-  ops.n_m2l = dim == 3 ? 343 : 49;
+  ops.n_m2l = dim == 3 ? 343 : 49 * (depth + 1);
   ops.off_m2m = ops.n_m2l;
   ops.off_l2l = ops.n_m2l + (1 << dim);
   ops.n_slots = ops.n_m2l + 2 * (1 << dim);
@@ -267,7 +273,7 @@ int build_op_tables(OpTables &ops, int dim, int p, const PassGeom &g, cudaStream
     size_t sh = sizeof(double) * 2 * (size_t)(2 * p + 1) * (2 * p + 2) / 2;
     k_build_ops3d<<<ops.n_slots, 256, sh, st>>>(ops.tab.ptr, p, K, KP, ops.n_m2l, a[0], a[1], a[2]);
   } else {
-    k_build_ops2d<<<ops.n_slots, 256, 0, st>>>(ops.tab.ptr, p, K, KP, ops.n_m2l, a[0], a[1]);
+    k_build_ops2d<<<ops.n_slots, 256, 0, st>>>(ops.tab.ptr, p, K, KP, ops.n_m2l, a[0], a[1], std::log(emax));
   }
   launches += 1;
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;

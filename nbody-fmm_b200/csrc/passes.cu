@@ -432,12 +432,95 @@ __global__ void k_l2p3d(const float4 *part, const int *leaf_of, int64_t n, int c
   far[i] = make_float4(gx * inv_s * inv_s, gy * inv_s * inv_s, gz * inv_s * inv_s, ph * inv_s);
 }
 
+// ------------------------------------------------------------------ 2D
+// P2M / L2P of the complex-log expansions (power_set2D.cpp:9-21,
+// local_set2D.cpp:60-69) with coefficients scaled by the cell size s:
+// a~_k = sum_i m_i ((z_i - c)/s)^k, stored [a_0, Re a_1, Im a_1, ...].
+__global__ void k_p2m2d(const float4 *part, const int *leaf_of, int64_t n, int cell0, float inv_s, int p, int KS,
+                        float *M) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  bool valid = i < n;
+  float4 q = valid ? part[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  int seg = valid ? leaf_of[i] : -1 - lane;
+  bool same[5];
+#pragma unroll
+  for (int o = 1, k = 0; o < 32; o <<= 1, ++k) {
+    int so = __shfl_down_sync(0xffffffffu, seg, o);
+    same[k] = (lane + o < 32) && so == seg;
+  }
+  int sp = __shfl_up_sync(0xffffffffu, seg, 1);
+  bool head = valid && (lane == 0 || sp != seg);
+  float *Mrow = M + (size_t)(valid ? seg - cell0 : 0) * KS;
+  const float x = q.x * inv_s, y = q.y * inv_s, w = q.w;
+  float v = seg_sum(w, same);
+  if (head) atomicAdd(Mrow, v);
+  float pr = w, pi = 0.f;  // w (z/s)^k
+  for (int k = 1; k <= p; ++k) {
+    const float nr = pr * x - pi * y, ni = pr * y + pi * x;
+    pr = nr;
+    pi = ni;
+    float vr = seg_sum(pr, same), vi = seg_sum(pi, same);
+    if (head) {
+      atomicAdd(Mrow + 2 * k - 1, vr);
+      atomicAdd(Mrow + 2 * k, vi);
+    }
+  }
+}
+
+// L^ = [Re b_0, Re b_1, Im b_1, ...] with b^_n = b_n s^n represents
+// sum_j m_j log(z - z_j); phi = -Re sum b^_n u^n and
+// grad = (1/s) (-Re, +Im)(sum n b^_n u^(n-1)), u = (z - c)/s.
+__global__ void k_l2p2d(const float4 *part, const int *leaf_of, int64_t n, int cell0, float inv_s, int p, int KS,
+                        const float *L, float4 *far) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 q = part[i];
+  const float *Lr = L + (size_t)(leaf_of[i] - cell0) * KS;
+  const float x = q.x * inv_s, y = q.y * inv_s;
+  float phr = Lr[0], dr = 0.f, di = 0.f, ur = 1.f, ui = 0.f;  // u^(n-1)
+  for (int k = 1; k <= p; ++k) {
+    const float br = Lr[2 * k - 1], bi = Lr[2 * k];
+    dr += k * (br * ur - bi * ui);
+    di += k * (br * ui + bi * ur);
+    const float nr = ur * x - ui * y, ni = ur * y + ui * x;
+    ur = nr;
+    ui = ni;
+    phr += br * ur - bi * ui;
+  }
+  far[i] = make_float4(-dr * inv_s, di * inv_s, 0.f, -phr);
+}
+
 // ------------------------------------------------------------------ P2P
 // Error-free sum: s + e == a + b exactly (Knuth's TwoSum).
 __device__ inline void two_sum(float a, float b, float &s, float &e) {
   s = a + b;
   float bb = s - a;
   e = (a - (s - bb)) + (b - bb);
+}
+
+// One pair: grad -= m d/|d|^3, phi += m/|d| (3D, leaf.cpp:118-142) or
+// grad -= m d/|d|^2, phi -= m log|d| (2D, leaf.cpp:81-95), r^2 -> r^2 + eps2.
+template <int DIM>
+__device__ inline void pair_acc(float rx, float ry, float rz, float w, float eps2, float &ax, float &ay, float &az,
+                                float &ph) {
+  if (DIM == 3) {
+    const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2)));
+    float inv = rsqrtf(r2);
+    inv = inv * fmaf(-0.5f * r2 * inv, inv, 1.5f);  // one Newton step
+    const float mi = w * inv;
+    const float mi3 = mi * inv * inv;
+    ax = fmaf(-rx, mi3, ax);
+    ay = fmaf(-ry, mi3, ay);
+    az = fmaf(-rz, mi3, az);
+    ph += mi;
+  } else {
+    const float r2 = fmaf(rx, rx, fmaf(ry, ry, eps2));
+    const float f = w / r2;
+    ax = fmaf(-rx, f, ax);
+    ay = fmaf(-ry, f, ay);
+    ph = fmaf(-0.5f * w, logf(r2), ph);
+  }
 }
 
 struct P2PArgs {
@@ -457,18 +540,19 @@ struct P2PArgs {
 
 // One warp per target leaf; the leaf's particles are spread over the lanes
 // (several lanes per particle for small leaves, each taking a share of the
-// sources).  Sources:
-//  - near field: the leaf itself (j != i) and its existing neighbours
-//    (leaf.cpp:118-142);
-// The direct far field (interaction-list pairs summed particle by particle)
-// has been added into `far` by k_direct_far before this kernel runs.
+// sources).  Sources: the leaf itself (j != i) and its existing neighbours
+// (leaf.cpp:118-142).  The direct far field (interaction-list pairs summed
+// particle by particle) has been added into `far` by k_direct_far before
+// this kernel runs; this kernel adds the near field and writes the output.
 //
 // Near-field precision: x_i - x_j = (t_i - shift) - s_j with t_i, s_j the
 // offsets from the two leaf centres and shift = c_s - c_t an exact multiple
 // of the leaf size.  Offsets are hi + lo FP32 pairs, the shift is hi + lo
 // from FP64, and (t_hi - shift_hi) is formed error-free (TwoSum), so each
 // difference is rounded once, relative to itself, whatever the separation.
-__global__ void k_p2p3d(P2PArgs a) {
+template <int DIM>
+__global__ void k_p2p(P2PArgs a) {
+  constexpr int NS = DIM == 3 ? 27 : 9;
   const int lane = threadIdx.x & 31;
   const int wl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (wl >= a.nleaves) return;
@@ -478,7 +562,7 @@ __global__ void k_p2p3d(P2PArgs a) {
   int Gl = 1;
   while (Gl * 2 * tp <= 32) Gl *= 2;
   const int tpp = 32 / Gl;
-  const int *cl = a.coll + (int64_t)g * 27;
+  const int *cl = a.coll + (int64_t)g * NS;
   bool bad = false;
   long long npairs = 0;
   for (int t0 = 0; t0 < nt; t0 += tpp) {
@@ -487,11 +571,11 @@ __global__ void k_p2p3d(P2PArgs a) {
     const int me_i = tb + (act ? ti : 0);
     const float4 me = a.part[me_i], mel = a.part_lo[me_i];
     float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
-    for (int s = 0; s < 27; ++s) {
+    for (int s = 0; s < NS; ++s) {
       const int S = cl[s];
       if (S < 0) continue;
       // shift = c_s - c_t in hi + lo
-      const double sx = (s % 3 - 1) * a.hx, sy = ((s / 3) % 3 - 1) * a.hy, sz = (s / 9 - 1) * a.hz;
+      const double sx = (s % 3 - 1) * a.hx, sy = ((s / 3) % 3 - 1) * a.hy, sz = DIM == 3 ? (s / 9 - 1) * a.hz : 0.0;
       const float shx = (float)sx, shy = (float)sy, shz = (float)sz;
       float tx, ty, tz, ex, ey, ez;
       two_sum(me.x, -shx, tx, ex);
@@ -508,15 +592,7 @@ __global__ void k_p2p3d(P2PArgs a) {
         const float rx = (tx - q.x) + (ex - ql.x);
         const float ry = (ty - q.y) + (ey - ql.y);
         const float rz = (tz - q.z) + (ez - ql.z);
-        const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, a.eps2)));
-        float inv = rsqrtf(r2);
-        inv = inv * fmaf(-0.5f * r2 * inv, inv, 1.5f);  // one Newton step
-        const float mi = q.w * inv;
-        const float mi3 = mi * inv * inv;
-        ax = fmaf(-rx, mi3, ax);
-        ay = fmaf(-ry, mi3, ay);
-        az = fmaf(-rz, mi3, az);
-        ph += mi;
+        pair_acc<DIM>(rx, ry, rz, q.w, a.eps2, ax, ay, az, ph);
       }
     }
     for (int o = 1; o < Gl; o <<= 1) {
@@ -529,9 +605,9 @@ __global__ void k_p2p3d(P2PArgs a) {
       const float4 f = a.far[me_i];
       const uint32_t o = a.perm[me_i];
       double vx = a.G * ((double)f.x + ax), vy = a.G * ((double)f.y + ay), vz = a.G * ((double)f.z + az);
-      a.acc[3 * (size_t)o] = vx;
-      a.acc[3 * (size_t)o + 1] = vy;
-      a.acc[3 * (size_t)o + 2] = vz;
+      a.acc[DIM * (size_t)o] = vx;
+      a.acc[DIM * (size_t)o + 1] = vy;
+      if (DIM == 3) a.acc[3 * (size_t)o + 2] = vz;
       if (a.pot) a.pot[o] = a.G * ((double)f.w + ph);
       bad |= !(isfinite(vx) && isfinite(vy) && isfinite(vz));
     }
@@ -544,21 +620,22 @@ __global__ void k_p2p3d(P2PArgs a) {
 // Offsets of every particle (leaf order) from the centre of its ancestor at
 // level d, FP32, with the mass: the frame in which pairs of level-d cells
 // are summed directly.
+template <int DIM>
 __global__ void k_level_offsets(const double *pos, const double *mass, const uint32_t *perm, const int *leaf_of,
                                 const uint64_t *ckey, int64_t n, int depth, int d, double lox, double loy, double loz,
                                 double ex, double ey, double ez, float4 *out) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint32_t qx, qy, qz;
-  morton_decode(3, ckey[leaf_of[i]], qx, qy, qz);
+  morton_decode(DIM, ckey[leaf_of[i]], qx, qy, qz);
   const int sh = depth - d;
   const double inv = ldexp(1.0, -d);
   const uint32_t j = perm[i];
   double cx = lox + ((double)(qx >> sh) + 0.5) * (ex * inv);
   double cy = loy + ((double)(qy >> sh) + 0.5) * (ey * inv);
-  double cz = loz + ((double)(qz >> sh) + 0.5) * (ez * inv);
-  out[i] = make_float4((float)(pos[3 * (size_t)j] - cx), (float)(pos[3 * (size_t)j + 1] - cy),
-                       (float)(pos[3 * (size_t)j + 2] - cz), (float)mass[j]);
+  double cz = DIM == 3 ? loz + ((double)(qz >> sh) + 0.5) * (ez * inv) : 0.0;
+  out[i] = make_float4((float)(pos[DIM * (size_t)j] - cx), (float)(pos[DIM * (size_t)j + 1] - cy),
+                       DIM == 3 ? (float)(pos[3 * (size_t)j + 2] - cz) : 0.f, (float)mass[j]);
 }
 
 struct DirectArgs {
@@ -573,25 +650,12 @@ struct DirectArgs {
   unsigned long long *pair_count;
 };
 
-__device__ inline void pair_acc(float rx, float ry, float rz, float w, float eps2, float &ax, float &ay, float &az,
-                                float &ph) {
-  const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2)));
-  float inv = rsqrtf(r2);
-  inv = inv * fmaf(-0.5f * r2 * inv, inv, 1.5f);
-  const float mi = w * inv;
-  const float mi3 = mi * inv * inv;
-  ax = fmaf(-rx, mi3, ax);
-  ay = fmaf(-ry, mi3, ay);
-  az = fmaf(-rz, mi3, az);
-  ph += mi;
-}
-
 // One warp per level-d target cell T with n_T <= direct_max: the sources are
 // the cells S of T's interaction list (node_i.cpp:39-43) with
 // n_T * n_S <= direct_max, exactly the pairs the M2L contraction skips.
 // Small T (NT <= 8 targets): every lane holds all targets and takes every
 // 32nd particle of the concatenated sources; larger T: lanes over targets.
-template <int NT>
+template <int NT, int DIM>
 __device__ void direct_small(const DirectArgs &a, int tb, int nt, const int *s_src, const float *s_shift,
                              const int *s_pref, int nsrc, int lane) {
   float tx[NT], ty[NT], tz[NT], ax[NT], ay[NT], az[NT], ph[NT];
@@ -611,7 +675,8 @@ __device__ void direct_small(const DirectArgs &a, int tb, int nt, const int *s_s
     const float4 q = a.off[j];
     const float qx = q.x + s_shift[3 * si], qy = q.y + s_shift[3 * si + 1], qz = q.z + s_shift[3 * si + 2];
 #pragma unroll
-    for (int k = 0; k < NT; ++k) pair_acc(tx[k] - qx, ty[k] - qy, tz[k] - qz, q.w, a.eps2, ax[k], ay[k], az[k], ph[k]);
+    for (int k = 0; k < NT; ++k)
+      pair_acc<DIM>(tx[k] - qx, ty[k] - qy, tz[k] - qz, q.w, a.eps2, ax[k], ay[k], az[k], ph[k]);
   }
 #pragma unroll
   for (int k = 0; k < NT; ++k) {
@@ -629,7 +694,9 @@ __device__ void direct_small(const DirectArgs &a, int tb, int nt, const int *s_s
   }
 }
 
+template <int DIM>
 __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
+  constexpr int NS = DIM == 3 ? 27 : 9, NC = 1 << DIM, NCAND = NS * NC, NR = (NCAND + 31) / 32;
   __shared__ int s_src_all[8][189];
   __shared__ float s_shift_all[8][3 * 189];
   __shared__ int s_pref_all[8][190];
@@ -643,29 +710,30 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   float *s_shift = s_shift_all[wib];
   int *s_pref = s_pref_all[wib];
   const int P = a.parent[T];
-  const int cls = (int)(a.ckey[T] & 7u);
-  const int *pc = a.coll + (int64_t)P * 27;
+  const int cls = (int)(a.ckey[T] & (uint64_t)(NC - 1));
+  const int *pc = a.coll + (int64_t)P * NS;
   int nsrc = 0;
   if (lane == 0) s_pref[0] = 0;
   // all candidate loads in flight at once: colleague, child, then counts
-  const int Qlane = lane < 27 ? pc[lane] : -1;
-  int qv[7], nsv[7];
+  const int Qlane = lane < NS ? pc[lane] : -1;
+  int qv[NR], nsv[NR];
 #pragma unroll
-  for (int r = 0; r < 7; ++r) {
+  for (int r = 0; r < NR; ++r) {
     const int cand = r * 32 + lane;
-    const int Q = __shfl_sync(0xffffffffu, Qlane, (cand >> 3) < 27 ? (cand >> 3) : 0);
-    qv[r] = (cand < 216 && Q >= 0) ? a.child[(int64_t)Q * 8 + (cand & 7)] : -1;
+    const int dl = cand / NC;
+    const int Q = __shfl_sync(0xffffffffu, Qlane, dl < NS ? dl : 0);
+    qv[r] = (cand < NCAND && Q >= 0) ? a.child[(int64_t)Q * NC + (cand % NC)] : -1;
   }
 #pragma unroll
-  for (int r = 0; r < 7; ++r) nsv[r] = qv[r] >= 0 ? a.pend[qv[r]] - a.pbeg[qv[r]] : 0;
+  for (int r = 0; r < NR; ++r) nsv[r] = qv[r] >= 0 ? a.pend[qv[r]] - a.pbeg[qv[r]] : 0;
 #pragma unroll
-  for (int r = 0; r < 7; ++r) {
+  for (int r = 0; r < NR; ++r) {
     const int cand = r * 32 + lane;
-    const int dl = cand >> 3, k = cand & 7;
+    const int dl = cand / NC, k = cand % NC;
     int q = qv[r];
     const int ddx = 2 * (dl % 3 - 1) + (k & 1) - (cls & 1);
     const int ddy = 2 * ((dl / 3) % 3 - 1) + ((k >> 1) & 1) - ((cls >> 1) & 1);
-    const int ddz = 2 * (dl / 9 - 1) + ((k >> 2) & 1) - ((cls >> 2) & 1);
+    const int ddz = DIM == 3 ? 2 * (dl / 9 - 1) + ((k >> 2) & 1) - ((cls >> 2) & 1) : 0;
     const bool adj = ddx >= -1 && ddx <= 1 && ddy >= -1 && ddy <= 1 && ddz >= -1 && ddz <= 1;
     if (q >= 0 && (adj || (long long)nt * nsv[r] > a.direct_max)) q = -1;
     const unsigned mask = __ballot_sync(0xffffffffu, q >= 0);
@@ -690,10 +758,10 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
     if (a.pair_count) atomicAdd(a.pair_count, (unsigned long long)((long long)nt * acc));
   }
   __syncwarp();
-  if (nt <= 1) direct_small<1>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
-  else if (nt <= 2) direct_small<2>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
-  else if (nt <= 4) direct_small<4>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
-  else if (nt <= 8) direct_small<8>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
+  if (nt <= 1) direct_small<1, DIM>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
+  else if (nt <= 2) direct_small<2, DIM>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
+  else if (nt <= 4) direct_small<4, DIM>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
+  else if (nt <= 8) direct_small<8, DIM>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
   else {
     // lanes over targets; every lane walks all sources (warp-uniform loads)
     for (int t0 = 0; t0 < nt; t0 += 32) {
@@ -705,7 +773,7 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
         const int jb = a.pbeg[s_src[si]], je = a.pend[s_src[si]];
         for (int j = jb; j < je; ++j) {
           const float4 q = a.off[j];
-          pair_acc(tx - q.x, ty - q.y, tz - q.z, q.w, a.eps2, ax, ay, az, ph);
+          pair_acc<DIM>(tx - q.x, ty - q.y, tz - q.z, q.w, a.eps2, ax, ay, az, ph);
         }
       }
       if (ti < nt) {
@@ -863,7 +931,8 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
 
   if (ev) cudaEventRecord(ev[1], st);
   // P2M
-  k_p2m3d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.M.ptr);
+  if (dim == 3) k_p2m3d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.M.ptr);
+  else k_p2m2d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.M.ptr);
   ws.launches += 1;
   // M2M, bottom-up
   for (int d = D - 1; d >= 2; --d) {
@@ -915,7 +984,10 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     if (rc) return rc;
   }
   // L2P
-  k_l2p3d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far);
+  if (dim == 3)
+    k_l2p3d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far);
+  else
+    k_l2p2d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far);
   ws.launches += 1;
   if (ev) cudaEventRecord(ev[4], st);
   // direct far field, level by level (levels >= 2 have interaction lists)
@@ -937,7 +1009,8 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
       if (d == D) {
         da.off = ws.part;
       } else {
-        k_level_offsets<<<cdiv(n, TPB), TPB, 0, st>>>(d_pos_g, d_mass_g, t.d_perm, ws.leaf_of, ws.cell_key, n, D, d,
+        auto lo_kern = dim == 3 ? k_level_offsets<3> : k_level_offsets<2>;
+        lo_kern<<<cdiv(n, TPB), TPB, 0, st>>>(d_pos_g, d_mass_g, t.d_perm, ws.leaf_of, ws.cell_key, n, D, d,
                                                       g.lo[0], g.lo[1], g.lo[2], g.ext[0], g.ext[1], g.ext[2],
                                                       eb.lvl_off.ptr);
         ws.launches += 1;
@@ -949,7 +1022,8 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
       da.hx = (float)(g.ext[0] * invd);
       da.hy = (float)(g.ext[1] * invd);
       da.hz = (float)(g.ext[2] * invd);
-      k_direct_far<<<cdiv((int64_t)da.count * 32, TPB), TPB, 0, st>>>(da);
+      if (dim == 3) k_direct_far<3><<<cdiv((int64_t)da.count * 32, TPB), TPB, 0, st>>>(da);
+      else k_direct_far<2><<<cdiv((int64_t)da.count * 32, TPB), TPB, 0, st>>>(da);
       ws.launches += 1;
     }
   }
@@ -980,7 +1054,8 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   pa.pot = d_pot;
   pa.err = ws.dev_err;
   pa.pair_count = ws.counters + 1;
-  k_p2p3d<<<cdiv((int64_t)pa.nleaves * 32, TPB), TPB, 0, st>>>(pa);
+  if (dim == 3) k_p2p<3><<<cdiv((int64_t)pa.nleaves * 32, TPB), TPB, 0, st>>>(pa);
+  else k_p2p<2><<<cdiv((int64_t)pa.nleaves * 32, TPB), TPB, 0, st>>>(pa);
   ws.launches += 1;
   if (ev) cudaEventRecord(ev[5], st);
   stats.n_cells = ncell;

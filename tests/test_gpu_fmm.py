@@ -56,8 +56,6 @@ def test_tree_matches_reference_fixture(name):
     z = golden("ref_trees.npz")
     pos = z[f"{name}/pos"]
     dim = pos.shape[1]
-    if dim == 2:
-        pytest.skip("2D tree build covered by test_gpu_fmm2d")
     with fmmgpu.Context(dim=dim, leaf_cap=int(z[f"{name}/T"])) as c:
         t = c.tree(pos)
     D = int(z[f"{name}/depth"])

@@ -1,0 +1,85 @@
+"""2D quadtree (complex-log) FMM on the GPU, through the C ABI.
+
+The reference's 2D operators converge (multipole_set2D.cpp, local_set2D.cpp),
+so here the GPU pass is held to the reference's own FMM::update at the same
+p and leaf capacity: relative L2 force error <= 1e-6 on the reference's
+fixture (uniform disk, p = 15, where the reference itself is accurate to
+~3e-8).  Against the FP64 oracle at the same p, leaf capacity and
+direct-pair rule: <= 1e-6 (FP32 arithmetic)."""
+import numpy as np
+import pytest
+from conftest import golden, rel_l2, tree_pairs_set
+
+import fmmgpu
+from fmmgpu import workloads
+
+pytestmark = pytest.mark.gpu
+
+
+def test_matches_reference_fmm_p15():
+    z = golden("ref_fmm2d.npz")
+    with fmmgpu.Context(dim=2, p=15, leaf_cap=16, G=1.0, direct_max=0) as c:
+        a = c.evaluate(z["pos"], z["mass"])
+    assert rel_l2(a, z["p15"]) < 1e-6
+
+
+@pytest.mark.parametrize("p", [2, 8])
+def test_matches_reference_fmm_low_p(oracle, p):
+    """At low p the reference's truncation error dominates; the GPU pass is
+    as close to the exact sum as the reference (geometric vs mass centres)."""
+    z = golden("ref_fmm2d.npz")
+    with fmmgpu.Context(dim=2, p=p, leaf_cap=16, G=1.0, direct_max=0) as c:
+        a = c.evaluate(z["pos"], z["mass"])
+    d = oracle.direct(z["pos"], z["mass"])
+    assert rel_l2(a, d) < 2.0 * rel_l2(z[f"p{p}"], d) + 1e-6
+
+
+@pytest.mark.parametrize("gen,n,p,T,dm", [("disk2d", 20000, 16, 32, 0), ("disk_clumps2d", 20000, 16, 32, 0),
+                                          ("disk_clumps2d", 30000, 12, 32, 40), ("uniform2d", 8000, 8, 16, 64)])
+def test_matches_oracle(oracle, gen, n, p, T, dm):
+    if gen == "uniform2d":
+        pos, m = workloads.uniform_cube(n, seed=4, dim=2)
+    else:
+        pos, m = workloads.WORKLOADS[gen](n, seed=4)
+    with fmmgpu.Context(dim=2, p=p, leaf_cap=T, G=1.0, direct_max=dm) as c:
+        a, ph = c.evaluate(pos, m, want_pot=True)
+    g, po = oracle.fmm(pos, m, p, T, want_pot=True, direct_max=dm)
+    assert rel_l2(a, g) < 1e-6
+    assert rel_l2(ph, po) < 1e-6
+
+
+def test_clumped_error_vs_direct(oracle):
+    """Disk + 64 Gaussian clumps (sigma 0.005), log-normal masses, p = 16,
+    leaf capacity 32, default direct-pair rule: error against the FP64 sum no
+    worse than the oracle's every-pair-by-M2L error."""
+    pos, m = workloads.disk_clumps_2d(40000, seed=3)
+    with fmmgpu.Context(dim=2, p=16, leaf_cap=32, G=1.0) as c:
+        a = c.evaluate(pos, m)
+        tg = np.arange(0, 40000, 11)
+        d = c.direct(pos, m, targets=tg)
+    og = oracle.fmm(pos, m, 16, 32)
+    assert rel_l2(a[tg], d) < 1.5 * rel_l2(og[tg], d) + 1e-6
+
+
+def test_tree_matches_oracle_2d(oracle):
+    pos, _ = workloads.disk_clumps_2d(30000, seed=8)
+    with fmmgpu.Context(dim=2, leaf_cap=32) as c:
+        t = c.tree(pos)
+    o = oracle.tree(pos, 32)
+    assert t["depth"] == o["depth"]
+    np.testing.assert_array_equal(t["leaf_keys"], o["leaf_keys"])
+    np.testing.assert_array_equal(t["perm"], o["perm"])
+    for d in range(o["depth"] + 1):
+        for kind in (0, 1):
+            assert tree_pairs_set(t, d, kind) == tree_pairs_set(o, d, kind), (d, kind)
+
+
+def test_two_d_edge_cases():
+    with fmmgpu.Context(dim=2, p=8, leaf_cap=8, G=1.0) as c:
+        a = c.evaluate(np.array([[0.0, 0.0], [2.0, 0.0]]), np.array([1.0, 3.0]))
+        np.testing.assert_allclose(a, [[1.5, 0.0], [-0.5, 0.0]], rtol=1e-6)
+        pos, m = workloads.uniform_disk_2d(3000, seed=2)
+        pos[:, 1] = 0.25  # a line: zero-extent axis
+        a = c.evaluate(pos, m)
+        d = c.direct(pos, m)
+        assert rel_l2(a, d) < 1e-3
