@@ -12,6 +12,7 @@
 #define FMM_DEV_ERR_NONFINITE_INPUT 1u
 #define FMM_DEV_ERR_NONFINITE_OUTPUT 2u
 #define FMM_DEV_ERR_LIST_OVERFLOW 4u
+#define FMM_DEV_ERR_TIMEOUT 8u
 
 namespace fmm {
 

@@ -25,7 +25,8 @@ struct ExpBuffers {
   DevBuf<int4> batches;
   DevBuf<uint32_t> cls_count;
   DevBuf<float4> lvl_off;
-  DevBuf<int> m2l_src, m2l_list, m2l_nslots;  // per M2L batch: resolved sources and present slots  // particle offsets from their level-d ancestor (direct far field)
+  DevBuf<int> m2l_src, m2l_list, m2l_nslots, m2l_tslot;  // per M2L batch: resolved sources and present slots
+  DevBuf<uint16_t> tc_img;  // BF16 split operator images for the tensor-core M2L  // particle offsets from their level-d ancestor (direct far field)
 };
 
 // Per-pass parameters.

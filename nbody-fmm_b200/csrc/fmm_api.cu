@@ -45,6 +45,8 @@ static int check_cfg(const fmm_config *c) {
   if (c->m2l_mode != FMM_M2L_FP32 && c->m2l_mode != FMM_M2L_TC) return FMM_ERR_INVALID_ARGUMENT;
   if (!(c->eps2 >= 0.0)) return FMM_ERR_INVALID_ARGUMENT;
   if (c->direct_max < -1) return FMM_ERR_INVALID_ARGUMENT;
+  if (c->m2l_mode == FMM_M2L_TC && (c->dim == 3 ? (c->p + 1) * (c->p + 1) : 2 * c->p + 1) > 128)
+    return FMM_ERR_UNSUPPORTED;  // tensor-core tiles hold K <= 128 (p <= 10 in 3D)
   return FMM_OK;
 }
 
@@ -131,6 +133,8 @@ int fmm_destroy(fmm_ctx *c) {
   c->eb.m2l_src.release();
   c->eb.m2l_list.release();
   c->eb.m2l_nslots.release();
+  c->eb.m2l_tslot.release();
+  c->eb.tc_img.release();
   for (auto *b : {&c->d_pos, &c->d_mass, &c->d_acc, &c->d_pot, &c->d_vel, &c->d_x0, &c->d_v0, &c->d_xs, &c->d_vs,
                   &c->d_asum, &c->d_vsum})
     b->release();
@@ -208,6 +212,7 @@ static int finish(fmm_ctx *c, cudaStream_t st) {
   }
   if (herr & FMM_DEV_ERR_NONFINITE_INPUT) return FMM_ERR_NONFINITE_INPUT;
   if (herr & FMM_DEV_ERR_NONFINITE_OUTPUT) return FMM_ERR_NONFINITE_OUTPUT;
+  if (herr & FMM_DEV_ERR_TIMEOUT) return FMM_ERR_TIMEOUT;
   return FMM_OK;
 }
 

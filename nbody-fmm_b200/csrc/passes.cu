@@ -15,6 +15,7 @@
 #include <vector>
 
 #include "expansions.cuh"
+#include "m2l_tc.cuh"
 
 namespace fmm {
 
@@ -282,24 +283,33 @@ static int launch_contract(const ContractArgs &a, int nb, cudaStream_t st, int64
 // Resolves the source cell of every (slot, target) of each M2L batch ahead of
 // the contraction (the lookups are chains of dependent loads, cheap when
 // thousands are in flight) and lists, per batch, the slots with at least one
-// source.  One block per batch.
-__global__ void k_m2l_sources(ContractArgs a, int *src_tab, int *slot_list, int *nslots_tab) {
+// source.  One block per batch of up to `tchunk` (64 or 128) targets; with
+// pair_count set it also counts the (target, source) pairs.
+__global__ void k_m2l_sources(ContractArgs a, int tchunk, int *src_tab, int *slot_list, int *nslots_tab,
+                              int *tslot_list, unsigned long long *pair_count) {
   __shared__ int s_flag[189];
-  __shared__ int s_tgt[CT_TGT];
+  __shared__ int s_tgt[128];
+  __shared__ int s_cnt;
   const int4 b = a.batches[blockIdx.x];
   const int tid = threadIdx.x;
   const int nsl = a.dim == 3 ? 189 : 27;
-  if (tid < CT_TGT) s_tgt[tid] = tid < b.y ? a.tlist[b.x + tid] : -1;
+  if (tid < tchunk) s_tgt[tid] = tid < b.y ? a.tlist[b.x + tid] : -1;
   for (int i = tid; i < 189; i += blockDim.x) s_flag[i] = 0;
+  if (tid == 0) s_cnt = 0;
   __syncthreads();
   const size_t base = (size_t)blockIdx.x * 189;
-  for (int e = tid; e < nsl * CT_TGT; e += blockDim.x) {
-    const int slot = e / CT_TGT, t = e % CT_TGT;
+  int cnt = 0;
+  for (int e = tid; e < nsl * tchunk; e += blockDim.x) {
+    const int slot = e / tchunk, t = e % tchunk;
     int src = -1, ts;
     if (s_tgt[t] >= 0) src = contract_source(a, s_tgt[t], slot, b.w, b.z, ts);
-    src_tab[(base + slot) * CT_TGT + t] = src;
-    if (src >= 0) s_flag[slot] = 1;
+    src_tab[(base + slot) * tchunk + t] = src;
+    if (src >= 0) {
+      s_flag[slot] = 1;
+      ++cnt;
+    }
   }
+  if (pair_count && cnt) atomicAdd(&s_cnt, cnt);
   __syncthreads();
   if (tid < 32) {
     int n = 0;
@@ -307,10 +317,17 @@ __global__ void k_m2l_sources(ContractArgs a, int *src_tab, int *slot_list, int 
       const int sl = c0 + tid;
       const bool f = sl < nsl && s_flag[sl];
       const unsigned m = __ballot_sync(0xffffffffu, f);
-      if (f) slot_list[base + n + __popc(m & ((1u << tid) - 1u))] = sl;
+      if (f) {
+        const int at = n + __popc(m & ((1u << tid) - 1u));
+        slot_list[base + at] = sl;
+        if (tslot_list) tslot_list[base + at] = (c_m2l_slots[a.dim - 2][b.w][sl] & 511) + b.z * a.level_stride;
+      }
       n += __popc(m);
     }
-    if (tid == 0) nslots_tab[blockIdx.x] = n;
+    if (tid == 0) {
+      nslots_tab[blockIdx.x] = n;
+      if (pair_count && s_cnt) atomicAdd(pair_count, (unsigned long long)s_cnt);
+    }
   }
 }
 
@@ -834,7 +851,6 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
                    const double *d_mass_g, int p, double eps2, double G,
                    const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, int64_t direct_max, cudaStream_t st,
                    fmm_stats &stats, cudaEvent_t *ev) {
-  (void)m2l_mode;
   const int dim = t.dim, D = t.depth, KS = ops.KS;
   const int64_t n = t.n;
   const int ncell = t.n_cells, cell0 = t.cell0;
@@ -842,6 +858,15 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   if (!eb.M.reserve((size_t)ncell * KS) || !eb.L.reserve((size_t)ncell * KS)) return FMM_ERR_OUT_OF_MEMORY;
   CUDA_TRY(cudaMemsetAsync(eb.M.ptr, 0, sizeof(float) * (size_t)ncell * KS, st));
   CUDA_TRY(cudaMemsetAsync(eb.L.ptr, 0, sizeof(float) * (size_t)ncell * KS, st));
+  // tensor-core M2L: 128-target batches, BF16 split operator images
+  const bool tc = m2l_mode == FMM_M2L_TC && ops.K <= 128;
+  const int tchunk = tc ? 128 : CT_TGT;
+  const int P16 = (ops.K + 15) & ~15;
+  if (tc && D >= 2) {
+    if (!eb.tc_img.reserve((size_t)ops.n_m2l * 3 * P16 * P16)) return FMM_ERR_OUT_OF_MEMORY;
+    int rc = tc_build_images(ops.tab.ptr, ops.n_m2l, ops.K, ops.KP, P16, eb.tc_img.ptr, st, ws.launches);
+    if (rc) return rc;
+  }
   const double emax = g.emax > 0 ? g.emax : 1.0;
   const double sD = std::ldexp(emax, -D);
   const float inv_sD = (float)(1.0 / sD);
@@ -883,12 +908,13 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     const int ncls = 1 << dim;
     for (int pass = 0; pass < 2; ++pass) {
       const uint32_t *h = hc + 256 * pass;
+      const int chunk = pass ? tchunk : CT_TGT;
       int off = 0;
       for (int d = 2; d <= D; ++d) {
         (pass ? m2l_b0 : lvl_b0)[d] = (int)hb.size();
         for (int c = 0; c < ncls; ++c) {
           int cnt = (int)h[(d << dim) | c];
-          for (int s0 = 0; s0 < cnt; s0 += CT_TGT) hb.push_back(make_int4(off + s0, std::min(CT_TGT, cnt - s0), d, c));
+          for (int s0 = 0; s0 < cnt; s0 += chunk) hb.push_back(make_int4(off + s0, std::min(chunk, cnt - s0), d, c));
           off += cnt;
         }
         (pass ? m2l_b1 : lvl_b1)[d] = (int)hb.size();
@@ -957,17 +983,38 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     c2.Y = eb.L.ptr;
     c2.batches = eb.batches.ptr + m2l_b0[2];
     const int nbm = m2l_b1[D] - m2l_b0[2];
-    if (!eb.m2l_src.reserve((size_t)nbm * 189 * CT_TGT) || !eb.m2l_list.reserve((size_t)nbm * 189) ||
-        !eb.m2l_nslots.reserve(nbm))
+    if (!eb.m2l_src.reserve((size_t)nbm * 189 * tchunk) || !eb.m2l_list.reserve((size_t)nbm * 189) ||
+        !eb.m2l_nslots.reserve(nbm) || !eb.m2l_tslot.reserve((size_t)nbm * 189))
       return FMM_ERR_OUT_OF_MEMORY;
     if (nbm > 0) {
-      k_m2l_sources<<<nbm, 256, 0, st>>>(c2, eb.m2l_src.ptr, eb.m2l_list.ptr, eb.m2l_nslots.ptr);
+      k_m2l_sources<<<nbm, 256, 0, st>>>(c2, tchunk, eb.m2l_src.ptr, eb.m2l_list.ptr, eb.m2l_nslots.ptr,
+                                         tc ? eb.m2l_tslot.ptr : nullptr, tc ? ws.counters : nullptr);
       ws.launches += 1;
     }
-    c2.src_tab = eb.m2l_src.ptr;
-    c2.slot_list = eb.m2l_list.ptr;
-    c2.nslots_tab = eb.m2l_nslots.ptr;
-    int rc = launch_contract(c2, nbm, st, ws.launches);
+    int rc;
+    if (tc) {
+      TcArgs ta;
+      ta.batches = c2.batches;
+      ta.tlist = tl_m2l;
+      ta.src_tab = eb.m2l_src.ptr;
+      ta.slot_list = eb.m2l_list.ptr;
+      ta.tslot_list = eb.m2l_tslot.ptr;
+      ta.nslots = eb.m2l_nslots.ptr;
+      ta.X = eb.M.ptr;
+      ta.Y = eb.L.ptr;
+      ta.bimg = eb.tc_img.ptr;
+      ta.cell0 = cell0;
+      ta.K = ops.K;
+      ta.KS = KS;
+      ta.P16 = P16;
+      ta.err = ws.dev_err;
+      rc = tc_launch_m2l(ta, nbm, st, ws.launches);
+    } else {
+      c2.src_tab = eb.m2l_src.ptr;
+      c2.slot_list = eb.m2l_list.ptr;
+      c2.nslots_tab = eb.m2l_nslots.ptr;
+      rc = launch_contract(c2, nbm, st, ws.launches);
+    }
     if (rc) return rc;
   }
   if (ev) cudaEventRecord(ev[3], st);
