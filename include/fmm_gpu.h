@@ -57,7 +57,8 @@ enum {
 /* M2L arithmetic. */
 enum {
   FMM_M2L_FP32 = 0,  /* SIMT FP32 batched contraction (plain GPU FMM) */
-  FMM_M2L_TC = 1     /* tcgen05 tensor-core contraction, split precision */
+  FMM_M2L_TC = 1     /* M2L, M2M and L2L as tcgen05 tensor-core contractions, 3xBF16 split precision
+                        with FP32 accumulation; K <= 176 (3D p <= 12) */
 };
 
 /* Direct-sum softening forms. */
@@ -99,7 +100,8 @@ typedef struct fmm_stats {
   double ms_downward;       /* L2L + L2P */
   double ms_p2p;
   double ms_total;          /* whole force pass (device time) */
-  double reserved[6];
+  int64_t m2l_tiles;        /* FMM_M2L_TC: 128-row (target batch, slot) tiles of the M2L contraction */
+  double reserved[5];
 } fmm_stats;
 
 typedef struct fmm_ctx fmm_ctx;

@@ -8,6 +8,7 @@
 #include "direct.cuh"
 #include "expansions.cuh"
 #include "fmm_gpu.h"
+#include "m2l_tc.cuh"
 
 namespace fmm {
 static thread_local std::string g_cuda_err;
@@ -45,8 +46,8 @@ static int check_cfg(const fmm_config *c) {
   if (c->m2l_mode != FMM_M2L_FP32 && c->m2l_mode != FMM_M2L_TC) return FMM_ERR_INVALID_ARGUMENT;
   if (!(c->eps2 >= 0.0)) return FMM_ERR_INVALID_ARGUMENT;
   if (c->direct_max < -1) return FMM_ERR_INVALID_ARGUMENT;
-  if (c->m2l_mode == FMM_M2L_TC && (c->dim == 3 ? (c->p + 1) * (c->p + 1) : 2 * c->p + 1) > 128)
-    return FMM_ERR_UNSUPPORTED;  // tensor-core tiles hold K <= 128 (p <= 10 in 3D)
+  if (c->m2l_mode == FMM_M2L_TC && (c->dim == 3 ? (c->p + 1) * (c->p + 1) : 2 * c->p + 1) > TC_MAX_P16)
+    return FMM_ERR_UNSUPPORTED;  // tensor-core tiles hold K <= 176 (p <= 12 in 3D)
   return FMM_OK;
 }
 
@@ -194,10 +195,11 @@ static int finish(fmm_ctx *c, cudaStream_t st) {
   unsigned int herr = 0;
   CUDA_TRY(cudaMemcpy(&herr, c->ws.dev_err, sizeof(herr), cudaMemcpyDeviceToHost));
   if (c->timing_pending) {
-    unsigned long long cnt[2] = {0, 0};
+    unsigned long long cnt[3] = {0, 0, 0};
     CUDA_TRY(cudaMemcpy(cnt, c->ws.counters, sizeof(cnt), cudaMemcpyDeviceToHost));
     c->stats.m2l_pairs = (int64_t)cnt[0];
     c->stats.p2p_pairs = (int64_t)cnt[1];
+    c->stats.m2l_tiles = (int64_t)cnt[2];
     float ms[5] = {0, 0, 0, 0, 0};
     for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], c->ev[i], c->ev[i + 1]);
     c->stats.ms_tree = ms[0];

@@ -1,38 +1,50 @@
-// M2L on the 5th-generation tensor cores (tcgen05, sm_100a).
+// Translations on the 5th-generation tensor cores (tcgen05, sm_100a): M2L,
+// M2M and L2L as batched dense contractions.
 //
-// A batch of 128 target cells of one level and one child class shares the
-// same interaction offsets, so for each offset slot present in the batch
-//   D[128 x N] += A_slot[128 x K] * B_slot[K x N]
-// where A_slot gathers each target's source multipole at that offset (zero
-// row if absent) and B_slot is the offset's M2L operator (transposed).  D
-// lives in tensor memory (TMEM) across all slots of the batch and is added
-// into the local expansions at the end.
+// A CTA takes up to 128 target cells that share their translation slots:
+//   M2L  cells of one level and one child class (same interaction offsets),
+//        one slot per offset present in the batch;
+//   M2M  parent cells of one level, one slot per child class;
+//   L2L  cells of one level and one child class, one slot (the parent).
+// For each slot it computes D[128 x N] = A_slot[128 x K] * B_slot[K x N],
+// where row r of A_slot is the source expansion of target r at that slot
+// (zero if absent) and B_slot the slot's operator (transposed), and adds D
+// to the running sum R.  D and R live in tensor memory (TMEM), lane r =
+// target r; R is written to the targets' expansions at the end.
 //
 // Precision: every FP32 operand x is split into three BF16 parts
 // x = x1 + x2 + x3 (8 significant bits each, 24 in all), and the product is
 // the sum of the six split products with total order <= 2
 // (x1y1 + x1y2 + x2y1 + x1y3 + x2y2 + x3y1); the dropped terms are below
 // 2^-24 relative.  The tensor core's own FP32 accumulation truncates at the
-// accumulator's magnitude, so each slot starts a fresh accumulator and
-// issues its split products smallest first; the slot's result is then read
-// out of TMEM and summed across slots in FP32 registers (round to nearest),
-// which keeps the contraction at FP32 accuracy.  The BF16 parts of the
-// operators are prepared once per pass (k_tc_images); those of the gathered
-// multipoles by the CTA.
+// accumulator's magnitude, so D starts afresh for every slot and takes its
+// split products smallest first; R += D is done by the threads in FP32
+// (round to nearest), which keeps the contraction at FP32 accuracy.
+//
+// Pipeline.  Thread 0 issues the MMAs.  The operator's BF16 images stream
+// through two shared-memory buffers by bulk asynchronous copies completing on
+// mbarriers (one split, or one split's half of the output columns when
+// P16 > 128, per copy), so the copy of the next image overlaps the MMAs of
+// the current one.  The threads prefetch the next slot's source rows into
+// registers while the MMAs run, then split them into the A operand once the
+// MMAs have released it.
 //
 // Shared-memory operands use the K-major layout without swizzle: 8-row x
 // 16-byte core matrices, rows of a core matrix contiguous, 8-row groups
-// SBO = 128 B apart and 16-byte K chunks LBO apart.  One thread issues the
-// MMAs and commits them to an mbarrier that all threads wait on with an
-// iteration limit; on timeout the kernel flags the device error word,
-// releases its TMEM and returns.
+// SBO = 128 B apart and 16-byte K chunks LBO apart.  Every wait on an
+// mbarrier gives up after about a second; the kernel then flags the device
+// error word, drains its copies (again with a limit), releases its TMEM and
+// returns.
 #include <cuda_bf16.h>
+
+#include <algorithm>
 
 #include "m2l_tc.cuh"
 
 namespace fmm {
 
 static constexpr int TC_M = 128;
+static constexpr int TC_MAX_SLOTS = 189;
 
 __device__ inline uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -54,9 +66,11 @@ __device__ inline void split3(float v, uint16_t &h, uint16_t &m, uint16_t &l) {
   l = __bfloat16_as_ushort(bl);
 }
 
-// Operator images: for each M2L table slot and split, element (n, k) of
-// B = T^T (n: output, k: input) at ((k/8) * (P16/8) + n/8) * 64 + (n%8) * 8 + k%8.
-__global__ void k_tc_images(const float *tab, int K, int KP, int P16, uint16_t *img) {
+// Operator images: for each table slot and split s, B = T^T (n: output,
+// k: input) cut into output tiles of N0 and P16 - N0 columns, each tile
+// contiguous; element (n, k) of a tile of width nw at
+// ((k/8) * (nw/8) + n/8) * 64 + (n%8) * 8 + k%8.
+__global__ void k_tc_images(const float *tab, int K, int KP, int P16, int N0, uint16_t *img) {
   const int slot = blockIdx.x;
   const size_t bsplit = (size_t)P16 * P16;
   const float *T = tab + (size_t)slot * K * KP;
@@ -66,11 +80,47 @@ __global__ void k_tc_images(const float *tab, int K, int KP, int P16, uint16_t *
     const float v = (n < K && k < K) ? T[(size_t)k * KP + n] : 0.f;
     uint16_t h, m, l;
     split3(v, h, m, l);
-    const size_t idx = ((size_t)(k / 8) * (P16 / 8) + n / 8) * 64 + (n % 8) * 8 + (k % 8);
+    const int j = n >= N0 ? 1 : 0;
+    const int nl = n - j * N0, nw = j ? P16 - N0 : N0;
+    const size_t idx = (j ? (size_t)P16 * N0 : 0) + ((size_t)(k / 8) * (nw / 8) + nl / 8) * 64 + (nl % 8) * 8 + (k % 8);
     out[idx] = h;
     out[bsplit + idx] = m;
     out[2 * bsplit + idx] = l;
   }
+}
+
+// ------------------------------------------------------------ primitives
+__device__ inline void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+// Waits for the completion of the phase with the given parity; false after
+// about 2^31 clocks (about a second).
+__device__ inline bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t addr = smem_u32(bar);
+  const long long t0 = clock64();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > (1ll << 31)) return false;
+  }
+}
+
+// Bulk copy global -> shared completing on an mbarrier (no multicast).
+__device__ inline void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
 }
 
 __device__ inline void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accum) {
@@ -83,6 +133,11 @@ __device__ inline void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
+__device__ inline void mma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
 __device__ inline void tmem_ld16(uint32_t addr, uint32_t *r) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
@@ -92,69 +147,150 @@ __device__ inline void tmem_ld16(uint32_t addr, uint32_t *r) {
       : "r"(addr));
 }
 
+__device__ inline void tmem_st16(uint32_t addr, const uint32_t *r) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16};" ::"r"(addr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+      "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+      : "memory");
+}
+
+__device__ inline void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ inline void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// ------------------------------------------------------------------ kernel
 template <int P16>
-__global__ void __launch_bounds__(128, 1) k_m2l_tc(TcArgs a) {
+__global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a) {
+  constexpr int NT = P16 > 128 ? 2 : 1;  // output tiles
+  constexpr int N0 = tc_n0(P16);
+  constexpr int N1 = P16 - N0;
+  constexpr int KC = P16 / 8;       // 16-byte K chunks
+  constexpr int KSTEPS = P16 / 16;  // MMA K steps
+  constexpr int ASPLIT = TC_M * P16;
+  constexpr int BTILE = P16 * N0;
+  constexpr int TILES = 3 * NT;  // operator copies per slot
+  constexpr uint32_t NCOLS = P16 <= 128 ? 256u : 512u;
+  constexpr uint32_t RCOL = NCOLS / 2;  // running sum R; D at column 0
+  constexpr uint32_t LBO_A = (TC_M / 8) * 128;
+
   extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ int s_tgt[TC_M];
-  __shared__ __align__(8) uint64_t s_mbar;
+  uint16_t *As = (uint16_t *)smem;  // 3 splits
+  uint16_t *Bs = As + 3 * ASPLIT;   // 2 buffers
+  __shared__ __align__(8) uint64_t s_full[2], s_mma[2], s_done;
   __shared__ uint32_t s_tmem;
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  constexpr int KC = P16 / 8;
-  float acc[P16];
-#pragma unroll
-  for (int j = 0; j < P16; ++j) acc[j] = 0.f;
-  const size_t asplit = (size_t)KC * (TC_M / 8) * 64;  // elements per A split
-  const size_t bsplit = (size_t)KC * (P16 / 8) * 64;
-  uint16_t *As = (uint16_t *)smem;
-  uint16_t *Bs = As + 3 * asplit;
-  const int nslots = a.nslots[blockIdx.x];
-  if (nslots == 0) return;
+  __shared__ int s_slot[TC_MAX_SLOTS], s_op[TC_MAX_SLOTS];
+  __shared__ int s_n;
+
+  const int tid = threadIdx.x, warp = tid >> 5;
   const int4 bt = a.batches[blockIdx.x];
-  s_tgt[tid] = tid < bt.y ? a.tlist[bt.x + tid] : -1;
-  const uint32_t ncols = P16 <= 128 ? 128u : 256u;
+  const size_t tbase = (size_t)blockIdx.x * TC_MAX_SLOTS;
+  const int tg = tid < bt.y ? (a.tlist ? a.tlist[bt.x + tid] : bt.x + tid) : -1;
+
+  // present slots and their operators
+  if (a.mode == TC_M2L) {
+    const int n = a.nslots[blockIdx.x];
+    for (int i = tid; i < n; i += TC_M) {
+      s_slot[i] = a.slot_list[tbase + i];
+      s_op[i] = a.tslot_list[tbase + i];
+    }
+    if (tid == 0) s_n = n;
+  } else if (a.mode == TC_M2M) {
+    int n = 0;
+    for (int s = 0; s < a.nchild; ++s) {
+      const int any = __syncthreads_or(tg >= 0 && a.cchild[(int64_t)tg * a.nchild + s] >= 0);
+      if (any) {
+        if (tid == 0) {
+          s_slot[n] = s;
+          s_op[n] = a.op_base + s;
+        }
+        ++n;
+      }
+    }
+    if (tid == 0) s_n = n;
+  } else {
+    if (tid == 0) {
+      s_slot[0] = 0;
+      s_op[0] = a.op_base + bt.w;
+      s_n = bt.y > 0 ? 1 : 0;
+    }
+  }
+  __syncthreads();
+  const int nslots = s_n;
+  if (nslots == 0) return;
+  if (tid == 0 && a.mode == TC_M2L && a.tiles) atomicAdd(a.tiles, (unsigned long long)nslots);
+
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                 "r"(ncols));
+                 "r"(NCOLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar)));
+    mbar_init(&s_full[0], 1);
+    mbar_init(&s_full[1], 1);
+    mbar_init(&s_mma[0], 1);
+    mbar_init(&s_mma[1], 1);
+    mbar_init(&s_done, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  asm volatile("tcgen05.fence::before_thread_sync;");
+  tc_fence_before();
   __syncthreads();
-  asm volatile("tcgen05.fence::after_thread_sync;");
+  tc_fence_after();
   const uint32_t tmem = s_tmem;
-  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(P16 >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
-  const uint32_t lboA = (TC_M / 8) * 128, lboB = (P16 / 8) * 128;
-  const size_t tbase = (size_t)blockIdx.x * 189;
-  uint32_t phase = 0;
-  bool ok = true;
-  for (int i = 0; i < nslots && ok; ++i) {
-    const int slot = a.slot_list[tbase + i];
-    const int ts = a.tslot_list[tbase + i];
-    // operator image: 3 splits, contiguous
-    const uint16_t *bsrc = a.bimg + (size_t)ts * 3 * bsplit;
-    const int n16 = (int)(3 * bsplit * 2 / 16);
-    for (int c = tid; c < n16; c += TC_M) {
-      unsigned d = smem_u32(Bs + 8 * (size_t)c);
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(bsrc + 8 * (size_t)c));
-    }
-    asm volatile("cp.async.commit_group;\n" ::);
-    // gathered source multipole of this thread's target row, split in three
-    const int src = a.src_tab[(tbase + slot) * TC_M + tid];
-    const float *xr = src >= 0 ? a.X + (size_t)(src - a.cell0) * a.KS : nullptr;
-    for (int kc = 0; kc < KC; ++kc) {
-      float v[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int k = kc * 8 + j;
-        v[j] = (xr && k < a.KS) ? xr[k] : 0.f;
+  const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
+  const int total = nslots * TILES;
+
+  // operator copy g (slot g / TILES; splits in the order 2, 1, 0; tiles 0, 1)
+  auto load_tile = [&](int g) {
+    const int i = g / TILES, t = g % TILES;
+    const int s = 2 - t / NT, j = t % NT;
+    const uint32_t bytes = (uint32_t)(P16 * (j ? N1 : N0) * 2);
+    const uint16_t *src =
+        a.bimg + (size_t)s_op[i] * 3 * P16 * P16 + (size_t)s * P16 * P16 + (j ? (size_t)P16 * N0 : 0);
+    bulk_load(Bs + (g & 1) * BTILE, src, bytes, &s_full[g & 1]);
+  };
+  // the MMAs of operator copy g: B split s against A splits 2 - s .. 0
+  auto mma_tile = [&](int g) {
+    const int t = g % TILES;
+    const int s = 2 - t / NT, j = t % NT;
+    const int nw = j ? N1 : N0;
+    const uint32_t idesc =
+        (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nw >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
+    const uint32_t lbo_b = (uint32_t)(nw / 8) * 128;
+    const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs + (g & 1) * BTILE);
+    for (int sa = 2 - s; sa >= 0; --sa)
+      for (int ks = 0; ks < KSTEPS; ++ks) {
+        const uint64_t ad = smem_desc(a0 + (uint32_t)(sa * ASPLIT * 2) + ks * 2 * LBO_A, LBO_A, 128);
+        const uint64_t bd = smem_desc(b0 + ks * 2 * lbo_b, lbo_b, 128);
+        const uint32_t acc = (s == 2 && sa == 0 && ks == 0) ? 0u : 1u;
+        mma_bf16(tmem + (j ? (uint32_t)N0 : 0u), ad, bd, idesc, acc);
       }
+    mma_commit(&s_mma[g & 1]);
+  };
+
+  // source row of this thread's target for slot i
+  float4 rv[P16 / 4];
+  auto fetch = [&](int i) {
+    int src = -1;
+    if (tg >= 0) {
+      const int sl = s_slot[i];
+      if (a.mode == TC_M2L) src = a.src_tab[(tbase + sl) * TC_M + tid];
+      else if (a.mode == TC_M2M) src = a.cchild[(int64_t)tg * a.nchild + sl];
+      else src = a.cparent[tg];
+    }
+    const float4 *xr = (const float4 *)(a.X + (size_t)(src >= 0 ? src - a.cell0 : 0) * a.KS);
+#pragma unroll
+    for (int q = 0; q < P16 / 4; ++q) rv[q] = (src >= 0 && 4 * q < a.KS) ? xr[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+  };
+  auto write_a = [&]() {
+#pragma unroll
+    for (int kc = 0; kc < KC; ++kc) {
+      float v[8] = {rv[2 * kc].x, rv[2 * kc].y, rv[2 * kc].z, rv[2 * kc].w,
+                    rv[2 * kc + 1].x, rv[2 * kc + 1].y, rv[2 * kc + 1].z, rv[2 * kc + 1].w};
       uint16_t h[8], m[8], l[8];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) split3(v[j], h[j], m[j], l[j]);
-      const size_t off = (size_t)kc * (TC_M / 8) * 64 + (size_t)(tid / 8) * 64 + (tid % 8) * 8;
+      for (int e = 0; e < 8; ++e) split3(kc * 8 + e < a.K ? v[e] : 0.f, h[e], m[e], l[e]);
+      const size_t off = ((size_t)kc * (TC_M / 8) + tid / 8) * 64 + (tid % 8) * 8;
       uint4 ph, pm, pl;
       ph.x = h[0] | ((uint32_t)h[1] << 16); ph.y = h[2] | ((uint32_t)h[3] << 16);
       ph.z = h[4] | ((uint32_t)h[5] << 16); ph.w = h[6] | ((uint32_t)h[7] << 16);
@@ -163,101 +299,130 @@ __global__ void __launch_bounds__(128, 1) k_m2l_tc(TcArgs a) {
       pl.x = l[0] | ((uint32_t)l[1] << 16); pl.y = l[2] | ((uint32_t)l[3] << 16);
       pl.z = l[4] | ((uint32_t)l[5] << 16); pl.w = l[6] | ((uint32_t)l[7] << 16);
       *(uint4 *)(As + off) = ph;
-      *(uint4 *)(As + asplit + off) = pm;
-      *(uint4 *)(As + 2 * asplit + off) = pl;
+      *(uint4 *)(As + ASPLIT + off) = pm;
+      *(uint4 *)(As + 2 * ASPLIT + off) = pl;
     }
-    asm volatile("cp.async.wait_group 0;\n" ::);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  };
+
+  int nl = 0, nwait = 0;  // thread 0: copies issued, copies waited for
+  if (tid == 0) {
+    load_tile(0);
+    if (total > 1) load_tile(1);
+    nl = total > 1 ? 2 : 1;
+  }
+  fetch(0);
+  bool ok = true;
+  for (int i = 0; i < nslots; ++i) {
+    write_a();
+    tc_fence_before();
     __syncthreads();
+    tc_fence_after();
+    if (i + 1 < nslots) fetch(i + 1);  // in flight during the MMAs
     if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;");
-      const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs);
-      // smallest split products first: (x3,y1) (x2,y2) (x1,y3) (x2,y1) (x1,y2) (x1,y1)
-      const int pa[6] = {2, 1, 0, 1, 0, 0}, pb[6] = {0, 1, 2, 0, 1, 0};
-#pragma unroll
-      for (int pr = 0; pr < 6; ++pr)
-        for (int ks = 0; ks < P16 / 16; ++ks) {
-          const uint64_t ad = smem_desc(a0 + (uint32_t)(pa[pr] * asplit * 2) + ks * 2 * lboA, lboA, 128);
-          const uint64_t bd = smem_desc(b0 + (uint32_t)(pb[pr] * bsplit * 2) + ks * 2 * lboB, lboB, 128);
-          mma_bf16(tmem, ad, bd, idesc, (ks > 0 || pr > 0) ? 1u : 0u);
+      for (int t = 0; t < TILES && ok; ++t) {
+        const int g = i * TILES + t;
+        if (!mbar_wait(&s_full[g & 1], (g >> 1) & 1)) {
+          ok = false;
+          break;
         }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_u32(&s_mbar))
-                   : "memory");
-    }
-    // the operands are reused for the next slot only after the MMAs finish
-    uint32_t done = 0;
-    for (long long it = 0; !done; ++it) {
-      asm volatile(
-          "{\n\t.reg .pred P1;\n\t"
-          "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-          "selp.b32 %0, 1, 0, P1;\n\t}"
-          : "=r"(done)
-          : "r"(smem_u32(&s_mbar)), "r"(phase)
-          : "memory");
-      if (!done && it > (1ll << 22)) {
-        ok = false;
-        break;
+        nwait = g + 1;
+        mma_tile(g);
+        if (nl == g + 1 && nl < total && g >= 1) {  // the buffer of copy g - 1 takes copy g + 1
+          if (!mbar_wait(&s_mma[(g - 1) & 1], ((g - 1) >> 1) & 1)) {
+            ok = false;
+            break;
+          }
+          load_tile(nl++);
+        }
       }
+      mma_commit(&s_done);  // also when stopping early, so that nobody waits in vain
     }
-    phase ^= 1u;
-    // tcgen05.ld is warp-collective: read only when the whole warp saw the commit
-    const bool wdone = __all_sync(0xffffffffu, done != 0);
-    if (!wdone) ok = false;
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    if (wdone) {
-      // this slot's contribution, added in FP32 registers
+    const bool dn = mbar_wait(&s_done, (uint32_t)(i & 1));
+    // tcgen05.ld/st are warp-collective: the whole warp goes on only if it saw the commit
+    const bool wd = __all_sync(0xffffffffu, dn);
+    if (!wd) ok = false;
+    tc_fence_after();
+    if (wd) {
 #pragma unroll
       for (int c0 = 0; c0 < P16; c0 += 16) {
-        uint32_t r[16];
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, r);
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        uint32_t d[16];
+        tmem_ld16(tmem + lane_off + (uint32_t)c0, d);
+        if (i > 0) {
+          uint32_t r[16];
+          tmem_ld16(tmem + lane_off + RCOL + (uint32_t)c0, r);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int j = 0; j < 16; ++j) acc[c0 + j] += __uint_as_float(r[j]);
+          for (int e = 0; e < 16; ++e) d[e] = __float_as_uint(__uint_as_float(d[e]) + __uint_as_float(r[e]));
+        } else {
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        }
+        tmem_st16(tmem + lane_off + RCOL + (uint32_t)c0, d);
       }
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
     }
-    asm volatile("tcgen05.fence::before_thread_sync;");
-    ok = __syncthreads_and(ok);  // every thread leaves the loop at the same slot
+    // all MMAs of slot i are done: the buffer of its last copy takes the next one
+    if (tid == 0 && ok && nl < total && nl == (i + 1) * TILES + 1) load_tile(nl++);
+    tc_fence_before();
+    ok = __syncthreads_and(ok);
+    if (!ok) break;
   }
+
   if (ok) {
-    const int tg = s_tgt[warp * 32 + lane];
-    if (tg >= 0) {
-      float *y = a.Y + (size_t)(tg - a.cell0) * a.KS;
+    tc_fence_after();
+    float *y = a.Y + (size_t)(tg >= 0 ? tg - a.cell0 : 0) * a.KS;
 #pragma unroll
-      for (int j = 0; j < P16; ++j)
-        if (j < a.K) y[j] += acc[j];
+    for (int c0 = 0; c0 < P16; c0 += 16) {
+      uint32_t r[16];
+      tmem_ld16(tmem + lane_off + RCOL + (uint32_t)c0, r);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (tg >= 0) {
+#pragma unroll
+        for (int e = 0; e < 16; ++e)
+          if (c0 + e < a.K) y[c0 + e] += __uint_as_float(r[e]);
+      }
     }
   } else if (tid == 0) {
     atomicOr(a.err, FMM_DEV_ERR_TIMEOUT);
+    for (int g = nwait; g < nl; ++g)  // copies still in flight
+      if (!mbar_wait(&s_full[g & 1], (g >> 1) & 1)) break;
   }
-  asm volatile("tcgen05.fence::before_thread_sync;");
+  tc_fence_before();
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOLS));
 }
 
-size_t tc_smem_bytes(int P16) { return (size_t)3 * P16 * TC_M * 2 + (size_t)3 * P16 * P16 * 2; }
+// ------------------------------------------------------------------ host
+static size_t tc_dyn_smem(int P16) {
+  return (size_t)3 * TC_M * P16 * 2 + (size_t)2 * P16 * tc_n0(P16) * 2;
+}
 
-int tc_build_images(const float *tab, int n_m2l, int K, int KP, int P16, uint16_t *img, cudaStream_t st,
+size_t tc_smem_bytes(int P16) { return tc_dyn_smem(P16); }
+
+int tc_build_images(const float *tab, int n_slots, int K, int KP, int P16, uint16_t *img, cudaStream_t st,
                     int64_t &launches) {
-  k_tc_images<<<n_m2l, 256, 0, st>>>(tab, K, KP, P16, img);
+  k_tc_images<<<n_slots, 256, 0, st>>>(tab, K, KP, P16, tc_n0(P16), img);
   launches += 1;
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
 }
 
 template <int P16>
 static int tc_launch_p(const TcArgs &a, int nb, cudaStream_t st) {
-  const size_t sh = tc_smem_bytes(P16);
+  // at most two CTAs per SM (each holds 256 TMEM columns), one when a CTA
+  // holds 512
+  size_t sh = tc_dyn_smem(P16);
+  sh = std::max(sh, P16 <= 128 ? (size_t)80 * 1024 : (size_t)120 * 1024);
   static size_t attr = 0;
   if (attr < sh) {
-    if (cudaFuncSetAttribute(k_m2l_tc<P16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess)
+    if (cudaFuncSetAttribute(k_tc_translate<P16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess)
       return FMM_ERR_CUDA;
     attr = sh;
   }
-  k_m2l_tc<P16><<<nb, TC_M, sh, st>>>(a);
+  k_tc_translate<P16><<<nb, TC_M, sh, st>>>(a);
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
 }
 
-int tc_launch_m2l(const TcArgs &a, int nb, cudaStream_t st, int64_t &launches) {
+int tc_launch(const TcArgs &a, int nb, cudaStream_t st, int64_t &launches) {
   if (nb <= 0) return FMM_OK;
   launches += 1;
   switch (a.P16) {
@@ -269,6 +434,9 @@ int tc_launch_m2l(const TcArgs &a, int nb, cudaStream_t st, int64_t &launches) {
     case 96: return tc_launch_p<96>(a, nb, st);
     case 112: return tc_launch_p<112>(a, nb, st);
     case 128: return tc_launch_p<128>(a, nb, st);
+    case 144: return tc_launch_p<144>(a, nb, st);
+    case 160: return tc_launch_p<160>(a, nb, st);
+    case 176: return tc_launch_p<176>(a, nb, st);
     default: return FMM_ERR_UNSUPPORTED;
   }
 }

@@ -1,26 +1,41 @@
-// Tensor-core (tcgen05) M2L contraction.
+// Translations (M2L, M2M, L2L) on the 5th-generation tensor cores (tcgen05).
 #pragma once
 #include "tree.cuh"
 
 namespace fmm {
 
+enum { TC_M2L = 0, TC_M2M = 1, TC_L2L = 2 };
+
+// Largest padded expansion length the tensor-core kernel takes (K <= 176:
+// 3D p <= 12, 2D p <= 87).
+static constexpr int TC_MAX_P16 = 176;
+
 struct TcArgs {
-  const int4 *batches;      // {tlist offset, count, level, class}, 128 targets each
-  const int *tlist;         // class-grouped M2L target cells
-  const int *src_tab;       // [batch][slot][128] source cell per target, -1 if none
-  const int *slot_list;     // [batch][i] present slots
-  const int *tslot_list;    // [batch][i] operator-table slot of each present slot
-  const int *nslots;        // [batch]
-  const float *X;           // multipoles, KS floats per cell
-  float *Y;                 // local expansions (accumulated into)
-  const uint16_t *bimg;     // BF16 operator images, 3 splits per table slot
+  int mode;                 // TC_M2L, TC_M2M or TC_L2L
+  const int4 *batches;      // {first, count, level, class}, up to 128 targets each
+  const int *tlist;         // target cells (M2L, L2L); null for M2M (cells first + row)
+  const int *src_tab;       // M2L: [batch][slot][128] source cell per target, -1 if none
+  const int *slot_list;     // M2L: [batch][i] present slots
+  const int *tslot_list;    // M2L: [batch][i] operator-table slot of each present slot
+  const int *nslots;        // M2L: [batch]
+  const int *cchild;        // M2M: children of each cell (nchild per cell, -1 if absent)
+  const int *cparent;       // L2L: parent of each cell
+  int nchild;               // 8 in 3D, 4 in 2D
+  int op_base;              // M2M / L2L: operator-table slot of child class 0
+  const float *X;           // source expansions, KS floats per cell
+  float *Y;                 // target expansions (accumulated into)
+  const uint16_t *bimg;     // BF16 split operator images, 3 * P16^2 per table slot
   int cell0, K, KS, P16;    // P16 = K rounded up to 16
   unsigned int *err;
+  unsigned long long *tiles;  // M2L: number of (batch, slot) tiles contracted (nullable)
 };
 
+// Width of the first output tile: one tile up to 128 columns, else two.
+__host__ __device__ constexpr int tc_n0(int P16) { return P16 <= 128 ? P16 : ((P16 / 2 + 15) & ~15); }
+
 size_t tc_smem_bytes(int P16);
-int tc_build_images(const float *tab, int n_m2l, int K, int KP, int P16, uint16_t *img, cudaStream_t st,
+int tc_build_images(const float *tab, int n_slots, int K, int KP, int P16, uint16_t *img, cudaStream_t st,
                     int64_t &launches);
-int tc_launch_m2l(const TcArgs &a, int nb, cudaStream_t st, int64_t &launches);
+int tc_launch(const TcArgs &a, int nb, cudaStream_t st, int64_t &launches);
 
 }  // namespace fmm

@@ -858,13 +858,13 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   if (!eb.M.reserve((size_t)ncell * KS) || !eb.L.reserve((size_t)ncell * KS)) return FMM_ERR_OUT_OF_MEMORY;
   CUDA_TRY(cudaMemsetAsync(eb.M.ptr, 0, sizeof(float) * (size_t)ncell * KS, st));
   CUDA_TRY(cudaMemsetAsync(eb.L.ptr, 0, sizeof(float) * (size_t)ncell * KS, st));
-  // tensor-core M2L: 128-target batches, BF16 split operator images
-  const bool tc = m2l_mode == FMM_M2L_TC && ops.K <= 128;
-  const int tchunk = tc ? 128 : CT_TGT;
+  // tensor-core translations: 128-target batches, BF16 split operator images
   const int P16 = (ops.K + 15) & ~15;
+  const bool tc = m2l_mode == FMM_M2L_TC && P16 <= TC_MAX_P16;
+  const int tchunk = tc ? 128 : CT_TGT;
   if (tc && D >= 2) {
-    if (!eb.tc_img.reserve((size_t)ops.n_m2l * 3 * P16 * P16)) return FMM_ERR_OUT_OF_MEMORY;
-    int rc = tc_build_images(ops.tab.ptr, ops.n_m2l, ops.K, ops.KP, P16, eb.tc_img.ptr, st, ws.launches);
+    if (!eb.tc_img.reserve((size_t)ops.n_slots * 3 * P16 * P16)) return FMM_ERR_OUT_OF_MEMORY;
+    int rc = tc_build_images(ops.tab.ptr, ops.n_slots, ops.K, ops.KP, P16, eb.tc_img.ptr, st, ws.launches);
     if (rc) return rc;
   }
   const double emax = g.emax > 0 ? g.emax : 1.0;
@@ -908,7 +908,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     const int ncls = 1 << dim;
     for (int pass = 0; pass < 2; ++pass) {
       const uint32_t *h = hc + 256 * pass;
-      const int chunk = pass ? tchunk : CT_TGT;
+      const int chunk = tchunk;
       int off = 0;
       for (int d = 2; d <= D; ++d) {
         (pass ? m2l_b0 : lvl_b0)[d] = (int)hb.size();
@@ -925,8 +925,8 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   std::vector<int> m2m_b0(D + 1, 0), m2m_b1(D + 1, 0);
   for (int d = D - 1; d >= 2; --d) {
     m2m_b0[d] = (int)hb.size();
-    for (int s = 0; s < t.level_count[d]; s += CT_TGT)
-      hb.push_back(make_int4(t.level_off[d] + s, std::min(CT_TGT, t.level_count[d] - s), d, -1));
+    for (int s = 0; s < t.level_count[d]; s += tchunk)
+      hb.push_back(make_int4(t.level_off[d] + s, std::min(tchunk, t.level_count[d] - s), d, -1));
     m2m_b1[d] = (int)hb.size();
   }
   if (!eb.batches.reserve(hb.size() + 1)) return FMM_ERR_OUT_OF_MEMORY;
@@ -953,7 +953,17 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   ca.dim = dim;
   ca.level_stride = dim == 2 ? 49 : 0;
   ca.pair_count = ws.counters;
-  CUDA_TRY(cudaMemsetAsync(ws.counters, 0, 2 * sizeof(unsigned long long), st));
+  CUDA_TRY(cudaMemsetAsync(ws.counters, 0, 3 * sizeof(unsigned long long), st));
+  TcArgs ta{};
+  ta.cchild = ws.cell_child;
+  ta.cparent = ws.cell_parent;
+  ta.nchild = 1 << dim;
+  ta.bimg = eb.tc_img.ptr;
+  ta.cell0 = cell0;
+  ta.K = ops.K;
+  ta.KS = KS;
+  ta.P16 = P16;
+  ta.err = ws.dev_err;
 
   if (ev) cudaEventRecord(ev[1], st);
   // P2M
@@ -961,7 +971,17 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   else k_p2m2d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.M.ptr);
   ws.launches += 1;
   // M2M, bottom-up
-  for (int d = D - 1; d >= 2; --d) {
+  for (int d = D - 1; d >= 2 && tc; --d) {
+    TcArgs t2 = ta;
+    t2.mode = TC_M2M;
+    t2.batches = eb.batches.ptr + m2m_b0[d];
+    t2.op_base = ops.off_m2m;
+    t2.X = eb.M.ptr;
+    t2.Y = eb.M.ptr;
+    int rc = tc_launch(t2, m2m_b1[d] - m2m_b0[d], st, ws.launches);
+    if (rc) return rc;
+  }
+  for (int d = D - 1; d >= 2 && !tc; --d) {
     ca.mode = MODE_M2M;
     ca.slot_base = ops.off_m2m;
     ca.tlist = nullptr;
@@ -993,22 +1013,18 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     }
     int rc;
     if (tc) {
-      TcArgs ta;
-      ta.batches = c2.batches;
-      ta.tlist = tl_m2l;
-      ta.src_tab = eb.m2l_src.ptr;
-      ta.slot_list = eb.m2l_list.ptr;
-      ta.tslot_list = eb.m2l_tslot.ptr;
-      ta.nslots = eb.m2l_nslots.ptr;
-      ta.X = eb.M.ptr;
-      ta.Y = eb.L.ptr;
-      ta.bimg = eb.tc_img.ptr;
-      ta.cell0 = cell0;
-      ta.K = ops.K;
-      ta.KS = KS;
-      ta.P16 = P16;
-      ta.err = ws.dev_err;
-      rc = tc_launch_m2l(ta, nbm, st, ws.launches);
+      TcArgs t2 = ta;
+      t2.mode = TC_M2L;
+      t2.batches = c2.batches;
+      t2.tlist = tl_m2l;
+      t2.src_tab = eb.m2l_src.ptr;
+      t2.slot_list = eb.m2l_list.ptr;
+      t2.tslot_list = eb.m2l_tslot.ptr;
+      t2.nslots = eb.m2l_nslots.ptr;
+      t2.X = eb.M.ptr;
+      t2.Y = eb.L.ptr;
+      t2.tiles = ws.counters + 2;
+      rc = tc_launch(t2, nbm, st, ws.launches);
     } else {
       c2.src_tab = eb.m2l_src.ptr;
       c2.slot_list = eb.m2l_list.ptr;
@@ -1019,7 +1035,18 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   }
   if (ev) cudaEventRecord(ev[3], st);
   // L2L, top-down
-  for (int d = 3; d <= D; ++d) {
+  for (int d = 3; d <= D && tc; ++d) {
+    TcArgs t2 = ta;
+    t2.mode = TC_L2L;
+    t2.batches = eb.batches.ptr + lvl_b0[d];
+    t2.tlist = tl;
+    t2.op_base = ops.off_l2l;
+    t2.X = eb.L.ptr;
+    t2.Y = eb.L.ptr;
+    int rc = tc_launch(t2, lvl_b1[d] - lvl_b0[d], st, ws.launches);
+    if (rc) return rc;
+  }
+  for (int d = 3; d <= D && !tc; ++d) {
     ContractArgs c2 = ca;
     c2.mode = MODE_L2L;
     c2.slot_base = ops.off_l2l;
