@@ -26,7 +26,8 @@ struct ExpBuffers {
   DevBuf<uint32_t> cls_count;
   DevBuf<float4> lvl_off;
   DevBuf<int> m2l_src, m2l_list, m2l_nslots, m2l_tslot;  // per M2L batch: resolved sources and present slots
-  DevBuf<uint16_t> tc_img;  // BF16 split operator images for the tensor-core M2L  // particle offsets from their level-d ancestor (direct far field)
+  DevBuf<uint16_t> tc_img;
+  DevBuf<unsigned int> tc_work;  // zeroed work counters of the tensor-core launches  // BF16 split operator images for the tensor-core M2L  // particle offsets from their level-d ancestor (direct far field)
 };
 
 // Per-pass parameters.

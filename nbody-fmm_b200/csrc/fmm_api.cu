@@ -136,6 +136,7 @@ int fmm_destroy(fmm_ctx *c) {
   c->eb.m2l_nslots.release();
   c->eb.m2l_tslot.release();
   c->eb.tc_img.release();
+  c->eb.tc_work.release();
   for (auto *b : {&c->d_pos, &c->d_mass, &c->d_acc, &c->d_pot, &c->d_vel, &c->d_x0, &c->d_v0, &c->d_xs, &c->d_vs,
                   &c->d_asum, &c->d_vsum})
     b->release();

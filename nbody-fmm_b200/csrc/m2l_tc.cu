@@ -4,7 +4,8 @@
 // A CTA takes up to 128 target cells that share their translation slots:
 //   M2L  cells of one level and one child class (same interaction offsets),
 //        one slot per offset present in the batch;
-//   M2M  parent cells of one level, one slot per child class;
+//   M2M  cells of one level and one child class, one slot: the rows are the
+//        children and the results are added into their parents;
 //   L2L  cells of one level and one child class, one slot (the parent).
 // For each slot it computes D[128 x N] = A_slot[128 x K] * B_slot[K x N],
 // where row r of A_slot is the source expansion of target r at that slot
@@ -160,8 +161,12 @@ __device__ inline void tc_fence_before() { asm volatile("tcgen05.fence::before_t
 __device__ inline void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 // ------------------------------------------------------------------ kernel
+// Persistent: each CTA takes batches from the launch's work counter and runs
+// their slots as one stream, so the operator copies and the source-row
+// prefetch of the next batch overlap the MMAs of the current one.  Batch
+// metadata is double-buffered in shared memory (current, next).
 template <int P16>
-__global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a) {
+__global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsigned int *work) {
   constexpr int NT = P16 > 128 ? 2 : 1;  // output tiles
   constexpr int N0 = tc_n0(P16);
   constexpr int N1 = P16 - N0;
@@ -179,46 +184,57 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a) {
   uint16_t *Bs = As + 3 * ASPLIT;   // 2 buffers
   __shared__ __align__(8) uint64_t s_full[2], s_mma[2], s_done;
   __shared__ uint32_t s_tmem;
-  __shared__ int s_slot[TC_MAX_SLOTS], s_op[TC_MAX_SLOTS];
-  __shared__ int s_n;
+  __shared__ int s_slot[2][TC_MAX_SLOTS], s_op[2][TC_MAX_SLOTS];
+  __shared__ int s_n[2], s_b[2];
+  __shared__ int s_grab;
 
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int4 bt = a.batches[blockIdx.x];
-  const size_t tbase = (size_t)blockIdx.x * TC_MAX_SLOTS;
-  const int tg = tid < bt.y ? (a.tlist ? a.tlist[bt.x + tid] : bt.x + tid) : -1;
 
-  // present slots and their operators
-  if (a.mode == TC_M2L) {
-    const int n = a.nslots[blockIdx.x];
-    for (int i = tid; i < n; i += TC_M) {
-      s_slot[i] = a.slot_list[tbase + i];
-      s_op[i] = a.tslot_list[tbase + i];
-    }
-    if (tid == 0) s_n = n;
-  } else if (a.mode == TC_M2M) {
-    int n = 0;
-    for (int s = 0; s < a.nchild; ++s) {
-      const int any = __syncthreads_or(tg >= 0 && a.cchild[(int64_t)tg * a.nchild + s] >= 0);
-      if (any) {
+  // Takes the next batch with at least one slot into metadata buffer `buf`
+  // (s_n[buf] = 0 when the work is exhausted); returns this thread's target.
+  auto load_meta = [&](int buf) -> int {
+    while (true) {
+      if (tid == 0) s_grab = (int)atomicAdd(work, 1u);
+      __syncthreads();
+      const int b = s_grab;
+      if (b >= nb) {
         if (tid == 0) {
-          s_slot[n] = s;
-          s_op[n] = a.op_base + s;
+          s_n[buf] = 0;
+          s_b[buf] = -1;
         }
-        ++n;
+        __syncthreads();
+        return -1;
       }
+      const int4 bt = a.batches[b];
+      const int tg = tid < bt.y ? (a.tlist ? a.tlist[bt.x + tid] : bt.x + tid) : -1;
+      int n = 0;
+      if (a.mode == TC_M2L) {
+        n = a.nslots[b];
+        const size_t tb = (size_t)b * TC_MAX_SLOTS;
+        for (int i = tid; i < n; i += TC_M) {
+          s_slot[buf][i] = a.slot_list[tb + i];
+          s_op[buf][i] = a.tslot_list[tb + i];
+        }
+      } else {
+        if (tid == 0) {
+          s_slot[buf][0] = 0;
+          s_op[buf][0] = a.op_base + bt.w;
+        }
+        n = bt.y > 0 ? 1 : 0;
+      }
+      if (tid == 0) {
+        s_n[buf] = n;
+        s_b[buf] = b;
+        if (n && a.mode == TC_M2L && a.tiles) atomicAdd(a.tiles, (unsigned long long)n);
+      }
+      __syncthreads();  // also keeps s_grab until everyone has read it
+      if (n) return tg;
     }
-    if (tid == 0) s_n = n;
-  } else {
-    if (tid == 0) {
-      s_slot[0] = 0;
-      s_op[0] = a.op_base + bt.w;
-      s_n = bt.y > 0 ? 1 : 0;
-    }
-  }
-  __syncthreads();
-  const int nslots = s_n;
-  if (nslots == 0) return;
-  if (tid == 0 && a.mode == TC_M2L && a.tiles) atomicAdd(a.tiles, (unsigned long long)nslots);
+  };
+
+  int tg_cur = load_meta(0);
+  if (s_n[0] == 0) return;
+  int tg_nxt = load_meta(1);
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
@@ -238,20 +254,25 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a) {
   tc_fence_after();
   const uint32_t tmem = s_tmem;
   const uint32_t lane_off = (uint32_t)(warp * 32) << 16;
-  const int total = nslots * TILES;
 
-  // operator copy g (slot g / TILES; splits in the order 2, 1, 0; tiles 0, 1)
-  auto load_tile = [&](int g) {
-    const int i = g / TILES, t = g % TILES;
+  // Stream bookkeeping: the current batch (buffer c) starts at tile t_cur,
+  // the next (buffer c ^ 1) at t_nxt; tiles end at t_end.
+  int c = 0;
+  long long t_cur = 0, t_nxt = (long long)s_n[0] * TILES, t_end = t_nxt + (long long)s_n[1] * TILES;
+
+  // operator copy g (splits in the order 2, 1, 0; output tiles 0, 1)
+  auto load_tile = [&](long long g) {
+    const int buf = g < t_nxt ? c : c ^ 1;
+    const int i = (int)((g - (g < t_nxt ? t_cur : t_nxt)) / TILES), t = (int)(g % TILES);
     const int s = 2 - t / NT, j = t % NT;
     const uint32_t bytes = (uint32_t)(P16 * (j ? N1 : N0) * 2);
     const uint16_t *src =
-        a.bimg + (size_t)s_op[i] * 3 * P16 * P16 + (size_t)s * P16 * P16 + (j ? (size_t)P16 * N0 : 0);
+        a.bimg + (size_t)s_op[buf][i] * 3 * P16 * P16 + (size_t)s * P16 * P16 + (j ? (size_t)P16 * N0 : 0);
     bulk_load(Bs + (g & 1) * BTILE, src, bytes, &s_full[g & 1]);
   };
   // the MMAs of operator copy g: B split s against A splits 2 - s .. 0
-  auto mma_tile = [&](int g) {
-    const int t = g % TILES;
+  auto mma_tile = [&](long long g) {
+    const int t = (int)(g % TILES);
     const int s = 2 - t / NT, j = t % NT;
     const int nw = j ? N1 : N0;
     const uint32_t idesc =
@@ -268,14 +289,14 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a) {
     mma_commit(&s_mma[g & 1]);
   };
 
-  // source row of this thread's target for slot i
+  // source row of target `tg` for slot i of metadata buffer `buf`
   float4 rv[P16 / 4];
-  auto fetch = [&](int i) {
+  auto fetch = [&](int buf, int i, int tg) {
     int src = -1;
     if (tg >= 0) {
-      const int sl = s_slot[i];
-      if (a.mode == TC_M2L) src = a.src_tab[(tbase + sl) * TC_M + tid];
-      else if (a.mode == TC_M2M) src = a.cchild[(int64_t)tg * a.nchild + sl];
+      const int sl = s_slot[buf][i];
+      if (a.mode == TC_M2L) src = a.src_tab[((size_t)s_b[buf] * TC_MAX_SLOTS + sl) * TC_M + tid];
+      else if (a.mode == TC_M2M) src = tg;
       else src = a.cparent[tg];
     }
     const float4 *xr = (const float4 *)(a.X + (size_t)(src >= 0 ? src - a.cell0 : 0) * a.KS);
@@ -305,87 +326,111 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   };
 
-  int nl = 0, nwait = 0;  // thread 0: copies issued, copies waited for
+  long long nl = 0, nwait = 0;  // thread 0: copies issued, copies waited for
+  long long sidx = 0;           // slots done by this CTA (parity of s_done)
   if (tid == 0) {
     load_tile(0);
-    if (total > 1) load_tile(1);
-    nl = total > 1 ? 2 : 1;
+    load_tile(1);  // every slot has three or more copies
+    nl = 2;
   }
-  fetch(0);
+  fetch(0, 0, tg_cur);
   bool ok = true;
-  for (int i = 0; i < nslots; ++i) {
-    write_a();
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    if (i + 1 < nslots) fetch(i + 1);  // in flight during the MMAs
-    if (tid == 0) {
-      for (int t = 0; t < TILES && ok; ++t) {
-        const int g = i * TILES + t;
-        if (!mbar_wait(&s_full[g & 1], (g >> 1) & 1)) {
-          ok = false;
-          break;
-        }
-        nwait = g + 1;
-        mma_tile(g);
-        if (nl == g + 1 && nl < total && g >= 1) {  // the buffer of copy g - 1 takes copy g + 1
-          if (!mbar_wait(&s_mma[(g - 1) & 1], ((g - 1) >> 1) & 1)) {
+  while (ok) {
+    const int n = s_n[c];
+    for (int j = 0; j < n; ++j, ++sidx) {
+      write_a();
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
+      // rows of the next slot, in flight during the MMAs
+      if (j + 1 < n) fetch(c, j + 1, tg_cur);
+      else if (s_n[c ^ 1]) fetch(c ^ 1, 0, tg_nxt);
+      if (tid == 0) {
+        for (int t = 0; t < TILES && ok; ++t) {
+          const long long g = t_cur + (long long)j * TILES + t;
+          if (!mbar_wait(&s_full[g & 1], (uint32_t)((g >> 1) & 1))) {
             ok = false;
             break;
           }
-          load_tile(nl++);
+          nwait = g + 1;
+          mma_tile(g);
+          if (nl == g + 1 && nl < t_end && g >= 1) {  // the buffer of copy g - 1 takes copy g + 1
+            if (!mbar_wait(&s_mma[(g - 1) & 1], (uint32_t)(((g - 1) >> 1) & 1))) {
+              ok = false;
+              break;
+            }
+            load_tile(nl++);
+          }
         }
+        mma_commit(&s_done);  // also when stopping early, so that nobody waits in vain
       }
-      mma_commit(&s_done);  // also when stopping early, so that nobody waits in vain
+      const bool dn = mbar_wait(&s_done, (uint32_t)(sidx & 1));
+      // tcgen05.ld/st are warp-collective: the whole warp goes on only if it saw the commit
+      const bool wd = __all_sync(0xffffffffu, dn);
+      if (!wd) ok = false;
+      tc_fence_after();
+      if (wd) {
+#pragma unroll
+        for (int c0 = 0; c0 < P16; c0 += 16) {
+          uint32_t d[16];
+          tmem_ld16(tmem + lane_off + (uint32_t)c0, d);
+          if (j > 0) {
+            uint32_t r[16];
+            tmem_ld16(tmem + lane_off + RCOL + (uint32_t)c0, r);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int e = 0; e < 16; ++e) d[e] = __float_as_uint(__uint_as_float(d[e]) + __uint_as_float(r[e]));
+          } else {
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          }
+          tmem_st16(tmem + lane_off + RCOL + (uint32_t)c0, d);
+        }
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      }
+      // all MMAs of this slot are done: the buffer of its last copy takes the next one
+      const long long g_end = t_cur + (long long)(j + 1) * TILES;
+      if (tid == 0 && ok && nl < t_end && nl == g_end + 1) load_tile(nl++);
+      tc_fence_before();
+      ok = __syncthreads_and(ok);
+      if (!ok) break;
     }
-    const bool dn = mbar_wait(&s_done, (uint32_t)(i & 1));
-    // tcgen05.ld/st are warp-collective: the whole warp goes on only if it saw the commit
-    const bool wd = __all_sync(0xffffffffu, dn);
-    if (!wd) ok = false;
+    if (!ok) break;
+    // epilogue: R into the targets' expansions (fire-and-forget vector
+    // reductions; M2M rows of several batches meet in one parent)
     tc_fence_after();
-    if (wd) {
+    {
+      const int dst = a.mode == TC_M2M ? (tg_cur >= 0 ? a.cparent[tg_cur] : -1) : tg_cur;
+      float *y = a.Y + (size_t)(dst >= 0 ? dst - a.cell0 : 0) * a.KS;
 #pragma unroll
       for (int c0 = 0; c0 < P16; c0 += 16) {
-        uint32_t d[16];
-        tmem_ld16(tmem + lane_off + (uint32_t)c0, d);
-        if (i > 0) {
-          uint32_t r[16];
-          tmem_ld16(tmem + lane_off + RCOL + (uint32_t)c0, r);
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        uint32_t r[16];
+        tmem_ld16(tmem + lane_off + RCOL + (uint32_t)c0, r);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (dst >= 0) {
 #pragma unroll
-          for (int e = 0; e < 16; ++e) d[e] = __float_as_uint(__uint_as_float(d[e]) + __uint_as_float(r[e]));
-        } else {
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          for (int q = 0; q < 4; ++q)
+            if (c0 + 4 * q < a.KS)
+              asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(y + c0 + 4 * q), "r"(r[4 * q]),
+                           "r"(r[4 * q + 1]), "r"(r[4 * q + 2]), "r"(r[4 * q + 3])
+                           : "memory");
         }
-        tmem_st16(tmem + lane_off + RCOL + (uint32_t)c0, d);
       }
-      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
     }
-    // all MMAs of slot i are done: the buffer of its last copy takes the next one
-    if (tid == 0 && ok && nl < total && nl == (i + 1) * TILES + 1) load_tile(nl++);
     tc_fence_before();
-    ok = __syncthreads_and(ok);
-    if (!ok) break;
+    // advance: the next batch becomes current; take the one after it
+    if (s_n[c ^ 1] == 0) break;
+    c ^= 1;
+    tg_cur = tg_nxt;
+    t_cur = t_nxt;
+    t_nxt = t_end;
+    tg_nxt = load_meta(c ^ 1);  // syncs: everyone has finished the epilogue's TMEM reads
+    t_end = t_nxt + (long long)s_n[c ^ 1] * TILES;
   }
 
-  if (ok) {
-    tc_fence_after();
-    float *y = a.Y + (size_t)(tg >= 0 ? tg - a.cell0 : 0) * a.KS;
-#pragma unroll
-    for (int c0 = 0; c0 < P16; c0 += 16) {
-      uint32_t r[16];
-      tmem_ld16(tmem + lane_off + RCOL + (uint32_t)c0, r);
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (tg >= 0) {
-#pragma unroll
-        for (int e = 0; e < 16; ++e)
-          if (c0 + e < a.K) y[c0 + e] += __uint_as_float(r[e]);
-      }
-    }
-  } else if (tid == 0) {
+  if (!ok && tid == 0) {
     atomicOr(a.err, FMM_DEV_ERR_TIMEOUT);
-    for (int g = nwait; g < nl; ++g)  // copies still in flight
-      if (!mbar_wait(&s_full[g & 1], (g >> 1) & 1)) break;
+    for (long long g = nwait; g < nl; ++g)  // copies still in flight
+      if (!mbar_wait(&s_full[g & 1], (uint32_t)((g >> 1) & 1))) break;
   }
   tc_fence_before();
   __syncthreads();
@@ -407,36 +452,45 @@ int tc_build_images(const float *tab, int n_slots, int K, int KP, int P16, uint1
 }
 
 template <int P16>
-static int tc_launch_p(const TcArgs &a, int nb, cudaStream_t st) {
+static int tc_launch_p(const TcArgs &a, int nb, unsigned int *work, cudaStream_t st) {
   // at most two CTAs per SM (each holds 256 TMEM columns), one when a CTA
   // holds 512
   size_t sh = tc_dyn_smem(P16);
   sh = std::max(sh, P16 <= 128 ? (size_t)80 * 1024 : (size_t)120 * 1024);
   static size_t attr = 0;
+  static int per_sm = 0;
   if (attr < sh) {
     if (cudaFuncSetAttribute(k_tc_translate<P16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess)
       return FMM_ERR_CUDA;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_translate<P16>, TC_M, sh) != cudaSuccess ||
+        per_sm < 1)
+      return FMM_ERR_CUDA;
     attr = sh;
   }
-  k_tc_translate<P16><<<nb, TC_M, sh, st>>>(a);
+  int dev = 0, nsm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return FMM_ERR_CUDA;
+  const int grid = std::min(nb, per_sm * nsm);
+  k_tc_translate<P16><<<grid, TC_M, sh, st>>>(a, nb, work);
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
 }
 
-int tc_launch(const TcArgs &a, int nb, cudaStream_t st, int64_t &launches) {
+int tc_launch(const TcArgs &a, int nb, unsigned int *work, cudaStream_t st, int64_t &launches) {
   if (nb <= 0) return FMM_OK;
   launches += 1;
   switch (a.P16) {
-    case 16: return tc_launch_p<16>(a, nb, st);
-    case 32: return tc_launch_p<32>(a, nb, st);
-    case 48: return tc_launch_p<48>(a, nb, st);
-    case 64: return tc_launch_p<64>(a, nb, st);
-    case 80: return tc_launch_p<80>(a, nb, st);
-    case 96: return tc_launch_p<96>(a, nb, st);
-    case 112: return tc_launch_p<112>(a, nb, st);
-    case 128: return tc_launch_p<128>(a, nb, st);
-    case 144: return tc_launch_p<144>(a, nb, st);
-    case 160: return tc_launch_p<160>(a, nb, st);
-    case 176: return tc_launch_p<176>(a, nb, st);
+    case 16: return tc_launch_p<16>(a, nb, work, st);
+    case 32: return tc_launch_p<32>(a, nb, work, st);
+    case 48: return tc_launch_p<48>(a, nb, work, st);
+    case 64: return tc_launch_p<64>(a, nb, work, st);
+    case 80: return tc_launch_p<80>(a, nb, work, st);
+    case 96: return tc_launch_p<96>(a, nb, work, st);
+    case 112: return tc_launch_p<112>(a, nb, work, st);
+    case 128: return tc_launch_p<128>(a, nb, work, st);
+    case 144: return tc_launch_p<144>(a, nb, work, st);
+    case 160: return tc_launch_p<160>(a, nb, work, st);
+    case 176: return tc_launch_p<176>(a, nb, work, st);
     default: return FMM_ERR_UNSUPPORTED;
   }
 }

@@ -12,14 +12,14 @@ static constexpr int TC_MAX_P16 = 176;
 
 struct TcArgs {
   int mode;                 // TC_M2L, TC_M2M or TC_L2L
-  const int4 *batches;      // {first, count, level, class}, up to 128 targets each
-  const int *tlist;         // target cells (M2L, L2L); null for M2M (cells first + row)
+  const int4 *batches;      // {tlist offset, count, level, class}, up to 128 cells each
+  const int *tlist;         // class-grouped cells: targets (M2L, L2L) or children (M2M)
   const int *src_tab;       // M2L: [batch][slot][128] source cell per target, -1 if none
   const int *slot_list;     // M2L: [batch][i] present slots
   const int *tslot_list;    // M2L: [batch][i] operator-table slot of each present slot
   const int *nslots;        // M2L: [batch]
-  const int *cchild;        // M2M: children of each cell (nchild per cell, -1 if absent)
-  const int *cparent;       // L2L: parent of each cell
+  const int *cchild;        // children of each cell (nchild per cell, -1 if absent)
+  const int *cparent;       // parent of each cell (M2M destination, L2L source)
   int nchild;               // 8 in 3D, 4 in 2D
   int op_base;              // M2M / L2L: operator-table slot of child class 0
   const float *X;           // source expansions, KS floats per cell
@@ -36,6 +36,11 @@ __host__ __device__ constexpr int tc_n0(int P16) { return P16 <= 128 ? P16 : ((P
 size_t tc_smem_bytes(int P16);
 int tc_build_images(const float *tab, int n_slots, int K, int KP, int P16, uint16_t *img, cudaStream_t st,
                     int64_t &launches);
-int tc_launch(const TcArgs &a, int nb, cudaStream_t st, int64_t &launches);
+// Launches one translation pass over nb batches; `work` is a zeroed device
+// counter the persistent CTAs take batches from.
+int tc_launch(const TcArgs &a, int nb, unsigned int *work, cudaStream_t st, int64_t &launches);
+
+// Work counters per pass (one per launch).
+static constexpr int TC_MAX_LAUNCHES = 80;
 
 }  // namespace fmm

@@ -671,7 +671,8 @@ struct DirectArgs {
 // the cells S of T's interaction list (node_i.cpp:39-43) with
 // n_T * n_S <= direct_max, exactly the pairs the M2L contraction skips.
 // Small T (NT <= 8 targets): every lane holds all targets and takes every
-// 32nd particle of the concatenated sources; larger T: lanes over targets.
+// 32nd particle of the concatenated sources; larger T: one or more lanes per
+// target over sources staged through shared memory.
 template <int NT, int DIM>
 __device__ void direct_small(const DirectArgs &a, int tb, int nt, const int *s_src, const float *s_shift,
                              const int *s_pref, int nsrc, int lane) {
@@ -717,6 +718,7 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   __shared__ int s_src_all[8][189];
   __shared__ float s_shift_all[8][3 * 189];
   __shared__ int s_pref_all[8][190];
+  __shared__ float4 s_stage_all[8][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int wl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (wl >= a.count) return;
@@ -780,20 +782,43 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   else if (nt <= 4) direct_small<4, DIM>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
   else if (nt <= 8) direct_small<8, DIM>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
   else {
-    // lanes over targets; every lane walks all sources (warp-uniform loads)
-    for (int t0 = 0; t0 < nt; t0 += 32) {
-      const int ti = t0 + lane;
+    // Gl lanes per target (Gl * min(nt, 32) <= 32); the sources pass through
+    // shared memory 32 at a time, each lane taking every Gl-th of them
+    const int tp = nt < 32 ? nt : 32;
+    int Gl = 1;
+    while (Gl * 2 * tp <= 32) Gl *= 2;
+    const int tpp = 32 / Gl;
+    const int total = s_pref[nsrc];
+    float4 *stage = s_stage_all[wib];
+    for (int t0 = 0; t0 < nt; t0 += tpp) {
+      const int ti = t0 + lane / Gl, sub = lane % Gl;
       const float4 t = a.off[tb + (ti < nt ? ti : 0)];
       float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
-      for (int si = 0; si < nsrc; ++si) {
-        const float tx = t.x - s_shift[3 * si], ty = t.y - s_shift[3 * si + 1], tz = t.z - s_shift[3 * si + 2];
-        const int jb = a.pbeg[s_src[si]], je = a.pend[s_src[si]];
-        for (int j = jb; j < je; ++j) {
-          const float4 q = a.off[j];
-          pair_acc<DIM>(tx - q.x, ty - q.y, tz - q.z, q.w, a.eps2, ax, ay, az, ph);
+      int si = 0;
+      for (int f0 = 0; f0 < total; f0 += 32) {
+        const int f = f0 + lane;
+        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (f < total) {
+          while (f >= s_pref[si + 1]) ++si;
+          const float4 qq = a.off[a.pbeg[s_src[si]] + (f - s_pref[si])];
+          q = make_float4(qq.x + s_shift[3 * si], qq.y + s_shift[3 * si + 1], qq.z + s_shift[3 * si + 2], qq.w);
         }
+        stage[lane] = q;
+        __syncwarp();
+        const int cnt = min(32, total - f0);
+        for (int k = sub; k < cnt; k += Gl) {
+          const float4 sq = stage[k];
+          pair_acc<DIM>(t.x - sq.x, t.y - sq.y, t.z - sq.z, sq.w, a.eps2, ax, ay, az, ph);
+        }
+        __syncwarp();
       }
-      if (ti < nt) {
+      for (int o = 1; o < Gl; o <<= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+        ph += __shfl_xor_sync(0xffffffffu, ph, o);
+      }
+      if (ti < nt && sub == 0) {
         float4 f0 = a.far[tb + ti];
         a.far[tb + ti] = make_float4(f0.x + ax, f0.y + ay, f0.z + az, f0.w + ph);
       }
@@ -862,8 +887,12 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   const int P16 = (ops.K + 15) & ~15;
   const bool tc = m2l_mode == FMM_M2L_TC && P16 <= TC_MAX_P16;
   const int tchunk = tc ? 128 : CT_TGT;
+  int tc_k = 0;  // tensor-core launches so far (work counter index)
   if (tc && D >= 2) {
-    if (!eb.tc_img.reserve((size_t)ops.n_slots * 3 * P16 * P16)) return FMM_ERR_OUT_OF_MEMORY;
+    if (!eb.tc_img.reserve((size_t)ops.n_slots * 3 * P16 * P16) || !eb.tc_work.reserve(TC_MAX_LAUNCHES))
+      return FMM_ERR_OUT_OF_MEMORY;
+    if (2 * D + 1 > TC_MAX_LAUNCHES) return FMM_ERR_UNSUPPORTED;
+    CUDA_TRY(cudaMemsetAsync(eb.tc_work.ptr, 0, TC_MAX_LAUNCHES * sizeof(unsigned int), st));
     int rc = tc_build_images(ops.tab.ptr, ops.n_slots, ops.K, ops.KP, P16, eb.tc_img.ptr, st, ws.launches);
     if (rc) return rc;
   }
@@ -971,14 +1000,15 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   else k_p2m2d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.M.ptr);
   ws.launches += 1;
   // M2M, bottom-up
-  for (int d = D - 1; d >= 2 && tc; --d) {
+  for (int d = D - 1; d >= 2 && tc; --d) {  // children of level d + 1 by class
     TcArgs t2 = ta;
     t2.mode = TC_M2M;
-    t2.batches = eb.batches.ptr + m2m_b0[d];
+    t2.batches = eb.batches.ptr + lvl_b0[d + 1];
+    t2.tlist = tl;
     t2.op_base = ops.off_m2m;
     t2.X = eb.M.ptr;
     t2.Y = eb.M.ptr;
-    int rc = tc_launch(t2, m2m_b1[d] - m2m_b0[d], st, ws.launches);
+    int rc = tc_launch(t2, lvl_b1[d + 1] - lvl_b0[d + 1], eb.tc_work.ptr + tc_k++, st, ws.launches);
     if (rc) return rc;
   }
   for (int d = D - 1; d >= 2 && !tc; --d) {
@@ -1024,7 +1054,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
       t2.X = eb.M.ptr;
       t2.Y = eb.L.ptr;
       t2.tiles = ws.counters + 2;
-      rc = tc_launch(t2, nbm, st, ws.launches);
+      rc = tc_launch(t2, nbm, eb.tc_work.ptr + tc_k++, st, ws.launches);
     } else {
       c2.src_tab = eb.m2l_src.ptr;
       c2.slot_list = eb.m2l_list.ptr;
@@ -1043,7 +1073,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     t2.op_base = ops.off_l2l;
     t2.X = eb.L.ptr;
     t2.Y = eb.L.ptr;
-    int rc = tc_launch(t2, lvl_b1[d] - lvl_b0[d], st, ws.launches);
+    int rc = tc_launch(t2, lvl_b1[d] - lvl_b0[d], eb.tc_work.ptr + tc_k++, st, ws.launches);
     if (rc) return rc;
   }
   for (int d = 3; d <= D && !tc; ++d) {
