@@ -635,32 +635,45 @@ __global__ void k_p2p(P2PArgs a) {
 
 // --------------------------------------------------------- direct far field
 // Offsets of every particle (leaf order) from the centre of its ancestor at
-// level d, FP32, with the mass: the frame in which pairs of level-d cells
-// are summed directly.
+// each level d in [d0, d1], FP32, with the mass: the frames in which pairs of
+// level-d cells are summed directly.  out[(d - d0) * n + i].
 template <int DIM>
 __global__ void k_level_offsets(const double *pos, const double *mass, const uint32_t *perm, const int *leaf_of,
-                                const uint64_t *ckey, int64_t n, int depth, int d, double lox, double loy, double loz,
-                                double ex, double ey, double ez, float4 *out) {
+                                const uint64_t *ckey, int64_t n, int depth, int d0, int d1, double lox, double loy,
+                                double loz, double ex, double ey, double ez, float4 *out) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint32_t qx, qy, qz;
   morton_decode(DIM, ckey[leaf_of[i]], qx, qy, qz);
-  const int sh = depth - d;
-  const double inv = ldexp(1.0, -d);
   const uint32_t j = perm[i];
-  double cx = lox + ((double)(qx >> sh) + 0.5) * (ex * inv);
-  double cy = loy + ((double)(qy >> sh) + 0.5) * (ey * inv);
-  double cz = DIM == 3 ? loz + ((double)(qz >> sh) + 0.5) * (ez * inv) : 0.0;
-  out[i] = make_float4((float)(pos[DIM * (size_t)j] - cx), (float)(pos[DIM * (size_t)j + 1] - cy),
-                       DIM == 3 ? (float)(pos[3 * (size_t)j + 2] - cz) : 0.f, (float)mass[j]);
+  const double px = pos[DIM * (size_t)j], py = pos[DIM * (size_t)j + 1], pz = DIM == 3 ? pos[3 * (size_t)j + 2] : 0.0;
+  const float w = (float)mass[j];
+  for (int d = d0; d <= d1; ++d) {
+    const int sh = depth - d;
+    const double inv = ldexp(1.0, -d);
+    const double cx = lox + ((double)(qx >> sh) + 0.5) * (ex * inv);
+    const double cy = loy + ((double)(qy >> sh) + 0.5) * (ey * inv);
+    const double cz = DIM == 3 ? loz + ((double)(qz >> sh) + 0.5) * (ez * inv) : 0.0;
+    out[(size_t)(d - d0) * n + i] =
+        make_float4((float)(px - cx), (float)(py - cy), DIM == 3 ? (float)(pz - cz) : 0.f, w);
+  }
 }
 
+__device__ inline void red_add4(float4 *p, float x, float y, float z, float w) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(x), "f"(y), "f"(z), "f"(w) : "memory");
+}
+
+static constexpr int DF_MAX_LEVELS = 33;
+
 struct DirectArgs {
-  int first, count, depth_d;  // cells of level d: [first, first + count)
+  // levels of the launch, coarse first: warps [w0[k], w0[k+1]) take the
+  // cells first[k] + (warp - w0[k])
+  int nlev;
+  int first[DF_MAX_LEVELS], w0[DF_MAX_LEVELS + 1];
+  const float4 *off[DF_MAX_LEVELS];  // particle offsets from their level-d ancestor's centre
+  float h[DF_MAX_LEVELS][3];         // level-d cell size
   const int *pbeg, *pend, *coll, *parent, *child;
   const uint64_t *ckey;
-  const float4 *off;  // particle offsets from their level-d ancestor's centre
-  float hx, hy, hz;   // level-d cell size
   float eps2;
   long long direct_max;
   float4 *far;
@@ -674,12 +687,12 @@ struct DirectArgs {
 // 32nd particle of the concatenated sources; larger T: one or more lanes per
 // target over sources staged through shared memory.
 template <int NT, int DIM>
-__device__ void direct_small(const DirectArgs &a, int tb, int nt, const int *s_src, const float *s_shift,
-                             const int *s_pref, int nsrc, int lane) {
+__device__ void direct_small(const DirectArgs &a, const float4 *off, int tb, int nt, const int *s_src,
+                             const float *s_shift, const int *s_pref, int nsrc, int lane) {
   float tx[NT], ty[NT], tz[NT], ax[NT], ay[NT], az[NT], ph[NT];
 #pragma unroll
   for (int k = 0; k < NT; ++k) {
-    float4 t = a.off[tb + (k < nt ? k : 0)];
+    float4 t = off[tb + (k < nt ? k : 0)];
     tx[k] = t.x;
     ty[k] = t.y;
     tz[k] = t.z;
@@ -690,7 +703,7 @@ __device__ void direct_small(const DirectArgs &a, int tb, int nt, const int *s_s
   for (int f = lane; f < total; f += 32) {
     while (f >= s_pref[si + 1]) ++si;
     const int j = a.pbeg[s_src[si]] + (f - s_pref[si]);
-    const float4 q = a.off[j];
+    const float4 q = off[j];
     const float qx = q.x + s_shift[3 * si], qy = q.y + s_shift[3 * si + 1], qz = q.z + s_shift[3 * si + 2];
 #pragma unroll
     for (int k = 0; k < NT; ++k)
@@ -705,10 +718,7 @@ __device__ void direct_small(const DirectArgs &a, int tb, int nt, const int *s_s
       az[k] += __shfl_xor_sync(0xffffffffu, az[k], o);
       ph[k] += __shfl_xor_sync(0xffffffffu, ph[k], o);
     }
-    if (lane == k && k < nt) {
-      float4 f0 = a.far[tb + k];
-      a.far[tb + k] = make_float4(f0.x + ax[k], f0.y + ay[k], f0.z + az[k], f0.w + ph[k]);
-    }
+    if (lane == k && k < nt) red_add4(a.far + tb + k, ax[k], ay[k], az[k], ph[k]);
   }
 }
 
@@ -721,8 +731,12 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   __shared__ float4 s_stage_all[8][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int wl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (wl >= a.count) return;
-  const int T = a.first + wl;
+  if (wl >= a.w0[a.nlev]) return;
+  int lv = 0;
+  while (wl >= a.w0[lv + 1]) ++lv;
+  const int T = a.first[lv] + (wl - a.w0[lv]);
+  const float4 *off = a.off[lv];
+  const float hx = a.h[lv][0], hy = a.h[lv][1], hz = a.h[lv][2];
   const int tb = a.pbeg[T], nt = a.pend[T] - tb;
   if ((long long)nt > a.direct_max) return;
   int *s_src = s_src_all[wib];
@@ -759,9 +773,9 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
     const int pos = nsrc + __popc(mask & ((1u << lane) - 1u));
     if (q >= 0) {
       s_src[pos] = q;
-      s_shift[3 * pos] = ddx * a.hx;  // c_S - c_T
-      s_shift[3 * pos + 1] = ddy * a.hy;
-      s_shift[3 * pos + 2] = ddz * a.hz;
+      s_shift[3 * pos] = ddx * hx;  // c_S - c_T
+      s_shift[3 * pos + 1] = ddy * hy;
+      s_shift[3 * pos + 2] = ddz * hz;
       s_pref[pos + 1] = nsv[r];  // counts, turned into a prefix sum below
     }
     nsrc += __popc(mask);
@@ -777,10 +791,10 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
     if (a.pair_count) atomicAdd(a.pair_count, (unsigned long long)((long long)nt * acc));
   }
   __syncwarp();
-  if (nt <= 1) direct_small<1, DIM>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
-  else if (nt <= 2) direct_small<2, DIM>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
-  else if (nt <= 4) direct_small<4, DIM>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
-  else if (nt <= 8) direct_small<8, DIM>(a, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
+  if (nt <= 1) direct_small<1, DIM>(a, off, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
+  else if (nt <= 2) direct_small<2, DIM>(a, off, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
+  else if (nt <= 4) direct_small<4, DIM>(a, off, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
+  else if (nt <= 8) direct_small<8, DIM>(a, off, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
   else {
     // Gl lanes per target (Gl * min(nt, 32) <= 32); the sources pass through
     // shared memory 32 at a time, each lane taking every Gl-th of them
@@ -792,7 +806,7 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
     float4 *stage = s_stage_all[wib];
     for (int t0 = 0; t0 < nt; t0 += tpp) {
       const int ti = t0 + lane / Gl, sub = lane % Gl;
-      const float4 t = a.off[tb + (ti < nt ? ti : 0)];
+      const float4 t = off[tb + (ti < nt ? ti : 0)];
       float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
       int si = 0;
       for (int f0 = 0; f0 < total; f0 += 32) {
@@ -800,7 +814,7 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
         float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
         if (f < total) {
           while (f >= s_pref[si + 1]) ++si;
-          const float4 qq = a.off[a.pbeg[s_src[si]] + (f - s_pref[si])];
+          const float4 qq = off[a.pbeg[s_src[si]] + (f - s_pref[si])];
           q = make_float4(qq.x + s_shift[3 * si], qq.y + s_shift[3 * si + 1], qq.z + s_shift[3 * si + 2], qq.w);
         }
         stage[lane] = q;
@@ -818,10 +832,7 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
         az += __shfl_xor_sync(0xffffffffu, az, o);
         ph += __shfl_xor_sync(0xffffffffu, ph, o);
       }
-      if (ti < nt && sub == 0) {
-        float4 f0 = a.far[tb + ti];
-        a.far[tb + ti] = make_float4(f0.x + ax, f0.y + ay, f0.z + az, f0.w + ph);
-      }
+      if (ti < nt && sub == 0) red_add4(a.far + tb + ti, ax, ay, az, ph);
     }
   }
 }
@@ -1094,9 +1105,17 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     k_l2p2d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far);
   ws.launches += 1;
   if (ev) cudaEventRecord(ev[4], st);
-  // direct far field, level by level (levels >= 2 have interaction lists)
+  // direct far field, all levels >= 2 (they have interaction lists) in one
+  // launch, coarse levels first so that their long warps start early
   if (direct_max > 0 && D >= 2) {
-    if (!eb.lvl_off.reserve((size_t)n)) return FMM_ERR_OUT_OF_MEMORY;
+    if (D + 1 > DF_MAX_LEVELS) return FMM_ERR_UNSUPPORTED;
+    if (D > 2) {
+      if (!eb.lvl_off.reserve((size_t)n * (D - 2))) return FMM_ERR_OUT_OF_MEMORY;
+      auto lo_kern = dim == 3 ? k_level_offsets<3> : k_level_offsets<2>;
+      lo_kern<<<cdiv(n, TPB), TPB, 0, st>>>(d_pos_g, d_mass_g, t.d_perm, ws.leaf_of, ws.cell_key, n, D, 2, D - 1,
+                                            g.lo[0], g.lo[1], g.lo[2], g.ext[0], g.ext[1], g.ext[2], eb.lvl_off.ptr);
+      ws.launches += 1;
+    }
     DirectArgs da;
     da.pbeg = ws.cell_pbeg;
     da.pend = ws.cell_pend;
@@ -1108,28 +1127,23 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     da.direct_max = direct_max;
     da.far = ws.far;
     da.pair_count = ws.counters + 1;
-    for (int d = D; d >= 2; --d) {
+    da.nlev = 0;
+    int64_t nw = 0;
+    for (int d = 2; d <= D; ++d) {
+      const int k = da.nlev++;
       const double invd = std::ldexp(1.0, -d);
-      if (d == D) {
-        da.off = ws.part;
-      } else {
-        auto lo_kern = dim == 3 ? k_level_offsets<3> : k_level_offsets<2>;
-        lo_kern<<<cdiv(n, TPB), TPB, 0, st>>>(d_pos_g, d_mass_g, t.d_perm, ws.leaf_of, ws.cell_key, n, D, d,
-                                                      g.lo[0], g.lo[1], g.lo[2], g.ext[0], g.ext[1], g.ext[2],
-                                                      eb.lvl_off.ptr);
-        ws.launches += 1;
-        da.off = eb.lvl_off.ptr;
-      }
-      da.first = t.level_off[d];
-      da.count = t.level_count[d];
-      da.depth_d = d;
-      da.hx = (float)(g.ext[0] * invd);
-      da.hy = (float)(g.ext[1] * invd);
-      da.hz = (float)(g.ext[2] * invd);
-      if (dim == 3) k_direct_far<3><<<cdiv((int64_t)da.count * 32, TPB), TPB, 0, st>>>(da);
-      else k_direct_far<2><<<cdiv((int64_t)da.count * 32, TPB), TPB, 0, st>>>(da);
-      ws.launches += 1;
+      da.first[k] = t.level_off[d];
+      da.w0[k] = (int)nw;
+      da.off[k] = d == D ? ws.part : eb.lvl_off.ptr + (size_t)(d - 2) * n;
+      da.h[k][0] = (float)(g.ext[0] * invd);
+      da.h[k][1] = (float)(g.ext[1] * invd);
+      da.h[k][2] = (float)(g.ext[2] * invd);
+      nw += t.level_count[d];
     }
+    da.w0[da.nlev] = (int)nw;
+    if (dim == 3) k_direct_far<3><<<cdiv(nw * 32, TPB), TPB, 0, st>>>(da);
+    else k_direct_far<2><<<cdiv(nw * 32, TPB), TPB, 0, st>>>(da);
+    ws.launches += 1;
   }
   // P2P + output
   const double inv2D = std::ldexp(1.0, -D);
