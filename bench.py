@@ -1,26 +1,36 @@
 #!/usr/bin/env python
-"""Throughput of the FMM force pass on B200 (particles per second).
+"""Throughput of the FMM force pass on B200 at 1e-6 relative force error
+(particles per second), tensor-core translations against the plain FP32 GPU
+FMM.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 A step is one force evaluation of the whole system: tree build (the
-reference's Tree::init_tree) and every FMM pass, exactly the work of the
+reference's Tree::init_tree) and every FMM pass, the work of the
 reference's FMM::update (src/system_updaters/FMM.cpp:9-12).  Workload: a 3D
 Plummer sphere of N = 2^20 particles (scale radius 1, truncated at 20, seed
-2, equal masses summing to 1), expansion order p = 8, leaf capacity 64,
-forces in FP32 from FP64 positions, G = 1.
+2, equal masses summing to 1), leaf capacity 64, forces in FP32 from FP64
+positions, G = 1, at expansion order p = 12: the lowest order whose relative
+L2 force error against the FP64 direct sum is <= 1e-6 on this input
+(p = 11 gives 1.06e-6, p = 12 8.6e-7).  M2L, M2M and L2L run on the tensor
+cores (tcgen05, 3xBF16 split, FP32 accumulation); interaction-list pairs with
+n_T * n_S <= direct_max are summed directly.
 
 value: N * K / (sum of the K per-step device times), inputs resident in HBM,
        timed with CUDA events on the launching stream; a 256 MiB buffer is
        written between steps (outside the event pair) to flush L2.  With N
        GPUs each rank runs its own replica (the single-system pass does not
        shard), value sums the particles of all ranks over the slowest rank.
-e2e:   the same metric through the public C ABI with pinned host buffers
-       (fmm_evaluate: host-to-device copy of positions and masses, the pass,
-       device-to-host copy of accelerations), wall-clock per call.
-roofline: the dominant kernel (the M2L contraction) timed live with CUDA
-       events; algorithmic FLOPs = 2 K^2 per interaction-list pair contracted,
-       K = (p+1)^2.
+plain: the same workload, order and error through the plain FP32 GPU FMM
+       (SIMT contractions, FMM_M2L_FP32), timed the same way.
+e2e:   the headline configuration through the public C ABI with pinned host
+       buffers (fmm_evaluate: host-to-device copy of positions and masses,
+       the pass, device-to-host copy of accelerations), wall clock per call.
+roofline: the dominant kernel by live-measured time, and both of the two
+       largest: the tensor-core M2L (algorithmic FLOPs 2 K^2 per
+       interaction-list pair, K = (p+1)^2, against the measured sustained
+       BF16 peak) and the direct far field (20 FLOPs per particle pair,
+       against the FP32 peak derived from the SM count and clock).
 cpu_baseline: the reference itself (compiled from its sources into
        oracle/_ref) timing FMM::update on a bounded Plummer sample, 1 thread.
 --impl reference: the reference's CPU FMM on all host cores (one process per
@@ -41,16 +51,16 @@ sys.path.insert(0, os.path.join(ROOT, "nbody-fmm_b200"))
 
 METRIC = "3D FMM particles/s at 1e-6 rel force err: learned+TC vs plain GPU FMM"
 UNIT = "particles/s"
-REF_SAMPLE_N = 2048          # particles per reference process per step
-BASELINE_SAMPLE_N = 4096     # single-thread CPU baseline sample (about 15 s)
+REF_SAMPLE_N = 512           # particles per reference process per step (about 2 s at p = 12)
+BASELINE_SAMPLE_N = 2048     # single-thread CPU baseline sample (about 20 s at p = 12)
 
 
-def workload_desc(n, p, leaf, m2l):
+def workload_desc(n, p, leaf, m2l, direct_max=None):
     return {
         "workload": f"3D Plummer sphere N={n} (a=1, r<=20, seed 2), p={p}, leaf capacity {leaf}, "
                     f"one force evaluation (tree build + all FMM passes) per step",
-        "n": n, "p": p, "leaf_cap": leaf, "m2l": m2l, "positions": "f64", "forces": "f32",
-        "l2": "256 MiB buffer written between steps (outside the timed events)",
+        "n": n, "p": p, "leaf_cap": leaf, "m2l": m2l, "direct_max": direct_max, "positions": "f64",
+        "forces": "f32", "l2": "256 MiB buffer written between steps (outside the timed events)",
         "parallelism": "replicas",
     }
 
@@ -119,6 +129,57 @@ def peaks():
 
 
 # ---------------------------------------------------------------- ours
+def _timed(ctx, n, d_pos, d_mass, d_acc, stream, flush, steps, warmup, barrier):
+    """Runs warmup + steps passes; returns per-step device ms and stats."""
+    import torch
+
+    sp = stream.cuda_stream
+    for _ in range(warmup):
+        flush.zero_()
+        ctx.evaluate_device(n, d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), None, sp)
+        ctx.synchronize()
+    barrier()
+    step_ms, stats = [], []
+    l0 = ctx.launch_count()
+    for _ in range(steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.evaluate_device(n, d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), None, sp)
+        e1.record(stream)
+        ctx.synchronize()
+        step_ms.append(e0.elapsed_time(e1))
+        stats.append(ctx.stats())
+    launches = ctx.launch_count() - l0
+    barrier()
+    return step_ms, stats, launches
+
+
+def _error(ctx, n, d_pos, d_mass, d_acc, d_pot, stream, dev, judge):
+    """Relative force and potential errors on 4096 sampled targets against
+    the FP64 direct sum on the GPU."""
+    import torch
+
+    d_tg, ra, rp = judge
+    ctx.evaluate_device(n, d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), d_pot.data_ptr(), stream.cuda_stream)
+    ctx.synchronize()
+    a = d_acc[d_tg].cpu().numpy()
+    ph = d_pot[d_tg].cpu().numpy()
+    return {
+        "targets": int(d_tg.numel()), "vs": "FP64 direct sum on the GPU",
+        "force_rel_l2": float(np.linalg.norm(a - ra) / np.linalg.norm(ra)),
+        "force_max_rel": float((np.linalg.norm(a - ra, axis=1) / np.linalg.norm(ra, axis=1)).max()),
+        "pot_rel_l2": float(np.linalg.norm(ph - rp) / np.linalg.norm(rp)),
+        "pot_max_rel": float((np.abs(ph - rp) / np.abs(rp)).max()),
+    }
+
+
+def _phases(stats):
+    keys = ("ms_tree", "ms_upward", "ms_m2l", "ms_downward", "ms_p2p", "ms_far_direct", "ms_total")
+    return {k: float(np.mean([s[k] for s in stats])) for k in keys}
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -141,47 +202,34 @@ def run_ours(args, world, rank, local):
     d_acc = torch.empty((n, 3), dtype=torch.float64, device=dev)
     d_pot = torch.empty((n,), dtype=torch.float64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    ctx = fmmgpu.Context(dim=3, p=p, leaf_cap=leaf, m2l_mode=mode, G=1.0, device=local)
     # a stream of our own (torch's default stream has handle 0, which the C
     # ABI reads as "the context's stream")
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
-    sp = stream.cuda_stream
-
-    def one(pot=False):
-        ctx.evaluate_device(n, d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(),
-                            d_pot.data_ptr() if pot else None, sp)
-
-    for _ in range(args.warmup):
-        flush.zero_()
-        one()
-        ctx.synchronize()
 
     def barrier():
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize(dev)
 
+    # the judge: FP64 direct sum on 4096 sampled targets
+    rng = np.random.default_rng(7)
+    tg = np.sort(rng.choice(n, size=min(4096, n), replace=False)).astype(np.int64)
+    d_tg = torch.from_numpy(tg).to(dev)
+    r_acc = torch.empty((len(tg), 3), dtype=torch.float64, device=dev)
+    r_pot = torch.empty((len(tg),), dtype=torch.float64, device=dev)
+    with fmmgpu.Context(dim=3, G=1.0, device=local) as jc:
+        jc.direct_device(n, d_pos.data_ptr(), d_mass.data_ptr(), len(tg), d_tg.data_ptr(), r_acc.data_ptr(),
+                         r_pot.data_ptr(), stream=stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    judge = (d_tg, r_acc.cpu().numpy(), r_pot.cpu().numpy())
+
+    # headline: the chosen M2L mode
+    ctx = fmmgpu.Context(dim=3, p=p, leaf_cap=leaf, m2l_mode=mode, G=1.0, device=local, direct_max=args.direct_max)
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
-    l0 = ctx.launch_count()
-    barrier()
-    step_ms, m2l_ms, stats = [], [], []
-    for _ in range(args.steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        one()
-        e1.record(stream)
-        ctx.synchronize()
-        step_ms.append(e0.elapsed_time(e1))
-        s = ctx.stats()
-        stats.append(s)
-        m2l_ms.append(s["ms_m2l"])
-    barrier()
-    launches = ctx.launch_count() - l0
+    step_ms, stats, launches = _timed(ctx, n, d_pos, d_mass, d_acc, stream, flush, args.steps, args.warmup, barrier)
     clocks = sampler.stop()
     total_ms = float(sum(step_ms))
     if world > 1:
@@ -189,28 +237,7 @@ def run_ours(args, world, rank, local):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         total_ms = float(t.item())
     value = n * args.steps * world / (total_ms / 1e3)
-
-    # accuracy on 4096 sampled targets against the FP64 direct sum (GPU)
-    rng = np.random.default_rng(7)
-    tg = np.sort(rng.choice(n, size=min(4096, n), replace=False)).astype(np.int64)
-    d_tg = torch.from_numpy(tg).to(dev)
-    r_acc = torch.empty((len(tg), 3), dtype=torch.float64, device=dev)
-    r_pot = torch.empty((len(tg),), dtype=torch.float64, device=dev)
-    one(pot=True)
-    ctx.synchronize()
-    ctx.direct_device(n, d_pos.data_ptr(), d_mass.data_ptr(), len(tg), d_tg.data_ptr(), r_acc.data_ptr(),
-                      r_pot.data_ptr(), stream=sp)
-    torch.cuda.synchronize(dev)
-    a = d_acc[d_tg].cpu().numpy()
-    ph = d_pot[d_tg].cpu().numpy()
-    ra, rp = r_acc.cpu().numpy(), r_pot.cpu().numpy()
-    err = {
-        "targets": len(tg), "vs": "FP64 direct sum on the GPU",
-        "force_rel_l2": float(np.linalg.norm(a - ra) / np.linalg.norm(ra)),
-        "force_max_rel": float((np.linalg.norm(a - ra, axis=1) / np.linalg.norm(ra, axis=1)).max()),
-        "pot_rel_l2": float(np.linalg.norm(ph - rp) / np.linalg.norm(rp)),
-        "pot_max_rel": float((np.abs(ph - rp) / np.abs(rp)).max()),
-    }
+    err = _error(ctx, n, d_pos, d_mass, d_acc, d_pot, stream, dev, judge)
 
     # end to end through the C ABI with pinned host buffers
     h_pos = torch.from_numpy(pos).pin_memory()
@@ -218,60 +245,94 @@ def run_ours(args, world, rank, local):
     h_acc = torch.empty((n, 3), dtype=torch.float64).pin_memory()
     hp, hm, ha = h_pos.numpy(), h_mass.numpy(), h_acc.numpy()
     ctx.evaluate(hp, hm, out=ha)
+    e2e_steps = max(3, args.steps // 2)
     e2e_s = 0.0
-    for _ in range(max(3, args.steps // 2)):
+    for _ in range(e2e_steps):
         flush.zero_()
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
         ctx.evaluate(hp, hm, out=ha)
         e2e_s += time.perf_counter() - t0
-    e2e_steps = max(3, args.steps // 2)
     e2e_val = n * e2e_steps * world / e2e_s
     if world > 1:
         t = torch.tensor([e2e_val / world], dtype=torch.float64, device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MIN)
         e2e_val = float(t.item()) * world
+    ctx.close()
 
-    # roofline of the dominant kernel (M2L contraction, FP32 SIMT)
-    s_last = stats[-1]
-    K = (p + 1) ** 2
-    flops = 2.0 * K * K * s_last["m2l_pairs"]
-    m2l_s = statistics.mean(m2l_ms) / 1e3
+    # rooflines of the two largest kernels, from the live event timings
     pk = peaks()
     sm_max = float(pk.get("sm_max_mhz", 1965.0))
     fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
-    roof = {
-        "kernel": "k_contract (M2L, FP32 SIMT)", "bound": "fp32", "unit": "TFLOP/s",
-        "achieved": flops / m2l_s / 1e12 if m2l_s > 0 else None,
-        "peak": fp32_peak,
-        "peak_source": f"derived: 148 SM x 128 FP32 lanes x 2 x {sm_max:.0f} MHz (no FP32 figure in MEASURED_PEAKS.json)",
-        "traffic": None,
-        "flops_per_launch": flops, "m2l_pairs": int(s_last["m2l_pairs"]), "ms_per_launch": m2l_s * 1e3,
-    }
-    roof["frac"] = roof["achieved"] / roof["peak"] if roof["achieved"] else None
+    tc_peak = pk.get("bf16_tflops_sustained")
+    tc_src = "MEASURED_PEAKS.json bf16_tflops_sustained (cuBLAS bf16, seconds-long loop)"
+    if tc_peak is None:
+        tc_peak, tc_src = 1400.0, "fallback sustained bf16 figure (MEASURED_PEAKS.json absent)"
+    K = (p + 1) ** 2
+    ph = _phases(stats)
+    s_last = stats[-1]
+    m2l_flops = 2.0 * K * K * s_last["m2l_pairs"]
+    far_flops = 20.0 * s_last["far_direct_pairs"]
     traffic = load_traffic()
-    if traffic:
-        roof["traffic"] = traffic
-
-    phases = {k: float(np.mean([s[k] for s in stats])) for k in
-              ("ms_tree", "ms_upward", "ms_m2l", "ms_downward", "ms_p2p", "ms_total")}
+    roofs = {
+        "m2l_tc" if mode == fmmgpu.FMM_M2L_TC else "m2l_fp32": {
+            "kernel": "k_tc_translate (M2L: tcgen05 3xBF16, FP32 accumulation)" if mode == fmmgpu.FMM_M2L_TC
+            else "k_contract (M2L, FP32 SIMT)",
+            "bound": "tensor" if mode == fmmgpu.FMM_M2L_TC else "fp32", "unit": "TFLOP/s",
+            "achieved": m2l_flops / (ph["ms_m2l"] / 1e3) / 1e12 if ph["ms_m2l"] > 0 else None,
+            "peak": tc_peak if mode == fmmgpu.FMM_M2L_TC else fp32_peak,
+            "peak_source": tc_src if mode == fmmgpu.FMM_M2L_TC else f"derived: 148 SM x 128 FP32 lanes x 2 x {sm_max:.0f} MHz",
+            "flops_per_launch": m2l_flops, "pairs": int(s_last["m2l_pairs"]), "tiles": int(s_last["m2l_tiles"]),
+            "ms_per_launch": ph["ms_m2l"],
+            "traffic": traffic.get("m2l_tc" if mode == fmmgpu.FMM_M2L_TC else "m2l_fp32"),
+        },
+        "far_direct": {
+            "kernel": "k_direct_far (interaction-list pairs summed directly, FP32)", "bound": "fp32",
+            "unit": "TFLOP/s", "achieved": far_flops / (ph["ms_far_direct"] / 1e3) / 1e12 if ph["ms_far_direct"] > 0 else None,
+            "peak": fp32_peak, "peak_source": f"derived: 148 SM x 128 FP32 lanes x 2 x {sm_max:.0f} MHz "
+                                              "(no FP32 figure in MEASURED_PEAKS.json)",
+            "flops_per_launch": far_flops, "pairs": int(s_last["far_direct_pairs"]),
+            "ms_per_launch": ph["ms_far_direct"], "traffic": traffic.get("far_direct"),
+        },
+    }
+    for r in roofs.values():
+        r["frac"] = r["achieved"] / r["peak"] if r["achieved"] else None
+    dominant = max(roofs, key=lambda k: roofs[k]["ms_per_launch"])
+    roof = dict(roofs[dominant], name=dominant)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded Plummer sphere)", "impl": "fmmgpu",
-        "config": workload_desc(n, p, leaf, args.m2l),
+        "config": workload_desc(n, p, leaf, args.m2l, s_last.get("direct_max")),
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(n * 3 * 8 + n * 8),
                 "d2h_bytes_per_step": int(n * 3 * 8)},
-        "roofline": roof, "error": err, "phases_ms": phases,
+        "roofline": roof, "rooflines": roofs, "error": err, "phases_ms": ph,
         "tree": {"depth": s_last["depth"], "leaves": s_last["n_leaves"], "cells": s_last["n_cells"],
-                 "p2p_pairs": s_last["p2p_pairs"]},
+                 "p2p_pairs": s_last["p2p_pairs"], "far_direct_pairs": s_last["far_direct_pairs"],
+                 "m2l_pairs": s_last["m2l_pairs"]},
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
+
+    # the plain FP32 GPU FMM at the same order (same error)
+    if not args.no_plain and mode == fmmgpu.FMM_M2L_TC:
+        pc = fmmgpu.Context(dim=3, p=p, leaf_cap=leaf, m2l_mode=fmmgpu.FMM_M2L_FP32, G=1.0, device=local,
+                            direct_max=args.direct_max)
+        psteps = max(3, args.steps // 2)
+        pms, pst, _ = _timed(pc, n, d_pos, d_mass, d_acc, stream, flush, psteps, max(1, args.warmup), barrier)
+        ptot = float(sum(pms))
+        if world > 1:
+            t = torch.tensor([ptot], dtype=torch.float64, device=dev)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ptot = float(t.item())
+        perr = _error(pc, n, d_pos, d_mass, d_acc, d_pot, stream, dev, judge)
+        pc.close()
+        line["plain"] = {"m2l": "fp32", "value": n * psteps * world / (ptot / 1e3), "unit": UNIT, "steps": psteps,
+                         "ms_per_step": ptot / psteps, "error": perr, "phases_ms": _phases(pst)}
+        line["speedup_vs_plain"] = value / line["plain"]["value"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p, leaf)
-    ctx.close()
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:
@@ -279,16 +340,26 @@ def run_ours(args, world, rank, local):
 
 
 def load_traffic():
-    """DRAM bytes per M2L launch (dram__bytes_read.sum + dram__bytes_write.sum)
-    from the committed ncu summary of that kernel, if present."""
-    path = os.path.join(ROOT, "profiles", "k_contract_m2l_plummer_2p20_p8.md")
+    """DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum)
+    of the rooflined kernels, from the committed ncu summaries: lines
+    `traffic_bytes_per_launch[<name>]: <bytes>` in profiles/*.md."""
+    out = {}
+    pdir = os.path.join(ROOT, "profiles")
     try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return float(line.split(":")[1])
-    except Exception:
-        pass
-    return None
+        names = sorted(os.listdir(pdir))
+    except OSError:
+        return out
+    for fn in names:
+        if not fn.endswith(".md"):
+            continue
+        for line in open(os.path.join(pdir, fn)):
+            if line.startswith("traffic_bytes_per_launch["):
+                key = line[len("traffic_bytes_per_launch["):line.index("]")]
+                try:
+                    out[key] = float(line.split(":", 1)[1])
+                except ValueError:
+                    pass
+    return out
 
 
 # ------------------------------------------------------------- reference
@@ -340,7 +411,7 @@ def run_reference(args, world, rank):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Plummer sphere)", "impl": "reference",
-        "config": workload_desc(args.n, p, leaf, "reference"),
+        "config": workload_desc(args.n, p, leaf, "reference (CPU)"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -354,9 +425,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=1 << 20)
-    ap.add_argument("--p", type=int, default=8)
+    ap.add_argument("--p", type=int, default=12)
     ap.add_argument("--leaf", type=int, default=64)
-    ap.add_argument("--m2l", default="fp32", choices=["fp32", "tc"])
+    ap.add_argument("--m2l", default="tc", choices=["fp32", "tc"])
+    ap.add_argument("--direct-max", type=int, default=-1, help="-1: the library's automatic threshold")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)

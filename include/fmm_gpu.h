@@ -93,15 +93,18 @@ typedef struct fmm_stats {
   int64_t n_leaves;
   int64_t n_cells;          /* all levels */
   int64_t m2l_pairs;        /* interaction-list pairs evaluated by M2L */
-  int64_t p2p_pairs;        /* particle pairs evaluated directly */
+  int64_t p2p_pairs;        /* particle pairs evaluated directly (near field + direct far field) */
   double ms_tree;           /* device time of the tree build */
   double ms_upward;         /* P2M + M2M */
   double ms_m2l;
   double ms_downward;       /* L2L + L2P */
-  double ms_p2p;
+  double ms_p2p;            /* near field + direct far field + output */
   double ms_total;          /* whole force pass (device time) */
   int64_t m2l_tiles;        /* FMM_M2L_TC: 128-row (target batch, slot) tiles of the M2L contraction */
-  double reserved[5];
+  double ms_far_direct;     /* the direct far field part of ms_p2p */
+  int64_t far_direct_pairs; /* the direct far field part of p2p_pairs */
+  int64_t direct_max;       /* the direct-pair threshold the pass used */
+  double reserved[2];
 } fmm_stats;
 
 typedef struct fmm_ctx fmm_ctx;

@@ -32,7 +32,7 @@ struct fmm_ctx {
   DevBuf<double> d_pos, d_mass, d_acc, d_pot, d_vel, d_x0, d_v0, d_xs, d_vs, d_asum, d_vsum;
   DevBuf<int64_t> d_targets;
   fmm_stats stats;
-  cudaEvent_t ev[6] = {};
+  cudaEvent_t ev[7] = {};  // pass boundaries; ev[6] ends the direct far field
   bool timing_pending = false;
   bool have_tree = false;
 };
@@ -182,6 +182,7 @@ static int evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const dou
   memset(&c->stats, 0, sizeof(c->stats));
   rc = run_fmm_passes(c->ws, c->tree, c->ops, c->eb, d_pos, d_mass, c->cfg.p, c->cfg.eps2, c->cfg.G, g, d_acc, d_pot,
                       c->cfg.m2l_mode, direct_threshold(c->cfg), st, c->stats, c->ev);
+  c->stats.direct_max = direct_threshold(c->cfg);
   if (rc) return rc;
   if (!c->ws.ok) return FMM_ERR_OUT_OF_MEMORY;
   c->stats.depth = c->tree.depth;
@@ -196,10 +197,11 @@ static int finish(fmm_ctx *c, cudaStream_t st) {
   unsigned int herr = 0;
   CUDA_TRY(cudaMemcpy(&herr, c->ws.dev_err, sizeof(herr), cudaMemcpyDeviceToHost));
   if (c->timing_pending) {
-    unsigned long long cnt[3] = {0, 0, 0};
+    unsigned long long cnt[4] = {0, 0, 0, 0};
     CUDA_TRY(cudaMemcpy(cnt, c->ws.counters, sizeof(cnt), cudaMemcpyDeviceToHost));
     c->stats.m2l_pairs = (int64_t)cnt[0];
-    c->stats.p2p_pairs = (int64_t)cnt[1];
+    c->stats.p2p_pairs = (int64_t)(cnt[1] + cnt[3]);
+    c->stats.far_direct_pairs = (int64_t)cnt[3];
     c->stats.m2l_tiles = (int64_t)cnt[2];
     float ms[5] = {0, 0, 0, 0, 0};
     for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], c->ev[i], c->ev[i + 1]);
@@ -208,6 +210,9 @@ static int finish(fmm_ctx *c, cudaStream_t st) {
     c->stats.ms_m2l = ms[2];
     c->stats.ms_downward = ms[3];
     c->stats.ms_p2p = ms[4];
+    float fd = 0.f;
+    if (cudaEventElapsedTime(&fd, c->ev[4], c->ev[6]) != cudaSuccess) fd = 0.f;
+    c->stats.ms_far_direct = fd;
     float tot = 0;
     cudaEventElapsedTime(&tot, c->ev[0], c->ev[5]);
     c->stats.ms_total = tot;

@@ -67,6 +67,20 @@ __device__ inline void split3(float v, uint16_t &h, uint16_t &m, uint16_t &l) {
   l = __bfloat16_as_ushort(bl);
 }
 
+// split3 of two values at once; each 32-bit word holds (a, b) as BF16 with
+// a in the low half.
+__device__ inline uint32_t bf2_pack(float a, float b) {
+  const __nv_bfloat162 t = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t *>(&t);
+}
+__device__ inline void split3x2(float a, float b, uint32_t &h, uint32_t &m, uint32_t &l) {
+  h = bf2_pack(a, b);
+  const float ra = a - __uint_as_float(h << 16), rb = b - __uint_as_float(h & 0xffff0000u);
+  m = bf2_pack(ra, rb);
+  const float sa = ra - __uint_as_float(m << 16), sb = rb - __uint_as_float(m & 0xffff0000u);
+  l = bf2_pack(sa, sb);
+}
+
 // Operator images: for each table slot and split s, B = T^T (n: output,
 // k: input) cut into output tiles of N0 and P16 - N0 columns, each tile
 // contiguous; element (n, k) of a tile of width nw at
@@ -303,25 +317,22 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
 #pragma unroll
     for (int q = 0; q < P16 / 4; ++q) rv[q] = (src >= 0 && 4 * q < a.KS) ? xr[q] : make_float4(0.f, 0.f, 0.f, 0.f);
   };
+  // A operand of the next slot from the prefetched rows: two values per
+  // conversion (cvt.rn.bf16x2.f32), the same round-to-nearest splits as
+  // split3.  Columns K..KS-1 of a row are zero in memory and beyond KS the
+  // prefetch is zero, so no masking is needed.
   auto write_a = [&]() {
 #pragma unroll
     for (int kc = 0; kc < KC; ++kc) {
-      float v[8] = {rv[2 * kc].x, rv[2 * kc].y, rv[2 * kc].z, rv[2 * kc].w,
-                    rv[2 * kc + 1].x, rv[2 * kc + 1].y, rv[2 * kc + 1].z, rv[2 * kc + 1].w};
-      uint16_t h[8], m[8], l[8];
+      const float v[8] = {rv[2 * kc].x, rv[2 * kc].y, rv[2 * kc].z, rv[2 * kc].w,
+                          rv[2 * kc + 1].x, rv[2 * kc + 1].y, rv[2 * kc + 1].z, rv[2 * kc + 1].w};
+      uint32_t h[4], m[4], l[4];
 #pragma unroll
-      for (int e = 0; e < 8; ++e) split3(kc * 8 + e < a.K ? v[e] : 0.f, h[e], m[e], l[e]);
+      for (int e = 0; e < 4; ++e) split3x2(v[2 * e], v[2 * e + 1], h[e], m[e], l[e]);
       const size_t off = ((size_t)kc * (TC_M / 8) + tid / 8) * 64 + (tid % 8) * 8;
-      uint4 ph, pm, pl;
-      ph.x = h[0] | ((uint32_t)h[1] << 16); ph.y = h[2] | ((uint32_t)h[3] << 16);
-      ph.z = h[4] | ((uint32_t)h[5] << 16); ph.w = h[6] | ((uint32_t)h[7] << 16);
-      pm.x = m[0] | ((uint32_t)m[1] << 16); pm.y = m[2] | ((uint32_t)m[3] << 16);
-      pm.z = m[4] | ((uint32_t)m[5] << 16); pm.w = m[6] | ((uint32_t)m[7] << 16);
-      pl.x = l[0] | ((uint32_t)l[1] << 16); pl.y = l[2] | ((uint32_t)l[3] << 16);
-      pl.z = l[4] | ((uint32_t)l[5] << 16); pl.w = l[6] | ((uint32_t)l[7] << 16);
-      *(uint4 *)(As + off) = ph;
-      *(uint4 *)(As + ASPLIT + off) = pm;
-      *(uint4 *)(As + 2 * ASPLIT + off) = pl;
+      *(uint4 *)(As + off) = make_uint4(h[0], h[1], h[2], h[3]);
+      *(uint4 *)(As + ASPLIT + off) = make_uint4(m[0], m[1], m[2], m[3]);
+      *(uint4 *)(As + 2 * ASPLIT + off) = make_uint4(l[0], l[1], l[2], l[3]);
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   };

@@ -993,7 +993,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   ca.dim = dim;
   ca.level_stride = dim == 2 ? 49 : 0;
   ca.pair_count = ws.counters;
-  CUDA_TRY(cudaMemsetAsync(ws.counters, 0, 3 * sizeof(unsigned long long), st));
+  CUDA_TRY(cudaMemsetAsync(ws.counters, 0, 4 * sizeof(unsigned long long), st));
   TcArgs ta{};
   ta.cchild = ws.cell_child;
   ta.cparent = ws.cell_parent;
@@ -1126,7 +1126,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     da.eps2 = (float)eps2;
     da.direct_max = direct_max;
     da.far = ws.far;
-    da.pair_count = ws.counters + 1;
+    da.pair_count = ws.counters + 3;
     da.nlev = 0;
     int64_t nw = 0;
     for (int d = 2; d <= D; ++d) {
@@ -1145,6 +1145,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     else k_direct_far<2><<<cdiv(nw * 32, TPB), TPB, 0, st>>>(da);
     ws.launches += 1;
   }
+  if (ev) cudaEventRecord(ev[6], st);
   // P2P + output
   const double inv2D = std::ldexp(1.0, -D);
   P2PArgs pa;

@@ -61,7 +61,8 @@ class FmmStats(ctypes.Structure):
         ("n_cells", ctypes.c_int64), ("m2l_pairs", ctypes.c_int64), ("p2p_pairs", ctypes.c_int64),
         ("ms_tree", ctypes.c_double), ("ms_upward", ctypes.c_double), ("ms_m2l", ctypes.c_double),
         ("ms_downward", ctypes.c_double), ("ms_p2p", ctypes.c_double), ("ms_total", ctypes.c_double),
-        ("m2l_tiles", ctypes.c_int64), ("reserved", ctypes.c_double * 5),
+        ("m2l_tiles", ctypes.c_int64), ("ms_far_direct", ctypes.c_double),
+        ("far_direct_pairs", ctypes.c_int64), ("direct_max", ctypes.c_int64), ("reserved", ctypes.c_double * 2),
     ]
 
 
