@@ -684,10 +684,10 @@ struct DirectArgs {
 // the cells S of T's interaction list (node_i.cpp:39-43) with
 // n_T * n_S <= direct_max, exactly the pairs the M2L contraction skips.
 // Small T (NT <= 8 targets): every lane holds all targets and takes every
-// 32nd particle of the concatenated sources; larger T: one or more lanes per
-// target over sources staged through shared memory.
+// 32nd particle of the concatenated sources; larger T: register-blocked
+// target groups over sources staged through shared memory.
 template <int NT, int DIM>
-__device__ void direct_small(const DirectArgs &a, const float4 *off, int tb, int nt, const int *s_src,
+__device__ void direct_small(const DirectArgs &a, const float4 *off, int tb, int nt, const int *s_pb,
                              const float *s_shift, const int *s_pref, int nsrc, int lane) {
   float tx[NT], ty[NT], tz[NT], ax[NT], ay[NT], az[NT], ph[NT];
 #pragma unroll
@@ -702,7 +702,7 @@ __device__ void direct_small(const DirectArgs &a, const float4 *off, int tb, int
   int si = 0;
   for (int f = lane; f < total; f += 32) {
     while (f >= s_pref[si + 1]) ++si;
-    const int j = a.pbeg[s_src[si]] + (f - s_pref[si]);
+    const int j = s_pb[si] + (f - s_pref[si]);
     const float4 q = off[j];
     const float qx = q.x + s_shift[3 * si], qy = q.y + s_shift[3 * si + 1], qz = q.z + s_shift[3 * si + 2];
 #pragma unroll
@@ -722,10 +722,75 @@ __device__ void direct_small(const DirectArgs &a, const float4 *off, int tb, int
   }
 }
 
+// Larger T: each lane holds R targets and takes every Gl-th source of the
+// chunks of 32 staged through shared memory; ceil(nt / R) target groups of
+// Gl lanes, 32 / Gl groups per round.
+template <int R, int DIM>
+__device__ void direct_blocked(const DirectArgs &a, const float4 *off, int tb, int nt, int Gl, const int *s_pb,
+                               const float *s_shift, const int *s_pref, int nsrc, int lane, float4 *stage) {
+  const int groups = (nt + R - 1) / R, gpr = 32 / Gl;
+  const int total = s_pref[nsrc];
+  for (int g0 = 0; g0 < groups; g0 += gpr) {
+    const int gi = g0 + lane / Gl, sub = lane % Gl;
+    float tx[R], ty[R], tz[R], ax[R], ay[R], az[R], ph[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int ti = gi * R + r;
+      const float4 t = off[tb + (gi < groups && ti < nt ? ti : 0)];
+      tx[r] = t.x;
+      ty[r] = t.y;
+      tz[r] = t.z;
+      ax[r] = ay[r] = az[r] = ph[r] = 0.f;
+    }
+    int si = 0;
+    for (int f0 = 0; f0 < total; f0 += 32) {
+      const int f = f0 + lane;
+      float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (f < total) {
+        while (f >= s_pref[si + 1]) ++si;
+        const float4 qq = off[s_pb[si] + (f - s_pref[si])];
+        q = make_float4(qq.x + s_shift[3 * si], qq.y + s_shift[3 * si + 1], qq.z + s_shift[3 * si + 2], qq.w);
+      }
+      stage[lane] = q;
+      __syncwarp();
+      const int cnt = min(32, total - f0);
+      for (int k = sub; k < cnt; k += Gl) {
+        const float4 sq = stage[k];
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+          pair_acc<DIM>(tx[r] - sq.x, ty[r] - sq.y, tz[r] - sq.z, sq.w, a.eps2, ax[r], ay[r], az[r], ph[r]);
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      for (int o = 1; o < Gl; o <<= 1) {
+        ax[r] += __shfl_xor_sync(0xffffffffu, ax[r], o);
+        ay[r] += __shfl_xor_sync(0xffffffffu, ay[r], o);
+        az[r] += __shfl_xor_sync(0xffffffffu, az[r], o);
+        ph[r] += __shfl_xor_sync(0xffffffffu, ph[r], o);
+      }
+      const int ti = gi * R + r;
+      if (sub == 0 && gi < groups && ti < nt) red_add4(a.far + tb + ti, ax[r], ay[r], az[r], ph[r]);
+    }
+  }
+}
+
+// Lanes per target group for R targets per lane (largest power of two with
+// ceil(nt / R) * Gl <= 32), and the work of the busiest lane in units of
+// the source count.
+__device__ inline void blocked_shape(int nt, int R, int &Gl, float &cost) {
+  const int groups = (nt + R - 1) / R;
+  Gl = 1;
+  while (Gl * 2 * groups <= 32) Gl *= 2;
+  const int rounds = (groups + 32 / Gl - 1) / (32 / Gl);
+  cost = (float)(rounds * R) / (float)Gl;
+}
+
 template <int DIM>
 __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   constexpr int NS = DIM == 3 ? 27 : 9, NC = 1 << DIM, NCAND = NS * NC, NR = (NCAND + 31) / 32;
-  __shared__ int s_src_all[8][189];
+  __shared__ int s_pb_all[8][189];
   __shared__ float s_shift_all[8][3 * 189];
   __shared__ int s_pref_all[8][190];
   __shared__ float4 s_stage_all[8][32];
@@ -739,17 +804,17 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   const float hx = a.h[lv][0], hy = a.h[lv][1], hz = a.h[lv][2];
   const int tb = a.pbeg[T], nt = a.pend[T] - tb;
   if ((long long)nt > a.direct_max) return;
-  int *s_src = s_src_all[wib];
+  int *s_pb = s_pb_all[wib];
   float *s_shift = s_shift_all[wib];
   int *s_pref = s_pref_all[wib];
   const int P = a.parent[T];
   const int cls = (int)(a.ckey[T] & (uint64_t)(NC - 1));
   const int *pc = a.coll + (int64_t)P * NS;
-  int nsrc = 0;
+  int nsrc = 0, ptotal = 0;
   if (lane == 0) s_pref[0] = 0;
   // all candidate loads in flight at once: colleague, child, then counts
   const int Qlane = lane < NS ? pc[lane] : -1;
-  int qv[NR], nsv[NR];
+  int qv[NR], nsv[NR], pbv[NR];
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
     const int cand = r * 32 + lane;
@@ -758,7 +823,10 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
     qv[r] = (cand < NCAND && Q >= 0) ? a.child[(int64_t)Q * NC + (cand % NC)] : -1;
   }
 #pragma unroll
-  for (int r = 0; r < NR; ++r) nsv[r] = qv[r] >= 0 ? a.pend[qv[r]] - a.pbeg[qv[r]] : 0;
+  for (int r = 0; r < NR; ++r) {
+    pbv[r] = qv[r] >= 0 ? a.pbeg[qv[r]] : 0;
+    nsv[r] = qv[r] >= 0 ? a.pend[qv[r]] - pbv[r] : 0;
+  }
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
     const int cand = r * 32 + lane;
@@ -771,69 +839,56 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
     if (q >= 0 && (adj || (long long)nt * nsv[r] > a.direct_max)) q = -1;
     const unsigned mask = __ballot_sync(0xffffffffu, q >= 0);
     const int pos = nsrc + __popc(mask & ((1u << lane) - 1u));
+    int x = q >= 0 ? nsv[r] : 0;  // inclusive scan of the kept counts
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
     if (q >= 0) {
-      s_src[pos] = q;
+      s_pb[pos] = pbv[r];
       s_shift[3 * pos] = ddx * hx;  // c_S - c_T
       s_shift[3 * pos + 1] = ddy * hy;
       s_shift[3 * pos + 2] = ddz * hz;
-      s_pref[pos + 1] = nsv[r];  // counts, turned into a prefix sum below
+      s_pref[pos + 1] = ptotal + x;
     }
+    ptotal += __shfl_sync(0xffffffffu, x, 31);
     nsrc += __popc(mask);
   }
   __syncwarp();
   if (nsrc == 0) return;
-  if (lane == 0) {
-    int acc = 0;
-    for (int k = 1; k <= nsrc; ++k) {
-      acc += s_pref[k];
-      s_pref[k] = acc;
-    }
-    if (a.pair_count) atomicAdd(a.pair_count, (unsigned long long)((long long)nt * acc));
+  if (lane == 0 && a.pair_count) atomicAdd(a.pair_count, (unsigned long long)((long long)nt * ptotal));
+  switch (nt) {
+    case 1: direct_small<1, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
+    case 2: direct_small<2, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
+    case 3: direct_small<3, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
+    case 4: direct_small<4, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
+    case 5: direct_small<5, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
+    case 6: direct_small<6, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
+    case 7: direct_small<7, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
+    case 8: direct_small<8, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
+    default: break;
   }
-  __syncwarp();
-  if (nt <= 1) direct_small<1, DIM>(a, off, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
-  else if (nt <= 2) direct_small<2, DIM>(a, off, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
-  else if (nt <= 4) direct_small<4, DIM>(a, off, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
-  else if (nt <= 8) direct_small<8, DIM>(a, off, tb, nt, s_src, s_shift, s_pref, nsrc, lane);
-  else {
-    // Gl lanes per target (Gl * min(nt, 32) <= 32); the sources pass through
-    // shared memory 32 at a time, each lane taking every Gl-th of them
-    const int tp = nt < 32 ? nt : 32;
-    int Gl = 1;
-    while (Gl * 2 * tp <= 32) Gl *= 2;
-    const int tpp = 32 / Gl;
-    const int total = s_pref[nsrc];
-    float4 *stage = s_stage_all[wib];
-    for (int t0 = 0; t0 < nt; t0 += tpp) {
-      const int ti = t0 + lane / Gl, sub = lane % Gl;
-      const float4 t = off[tb + (ti < nt ? ti : 0)];
-      float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
-      int si = 0;
-      for (int f0 = 0; f0 < total; f0 += 32) {
-        const int f = f0 + lane;
-        float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (f < total) {
-          while (f >= s_pref[si + 1]) ++si;
-          const float4 qq = off[a.pbeg[s_src[si]] + (f - s_pref[si])];
-          q = make_float4(qq.x + s_shift[3 * si], qq.y + s_shift[3 * si + 1], qq.z + s_shift[3 * si + 2], qq.w);
-        }
-        stage[lane] = q;
-        __syncwarp();
-        const int cnt = min(32, total - f0);
-        for (int k = sub; k < cnt; k += Gl) {
-          const float4 sq = stage[k];
-          pair_acc<DIM>(t.x - sq.x, t.y - sq.y, t.z - sq.z, sq.w, a.eps2, ax, ay, az, ph);
-        }
-        __syncwarp();
-      }
-      for (int o = 1; o < Gl; o <<= 1) {
-        ax += __shfl_xor_sync(0xffffffffu, ax, o);
-        ay += __shfl_xor_sync(0xffffffffu, ay, o);
-        az += __shfl_xor_sync(0xffffffffu, az, o);
-        ph += __shfl_xor_sync(0xffffffffu, ph, o);
-      }
-      if (ti < nt && sub == 0) red_add4(a.far + tb + ti, ax, ay, az, ph);
+  // larger T: the register blocking R in 1..4 that minimises the busiest lane's work
+  int bestR = 1, bestG = 1;
+  float best = 1e30f;
+#pragma unroll
+  for (int R = 1; R <= 4; ++R) {
+    int G;
+    float c;
+    blocked_shape(nt, R, G, c);
+    if (c < best) {
+      best = c;
+      bestR = R;
+      bestG = G;
     }
+  }
+  float4 *stage = s_stage_all[wib];
+  switch (bestR) {
+    case 1: direct_blocked<1, DIM>(a, off, tb, nt, bestG, s_pb, s_shift, s_pref, nsrc, lane, stage); break;
+    case 2: direct_blocked<2, DIM>(a, off, tb, nt, bestG, s_pb, s_shift, s_pref, nsrc, lane, stage); break;
+    case 3: direct_blocked<3, DIM>(a, off, tb, nt, bestG, s_pb, s_shift, s_pref, nsrc, lane, stage); break;
+    default: direct_blocked<4, DIM>(a, off, tb, nt, bestG, s_pb, s_shift, s_pref, nsrc, lane, stage); break;
   }
 }
 
