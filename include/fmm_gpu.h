@@ -54,6 +54,28 @@ enum {
   FMM_ERR_TOO_LARGE = -10         /* request larger than fmm_direct_noalloc's fixed scratch */
 };
 
+/* Order of each M2L pair (FMM_M2L_TC).  FIXED: every pair at p.  GEOMETRIC:
+   a pair whose cells are R cell sizes apart is evaluated at the order that
+   gives the closest offset's (R = 2) truncation bound at p, plus
+   order_margin, clamped to [min(4, p), p].  LEARNED (3D): an MLP set with
+   fmm_order_set_model predicts each pair's truncation error at orders 4..12
+   and the pair takes the lowest order within its share of order_tol (a
+   relative L2 force budget, shared by the pairs through the RMS force of the
+   previous evaluation; the first evaluation of a system runs at p).  With
+   judge_samples > 0 every learned-order evaluation is checked on that many
+   targets against the FP64 direct sum and, if their relative L2 error
+   exceeds judge_budget, evaluated again at fixed p (fmm_stats.order_fallbacks). */
+enum {
+  FMM_ORDER_FIXED = 0,
+  FMM_ORDER_GEOMETRIC = 1,
+  FMM_ORDER_LEARNED = 2
+};
+
+/* The order model: a 32 -> 64 -> 64 -> 9 MLP (ReLU), weights used in BF16. */
+#define FMM_ORDER_NPARAM 7312
+#define FMM_ORDER_NFEAT 32
+#define FMM_ORDER_NOUT 9
+
 /* M2L arithmetic. */
 enum {
   FMM_M2L_FP32 = 0,  /* SIMT FP32 batched contraction (plain GPU FMM) */
@@ -84,7 +106,12 @@ typedef struct fmm_config {
   int32_t direct_max; /* interaction-list pairs (target, source) with n_target * n_source <= direct_max
                          are summed directly (exactly) instead of through M2L; 0 = every pair by M2L
                          as in the reference; -1 = automatic */
-  int32_t reserved[6];
+  int32_t order_mode; /* FMM_ORDER_*: expansion order of each M2L pair (tensor-core mode only) */
+  int32_t order_margin; /* FMM_ORDER_GEOMETRIC: orders added to each reduced pair order */
+  float order_tol;      /* FMM_ORDER_LEARNED: relative L2 force budget of the reduced orders (default 5e-7) */
+  int32_t judge_samples;/* FMM_ORDER_LEARNED: targets checked against the FP64 direct sum (0 = no check) */
+  float judge_budget;   /* FMM_ORDER_LEARNED: relative L2 error above which the evaluation is redone at p */
+  int32_t reserved[1];
 } fmm_config;
 
 typedef struct fmm_stats {
@@ -104,7 +131,8 @@ typedef struct fmm_stats {
   double ms_far_direct;     /* the direct far field part of ms_p2p */
   int64_t far_direct_pairs; /* the direct far field part of p2p_pairs */
   int64_t direct_max;       /* the direct-pair threshold the pass used */
-  double reserved[2];
+  double judge_rel_l2;      /* FMM_ORDER_LEARNED with judge_samples: the checked relative L2 error */
+  int64_t order_fallbacks;  /* FMM_ORDER_LEARNED: 1 if the judge sent the evaluation back to fixed p */
 } fmm_stats;
 
 typedef struct fmm_ctx fmm_ctx;
@@ -193,6 +221,26 @@ FMM_API int fmm_last_stats(fmm_ctx *ctx, fmm_stats *out);
 /* Number of kernel launches the library issued since the context was
  * created (all entry points). */
 FMM_API int64_t fmm_launch_count(fmm_ctx *ctx);
+
+/* Learned pair orders.  Parameters are FMM_ORDER_NPARAM floats (host). */
+FMM_API int fmm_order_set_model(fmm_ctx *ctx, const float *params, int32_t nparams);
+FMM_API int fmm_order_get_model(fmm_ctx *ctx, float *params, int32_t nparams);
+/* One force evaluation (fixed p; 3D, FMM_M2L_TC) that samples npairs of its
+   M2L pairs and writes their features (d_feat, npairs x FMM_ORDER_NFEAT) and
+   the base-10 logarithms of their FP64 truncation errors at orders 4..12
+   over the pair's monopole scale (d_labels, npairs x FMM_ORDER_NOUT).  Rows
+   where the draw found no pair are all zero.  Device buffers; synchronous. */
+FMM_API int fmm_order_collect(fmm_ctx *ctx, int64_t n, const double *d_pos, const double *d_mass, int32_t npairs,
+                              uint64_t seed, float *d_feat, float *d_labels, void *stream);
+/* Trains the context's model in place on the GPU (Adam, mean squared error
+   of the predicted logarithms; device data, rows used in order);
+   loss_out (host, epochs floats) receives the mean loss of each epoch. */
+FMM_API int fmm_order_train(fmm_ctx *ctx, const float *d_feat, const float *d_labels, int32_t n, int32_t epochs,
+                            int32_t batch, float lr, float *loss_out);
+/* Predictions (n x FMM_ORDER_NOUT), the mean squared error and its gradient
+   with respect to the parameters, for n rows (device buffers). */
+FMM_API int fmm_order_forward_grad(const float *d_feat, const float *d_labels, int32_t n, const float *d_params,
+                                   float *d_pred, float *d_grad, float *d_loss, void *stream);
 
 #ifdef __cplusplus
 }

@@ -1,5 +1,6 @@
 // Expansion passes (P2M, M2M, M2L, L2L, L2P) and the near field.
 #pragma once
+#include "order.cuh"
 #include "tree.cuh"
 
 namespace fmm {
@@ -14,6 +15,7 @@ struct OpTables {
   int n_m2l = 0, off_m2m = 0, off_l2l = 0, n_slots = 0;
   DevBuf<float> tab;        // n_slots * K * KP
   DevBuf<double> scratch;   // FP64 staging
+  DevBuf<double> tab64;     // FP64 copy of the 3D M2L operators (training-pair probe only)
 };
 
 struct ExpBuffers {
@@ -27,7 +29,11 @@ struct ExpBuffers {
   DevBuf<float4> lvl_off;
   DevBuf<int> m2l_src, m2l_list, m2l_nslots, m2l_tslot;  // per M2L batch: resolved sources and present slots
   DevBuf<uint16_t> tc_img;
-  DevBuf<unsigned int> tc_work;  // zeroed work counters of the tensor-core launches  // BF16 split operator images for the tensor-core M2L  // particle offsets from their level-d ancestor (direct far field)
+  DevBuf<unsigned int> tc_work;  // zeroed work counters of the tensor-core launches
+  DevBuf<uint8_t> order_p16;     // per M2L operator slot: padded width of its pair order
+  DevBuf<uint8_t> m2l_w;         // per M2L batch and present slot: padded width of its order
+  DevBuf<float> cf;              // learned orders: per-cell features (ORD_CF floats per cell)
+  DevBuf<double> frms;           // learned orders: [0] F_rms of the previous pass (G = 1), [1] scratch  // BF16 split operator images for the tensor-core M2L  // particle offsets from their level-d ancestor (direct far field)
 };
 
 // Per-pass parameters.
@@ -35,12 +41,29 @@ struct PassGeom {
   double lo[3], ext[3], emax;
 };
 
-int build_op_tables(OpTables &ops, int dim, int p, int depth, const PassGeom &g, cudaStream_t st, int64_t &launches);
+int build_op_tables(OpTables &ops, int dim, int p, int depth, const PassGeom &g, cudaStream_t st, int64_t &launches,
+                    bool want64 = false);
+
+// Learned-order settings of a pass, and the training-pair collection hook.
+struct OrderOpts {
+  int mode = 0;            // FMM_ORDER_*
+  int margin = 1;          // FMM_ORDER_GEOMETRIC
+  float tol = 5e-7f;       // FMM_ORDER_LEARNED: relative error budget of the truncation
+  const float *params = nullptr;  // FMM_ORDER_LEARNED: MLP parameters
+  // collection (nullptr: none): sample `npairs` M2L pairs, write their
+  // features and FP64 error labels
+  int npairs = 0;
+  unsigned long long seed = 0;
+  int *pairs = nullptr;
+  float *feat = nullptr, *labels = nullptr;
+  const double *pos = nullptr, *mass = nullptr;  // FP64 inputs for the probe
+  OrderGeom geom{};
+};
 void upload_class_tables();
 
 int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, const double *d_pos,
                    const double *d_mass, int p, double eps2, double G,
-                   const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, int64_t direct_max, cudaStream_t st,
-                   fmm_stats &stats, cudaEvent_t *ev);
+                   const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, int64_t direct_max,
+                   const OrderOpts &order, cudaStream_t st, fmm_stats &stats, cudaEvent_t *ev);
 
 }  // namespace fmm

@@ -1,4 +1,5 @@
 // C ABI of libfmmgpu.so (declared in include/fmm_gpu.h).
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -31,6 +32,14 @@ struct fmm_ctx {
   ExpBuffers eb;
   DevBuf<double> d_pos, d_mass, d_acc, d_pot, d_vel, d_x0, d_v0, d_xs, d_vs, d_asum, d_vsum;
   DevBuf<int64_t> d_targets;
+  // learned pair orders
+  DevBuf<float> order_params;
+  bool has_model = false;
+  int64_t frms_n = -1;         // system size the cached F_rms belongs to
+  DevBuf<int64_t> judge_tg;    // judge targets of (judge_n, judge_k)
+  DevBuf<double> judge_ref, judge_sum;
+  int64_t judge_n = -1, judge_k = -1;
+  DevBuf<int> col_pairs;
   fmm_stats stats;
   cudaEvent_t ev[7] = {};  // pass boundaries; ev[6] ends the direct far field
   bool timing_pending = false;
@@ -48,6 +57,14 @@ static int check_cfg(const fmm_config *c) {
   if (c->direct_max < -1) return FMM_ERR_INVALID_ARGUMENT;
   if (c->m2l_mode == FMM_M2L_TC && (c->dim == 3 ? (c->p + 1) * (c->p + 1) : 2 * c->p + 1) > TC_MAX_P16)
     return FMM_ERR_UNSUPPORTED;  // tensor-core tiles hold K <= 176 (p <= 12 in 3D)
+  if (c->order_mode != FMM_ORDER_FIXED && c->order_mode != FMM_ORDER_GEOMETRIC && c->order_mode != FMM_ORDER_LEARNED)
+    return FMM_ERR_INVALID_ARGUMENT;
+  if (c->order_mode == FMM_ORDER_LEARNED && c->dim != 3) return FMM_ERR_UNSUPPORTED;
+  if (c->order_mode == FMM_ORDER_LEARNED && !(c->order_tol > 0.f)) return FMM_ERR_INVALID_ARGUMENT;
+  if (c->judge_samples < 0 || !(c->judge_budget > 0.f)) return FMM_ERR_INVALID_ARGUMENT;
+  if (c->order_mode != FMM_ORDER_FIXED && c->m2l_mode != FMM_M2L_TC)
+    return FMM_ERR_UNSUPPORTED;  // per-pair orders live in the tensor-core kernel; the plain FMM is fixed-p
+  if (c->order_margin < 0 || c->order_margin > FMM_MAX_P) return FMM_ERR_INVALID_ARGUMENT;
   return FMM_OK;
 }
 
@@ -82,6 +99,11 @@ int fmm_config_default(fmm_config *cfg) {
   cfg->G = 1.0;
   cfg->device = 0;
   cfg->direct_max = -1;
+  cfg->order_mode = FMM_ORDER_FIXED;
+  cfg->order_margin = 1;
+  cfg->order_tol = 5e-7f;
+  cfg->judge_samples = 0;
+  cfg->judge_budget = 1e-6f;
   return FMM_OK;
 }
 
@@ -137,6 +159,16 @@ int fmm_destroy(fmm_ctx *c) {
   c->eb.m2l_tslot.release();
   c->eb.tc_img.release();
   c->eb.tc_work.release();
+  c->eb.order_p16.release();
+  c->eb.m2l_w.release();
+  c->eb.cf.release();
+  c->eb.frms.release();
+  c->ops.tab64.release();
+  c->order_params.release();
+  c->judge_tg.release();
+  c->judge_ref.release();
+  c->judge_sum.release();
+  c->col_pairs.release();
   for (auto *b : {&c->d_pos, &c->d_mass, &c->d_acc, &c->d_pot, &c->d_vel, &c->d_x0, &c->d_v0, &c->d_xs, &c->d_vs,
                   &c->d_asum, &c->d_vsum})
     b->release();
@@ -159,12 +191,10 @@ static int64_t direct_threshold(const fmm_config &c) {
   return std::max<int64_t>(8, (int64_t)(2.0 * K * K / 20.0 / 2.5));
 }
 
-static int evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass, double *d_acc,
-                           double *d_pot, cudaStream_t st) {
+// One force pass: tree, operators, expansions, near field.
+static int pass(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass, double *d_acc, double *d_pot,
+                cudaStream_t st, const OrderOpts &oo, bool want64) {
   const int dim = c->cfg.dim;
-  if (n < 0 || n > (int64_t)INT32_MAX) return FMM_ERR_INVALID_ARGUMENT;
-  if (n == 0) return FMM_OK;
-  if (!d_pos || !d_mass || !d_acc) return FMM_ERR_INVALID_ARGUMENT;
   CUDA_TRY(cudaEventRecord(c->ev[0], st));
   int rc = build_tree(c->ws, c->tree, d_pos, d_mass, n, dim, c->cfg.leaf_cap, st);
   if (rc) return rc;
@@ -177,11 +207,15 @@ static int evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const dou
     g.ext[d] = d < dim ? c->tree.hi[d] - c->tree.lo[d] : 0.0;
     g.emax = std::max(g.emax, g.ext[d]);
   }
-  rc = build_op_tables(c->ops, dim, c->cfg.p, c->tree.depth, g, st, c->ws.launches);
+  rc = build_op_tables(c->ops, dim, c->cfg.p, c->tree.depth, g, st, c->ws.launches, want64);
   if (rc) return rc;
+  const double jr = c->stats.judge_rel_l2;
+  const int64_t fb = c->stats.order_fallbacks;
   memset(&c->stats, 0, sizeof(c->stats));
+  c->stats.judge_rel_l2 = jr;
+  c->stats.order_fallbacks = fb;
   rc = run_fmm_passes(c->ws, c->tree, c->ops, c->eb, d_pos, d_mass, c->cfg.p, c->cfg.eps2, c->cfg.G, g, d_acc, d_pot,
-                      c->cfg.m2l_mode, direct_threshold(c->cfg), st, c->stats, c->ev);
+                      c->cfg.m2l_mode, direct_threshold(c->cfg), oo, st, c->stats, c->ev);
   c->stats.direct_max = direct_threshold(c->cfg);
   if (rc) return rc;
   if (!c->ws.ok) return FMM_ERR_OUT_OF_MEMORY;
@@ -192,12 +226,80 @@ static int evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const dou
   return FMM_OK;
 }
 
+// Relative L2 error of d_acc on judge_samples targets against the FP64
+// direct sum (synchronous).
+static int judge(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass, const double *d_acc,
+                 cudaStream_t st, double &rel) {
+  const int dim = c->cfg.dim;
+  const int64_t k = std::min<int64_t>(c->cfg.judge_samples, n);
+  if (c->judge_n != n || c->judge_k != k) {
+    std::vector<int64_t> tg(k);
+    for (int64_t i = 0; i < k; ++i) tg[i] = (int64_t)(((double)i + 0.5) * (double)n / (double)k);
+    if (!c->judge_tg.reserve(k) || !c->judge_ref.reserve((size_t)k * dim) || !c->judge_sum.reserve(2))
+      return FMM_ERR_OUT_OF_MEMORY;
+    CUDA_TRY(cudaMemcpyAsync(c->judge_tg.ptr, tg.data(), sizeof(int64_t) * k, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    c->judge_n = n;
+    c->judge_k = k;
+  }
+  int rc = direct_sum(d_pos, d_mass, n, c->judge_tg.ptr, k, dim, c->cfg.eps2, FMM_SOFT_PLUMMER, c->cfg.G,
+                      c->judge_ref.ptr, nullptr, st, c->ws.launches);
+  if (rc) return rc;
+  rc = order_judge_compare(d_acc, c->judge_ref.ptr, c->judge_tg.ptr, k, dim, c->judge_sum.ptr, st, c->ws.launches);
+  if (rc) return rc;
+  double h[2] = {0.0, 0.0};
+  CUDA_TRY(cudaMemcpyAsync(h, c->judge_sum.ptr, sizeof(h), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  rel = h[1] > 0.0 ? std::sqrt(h[0] / h[1]) : 0.0;
+  return FMM_OK;
+}
+
+static int evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass, double *d_acc,
+                           double *d_pot, cudaStream_t st) {
+  if (n < 0 || n > (int64_t)INT32_MAX) return FMM_ERR_INVALID_ARGUMENT;
+  if (n == 0) return FMM_OK;
+  if (!d_pos || !d_mass || !d_acc) return FMM_ERR_INVALID_ARGUMENT;
+  OrderOpts oo;
+  oo.mode = c->cfg.order_mode;
+  oo.margin = c->cfg.order_margin;
+  oo.tol = c->cfg.order_tol;
+  const bool learned = c->cfg.order_mode == FMM_ORDER_LEARNED && c->cfg.m2l_mode == FMM_M2L_TC;
+  c->stats.judge_rel_l2 = 0.0;
+  c->stats.order_fallbacks = 0;
+  if (learned) {
+    if (!c->has_model) return FMM_ERR_INVALID_ARGUMENT;  // no order model set
+    oo.params = c->order_params.ptr;
+    if (!c->eb.frms.reserve(2)) return FMM_ERR_OUT_OF_MEMORY;
+    if (c->frms_n != n) {  // a new system: its first evaluation runs at fixed p
+      CUDA_TRY(cudaMemsetAsync(c->eb.frms.ptr, 0, 2 * sizeof(double), st));
+      c->frms_n = n;
+    }
+  }
+  int rc = pass(c, n, d_pos, d_mass, d_acc, d_pot, st, oo, false);
+  if (rc) return rc;
+  if (!learned) return FMM_OK;
+  if (c->cfg.judge_samples > 0) {
+    double rel = 0.0;
+    rc = judge(c, n, d_pos, d_mass, d_acc, st, rel);
+    if (rc) return rc;
+    c->stats.judge_rel_l2 = rel;
+    if (rel > c->cfg.judge_budget) {  // the judge rejects the reduced orders: fixed p
+      OrderOpts fx;
+      rc = pass(c, n, d_pos, d_mass, d_acc, d_pot, st, fx, false);
+      if (rc) return rc;
+      c->stats.order_fallbacks = 1;
+    }
+  }
+  // the RMS force the next evaluation budgets with
+  return order_force_rms(d_acc, n, c->cfg.dim, c->cfg.G, c->eb.frms.ptr + 1, c->eb.frms.ptr, st, c->ws.launches);
+}
+
 static int finish(fmm_ctx *c, cudaStream_t st) {
   CUDA_TRY(cudaStreamSynchronize(st));
   unsigned int herr = 0;
   CUDA_TRY(cudaMemcpy(&herr, c->ws.dev_err, sizeof(herr), cudaMemcpyDeviceToHost));
   if (c->timing_pending) {
-    unsigned long long cnt[4] = {0, 0, 0, 0};
+    unsigned long long cnt[4] = {0, 0, 0, 0};  // [4] (sum of n_T) stays on the device
     CUDA_TRY(cudaMemcpy(cnt, c->ws.counters, sizeof(cnt), cudaMemcpyDeviceToHost));
     c->stats.m2l_pairs = (int64_t)cnt[0];
     c->stats.p2p_pairs = (int64_t)(cnt[1] + cnt[3]);
@@ -453,5 +555,68 @@ int fmm_last_stats(fmm_ctx *c, fmm_stats *out) {
 }
 
 int64_t fmm_launch_count(fmm_ctx *c) { return c ? c->ws.launches : -1; }
+
+
+int fmm_order_set_model(fmm_ctx *c, const float *params, int32_t nparams) {
+  if (!c || !params || nparams != FMM_ORDER_NPARAM) return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  for (int i = 0; i < nparams; ++i)
+    if (!std::isfinite(params[i])) return FMM_ERR_INVALID_ARGUMENT;
+  if (!c->order_params.reserve(ORD_NPARAM)) return FMM_ERR_OUT_OF_MEMORY;
+  CUDA_TRY(cudaMemcpyAsync(c->order_params.ptr, params, sizeof(float) * ORD_NPARAM, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->has_model = true;
+  return FMM_OK;
+}
+
+int fmm_order_get_model(fmm_ctx *c, float *params, int32_t nparams) {
+  if (!c || !params || nparams != FMM_ORDER_NPARAM) return FMM_ERR_INVALID_ARGUMENT;
+  if (!c->has_model) return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  CUDA_TRY(cudaMemcpyAsync(params, c->order_params.ptr, sizeof(float) * ORD_NPARAM, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return FMM_OK;
+}
+
+int fmm_order_collect(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass, int32_t npairs,
+                      uint64_t seed, float *d_feat, float *d_labels, void *stream) {
+  if (!c || n <= 0 || n > (int64_t)INT32_MAX || npairs <= 0 || !d_pos || !d_mass || !d_feat || !d_labels)
+    return FMM_ERR_INVALID_ARGUMENT;
+  if (c->cfg.dim != 3 || c->cfg.m2l_mode != FMM_M2L_TC) return FMM_ERR_UNSUPPORTED;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  if (!c->col_pairs.reserve((size_t)npairs * 4) || !c->d_acc.reserve((size_t)n * 3)) return FMM_ERR_OUT_OF_MEMORY;
+  CUDA_TRY(cudaMemsetAsync(d_feat, 0, sizeof(float) * (size_t)npairs * ORD_NF, st));
+  CUDA_TRY(cudaMemsetAsync(d_labels, 0, sizeof(float) * (size_t)npairs * ORD_NQ, st));
+  OrderOpts oo;  // fixed order; collection hook on
+  oo.npairs = npairs;
+  oo.seed = seed;
+  oo.pairs = c->col_pairs.ptr;
+  oo.feat = d_feat;
+  oo.labels = d_labels;
+  int rc = pass(c, n, d_pos, d_mass, c->d_acc.ptr, nullptr, st, oo, true);
+  if (rc) return rc;
+  return finish(c, st);
+}
+
+int fmm_order_train(fmm_ctx *c, const float *d_feat, const float *d_labels, int32_t n, int32_t epochs, int32_t batch,
+                    float lr, float *loss_out) {
+  if (!c || !d_feat || !d_labels || n <= 0 || epochs <= 0 || batch <= 0 || !(lr > 0.f) || !loss_out)
+    return FMM_ERR_INVALID_ARGUMENT;
+  if (!c->has_model) return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  return order_train(d_feat, d_labels, n, epochs, batch, lr, c->order_params.ptr, loss_out, c->stream, c->ws.launches);
+}
+
+int fmm_order_forward_grad(const float *d_feat, const float *d_labels, int32_t n, const float *d_params, float *d_pred,
+                           float *d_grad, float *d_loss, void *stream) {
+  if (!d_feat || !d_labels || n <= 0 || !d_params || !d_grad || !d_loss) return FMM_ERR_INVALID_ARGUMENT;
+  int64_t launches = 0;
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = order_forward_grad(d_feat, d_labels, n, d_params, d_pred, d_grad, d_loss, st, launches);
+  if (rc) return rc;
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return FMM_OK;
+}
 
 }  // extern "C"

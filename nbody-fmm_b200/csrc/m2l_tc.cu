@@ -138,6 +138,10 @@ __device__ inline void bulk_load(void *dst, const void *src, uint32_t bytes, uin
       : "memory");
 }
 
+__device__ inline void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ inline void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accum) {
   asm volatile(
       "{\n\t"
@@ -185,7 +189,6 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
   constexpr int N0 = tc_n0(P16);
   constexpr int N1 = P16 - N0;
   constexpr int KC = P16 / 8;       // 16-byte K chunks
-  constexpr int KSTEPS = P16 / 16;  // MMA K steps
   constexpr int ASPLIT = TC_M * P16;
   constexpr int BTILE = P16 * N0;
   constexpr int TILES = 3 * NT;  // operator copies per slot
@@ -199,6 +202,7 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
   __shared__ __align__(8) uint64_t s_full[2], s_mma[2], s_done;
   __shared__ uint32_t s_tmem;
   __shared__ int s_slot[2][TC_MAX_SLOTS], s_op[2][TC_MAX_SLOTS];
+  __shared__ uint8_t s_w[2][TC_MAX_SLOTS];  // padded width of each slot's order
   __shared__ int s_n[2], s_b[2];
   __shared__ int s_grab;
 
@@ -228,11 +232,13 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
         for (int i = tid; i < n; i += TC_M) {
           s_slot[buf][i] = a.slot_list[tb + i];
           s_op[buf][i] = a.tslot_list[tb + i];
+          s_w[buf][i] = a.slot_p16 ? a.slot_p16[tb + i] : (uint8_t)P16;
         }
       } else {
         if (tid == 0) {
           s_slot[buf][0] = 0;
           s_op[buf][0] = a.op_base + bt.w;
+          s_w[buf][0] = (uint8_t)P16;
         }
         n = bt.y > 0 ? 1 : 0;
       }
@@ -274,32 +280,45 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
   int c = 0;
   long long t_cur = 0, t_nxt = (long long)s_n[0] * TILES, t_end = t_nxt + (long long)s_n[1] * TILES;
 
-  // operator copy g (splits in the order 2, 1, 0; output tiles 0, 1)
+  // operator copy g (splits in the order 2, 1, 0; output tiles 0, 1).  A
+  // slot of padded width w < P16 needs only the first w rows (k) of each
+  // tile, a contiguous prefix, and no second tile when w <= N0; an unneeded
+  // copy completes its barrier without data.
   auto load_tile = [&](long long g) {
     const int buf = g < t_nxt ? c : c ^ 1;
     const int i = (int)((g - (g < t_nxt ? t_cur : t_nxt)) / TILES), t = (int)(g % TILES);
     const int s = 2 - t / NT, j = t % NT;
-    const uint32_t bytes = (uint32_t)(P16 * (j ? N1 : N0) * 2);
+    const int w = s_w[buf][i];
+    if ((j ? w - N0 : w) <= 0) {
+      mbar_arrive(&s_full[g & 1]);
+      return;
+    }
+    const uint32_t bytes = (uint32_t)(w * (j ? N1 : N0) * 2);
     const uint16_t *src =
         a.bimg + (size_t)s_op[buf][i] * 3 * P16 * P16 + (size_t)s * P16 * P16 + (j ? (size_t)P16 * N0 : 0);
     bulk_load(Bs + (g & 1) * BTILE, src, bytes, &s_full[g & 1]);
   };
-  // the MMAs of operator copy g: B split s against A splits 2 - s .. 0
-  auto mma_tile = [&](long long g) {
+  // the MMAs of operator copy g for a slot of width w: B split s against A
+  // splits 2 - s .. 0, N = the tile's needed columns, w / 16 K steps
+  auto mma_tile = [&](long long g, int w) {
     const int t = (int)(g % TILES);
     const int s = 2 - t / NT, j = t % NT;
     const int nw = j ? N1 : N0;
-    const uint32_t idesc =
-        (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(nw >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
-    const uint32_t lbo_b = (uint32_t)(nw / 8) * 128;
-    const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs + (g & 1) * BTILE);
-    for (int sa = 2 - s; sa >= 0; --sa)
-      for (int ks = 0; ks < KSTEPS; ++ks) {
-        const uint64_t ad = smem_desc(a0 + (uint32_t)(sa * ASPLIT * 2) + ks * 2 * LBO_A, LBO_A, 128);
-        const uint64_t bd = smem_desc(b0 + ks * 2 * lbo_b, lbo_b, 128);
-        const uint32_t acc = (s == 2 && sa == 0 && ks == 0) ? 0u : 1u;
-        mma_bf16(tmem + (j ? (uint32_t)N0 : 0u), ad, bd, idesc, acc);
-      }
+    const int ncols = min(nw, j ? w - N0 : w);
+    if (ncols > 0) {
+      const uint32_t idesc =
+          (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(ncols >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
+      const uint32_t lbo_b = (uint32_t)(nw / 8) * 128;
+      const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs + (g & 1) * BTILE);
+      const int ksteps = w / 16;
+      for (int sa = 2 - s; sa >= 0; --sa)
+        for (int ks = 0; ks < ksteps; ++ks) {
+          const uint64_t ad = smem_desc(a0 + (uint32_t)(sa * ASPLIT * 2) + ks * 2 * LBO_A, LBO_A, 128);
+          const uint64_t bd = smem_desc(b0 + ks * 2 * lbo_b, lbo_b, 128);
+          const uint32_t acc = (s == 2 && sa == 0 && ks == 0) ? 0u : 1u;
+          mma_bf16(tmem + (j ? (uint32_t)N0 : 0u), ad, bd, idesc, acc);
+        }
+    }
     mma_commit(&s_mma[g & 1]);
   };
 
@@ -364,7 +383,7 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
             break;
           }
           nwait = g + 1;
-          mma_tile(g);
+          mma_tile(g, s_w[c][j]);
           if (nl == g + 1 && nl < t_end && g >= 1) {  // the buffer of copy g - 1 takes copy g + 1
             if (!mbar_wait(&s_mma[(g - 1) & 1], (uint32_t)(((g - 1) >> 1) & 1))) {
               ok = false;
@@ -381,20 +400,26 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
       if (!wd) ok = false;
       tc_fence_after();
       if (wd) {
+        const int w = s_w[c][j];  // D holds the slot's first w columns
 #pragma unroll
         for (int c0 = 0; c0 < P16; c0 += 16) {
-          uint32_t d[16];
-          tmem_ld16(tmem + lane_off + (uint32_t)c0, d);
-          if (j > 0) {
-            uint32_t r[16];
-            tmem_ld16(tmem + lane_off + RCOL + (uint32_t)c0, r);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          if (c0 < w) {
+            uint32_t d[16];
+            tmem_ld16(tmem + lane_off + (uint32_t)c0, d);
+            if (j > 0) {
+              uint32_t r[16];
+              tmem_ld16(tmem + lane_off + RCOL + (uint32_t)c0, r);
+              asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-            for (int e = 0; e < 16; ++e) d[e] = __float_as_uint(__uint_as_float(d[e]) + __uint_as_float(r[e]));
-          } else {
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+              for (int e = 0; e < 16; ++e) d[e] = __float_as_uint(__uint_as_float(d[e]) + __uint_as_float(r[e]));
+            } else {
+              asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            }
+            tmem_st16(tmem + lane_off + RCOL + (uint32_t)c0, d);
+          } else if (j == 0) {
+            const uint32_t z[16] = {};
+            tmem_st16(tmem + lane_off + RCOL + (uint32_t)c0, z);
           }
-          tmem_st16(tmem + lane_off + RCOL + (uint32_t)c0, d);
         }
         asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
       }

@@ -18,6 +18,8 @@ struct TcArgs {
   const int *slot_list;     // M2L: [batch][i] present slots
   const int *tslot_list;    // M2L: [batch][i] operator-table slot of each present slot
   const int *nslots;        // M2L: [batch]
+  const uint8_t *slot_p16;  // M2L: [batch][i] padded width (16 * ceil(K_i / 16)) of each present slot's
+                            // order, null = every slot at full order
   const int *cchild;        // children of each cell (nchild per cell, -1 if absent)
   const int *cparent;       // parent of each cell (M2M destination, L2L source)
   int nchild;               // 8 in 3D, 4 in 2D

@@ -102,7 +102,8 @@ __device__ inline cd op_coef(int kind, const cd *H, int k, int l, int n, int mp)
 }
 
 // One block per slot.  Builds K x KP (input-major) FP32 matrix.
-__global__ void k_build_ops3d(float *tab, int p, int K, int KP, int n_m2l, double ax, double ay, double az) {
+__global__ void k_build_ops3d(float *tab, double *tab64, int p, int K, int KP, int n_m2l, double ax, double ay,
+                              double az) {
   extern __shared__ cd H[];
   const int slot = blockIdx.x;
   int kind;
@@ -153,6 +154,7 @@ __global__ void k_build_ops3d(float *tab, int p, int K, int KP, int n_m2l, doubl
       }
     }
     T[e] = (float)val;
+    if (tab64 && slot < n_m2l) tab64[(size_t)slot * K * KP + e] = val;
   }
 }
 
@@ -253,7 +255,8 @@ __global__ void k_build_ops2d(float *tab, int p, int K, int KP, int n_m2l, doubl
   }
 }
 
-int build_op_tables(OpTables &ops, int dim, int p, int depth, const PassGeom &g, cudaStream_t st, int64_t &launches) {
+int build_op_tables(OpTables &ops, int dim, int p, int depth, const PassGeom &g, cudaStream_t st, int64_t &launches,
+                    bool want64) {
   int K = dim == 3 ? (p + 1) * (p + 1) : 2 * p + 1;
   int KP = 32 * ((K + 31) / 32);
   int KS = (K + 3) & ~3;
@@ -271,7 +274,12 @@ int build_op_tables(OpTables &ops, int dim, int p, int depth, const PassGeom &g,
   double a[3] = {g.ext[0] / emax, g.ext[1] / emax, dim == 3 ? g.ext[2] / emax : 0.0};
   if (dim == 3) {
     size_t sh = sizeof(double) * 2 * (size_t)(2 * p + 1) * (2 * p + 2) / 2;
-    k_build_ops3d<<<ops.n_slots, 256, sh, st>>>(ops.tab.ptr, p, K, KP, ops.n_m2l, a[0], a[1], a[2]);
+    double *t64 = nullptr;
+    if (want64) {
+      if (!ops.tab64.reserve((size_t)ops.n_m2l * K * KP)) return FMM_ERR_OUT_OF_MEMORY;
+      t64 = ops.tab64.ptr;
+    }
+    k_build_ops3d<<<ops.n_slots, 256, sh, st>>>(ops.tab.ptr, t64, p, K, KP, ops.n_m2l, a[0], a[1], a[2]);
   } else {
     k_build_ops2d<<<ops.n_slots, 256, 0, st>>>(ops.tab.ptr, p, K, KP, ops.n_m2l, a[0], a[1], std::log(emax));
   }

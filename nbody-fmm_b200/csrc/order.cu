@@ -1,0 +1,663 @@
+// Learned expansion order of each M2L pair: cell and pair features, the FP64
+// error probe that labels training pairs, the MLP (forward, backward, Adam)
+// and the hot-path inference that sets each M2L tile's order.
+//
+// MLP: 32 inputs -> 64 -> 64 -> 9, ReLU, weights and activations rounded to
+// BF16 (round to nearest) before every product, FP32 accumulation, FP32
+// biases; the FP32 master weights take the gradients (straight-through).
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "order.cuh"
+
+namespace fmm {
+
+__device__ inline float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+// ---------------------------------------------------------------- features
+__global__ void k_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int cell0,
+                                int p, int KS, float *cf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int c = first + i;
+  const float *m = M + (size_t)(c - cell0) * KS;
+  float *o = cf + (size_t)(c - cell0) * ORD_CF;
+  const float m0 = fabsf(m[0]);
+  o[0] = log2f(1.f + (float)(pend[c] - pbeg[c]));
+  for (int n = 1; n <= 12; ++n) {
+    float v = -30.f;
+    if (n <= p && m0 > 0.f) {
+      float s = m[re_idx(n, 0)] * m[re_idx(n, 0)];
+      for (int k = 1; k <= n; ++k) s += 2.f * (m[re_idx(n, k)] * m[re_idx(n, k)] + m[im_idx(n, k)] * m[im_idx(n, k)]);
+      v = s > 0.f ? fmaxf(log10f(sqrtf(s) / m0), -30.f) : -30.f;
+    }
+    o[n] = v;
+  }
+  for (int k = 13; k < ORD_CF; ++k) o[k] = 0.f;
+}
+
+// Features of pair (T, S) with source offset (dx, dy, dz) cells at `level`.
+__device__ inline void pair_features(const float *cfT, const float *cfS, int level, int dx, int dy, int dz, float ax,
+                                     float ay, float az, float *f) {
+  f[0] = level * (1.f / 16.f);
+  f[1] = cfT[0] * 0.125f;
+  f[2] = cfS[0] * 0.125f;
+  for (int k = 0; k < 12; ++k) f[3 + k] = cfS[1 + k] * 0.25f;
+  f[15] = cfT[1] * 0.25f;
+  f[16] = cfT[2] * 0.25f;
+  float e0 = fabsf((float)dx) * ax, e1 = fabsf((float)dy) * ay, e2 = fabsf((float)dz) * az;
+  const float R = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
+  f[17] = R * 0.25f;
+  if (e0 < e1) { const float t = e0; e0 = e1; e1 = t; }
+  if (e1 < e2) { const float t = e1; e1 = e2; e2 = t; }
+  if (e0 < e1) { const float t = e0; e0 = e1; e1 = t; }
+  f[18] = e0 * (1.f / 3.f);
+  f[19] = e1 * (1.f / 3.f);
+  f[20] = e2 * (1.f / 3.f);
+  const float diag = sqrtf(ax * ax + ay * ay + az * az);
+  f[21] = R > 0.f ? log10f(diag / R) : 0.f;
+  for (int k = 22; k < ORD_NF; ++k) f[k] = 0.f;
+}
+
+__device__ inline unsigned long long splitmix(unsigned long long x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+__global__ void k_order_sample(const int4 *batches, const int *tlist, const int *src_tab, const int *slot_list,
+                               const int *tslot_list, const int *nslots, int nbm, const int *pbeg, const int *pend,
+                               int n, unsigned long long seed, int max_nt, int max_ns, int4 *pairs) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const unsigned long long h = splitmix(seed * 0x100000001B3ull + (unsigned long long)k);
+  int4 out = make_int4(-1, -1, -1, -1);
+  const int b = (int)(h % (unsigned long long)nbm);
+  const int ns = nslots[b];
+  if (ns > 0) {
+    const int i = (int)((h >> 20) % (unsigned long long)ns);
+    const size_t base = (size_t)b * 189;
+    const int sl = slot_list[base + i];
+    const int4 bt = batches[b];
+    const int t = (int)((h >> 40) % (unsigned long long)bt.y);
+    const int T = tlist[bt.x + t];
+    const int S = src_tab[(base + sl) * 128 + t];
+    if (S >= 0 && pend[T] - pbeg[T] <= max_nt && pend[S] - pbeg[S] <= max_ns)
+      out = make_int4(T, S, tslot_list[base + i], bt.z);
+  }
+  pairs[k] = out;
+}
+
+__global__ void k_pair_features(const int4 *pairs, int n, const float *cf, int cell0, float ax, float ay, float az,
+                                float *feat) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  float f[ORD_NF];
+  const int4 pr = pairs[k];
+  if (pr.x < 0) {
+    for (int i = 0; i < ORD_NF; ++i) f[i] = 0.f;
+  } else {
+    const int o = pr.z;
+    pair_features(cf + (size_t)(pr.x - cell0) * ORD_CF, cf + (size_t)(pr.y - cell0) * ORD_CF, pr.w, o % 7 - 3,
+                  (o / 7) % 7 - 3, o / 49 - 3, ax, ay, az, f);
+  }
+  for (int i = 0; i < ORD_NF; ++i) feat[(size_t)k * ORD_NF + i] = f[i];
+}
+
+// ---------------------------------------------------------------- FP64 probe
+__device__ inline void lget_d(const double *L, int n, int m, double &re, double &im) {
+  if (m > n) {
+    re = im = 0.0;
+  } else if (m >= 0) {
+    re = L[re_idx(n, m)];
+    im = m ? L[im_idx(n, m)] : 0.0;
+  } else {  // L_n^-1 = -conj(L_n^1)
+    re = -L[re_idx(n, 1)];
+    im = L[im_idx(n, 1)];
+  }
+}
+
+// Gradient of the order-q local expansion L^ (scaled units) at x: the same
+// recurrences of the scaled regular harmonics as the FP32 L2P, in FP64.
+__device__ void l2p_grad_d(const double *L, int q, double x, double y, double z, double &gx, double &gy,
+                           double &gz) {
+  const double r2 = x * x + y * y + z * z;
+  double dre = 1.0, dim = 0.0;
+  gx = gy = gz = 0.0;
+  for (int m = 0; m <= q; ++m) {
+    if (m > 0) {
+      const double h = -0.5 / m;
+      const double nre = h * (x * dre - y * dim), nim = h * (x * dim + y * dre);
+      dre = nre;
+      dim = nim;
+    }
+    const double wm = m ? 2.0 : 1.0;
+    double p1re = dre, p1im = dim, p2re = 0.0, p2im = 0.0;
+    for (int l = m; l < q; ++l) {
+      double cre, cim;
+      if (l == m) {
+        cre = dre;
+        cim = dim;
+      } else {
+        const double den = (double)(l * l - m * m);
+        const double a1 = (2.0 * l - 1.0) * z / den, a2 = r2 / den;
+        cre = a1 * p1re - a2 * p2re;
+        cim = a1 * p1im - a2 * p2im;
+        p2re = p1re;
+        p2im = p1im;
+        p1re = cre;
+        p1im = cim;
+      }
+      double Ar, Ai, Mr, Mi, Pr, Pi;
+      lget_d(L, l + 1, m, Ar, Ai);
+      lget_d(L, l + 1, m - 1, Mr, Mi);
+      lget_d(L, l + 1, m + 1, Pr, Pi);
+      gz += wm * (Ar * cre - Ai * cim);
+      gx += wm * (0.5 * (Mr - Pr) * cre - 0.5 * (Mi - Pi) * cim);
+      gy += wm * 0.5 * ((Pr + Mr) * cim + (Pi + Mi) * cre);
+    }
+  }
+}
+
+static constexpr int PROBE_T = 256;
+static constexpr int PROBE_MAX_NT = 256;
+
+__global__ void __launch_bounds__(PROBE_T) k_probe(ProbeArgs a) {
+  extern __shared__ double sh[];
+  const int K = a.K;
+  double *Ms = sh;                              // [K]
+  double *Lq = Ms + K;                          // [ORD_NQ][K]
+  double *Fx = Lq + ORD_NQ * K;                 // [PROBE_MAX_NT][3]
+  double *e2 = Fx + 3 * PROBE_MAX_NT;           // [ORD_NQ]
+  double *wpart = e2 + ORD_NQ;                  // [8][K] per-warp P2M partials
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int4 pr = reinterpret_cast<const int4 *>(a.pairs)[blockIdx.x];
+  float *lab = a.labels + (size_t)blockIdx.x * ORD_NQ;
+  if (pr.x < 0) {
+    if (tid < ORD_NQ) lab[tid] = 0.f;
+    return;
+  }
+  const int T = pr.x, S = pr.y, d = pr.w;
+  const int tb = a.pbeg[T], nt = a.pend[T] - tb, sb = a.pbeg[S], nsrc = a.pend[S] - sb;
+  double cT[3], cS[3];
+  {
+    uint32_t q[3], r[3];
+    morton_decode(3, a.ckey[T], q[0], q[1], q[2]);
+    morton_decode(3, a.ckey[S], r[0], r[1], r[2]);
+    for (int k = 0; k < 3; ++k) {
+      const double sk = a.g.ext[k] * ldexp(1.0, -d);
+      cT[k] = a.g.lo[k] + (q[k] + 0.5) * sk;
+      cS[k] = a.g.lo[k] + (r[k] + 0.5) * sk;
+    }
+  }
+  const double s = a.g.emax * ldexp(1.0, -d), inv_s = 1.0 / s;
+  for (int i = tid; i < 8 * K; i += PROBE_T) wpart[i] = 0.0;
+  for (int i = tid; i < ORD_NQ; i += PROBE_T) e2[i] = 0.0;
+  __syncthreads();
+  // P2M in FP64 about c_S: M~_l^m = sum w conj(Rs_l^m((x - c_S) / s)), per-warp sums
+  for (int j0 = warp * 32; j0 < nsrc; j0 += PROBE_T) {
+    const int j = j0 + lane;
+    double x = 0.0, y = 0.0, z = 0.0, w = 0.0;
+    if (j < nsrc) {
+      const uint32_t o = a.perm[sb + j];
+      x = (a.pos[3 * (size_t)o] - cS[0]) * inv_s;
+      y = (a.pos[3 * (size_t)o + 1] - cS[1]) * inv_s;
+      z = (a.pos[3 * (size_t)o + 2] - cS[2]) * inv_s;
+      w = a.mass[o];
+    }
+    const double r2 = x * x + y * y + z * z;
+    double dre = 1.0, dim = 0.0;
+    for (int m = 0; m <= a.p; ++m) {
+      if (m > 0) {
+        const double h = -0.5 / m;
+        const double nre = h * (x * dre - y * dim), nim = h * (x * dim + y * dre);
+        dre = nre;
+        dim = nim;
+      }
+      double p1re = dre, p1im = dim, p2re = 0.0, p2im = 0.0;
+      for (int l = m; l <= a.p; ++l) {
+        double cre, cim;
+        if (l == m) {
+          cre = dre;
+          cim = dim;
+        } else {
+          const double den = (double)(l * l - m * m);
+          const double a1 = (2.0 * l - 1.0) * z / den, a2 = r2 / den;
+          cre = a1 * p1re - a2 * p2re;
+          cim = a1 * p1im - a2 * p2im;
+          p2re = p1re;
+          p2im = p1im;
+          p1re = cre;
+          p1im = cim;
+        }
+        double vr = w * cre, vi = -w * cim;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+          vr += __shfl_xor_sync(0xffffffffu, vr, o);
+          vi += __shfl_xor_sync(0xffffffffu, vi, o);
+        }
+        if (lane == 0) {
+          wpart[warp * K + re_idx(l, m)] += vr;
+          if (m) wpart[warp * K + im_idx(l, m)] += vi;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < K; i += PROBE_T) {
+    double v = 0.0;
+    for (int w = 0; w < 8; ++w) v += wpart[w * K + i];
+    Ms[i] = v;
+  }
+  __syncthreads();
+  // M2L at every order q: cumulative sums over the input degrees
+  const double *Tm = a.tab64 + (size_t)pr.z * K * a.KP;
+  for (int k = tid; k < K; k += PROBE_T) {
+    int dk = 0;
+    while ((dk + 1) * (dk + 1) <= k) ++dk;
+    double acc = 0.0;
+    for (int dn = 0; dn <= a.p; ++dn) {
+      for (int ni = dn * dn; ni < (dn + 1) * (dn + 1); ++ni) acc += Tm[(size_t)ni * a.KP + k] * Ms[ni];
+      if (dn >= ORD_QMIN && dn <= ORD_QMAX) Lq[(dn - ORD_QMIN) * K + k] = dk <= dn ? acc : 0.0;
+    }
+  }
+  // exact far field of S on the target particles (FP64)
+  const int ntc = min(nt, PROBE_MAX_NT);
+  for (int i = tid; i < ntc; i += PROBE_T) {
+    const uint32_t o = a.perm[tb + i];
+    const double xi = a.pos[3 * (size_t)o], yi = a.pos[3 * (size_t)o + 1], zi = a.pos[3 * (size_t)o + 2];
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    for (int j = 0; j < nsrc; ++j) {
+      const uint32_t u = a.perm[sb + j];
+      const double rx = xi - a.pos[3 * (size_t)u], ry = yi - a.pos[3 * (size_t)u + 1], rz = zi - a.pos[3 * (size_t)u + 2];
+      const double r2 = rx * rx + ry * ry + rz * rz;
+      const double inv = 1.0 / sqrt(r2);
+      const double w3 = a.mass[u] * inv * inv * inv;
+      fx -= rx * w3;
+      fy -= ry * w3;
+      fz -= rz * w3;
+    }
+    Fx[3 * i] = fx;
+    Fx[3 * i + 1] = fy;
+    Fx[3 * i + 2] = fz;
+  }
+  __syncthreads();
+  // truncated field at every order; squared error summed over the targets
+  const int qhi = min(a.p, ORD_QMAX);
+  const int nq = qhi - ORD_QMIN + 1;
+  for (int e = tid; e < ntc * nq; e += PROBE_T) {
+    const int i = e / nq, qi = e % nq;
+    const uint32_t o = a.perm[tb + i];
+    const double x = (a.pos[3 * (size_t)o] - cT[0]) * inv_s, y = (a.pos[3 * (size_t)o + 1] - cT[1]) * inv_s,
+                 z = (a.pos[3 * (size_t)o + 2] - cT[2]) * inv_s;
+    double gx, gy, gz;
+    l2p_grad_d(Lq + qi * K, ORD_QMIN + qi, x, y, z, gx, gy, gz);
+    const double s2 = inv_s * inv_s;
+    const double ex = gx * s2 - Fx[3 * i], ey = gy * s2 - Fx[3 * i + 1], ez = gz * s2 - Fx[3 * i + 2];
+    atomicAdd(&e2[qi], ex * ex + ey * ey + ez * ez);
+  }
+  __syncthreads();
+  if (tid < ORD_NQ) {
+    float v = 0.f;
+    if (tid < nq) {
+      double R2 = 0.0;
+      for (int k = 0; k < 3; ++k) R2 += (cS[k] - cT[k]) * (cS[k] - cT[k]);
+      const double scale = Ms[0] * sqrt((double)ntc) / R2;
+      const double rel = scale > 0.0 ? sqrt(e2[tid]) / scale : 0.0;
+      v = (float)log10(rel + 1e-30);
+    }
+    lab[tid] = v;
+  }
+}
+
+// ---------------------------------------------------------------- MLP
+// Forward pass of one row with parameters in shared memory (weights already
+// rounded to BF16).  h1, h2: BF16-rounded activations.
+__device__ inline void mlp_forward(const float *w, const float *x, float *h1, float *h2, float *y) {
+#pragma unroll 4
+  for (int j = 0; j < ORD_NH; ++j) {
+    float acc = w[ORD_B1 + j];
+#pragma unroll
+    for (int i = 0; i < ORD_NF; ++i) acc = fmaf(w[ORD_W1 + j * ORD_NF + i], x[i], acc);
+    h1[j] = bf16r(fmaxf(acc, 0.f));
+  }
+#pragma unroll 2
+  for (int j = 0; j < ORD_NH; ++j) {
+    float acc = w[ORD_B2 + j];
+#pragma unroll
+    for (int i = 0; i < ORD_NH; ++i) acc = fmaf(w[ORD_W2 + j * ORD_NH + i], h1[i], acc);
+    h2[j] = bf16r(fmaxf(acc, 0.f));
+  }
+#pragma unroll
+  for (int o = 0; o < ORD_NQ; ++o) {
+    float acc = w[ORD_B3 + o];
+#pragma unroll
+    for (int i = 0; i < ORD_NH; ++i) acc = fmaf(w[ORD_W3 + o * ORD_NH + i], h2[i], acc);
+    y[o] = acc;
+  }
+}
+
+// parameters into shared memory, weights rounded to BF16, biases FP32
+__device__ inline void load_params(const float *params, float *w) {
+  for (int i = threadIdx.x; i < ORD_NPARAM; i += blockDim.x) {
+    const bool bias = (i >= ORD_B1 && i < ORD_W2) || (i >= ORD_B2 && i < ORD_W3) || i >= ORD_B3;
+    w[i] = bias ? params[i] : bf16r(params[i]);
+  }
+}
+
+static constexpr int MLP_ROWS = 128;  // rows per training block
+
+// Forward + backward of MLP_ROWS rows per block; gradients of the mean
+// squared error (over rows_total rows and the ORD_NQ outputs) added into
+// grad, loss sum into *loss.  Rows at or beyond n are ignored.
+__global__ void __launch_bounds__(MLP_ROWS) k_mlp_grad(const float *feat, const float *labels, int n, int row0,
+                                                       int rows_total, const float *params, float *grad, float *loss,
+                                                       float *pred) {
+  extern __shared__ float shm[];
+  float *w = shm;                               // ORD_NPARAM
+  float *X = w + ORD_NPARAM;                    // [ROWS][NF]
+  float *H1 = X + MLP_ROWS * ORD_NF;            // [ROWS][NH]
+  float *H2 = H1 + MLP_ROWS * ORD_NH;           // [ROWS][NH]
+  float *D2 = H2 + MLP_ROWS * ORD_NH;           // [ROWS][NH] dL/d(pre-activation 2)
+  float *D1 = D2 + MLP_ROWS * ORD_NH;           // [ROWS][NH] dL/d(pre-activation 1)
+  float *DY = D1 + MLP_ROWS * ORD_NH;           // [ROWS][16]
+  const int t = threadIdx.x;
+  load_params(params, w);
+  __syncthreads();
+  const int r = row0 + blockIdx.x * MLP_ROWS + t;
+  const bool valid = r < n && r < row0 + rows_total;
+  float x[ORD_NF], h1[ORD_NH], h2[ORD_NH], y[ORD_NQ];
+  for (int i = 0; i < ORD_NF; ++i) x[i] = valid ? bf16r(feat[(size_t)r * ORD_NF + i]) : 0.f;
+  mlp_forward(w, x, h1, h2, y);
+  const float inv = 1.f / ((float)rows_total * ORD_NQ);
+  float l = 0.f;
+  for (int o = 0; o < 16; ++o) {
+    float dy = 0.f;
+    if (o < ORD_NQ && valid) {
+      const float lab = fmaxf(labels[(size_t)r * ORD_NQ + o], -16.f);
+      const float e = y[o] - lab;
+      l += e * e;
+      dy = 2.f * e * inv;
+      if (pred) pred[(size_t)r * ORD_NQ + o] = y[o];
+    }
+    DY[t * 16 + o] = dy;
+  }
+  if (valid) atomicAdd(loss, l * inv);
+  for (int i = 0; i < ORD_NF; ++i) X[t * ORD_NF + i] = x[i];
+  for (int i = 0; i < ORD_NH; ++i) {
+    H1[t * ORD_NH + i] = h1[i];
+    H2[t * ORD_NH + i] = h2[i];
+  }
+  // back through layer 3 and the second ReLU
+  for (int i = 0; i < ORD_NH; ++i) {
+    float g = 0.f;
+    for (int o = 0; o < ORD_NQ; ++o) g = fmaf(w[ORD_W3 + o * ORD_NH + i], DY[t * 16 + o], g);
+    D2[t * ORD_NH + i] = h2[i] > 0.f ? g : 0.f;
+  }
+  // back through layer 2 and the first ReLU
+  for (int i = 0; i < ORD_NH; ++i) {
+    float g = 0.f;
+    for (int j = 0; j < ORD_NH; ++j) g = fmaf(w[ORD_W2 + j * ORD_NH + i], D2[t * ORD_NH + j], g);
+    D1[t * ORD_NH + i] = h1[i] > 0.f ? g : 0.f;
+  }
+  __syncthreads();
+  // parameter gradients: sums over the block's rows
+  for (int e = t; e < ORD_NPARAM; e += MLP_ROWS) {
+    float g = 0.f;
+    if (e < ORD_B1) {
+      const int j = e / ORD_NF, i = e % ORD_NF;
+      for (int k = 0; k < MLP_ROWS; ++k) g = fmaf(D1[k * ORD_NH + j], X[k * ORD_NF + i], g);
+    } else if (e < ORD_W2) {
+      const int j = e - ORD_B1;
+      for (int k = 0; k < MLP_ROWS; ++k) g += D1[k * ORD_NH + j];
+    } else if (e < ORD_B2) {
+      const int j = (e - ORD_W2) / ORD_NH, i = (e - ORD_W2) % ORD_NH;
+      for (int k = 0; k < MLP_ROWS; ++k) g = fmaf(D2[k * ORD_NH + j], H1[k * ORD_NH + i], g);
+    } else if (e < ORD_W3) {
+      const int j = e - ORD_B2;
+      for (int k = 0; k < MLP_ROWS; ++k) g += D2[k * ORD_NH + j];
+    } else if (e < ORD_B3) {
+      const int o = (e - ORD_W3) / ORD_NH, i = (e - ORD_W3) % ORD_NH;
+      if (o < ORD_NQ)
+        for (int k = 0; k < MLP_ROWS; ++k) g = fmaf(DY[k * 16 + o], H2[k * ORD_NH + i], g);
+    } else {
+      const int o = e - ORD_B3;
+      if (o < ORD_NQ)
+        for (int k = 0; k < MLP_ROWS; ++k) g += DY[k * 16 + o];
+    }
+    if (g != 0.f) atomicAdd(&grad[e], g);
+  }
+}
+
+__global__ void k_adam(float *params, float *grad, float *m, float *v, int step, float lr, float b1, float b2,
+                       float eps) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ORD_NPARAM) return;
+  const bool pad = (i >= ORD_W3 + ORD_NQ * ORD_NH && i < ORD_B3) || i >= ORD_B3 + ORD_NQ;
+  const float g = pad ? 0.f : grad[i];
+  const float mi = b1 * m[i] + (1.f - b1) * g, vi = b2 * v[i] + (1.f - b2) * g * g;
+  m[i] = mi;
+  v[i] = vi;
+  const float mh = mi / (1.f - powf(b1, (float)step)), vh = vi / (1.f - powf(b2, (float)step));
+  if (!pad) params[i] -= lr * mh / (sqrtf(vh) + eps);
+  grad[i] = 0.f;
+}
+
+static size_t mlp_grad_smem() {
+  return sizeof(float) * ((size_t)ORD_NPARAM + MLP_ROWS * ORD_NF + 4 * MLP_ROWS * ORD_NH + MLP_ROWS * 16);
+}
+
+// ---------------------------------------------------------------- inference
+// One block per M2L batch, one thread per target row; for every present
+// slot each row predicts its pair's errors and takes the lowest order within
+// its budget; the slot takes the largest order of its rows.
+__global__ void __launch_bounds__(128) k_order_infer(InferArgs a) {
+  __shared__ float w[ORD_NPARAM];
+  __shared__ int s_q;
+  const int tid = threadIdx.x;
+  load_params(a.params, w);
+  const int4 bt = a.batches[blockIdx.x];
+  const int T = tid < bt.y ? a.tlist[bt.x + tid] : -1;
+  const int ns = a.nslots[blockIdx.x];
+  const size_t base = (size_t)blockIdx.x * 189;
+  const double frms = *a.frms;
+  const double pbar = a.n > 0 ? (double)(*a.nt_sum) / (double)a.n : 1.0;
+  const int pmax = a.p;
+  const float *cfT = T >= 0 ? a.cf + (size_t)(T - a.cell0) * ORD_CF : nullptr;
+  const float sd = (float)(a.emax * ldexp(1.0, -bt.z));  // isotropic scale of the level
+  __syncthreads();
+  for (int i = 0; i < ns; ++i) {
+    if (tid == 0) s_q = ORD_QMIN;
+    __syncthreads();
+    const int sl = a.slot_list[base + i];
+    const int o = a.tslot_list[base + i];
+    const int S = T >= 0 ? a.src_tab[(base + sl) * 128 + tid] : -1;
+    int q = ORD_QMIN;
+    if (S >= 0) {
+      if (!(frms > 0.0)) {
+        q = pmax;
+      } else {
+        const int dx = o % 7 - 3, dy = (o / 7) % 7 - 3, dz = o / 49 - 3;
+        float f[ORD_NF], h1[ORD_NH], h2[ORD_NH], y[ORD_NQ];
+        pair_features(cfT, a.cf + (size_t)(S - a.cell0) * ORD_CF, bt.z, dx, dy, dz, a.ax, a.ay, a.az, f);
+        for (int k = 0; k < ORD_NF; ++k) f[k] = bf16r(f[k]);
+        mlp_forward(w, f, h1, h2, y);
+        const float ex = dx * a.ax * sd, ey = dy * a.ay * sd, ez = dz * a.az * sd;
+        const float R2 = ex * ex + ey * ey + ez * ez;
+        const float ms = a.M[(size_t)(S - a.cell0) * a.KS];
+        const float thr = ms > 0.f ? log10f(a.tol * (float)frms * R2 / (ms * (float)sqrt(pbar))) : 30.f;
+        q = pmax;
+        for (int qq = ORD_QMIN; qq < pmax; ++qq)
+          if (y[qq - ORD_QMIN] <= thr) {
+            q = qq;
+            break;
+          }
+      }
+      atomicMax(&s_q, q);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      const int K = (s_q + 1) * (s_q + 1);
+      a.slot_p16[base + i] = (uint8_t)((K + 15) & ~15);
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- F_rms
+__global__ void k_force_sq(const double *acc, int64_t n, int dim, double invG2, double *out) {
+  double s = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double v = 0.0;
+    for (int d = 0; d < dim; ++d) v += acc[dim * i + d] * acc[dim * i + d];
+    s += v;
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s * invG2);
+}
+
+__global__ void k_force_rms_final(const double *sum, int64_t n, double *frms) {
+  *frms = n > 0 ? sqrt(*sum / (double)n) : 0.0;
+}
+
+__global__ void k_judge_compare(const double *acc, const double *ref, const int64_t *targets, int64_t nt, int dim,
+                                double *out) {
+  double e = 0.0, r = 0.0;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = targets[k];
+    for (int d = 0; d < dim; ++d) {
+      const double a = acc[dim * i + d], b = ref[dim * k + d];
+      e += (a - b) * (a - b);
+      r += b * b;
+    }
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    e += __shfl_xor_sync(0xffffffffu, e, o);
+    r += __shfl_xor_sync(0xffffffffu, r, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&out[0], e);
+    atomicAdd(&out[1], r);
+  }
+}
+
+// ---------------------------------------------------------------- host
+int order_judge_compare(const double *acc, const double *ref, const int64_t *targets, int64_t nt, int dim, double *out,
+                        cudaStream_t st, int64_t &launches) {
+  CUDA_TRY(cudaMemsetAsync(out, 0, 2 * sizeof(double), st));
+  k_judge_compare<<<std::max(1, std::min(cdiv(nt, 256), 148)), 256, 0, st>>>(acc, ref, targets, nt, dim, out);
+  launches += 1;
+  return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
+}
+
+int order_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int cell0, int p,
+                        int KS, float *cf, cudaStream_t st, int64_t &launches) {
+  if (count <= 0) return FMM_OK;
+  k_cell_features<<<cdiv(count, 256), 256, 0, st>>>(M, pbeg, pend, first, count, cell0, p, KS, cf);
+  launches += 1;
+  return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
+}
+
+int order_sample_pairs(const int4 *batches, const int *tlist, const int *src_tab, const int *slot_list,
+                       const int *tslot_list, const int *nslots, int nbm, const int *pbeg, const int *pend, int n,
+                       unsigned long long seed, int max_nt, int max_ns, int *pairs, cudaStream_t st,
+                       int64_t &launches) {
+  if (n <= 0 || nbm <= 0) return FMM_OK;
+  k_order_sample<<<cdiv(n, 256), 256, 0, st>>>(batches, tlist, src_tab, slot_list, tslot_list, nslots, nbm, pbeg,
+                                               pend, n, seed, max_nt, max_ns, reinterpret_cast<int4 *>(pairs));
+  launches += 1;
+  return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
+}
+
+int order_pair_features(const int *pairs, int n, const float *cf, int cell0, float ax, float ay, float az,
+                        float *feat, cudaStream_t st, int64_t &launches) {
+  if (n <= 0) return FMM_OK;
+  k_pair_features<<<cdiv(n, 256), 256, 0, st>>>(reinterpret_cast<const int4 *>(pairs), n, cf, cell0, ax, ay, az,
+                                                feat);
+  launches += 1;
+  return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
+}
+
+int order_probe_errors(const ProbeArgs &a, cudaStream_t st, int64_t &launches) {
+  if (a.n <= 0) return FMM_OK;
+  const size_t sh = sizeof(double) * ((size_t)a.K + ORD_NQ * (size_t)a.K + 3 * PROBE_MAX_NT + ORD_NQ + 8 * (size_t)a.K);
+  if (sh > 227 * 1024) return FMM_ERR_UNSUPPORTED;
+  if (cudaFuncSetAttribute(k_probe, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess)
+    return FMM_ERR_CUDA;
+  k_probe<<<a.n, PROBE_T, sh, st>>>(a);
+  launches += 1;
+  return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
+}
+
+int order_infer(const InferArgs &a, int nbm, cudaStream_t st, int64_t &launches) {
+  if (nbm <= 0) return FMM_OK;
+  k_order_infer<<<nbm, 128, 0, st>>>(a);
+  launches += 1;
+  return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
+}
+
+int order_forward_grad(const float *feat, const float *labels, int n, const float *params, float *pred, float *grad,
+                       float *loss, cudaStream_t st, int64_t &launches) {
+  if (n <= 0) return FMM_OK;
+  const size_t sh = mlp_grad_smem();
+  if (cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess)
+    return FMM_ERR_CUDA;
+  if (cudaMemsetAsync(grad, 0, sizeof(float) * ORD_NPARAM, st) != cudaSuccess ||
+      cudaMemsetAsync(loss, 0, sizeof(float), st) != cudaSuccess)
+    return FMM_ERR_CUDA;
+  k_mlp_grad<<<cdiv(n, MLP_ROWS), MLP_ROWS, sh, st>>>(feat, labels, n, 0, n, params, grad, loss, pred);
+  launches += 1;
+  return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
+}
+
+int order_train(const float *feat, const float *labels, int n, int epochs, int batch, float lr, float *params,
+                float *loss_out, cudaStream_t st, int64_t &launches) {
+  if (n <= 0 || epochs <= 0) return FMM_OK;
+  batch = std::max(MLP_ROWS, (batch / MLP_ROWS) * MLP_ROWS);
+  const size_t sh = mlp_grad_smem();
+  if (cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess)
+    return FMM_ERR_CUDA;
+  DevBuf<float> gbuf, mbuf, vbuf, lbuf;
+  if (!gbuf.reserve(ORD_NPARAM) || !mbuf.reserve(ORD_NPARAM) || !vbuf.reserve(ORD_NPARAM) || !lbuf.reserve(epochs))
+    return FMM_ERR_OUT_OF_MEMORY;
+  CUDA_TRY(cudaMemsetAsync(gbuf.ptr, 0, sizeof(float) * ORD_NPARAM, st));
+  CUDA_TRY(cudaMemsetAsync(mbuf.ptr, 0, sizeof(float) * ORD_NPARAM, st));
+  CUDA_TRY(cudaMemsetAsync(vbuf.ptr, 0, sizeof(float) * ORD_NPARAM, st));
+  CUDA_TRY(cudaMemsetAsync(lbuf.ptr, 0, sizeof(float) * epochs, st));
+  int step = 0;
+  const int steps_per_epoch = (n + batch - 1) / batch;
+  for (int e = 0; e < epochs; ++e) {
+    for (int s = 0; s < steps_per_epoch; ++s) {
+      const int row0 = s * batch, rows = std::min(batch, n - row0);
+      k_mlp_grad<<<cdiv(rows, MLP_ROWS), MLP_ROWS, sh, st>>>(feat, labels, n, row0, rows, params, gbuf.ptr,
+                                                              lbuf.ptr + e, nullptr);
+      k_adam<<<cdiv(ORD_NPARAM, 256), 256, 0, st>>>(params, gbuf.ptr, mbuf.ptr, vbuf.ptr, ++step, lr, 0.9f, 0.999f,
+                                                   1e-8f);
+      launches += 2;
+    }
+  }
+  CUDA_TRY(cudaGetLastError());
+  std::vector<float> hl(epochs);
+  CUDA_TRY(cudaMemcpyAsync(hl.data(), lbuf.ptr, sizeof(float) * epochs, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  for (int e = 0; e < epochs; ++e) loss_out[e] = hl[e] / (float)steps_per_epoch;
+  return FMM_OK;
+}
+
+int order_force_rms(const double *acc, int64_t n, int dim, double G, double *scratch, double *frms, cudaStream_t st,
+                    int64_t &launches) {
+  CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(double), st));
+  const double invG2 = G != 0.0 ? 1.0 / (G * G) : 1.0;
+  k_force_sq<<<std::min(cdiv(n, 256), 148 * 8), 256, 0, st>>>(acc, n, dim, invG2, scratch);
+  k_force_rms_final<<<1, 1, 0, st>>>(scratch, n, frms);
+  launches += 2;
+  return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
+}
+
+}  // namespace fmm

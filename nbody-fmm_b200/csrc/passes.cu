@@ -286,19 +286,25 @@ static int launch_contract(const ContractArgs &a, int nb, cudaStream_t st, int64
 // source.  One block per batch of up to `tchunk` (64 or 128) targets; with
 // pair_count set it also counts the (target, source) pairs.
 __global__ void k_m2l_sources(ContractArgs a, int tchunk, int *src_tab, int *slot_list, int *nslots_tab,
-                              int *tslot_list, unsigned long long *pair_count) {
+                              int *tslot_list, unsigned long long *pair_count, const uint8_t *order_p16,
+                              uint8_t *slot_p16, unsigned long long *nt_sum) {
   __shared__ int s_flag[189];
   __shared__ int s_tgt[128];
   __shared__ int s_cnt;
+  __shared__ unsigned long long s_nt;
   const int4 b = a.batches[blockIdx.x];
   const int tid = threadIdx.x;
   const int nsl = a.dim == 3 ? 189 : 27;
   if (tid < tchunk) s_tgt[tid] = tid < b.y ? a.tlist[b.x + tid] : -1;
   for (int i = tid; i < 189; i += blockDim.x) s_flag[i] = 0;
-  if (tid == 0) s_cnt = 0;
+  if (tid == 0) {
+    s_cnt = 0;
+    s_nt = 0;
+  }
   __syncthreads();
   const size_t base = (size_t)blockIdx.x * 189;
   int cnt = 0;
+  unsigned long long ntc = 0;
   for (int e = tid; e < nsl * tchunk; e += blockDim.x) {
     const int slot = e / tchunk, t = e % tchunk;
     int src = -1, ts;
@@ -307,9 +313,11 @@ __global__ void k_m2l_sources(ContractArgs a, int tchunk, int *src_tab, int *slo
     if (src >= 0) {
       s_flag[slot] = 1;
       ++cnt;
+      ntc += (unsigned long long)(a.cpend[s_tgt[t]] - a.cpbeg[s_tgt[t]]);
     }
   }
   if (pair_count && cnt) atomicAdd(&s_cnt, cnt);
+  if (nt_sum && ntc) atomicAdd(&s_nt, ntc);
   __syncthreads();
   if (tid < 32) {
     int n = 0;
@@ -320,13 +328,16 @@ __global__ void k_m2l_sources(ContractArgs a, int tchunk, int *src_tab, int *slo
       if (f) {
         const int at = n + __popc(m & ((1u << tid) - 1u));
         slot_list[base + at] = sl;
-        if (tslot_list) tslot_list[base + at] = (c_m2l_slots[a.dim - 2][b.w][sl] & 511) + b.z * a.level_stride;
+        const int ts = (c_m2l_slots[a.dim - 2][b.w][sl] & 511) + b.z * a.level_stride;
+        if (tslot_list) tslot_list[base + at] = ts;
+        if (slot_p16) slot_p16[base + at] = order_p16[ts];
       }
       n += __popc(m);
     }
     if (tid == 0) {
       nslots_tab[blockIdx.x] = n;
       if (pair_count && s_cnt) atomicAdd(pair_count, (unsigned long long)s_cnt);
+      if (nt_sum && s_nt) atomicAdd(nt_sum, s_nt);
     }
   }
 }
@@ -935,13 +946,49 @@ __global__ void k_class_hist(const uint64_t *keys, int n, uint32_t *hist) {
   if (h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
 }
 
+// ------------------------------------------------------------ pair orders
+// FMM_ORDER_GEOMETRIC: for every M2L operator slot (offset D of source from
+// target, in cell sizes), the order whose truncation bound rho^(q+1),
+// rho = (sum of the two cells' radii) / |D|, matches the closest offset's at
+// order p, plus `margin`, clamped to [min(4, p), p]; stored as the padded
+// width of that order's expansion length.
+__global__ void k_order_table(int dim, int p, int margin, int n_slots, int per_level, float ax, float ay, float az,
+                              uint8_t *out) {
+  __shared__ float s_ref;
+  const float diag = sqrtf(ax * ax + ay * ay + (dim == 3 ? az * az : 0.f));  // radius sum of two cells
+  if (threadIdx.x == 0) {
+    float ref = 0.f;
+    for (int t = 0; t < per_level; ++t) {
+      const int dx = t % 7 - 3, dy = (t / 7) % 7 - 3, dz = dim == 3 ? t / 49 - 3 : 0;
+      if (max(abs(dx), max(abs(dy), abs(dz))) < 2) continue;  // neighbours never interact by M2L
+      const float R = sqrtf(dx * dx * ax * ax + dy * dy * ay * ay + dz * dz * az * az);
+      ref = fmaxf(ref, diag / R);
+    }
+    s_ref = ref;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < n_slots; t += blockDim.x) {
+    const int o = t % per_level;
+    const int dx = o % 7 - 3, dy = (o / 7) % 7 - 3, dz = dim == 3 ? o / 49 - 3 : 0;
+    const float R = sqrtf(dx * dx * ax * ax + dy * dy * ay * ay + dz * dz * az * az);
+    const float rho = R > 0.f ? diag / R : 1.f;
+    int q = p;
+    if (rho < 1.f && s_ref < 1.f && max(abs(dx), max(abs(dy), abs(dz))) >= 2) {
+      q = (int)ceilf((p + 1) * logf(s_ref) / logf(rho)) - 1 + margin;
+      q = max(min(q, p), min(4, p));
+    }
+    const int K = dim == 3 ? (q + 1) * (q + 1) : 2 * q + 1;
+    out[t] = (uint8_t)((K + 15) & ~15);
+  }
+}
+
 // ------------------------------------------------------------ driver
 static inline float fmax3(float a, float b, float c) { return std::max(a, std::max(b, c)); }
 
 int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, const double *d_pos_g,
                    const double *d_mass_g, int p, double eps2, double G,
-                   const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, int64_t direct_max, cudaStream_t st,
-                   fmm_stats &stats, cudaEvent_t *ev) {
+                   const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, int64_t direct_max,
+                   const OrderOpts &order, cudaStream_t st, fmm_stats &stats, cudaEvent_t *ev) {
   const int dim = t.dim, D = t.depth, KS = ops.KS;
   const int64_t n = t.n;
   const int ncell = t.n_cells, cell0 = t.cell0;
@@ -1048,7 +1095,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   ca.dim = dim;
   ca.level_stride = dim == 2 ? 49 : 0;
   ca.pair_count = ws.counters;
-  CUDA_TRY(cudaMemsetAsync(ws.counters, 0, 4 * sizeof(unsigned long long), st));
+  CUDA_TRY(cudaMemsetAsync(ws.counters, 0, 8 * sizeof(unsigned long long), st));
   TcArgs ta{};
   ta.cchild = ws.cell_child;
   ta.cparent = ws.cell_parent;
@@ -1102,10 +1149,92 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     if (!eb.m2l_src.reserve((size_t)nbm * 189 * tchunk) || !eb.m2l_list.reserve((size_t)nbm * 189) ||
         !eb.m2l_nslots.reserve(nbm) || !eb.m2l_tslot.reserve((size_t)nbm * 189))
       return FMM_ERR_OUT_OF_MEMORY;
+    const bool geometric = tc && order.mode == FMM_ORDER_GEOMETRIC;
+    const bool learned = tc && dim == 3 && order.mode == FMM_ORDER_LEARNED && order.params;
+    const bool collect = tc && dim == 3 && order.npairs > 0 && ops.tab64.ptr;
+    const bool var_order = geometric || learned;
+    const float ax = (float)(g.ext[0] / emax), ay = (float)(g.ext[1] / emax),
+                az = (float)(dim == 3 ? g.ext[2] / emax : 0.0);
+    if (var_order && !eb.m2l_w.reserve((size_t)nbm * 189)) return FMM_ERR_OUT_OF_MEMORY;
+    if (geometric) {
+      if (!eb.order_p16.reserve(ops.n_m2l)) return FMM_ERR_OUT_OF_MEMORY;
+      k_order_table<<<1, 256, 0, st>>>(dim, p, order.margin, ops.n_m2l, dim == 3 ? 343 : 49, ax, ay, az,
+                                       eb.order_p16.ptr);
+      ws.launches += 1;
+    }
+    if (learned || collect) {
+      if (!eb.cf.reserve((size_t)ncell * ORD_CF)) return FMM_ERR_OUT_OF_MEMORY;
+      int rc = order_cell_features(eb.M.ptr, ws.cell_pbeg, ws.cell_pend, t.level_off[2], ntl, cell0, p, KS, eb.cf.ptr,
+                                   st, ws.launches);
+      if (rc) return rc;
+    }
     if (nbm > 0) {
       k_m2l_sources<<<nbm, 256, 0, st>>>(c2, tchunk, eb.m2l_src.ptr, eb.m2l_list.ptr, eb.m2l_nslots.ptr,
-                                         tc ? eb.m2l_tslot.ptr : nullptr, tc ? ws.counters : nullptr);
+                                         tc ? eb.m2l_tslot.ptr : nullptr, tc ? ws.counters : nullptr,
+                                         geometric ? eb.order_p16.ptr : nullptr, geometric ? eb.m2l_w.ptr : nullptr,
+                                         ws.counters + 4);
       ws.launches += 1;
+    }
+    if (learned && nbm > 0) {
+      if (!eb.frms.reserve(2)) return FMM_ERR_OUT_OF_MEMORY;
+      InferArgs ia;
+      ia.batches = c2.batches;
+      ia.tlist = tl_m2l;
+      ia.src_tab = eb.m2l_src.ptr;
+      ia.slot_list = eb.m2l_list.ptr;
+      ia.tslot_list = eb.m2l_tslot.ptr;
+      ia.nslots = eb.m2l_nslots.ptr;
+      ia.pbeg = ws.cell_pbeg;
+      ia.pend = ws.cell_pend;
+      ia.cf = eb.cf.ptr;
+      ia.M = eb.M.ptr;
+      ia.params = order.params;
+      ia.frms = eb.frms.ptr;
+      ia.nt_sum = ws.counters + 4;
+      ia.n = n;
+      ia.cell0 = cell0;
+      ia.KS = KS;
+      ia.p = p;
+      ia.dim = dim;
+      ia.tol = order.tol;
+      ia.ax = ax;
+      ia.ay = ay;
+      ia.az = az;
+      ia.emax = emax;
+      ia.slot_p16 = eb.m2l_w.ptr;
+      int rc = order_infer(ia, nbm, st, ws.launches);
+      if (rc) return rc;
+    }
+    if (collect && nbm > 0) {
+      int rc = order_sample_pairs(c2.batches, tl_m2l, eb.m2l_src.ptr, eb.m2l_list.ptr, eb.m2l_tslot.ptr,
+                                  eb.m2l_nslots.ptr, nbm, ws.cell_pbeg, ws.cell_pend, order.npairs, order.seed,
+                                  1 << 30, 1 << 17, order.pairs, st, ws.launches);
+      if (!rc)
+        rc = order_pair_features(order.pairs, order.npairs, eb.cf.ptr, cell0, ax, ay, az, order.feat, st,
+                                 ws.launches);
+      if (!rc) {
+        ProbeArgs pa;
+        pa.pairs = order.pairs;
+        pa.n = order.npairs;
+        pa.pos = d_pos_g;
+        pa.mass = d_mass_g;
+        pa.perm = t.d_perm;
+        pa.pbeg = ws.cell_pbeg;
+        pa.pend = ws.cell_pend;
+        pa.ckey = ws.cell_key;
+        pa.tab64 = ops.tab64.ptr;
+        pa.p = p;
+        pa.K = ops.K;
+        pa.KP = ops.KP;
+        for (int k = 0; k < 3; ++k) {
+          pa.g.lo[k] = g.lo[k];
+          pa.g.ext[k] = g.ext[k];
+        }
+        pa.g.emax = emax;
+        pa.labels = order.labels;
+        rc = order_probe_errors(pa, st, ws.launches);
+      }
+      if (rc) return rc;
     }
     int rc;
     if (tc) {
@@ -1120,6 +1249,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
       t2.X = eb.M.ptr;
       t2.Y = eb.L.ptr;
       t2.tiles = ws.counters + 2;
+      t2.slot_p16 = var_order ? eb.m2l_w.ptr : nullptr;
       rc = tc_launch(t2, nbm, eb.tc_work.ptr + tc_k++, st, ws.launches);
     } else {
       c2.src_tab = eb.m2l_src.ptr;

@@ -63,7 +63,8 @@ struct Workspace {
   DevBuf<double> bgeom;
   DevBuf<uint32_t> bscalars;
   DevBuf<unsigned int> berr;
-  DevBuf<unsigned long long> bcount;  // [0] M2L pairs, [1] P2P particle pairs
+  DevBuf<unsigned long long> bcount;  // [0] M2L pairs, [1] near-field pairs, [2] M2L tiles, [3] direct far-field
+                                      // pairs, [4] sum over M2L pairs of the target's particle count
 
   uint64_t *keyA = nullptr, *keyB = nullptr, *keyC = nullptr;
   uint32_t *valA = nullptr, *valB = nullptr, *valC = nullptr, *u32A = nullptr, *u32B = nullptr, *u32C = nullptr;
@@ -80,7 +81,7 @@ struct Workspace {
   bool ok = true;
 
   bool init_small() {
-    ok &= bbox.reserve(8) && bgeom.reserve(8) && bscalars.reserve(8) && berr.reserve(4) && bcount.reserve(4);
+    ok &= bbox.reserve(8) && bgeom.reserve(8) && bscalars.reserve(8) && berr.reserve(4) && bcount.reserve(8);
     counters = bcount.ptr;
     box_u64 = bbox.ptr;
     geom = bgeom.ptr;

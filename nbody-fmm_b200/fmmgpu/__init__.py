@@ -33,6 +33,13 @@ FMM_NOALLOC_MAX_TARGETS = 262144
 
 FMM_M2L_FP32 = 0
 FMM_M2L_TC = 1
+FMM_ORDER_FIXED = 0
+FMM_ORDER_GEOMETRIC = 1
+FMM_ORDER_LEARNED = 2
+FMM_ORDER_NPARAM = 7312
+FMM_ORDER_NFEAT = 32
+FMM_ORDER_NOUT = 9
+ORDER_MODEL_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "order_model.npy")
 FMM_SOFT_PLUMMER = 0
 FMM_SOFT_NAIVE_REF = 1
 FMM_INT_SYMPLECTIC_EULER = 0
@@ -43,7 +50,8 @@ EXPORTED = (
     "fmm_strerror", "fmm_version", "fmm_config_default", "fmm_create", "fmm_destroy", "fmm_evaluate",
     "fmm_evaluate_device", "fmm_synchronize", "fmm_direct", "fmm_direct_device", "fmm_integrate",
     "fmm_tree_build", "fmm_tree_depth", "fmm_tree_level_size", "fmm_tree_level_keys", "fmm_tree_leaves",
-    "fmm_tree_pairs", "fmm_last_stats", "fmm_launch_count", "fmm_direct_noalloc",
+    "fmm_tree_pairs", "fmm_last_stats", "fmm_launch_count", "fmm_direct_noalloc", "fmm_order_set_model",
+    "fmm_order_get_model", "fmm_order_collect", "fmm_order_train", "fmm_order_forward_grad",
 )
 
 
@@ -51,7 +59,9 @@ class FmmConfig(ctypes.Structure):
     _fields_ = [
         ("dim", ctypes.c_int32), ("p", ctypes.c_int32), ("leaf_cap", ctypes.c_int32), ("m2l_mode", ctypes.c_int32),
         ("eps2", ctypes.c_double), ("G", ctypes.c_double), ("device", ctypes.c_int32),
-        ("direct_max", ctypes.c_int32), ("reserved", ctypes.c_int32 * 6),
+        ("direct_max", ctypes.c_int32), ("order_mode", ctypes.c_int32), ("order_margin", ctypes.c_int32),
+        ("order_tol", ctypes.c_float), ("judge_samples", ctypes.c_int32), ("judge_budget", ctypes.c_float),
+        ("reserved", ctypes.c_int32 * 1),
     ]
 
 
@@ -62,7 +72,8 @@ class FmmStats(ctypes.Structure):
         ("ms_tree", ctypes.c_double), ("ms_upward", ctypes.c_double), ("ms_m2l", ctypes.c_double),
         ("ms_downward", ctypes.c_double), ("ms_p2p", ctypes.c_double), ("ms_total", ctypes.c_double),
         ("m2l_tiles", ctypes.c_int64), ("ms_far_direct", ctypes.c_double),
-        ("far_direct_pairs", ctypes.c_int64), ("direct_max", ctypes.c_int64), ("reserved", ctypes.c_double * 2),
+        ("far_direct_pairs", ctypes.c_int64), ("direct_max", ctypes.c_int64), ("judge_rel_l2", ctypes.c_double),
+        ("order_fallbacks", ctypes.c_int64),
     ]
 
 
@@ -110,6 +121,12 @@ def load_library(path=LIB_PATH):
     L.fmm_launch_count.argtypes = [_vp]
     L.fmm_direct_noalloc.argtypes = [ctypes.c_int32, ctypes.c_int64, _vp, _vp, ctypes.c_int64, _vp, ctypes.c_int32,
                                      ctypes.c_double, ctypes.c_double, _vp, _vp, _vp]
+    _f = ctypes.POINTER(ctypes.c_float)
+    L.fmm_order_set_model.argtypes = [_vp, _f, ctypes.c_int32]
+    L.fmm_order_get_model.argtypes = [_vp, _f, ctypes.c_int32]
+    L.fmm_order_collect.argtypes = [_vp, ctypes.c_int64, _vp, _vp, ctypes.c_int32, ctypes.c_uint64, _vp, _vp, _vp]
+    L.fmm_order_train.argtypes = [_vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, _f]
+    L.fmm_order_forward_grad.argtypes = [_vp, _vp, ctypes.c_int32, _vp, _vp, _vp, _vp, _vp]
     _lib = L
     return L
 
@@ -138,17 +155,25 @@ def direct_noalloc(dim, n, pos_ptr, mass_ptr, acc_ptr, pot_ptr=None, ntargets=0,
 class Context:
     """One FMM force evaluator on one GPU (fmm_create / fmm_destroy)."""
 
-    def __init__(self, dim=3, p=8, leaf_cap=64, m2l_mode=FMM_M2L_FP32, eps2=0.0, G=1.0, device=0, direct_max=-1):
+    def __init__(self, dim=3, p=8, leaf_cap=64, m2l_mode=FMM_M2L_FP32, eps2=0.0, G=1.0, device=0, direct_max=-1,
+                 order_mode=FMM_ORDER_FIXED, order_margin=1, order_tol=5e-7, judge_samples=0, judge_budget=1e-6,
+                 order_model=None):
         L = load_library()
         cfg = FmmConfig()
         _check(L.fmm_config_default(ctypes.byref(cfg)))
         cfg.dim, cfg.p, cfg.leaf_cap, cfg.m2l_mode = dim, p, leaf_cap, m2l_mode
         cfg.eps2, cfg.G, cfg.device, cfg.direct_max = eps2, G, device, direct_max
+        cfg.order_mode, cfg.order_margin = order_mode, order_margin
+        cfg.order_tol, cfg.judge_samples, cfg.judge_budget = order_tol, judge_samples, judge_budget
         h = _vp()
         _check(L.fmm_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
         self.dim = dim
         self.cfg = cfg
+        if order_model is None and order_mode == FMM_ORDER_LEARNED and os.path.exists(ORDER_MODEL_PATH):
+            order_model = np.load(ORDER_MODEL_PATH)
+        if order_model is not None:
+            self.set_order_model(order_model)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -255,3 +280,50 @@ class Context:
 
     def launch_count(self):
         return int(_lib.fmm_launch_count(self._h))
+
+    # ---- learned pair orders
+    def set_order_model(self, params):
+        """Loads the order MLP (FMM_ORDER_NPARAM floats, fmm_order_set_model)."""
+        params = np.ascontiguousarray(params, dtype=np.float32).ravel()
+        _check(_lib.fmm_order_set_model(self._h, _p(params, ctypes.POINTER(ctypes.c_float)), params.size))
+
+    def get_order_model(self):
+        out = np.zeros(FMM_ORDER_NPARAM, np.float32)
+        _check(_lib.fmm_order_get_model(self._h, _p(out, ctypes.POINTER(ctypes.c_float)), out.size))
+        return out
+
+    def order_collect(self, n, pos_ptr, mass_ptr, npairs, seed, feat_ptr, labels_ptr, stream=None):
+        """One fixed-order evaluation that writes the features and FP64
+        truncation-error labels of npairs sampled M2L pairs into device
+        buffers (fmm_order_collect)."""
+        _check(_lib.fmm_order_collect(self._h, n, pos_ptr, mass_ptr, npairs, seed, feat_ptr, labels_ptr, stream))
+
+    def order_train(self, feat_ptr, labels_ptr, n, epochs, batch=8192, lr=1e-3):
+        """Trains the loaded model in place on device data; returns the mean
+        loss of every epoch (fmm_order_train)."""
+        loss = np.zeros(epochs, np.float32)
+        _check(_lib.fmm_order_train(self._h, feat_ptr, labels_ptr, n, epochs, batch, lr,
+                                    _p(loss, ctypes.POINTER(ctypes.c_float))))
+        return loss
+
+
+def order_forward_grad(feat_ptr, labels_ptr, n, params_ptr, pred_ptr, grad_ptr, loss_ptr, stream=None):
+    """Predictions, mean squared error and its parameter gradient on device
+    buffers (fmm_order_forward_grad)."""
+    load_library()
+    _check(_lib.fmm_order_forward_grad(feat_ptr, labels_ptr, n, params_ptr, pred_ptr, grad_ptr, loss_ptr, stream))
+
+
+def order_init_params(seed=0):
+    """He-initialised MLP parameters in the library's flat layout (the rows
+    of W3 and b3 beyond the nine outputs are zero)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(FMM_ORDER_NPARAM, np.float32)
+    nf, nh = FMM_ORDER_NFEAT, 64
+    w1, b1 = 0, nh * nf
+    w2, b2 = b1 + nh, b1 + nh + nh * nh
+    w3, b3 = b2 + nh, b2 + nh + 16 * nh
+    p[w1:b1] = rng.normal(0.0, np.sqrt(2.0 / nf), nh * nf)
+    p[w2:b2] = rng.normal(0.0, np.sqrt(2.0 / nh), nh * nh)
+    p[w3:w3 + FMM_ORDER_NOUT * nh] = rng.normal(0.0, np.sqrt(1.0 / nh), FMM_ORDER_NOUT * nh)
+    return p
