@@ -58,10 +58,12 @@ enum {
    a pair whose cells are R cell sizes apart is evaluated at the order that
    gives the closest offset's (R = 2) truncation bound at p, plus
    order_margin, clamped to [min(4, p), p].  LEARNED (3D): an MLP set with
-   fmm_order_set_model predicts each pair's truncation error at orders 4..12
-   and the pair takes the lowest order within its share of order_tol (a
-   relative L2 force budget, shared by the pairs through the RMS force of the
-   previous evaluation; the first evaluation of a system runs at p).  With
+   fmm_order_set_model predicts, for each M2L tile (the targets of one tensor-
+   core tile at one interaction offset), its pairs' largest truncation error
+   at orders 4..12, and the tile takes the lowest order within the pairs'
+   share of order_tol (a relative L2 force budget, shared through the RMS
+   force of the previous evaluation; the first evaluation of a system runs
+   at p).  With
    judge_samples > 0 every learned-order evaluation is checked on that many
    targets against the FP64 direct sum and, if their relative L2 error
    exceeds judge_budget, evaluated again at fixed p (fmm_stats.order_fallbacks). */
@@ -225,12 +227,14 @@ FMM_API int64_t fmm_launch_count(fmm_ctx *ctx);
 /* Learned pair orders.  Parameters are FMM_ORDER_NPARAM floats (host). */
 FMM_API int fmm_order_set_model(fmm_ctx *ctx, const float *params, int32_t nparams);
 FMM_API int fmm_order_get_model(fmm_ctx *ctx, float *params, int32_t nparams);
-/* One force evaluation (fixed p; 3D, FMM_M2L_TC) that samples npairs of its
-   M2L pairs and writes their features (d_feat, npairs x FMM_ORDER_NFEAT) and
-   the base-10 logarithms of their FP64 truncation errors at orders 4..12
-   over the pair's monopole scale (d_labels, npairs x FMM_ORDER_NOUT).  Rows
-   where the draw found no pair are all zero.  Device buffers; synchronous. */
-FMM_API int fmm_order_collect(fmm_ctx *ctx, int64_t n, const double *d_pos, const double *d_mass, int32_t npairs,
+/* One force evaluation (fixed p; 3D, FMM_M2L_TC) that samples ntiles of its
+   M2L tiles (128 targets at one interaction offset) and writes their
+   features (d_feat, ntiles x FMM_ORDER_NFEAT) and labels (d_labels, ntiles x
+   FMM_ORDER_NOUT): for every order q in 4..12 the base-10 logarithm of the
+   largest over the tile's pairs of e(q) / sqrt(n_T) * R^2 / M_tot, e(q) the
+   pair's FP64 truncation error over its target particles (G = 1).  Rows
+   where the draw found no tile are all zero.  Device buffers; synchronous. */
+FMM_API int fmm_order_collect(fmm_ctx *ctx, int64_t n, const double *d_pos, const double *d_mass, int32_t ntiles,
                               uint64_t seed, float *d_feat, float *d_labels, void *stream);
 /* Trains the context's model in place on the GPU (Adam, mean squared error
    of the predicted logarithms; device data, rows used in order);

@@ -33,7 +33,8 @@ struct ExpBuffers {
   DevBuf<uint8_t> order_p16;     // per M2L operator slot: padded width of its pair order
   DevBuf<uint8_t> m2l_w;         // per M2L batch and present slot: padded width of its order
   DevBuf<float> cf;              // learned orders: per-cell features (ORD_CF floats per cell)
-  DevBuf<double> frms;           // learned orders: [0] F_rms of the previous pass (G = 1), [1] scratch  // BF16 split operator images for the tensor-core M2L  // particle offsets from their level-d ancestor (direct far field)
+  DevBuf<double> frms;           // learned orders: [0] F_rms of the previous pass (G = 1), [1] scratch,
+                                 // [2] total mass  // BF16 split operator images for the tensor-core M2L  // particle offsets from their level-d ancestor (direct far field)
 };
 
 // Per-pass parameters.
@@ -50,14 +51,14 @@ struct OrderOpts {
   int margin = 1;          // FMM_ORDER_GEOMETRIC
   float tol = 5e-7f;       // FMM_ORDER_LEARNED: relative error budget of the truncation
   const float *params = nullptr;  // FMM_ORDER_LEARNED: MLP parameters
-  // collection (nullptr: none): sample `npairs` M2L pairs, write their
+  // collection (ntiles = 0: none): sample `ntiles` M2L tiles, write their
   // features and FP64 error labels
-  int npairs = 0;
+  int ntiles = 0;
   unsigned long long seed = 0;
-  int *pairs = nullptr;
+  int *tiles = nullptr;          // [ntiles][2]
+  int *pairs = nullptr;          // [ntiles][128][4]
+  float *pair_labels = nullptr;  // [ntiles][128][ORD_NQ]
   float *feat = nullptr, *labels = nullptr;
-  const double *pos = nullptr, *mass = nullptr;  // FP64 inputs for the probe
-  OrderGeom geom{};
 };
 void upload_class_tables();
 

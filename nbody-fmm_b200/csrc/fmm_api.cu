@@ -39,7 +39,8 @@ struct fmm_ctx {
   DevBuf<int64_t> judge_tg;    // judge targets of (judge_n, judge_k)
   DevBuf<double> judge_ref, judge_sum;
   int64_t judge_n = -1, judge_k = -1;
-  DevBuf<int> col_pairs;
+  DevBuf<int> col_pairs, col_tiles;
+  DevBuf<float> col_plabels;
   fmm_stats stats;
   cudaEvent_t ev[7] = {};  // pass boundaries; ev[6] ends the direct far field
   bool timing_pending = false;
@@ -169,6 +170,8 @@ int fmm_destroy(fmm_ctx *c) {
   c->judge_ref.release();
   c->judge_sum.release();
   c->col_pairs.release();
+  c->col_tiles.release();
+  c->col_plabels.release();
   for (auto *b : {&c->d_pos, &c->d_mass, &c->d_acc, &c->d_pot, &c->d_vel, &c->d_x0, &c->d_v0, &c->d_xs, &c->d_vs,
                   &c->d_asum, &c->d_vsum})
     b->release();
@@ -269,9 +272,9 @@ static int evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const dou
   if (learned) {
     if (!c->has_model) return FMM_ERR_INVALID_ARGUMENT;  // no order model set
     oo.params = c->order_params.ptr;
-    if (!c->eb.frms.reserve(2)) return FMM_ERR_OUT_OF_MEMORY;
+    if (!c->eb.frms.reserve(3)) return FMM_ERR_OUT_OF_MEMORY;
     if (c->frms_n != n) {  // a new system: its first evaluation runs at fixed p
-      CUDA_TRY(cudaMemsetAsync(c->eb.frms.ptr, 0, 2 * sizeof(double), st));
+      CUDA_TRY(cudaMemsetAsync(c->eb.frms.ptr, 0, 3 * sizeof(double), st));
       c->frms_n = n;
     }
   }
@@ -578,20 +581,25 @@ int fmm_order_get_model(fmm_ctx *c, float *params, int32_t nparams) {
   return FMM_OK;
 }
 
-int fmm_order_collect(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass, int32_t npairs,
+int fmm_order_collect(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass, int32_t ntiles,
                       uint64_t seed, float *d_feat, float *d_labels, void *stream) {
-  if (!c || n <= 0 || n > (int64_t)INT32_MAX || npairs <= 0 || !d_pos || !d_mass || !d_feat || !d_labels)
+  if (!c || n <= 0 || n > (int64_t)INT32_MAX || ntiles <= 0 || ntiles > (1 << 20) || !d_pos || !d_mass || !d_feat ||
+      !d_labels)
     return FMM_ERR_INVALID_ARGUMENT;
   if (c->cfg.dim != 3 || c->cfg.m2l_mode != FMM_M2L_TC) return FMM_ERR_UNSUPPORTED;
   CUDA_TRY(cudaSetDevice(c->cfg.device));
   cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
-  if (!c->col_pairs.reserve((size_t)npairs * 4) || !c->d_acc.reserve((size_t)n * 3)) return FMM_ERR_OUT_OF_MEMORY;
-  CUDA_TRY(cudaMemsetAsync(d_feat, 0, sizeof(float) * (size_t)npairs * ORD_NF, st));
-  CUDA_TRY(cudaMemsetAsync(d_labels, 0, sizeof(float) * (size_t)npairs * ORD_NQ, st));
+  if (!c->col_tiles.reserve((size_t)ntiles * 2) || !c->col_pairs.reserve((size_t)ntiles * 128 * 4) ||
+      !c->col_plabels.reserve((size_t)ntiles * 128 * ORD_NQ) || !c->d_acc.reserve((size_t)n * 3))
+    return FMM_ERR_OUT_OF_MEMORY;
+  CUDA_TRY(cudaMemsetAsync(d_feat, 0, sizeof(float) * (size_t)ntiles * ORD_NF, st));
+  CUDA_TRY(cudaMemsetAsync(d_labels, 0, sizeof(float) * (size_t)ntiles * ORD_NQ, st));
   OrderOpts oo;  // fixed order; collection hook on
-  oo.npairs = npairs;
+  oo.ntiles = ntiles;
   oo.seed = seed;
+  oo.tiles = c->col_tiles.ptr;
   oo.pairs = c->col_pairs.ptr;
+  oo.pair_labels = c->col_plabels.ptr;
   oo.feat = d_feat;
   oo.labels = d_labels;
   int rc = pass(c, n, d_pos, d_mass, c->d_acc.ptr, nullptr, st, oo, true);

@@ -1,5 +1,5 @@
-// Learned expansion order of each M2L pair: cell and pair features, the FP64
-// error probe that labels training pairs, the MLP (forward, backward, Adam)
+// Learned expansion order of the M2L tiles: cell and tile features, the FP64
+// error probe that labels training tiles, the MLP (forward, backward, Adam)
 // and the hot-path inference that sets each M2L tile's order.
 //
 // MLP: 32 inputs -> 64 -> 64 -> 9, ReLU, weights and activations rounded to
@@ -18,8 +18,8 @@ namespace fmm {
 __device__ inline float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
 // ---------------------------------------------------------------- features
-__global__ void k_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int cell0,
-                                int p, int KS, float *cf) {
+__global__ void k_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int count2,
+                                int cell0, int p, int KS, float *cf, double *mtot) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const int c = first + i;
@@ -36,30 +36,9 @@ __global__ void k_cell_features(const float *M, const int *pbeg, const int *pend
     }
     o[n] = v;
   }
-  for (int k = 13; k < ORD_CF; ++k) o[k] = 0.f;
-}
-
-// Features of pair (T, S) with source offset (dx, dy, dz) cells at `level`.
-__device__ inline void pair_features(const float *cfT, const float *cfS, int level, int dx, int dy, int dz, float ax,
-                                     float ay, float az, float *f) {
-  f[0] = level * (1.f / 16.f);
-  f[1] = cfT[0] * 0.125f;
-  f[2] = cfS[0] * 0.125f;
-  for (int k = 0; k < 12; ++k) f[3 + k] = cfS[1 + k] * 0.25f;
-  f[15] = cfT[1] * 0.25f;
-  f[16] = cfT[2] * 0.25f;
-  float e0 = fabsf((float)dx) * ax, e1 = fabsf((float)dy) * ay, e2 = fabsf((float)dz) * az;
-  const float R = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
-  f[17] = R * 0.25f;
-  if (e0 < e1) { const float t = e0; e0 = e1; e1 = t; }
-  if (e1 < e2) { const float t = e1; e1 = e2; e2 = t; }
-  if (e0 < e1) { const float t = e0; e0 = e1; e1 = t; }
-  f[18] = e0 * (1.f / 3.f);
-  f[19] = e1 * (1.f / 3.f);
-  f[20] = e2 * (1.f / 3.f);
-  const float diag = sqrtf(ax * ax + ay * ay + az * az);
-  f[21] = R > 0.f ? log10f(diag / R) : 0.f;
-  for (int k = 22; k < ORD_NF; ++k) f[k] = 0.f;
+  o[13] = m0 > 0.f ? log10f(m0) : -30.f;
+  o[14] = o[15] = 0.f;
+  if (i < count2) atomicAdd(mtot, (double)m[0]);
 }
 
 __device__ inline unsigned long long splitmix(unsigned long long x) {
@@ -69,43 +48,129 @@ __device__ inline unsigned long long splitmix(unsigned long long x) {
   return x ^ (x >> 31);
 }
 
-__global__ void k_order_sample(const int4 *batches, const int *tlist, const int *src_tab, const int *slot_list,
-                               const int *tslot_list, const int *nslots, int nbm, const int *pbeg, const int *pend,
-                               int n, unsigned long long seed, int max_nt, int max_ns, int4 *pairs) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  const unsigned long long h = splitmix(seed * 0x100000001B3ull + (unsigned long long)k);
-  int4 out = make_int4(-1, -1, -1, -1);
-  const int b = (int)(h % (unsigned long long)nbm);
-  const int ns = nslots[b];
-  if (ns > 0) {
-    const int i = (int)((h >> 20) % (unsigned long long)ns);
-    const size_t base = (size_t)b * 189;
-    const int sl = slot_list[base + i];
-    const int4 bt = batches[b];
-    const int t = (int)((h >> 40) % (unsigned long long)bt.y);
-    const int T = tlist[bt.x + t];
-    const int S = src_tab[(base + sl) * 128 + t];
-    if (S >= 0 && pend[T] - pbeg[T] <= max_nt && pend[S] - pbeg[S] <= max_ns)
-      out = make_int4(T, S, tslot_list[base + i], bt.z);
-  }
-  pairs[k] = out;
+__device__ inline float warp_max(float v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
 }
 
-__global__ void k_pair_features(const int4 *pairs, int n, const float *cf, int cell0, float ax, float ay, float az,
-                                float *feat) {
+// Features of tile (batch b, present slot i), computed by one warp (lanes
+// over the 128 rows); every lane returns all of them.  Also returns the
+// offset slot and the level.
+__device__ void tile_features(const TileArgs &a, int b, int i, int lane, float *f, int &off, int &level) {
+  const int4 bt = a.batches[b];
+  const size_t base = (size_t)b * 189;
+  const int sl = a.slot_list[base + i];
+  off = a.tslot_list[base + i];
+  level = bt.z;
+  float mT = 0.f, mS = 0.f, sp1 = -30.f, sp2 = -30.f, mA[13];
+#pragma unroll
+  for (int n = 0; n < 13; ++n) mA[n] = -60.f;
+  int cnt = 0;
+  for (int r = lane; r < bt.y; r += 32) {
+    const int S = a.src_tab[(base + sl) * 128 + r];
+    if (S < 0) continue;
+    const int T = a.tlist[bt.x + r];
+    const float *cT = a.cf + (size_t)(T - a.cell0) * ORD_CF, *cS = a.cf + (size_t)(S - a.cell0) * ORD_CF;
+    mT = fmaxf(mT, cT[0]);
+    mS = fmaxf(mS, cS[0]);
+    sp1 = fmaxf(sp1, cT[1]);
+    sp2 = fmaxf(sp2, cT[2]);
+    const float l0 = cS[13];
+    mA[0] = fmaxf(mA[0], l0);
+#pragma unroll
+    for (int n = 1; n < 13; ++n) mA[n] = fmaxf(mA[n], l0 + cS[n]);
+    ++cnt;
+  }
+  mT = warp_max(mT);
+  mS = warp_max(mS);
+  sp1 = warp_max(sp1);
+  sp2 = warp_max(sp2);
+#pragma unroll
+  for (int n = 0; n < 13; ++n) mA[n] = warp_max(mA[n]);
+#pragma unroll
+  for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  const float lmt = log10f((float)fmax(*a.mtot, 1e-300));
+  f[0] = level * (1.f / 16.f);
+  f[1] = mT * 0.125f;
+  f[2] = mS * 0.125f;
+#pragma unroll
+  for (int n = 0; n < 13; ++n) f[3 + n] = fmaxf(mA[n] - lmt, -40.f) * 0.25f;
+  f[16] = sp1 * 0.25f;
+  f[17] = sp2 * 0.25f;
+  f[18] = cnt * (1.f / 128.f);
+  const int dx = off % 7 - 3, dy = (off / 7) % 7 - 3, dz = off / 49 - 3;
+  float e0 = fabsf((float)dx) * a.ax, e1 = fabsf((float)dy) * a.ay, e2 = fabsf((float)dz) * a.az;
+  const float R = sqrtf(e0 * e0 + e1 * e1 + e2 * e2);
+  f[19] = R * 0.25f;
+  if (e0 < e1) { const float t = e0; e0 = e1; e1 = t; }
+  if (e1 < e2) { const float t = e1; e1 = e2; e2 = t; }
+  if (e0 < e1) { const float t = e0; e0 = e1; e1 = t; }
+  f[20] = e0 * (1.f / 3.f);
+  f[21] = e1 * (1.f / 3.f);
+  f[22] = e2 * (1.f / 3.f);
+  const float diag = sqrtf(a.ax * a.ax + a.ay * a.ay + a.az * a.az);
+  f[23] = R > 0.f ? log10f(diag / R) : 0.f;
+#pragma unroll
+  for (int k = 24; k < ORD_NF; ++k) f[k] = 0.f;
+  if (cnt == 0) {
+#pragma unroll
+    for (int k = 0; k < ORD_NF; ++k) f[k] = 0.f;
+  }
+}
+
+// One warp per sampled tile.
+__global__ void k_order_sample_tiles(TileArgs a, int nbm, int n, unsigned long long seed, int2 *tiles, float *feat,
+                                     int4 *pairs) {
+  const int lane = threadIdx.x & 31;
+  const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (k >= n) return;
+  const unsigned long long h = splitmix(seed * 0x100000001B3ull + (unsigned long long)k);
+  const int b = (int)(h % (unsigned long long)nbm);
+  const int ns = a.nslots[b];
+  int4 *pr = pairs + (size_t)k * 128;
+  if (ns == 0) {
+    if (lane == 0) tiles[k] = make_int2(-1, -1);
+    for (int r = lane; r < 128; r += 32) pr[r] = make_int4(-1, -1, -1, -1);
+    for (int q = lane; q < ORD_NF; q += 32) feat[(size_t)k * ORD_NF + q] = 0.f;
+    return;
+  }
+  const int i = (int)((h >> 20) % (unsigned long long)ns);
+  float f[ORD_NF];
+  int off, level;
+  tile_features(a, b, i, lane, f, off, level);
+  if (lane == 0) tiles[k] = make_int2(b, i);
+  for (int q = 0; q < ORD_NF; ++q)
+    if (lane == q) feat[(size_t)k * ORD_NF + q] = f[q];
+  const int4 bt = a.batches[b];
+  const size_t base = (size_t)b * 189;
+  const int sl = a.slot_list[base + i];
+  for (int r = lane; r < 128; r += 32) {
+    int4 v = make_int4(-1, -1, -1, -1);
+    if (r < bt.y) {
+      const int S = a.src_tab[(base + sl) * 128 + r];
+      if (S >= 0) v = make_int4(a.tlist[bt.x + r], S, off, level);
+    }
+    pr[r] = v;
+  }
+}
+
+__global__ void k_tile_labels(const float *pl, int n, const double *mtot, float *labels, float *feat) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
-  float f[ORD_NF];
-  const int4 pr = pairs[k];
-  if (pr.x < 0) {
-    for (int i = 0; i < ORD_NF; ++i) f[i] = 0.f;
-  } else {
-    const int o = pr.z;
-    pair_features(cf + (size_t)(pr.x - cell0) * ORD_CF, cf + (size_t)(pr.y - cell0) * ORD_CF, pr.w, o % 7 - 3,
-                  (o / 7) % 7 - 3, o / 49 - 3, ax, ay, az, f);
+  const float lmt = log10f((float)fmax(*mtot, 1e-300));
+  float mx[ORD_NQ];
+  bool any = false;
+  for (int q = 0; q < ORD_NQ; ++q) mx[q] = -1e30f;
+  for (int r = 0; r < 128; ++r) {
+    const float *l = pl + ((size_t)k * 128 + r) * ORD_NQ;
+    if (l[0] < -1e29f) continue;
+    any = true;
+    for (int q = 0; q < ORD_NQ; ++q) mx[q] = fmaxf(mx[q], l[q]);
   }
-  for (int i = 0; i < ORD_NF; ++i) feat[(size_t)k * ORD_NF + i] = f[i];
+  for (int q = 0; q < ORD_NQ; ++q) labels[(size_t)k * ORD_NQ + q] = any ? mx[q] - lmt : 0.f;
+  if (!any)
+    for (int q = 0; q < ORD_NF; ++q) feat[(size_t)k * ORD_NF + q] = 0.f;
 }
 
 // ---------------------------------------------------------------- FP64 probe
@@ -178,7 +243,7 @@ __global__ void __launch_bounds__(PROBE_T) k_probe(ProbeArgs a) {
   const int4 pr = reinterpret_cast<const int4 *>(a.pairs)[blockIdx.x];
   float *lab = a.labels + (size_t)blockIdx.x * ORD_NQ;
   if (pr.x < 0) {
-    if (tid < ORD_NQ) lab[tid] = 0.f;
+    if (tid < ORD_NQ) lab[tid] = -1e30f;
     return;
   }
   const int T = pr.x, S = pr.y, d = pr.w;
@@ -306,9 +371,7 @@ __global__ void __launch_bounds__(PROBE_T) k_probe(ProbeArgs a) {
     if (tid < nq) {
       double R2 = 0.0;
       for (int k = 0; k < 3; ++k) R2 += (cS[k] - cT[k]) * (cS[k] - cT[k]);
-      const double scale = Ms[0] * sqrt((double)ntc) / R2;
-      const double rel = scale > 0.0 ? sqrt(e2[tid]) / scale : 0.0;
-      v = (float)log10(rel + 1e-30);
+      v = (float)log10(sqrt(e2[tid] / (double)ntc) * R2 + 1e-300);
     }
     lab[tid] = v;
   }
@@ -452,59 +515,86 @@ static size_t mlp_grad_smem() {
 }
 
 // ---------------------------------------------------------------- inference
-// One block per M2L batch, one thread per target row; for every present
-// slot each row predicts its pair's errors and takes the lowest order within
-// its budget; the slot takes the largest order of its rows.
-__global__ void __launch_bounds__(128) k_order_infer(InferArgs a) {
-  __shared__ float w[ORD_NPARAM];
-  __shared__ int s_q;
-  const int tid = threadIdx.x;
-  load_params(a.params, w);
-  const int4 bt = a.batches[blockIdx.x];
-  const int T = tid < bt.y ? a.tlist[bt.x + tid] : -1;
-  const int ns = a.nslots[blockIdx.x];
-  const size_t base = (size_t)blockIdx.x * 189;
+// One block per M2L batch; each warp takes present slots (tiles) in turn:
+// tile features, the MLP with the lanes over the hidden units (weights
+// transposed in shared memory), then the lowest order within the budget.
+static constexpr int INF_WARPS = 8;
+
+__global__ void __launch_bounds__(32 * INF_WARPS) k_order_infer(InferArgs a) {
+  __shared__ float w1t[ORD_NF * ORD_NH], w2t[ORD_NH * ORD_NH], w3t[ORD_NH * 16], bias[2 * ORD_NH + 16];
+  __shared__ float hs[INF_WARPS][2][ORD_NH];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < ORD_NH * ORD_NF; e += blockDim.x) {
+    const int j = e / ORD_NF, i = e % ORD_NF;
+    w1t[i * ORD_NH + j] = bf16r(a.params[ORD_W1 + e]);
+  }
+  for (int e = tid; e < ORD_NH * ORD_NH; e += blockDim.x) {
+    const int j = e / ORD_NH, i = e % ORD_NH;
+    w2t[i * ORD_NH + j] = bf16r(a.params[ORD_W2 + e]);
+  }
+  for (int e = tid; e < 16 * ORD_NH; e += blockDim.x) {
+    const int o = e / ORD_NH, i = e % ORD_NH;
+    w3t[i * 16 + o] = bf16r(a.params[ORD_W3 + e]);
+  }
+  for (int e = tid; e < ORD_NH; e += blockDim.x) {
+    bias[e] = a.params[ORD_B1 + e];
+    bias[ORD_NH + e] = a.params[ORD_B2 + e];
+  }
+  if (tid < 16) bias[2 * ORD_NH + tid] = a.params[ORD_B3 + tid];
+  __syncthreads();
+  const int b = blockIdx.x;
+  const int ns = a.t.nslots[b];
+  const size_t base = (size_t)b * 189;
   const double frms = *a.frms;
   const double pbar = a.n > 0 ? (double)(*a.nt_sum) / (double)a.n : 1.0;
-  const int pmax = a.p;
-  const float *cfT = T >= 0 ? a.cf + (size_t)(T - a.cell0) * ORD_CF : nullptr;
-  const float sd = (float)(a.emax * ldexp(1.0, -bt.z));  // isotropic scale of the level
-  __syncthreads();
-  for (int i = 0; i < ns; ++i) {
-    if (tid == 0) s_q = ORD_QMIN;
-    __syncthreads();
-    const int sl = a.slot_list[base + i];
-    const int o = a.tslot_list[base + i];
-    const int S = T >= 0 ? a.src_tab[(base + sl) * 128 + tid] : -1;
-    int q = ORD_QMIN;
-    if (S >= 0) {
-      if (!(frms > 0.0)) {
-        q = pmax;
-      } else {
-        const int dx = o % 7 - 3, dy = (o / 7) % 7 - 3, dz = o / 49 - 3;
-        float f[ORD_NF], h1[ORD_NH], h2[ORD_NH], y[ORD_NQ];
-        pair_features(cfT, a.cf + (size_t)(S - a.cell0) * ORD_CF, bt.z, dx, dy, dz, a.ax, a.ay, a.az, f);
-        for (int k = 0; k < ORD_NF; ++k) f[k] = bf16r(f[k]);
-        mlp_forward(w, f, h1, h2, y);
-        const float ex = dx * a.ax * sd, ey = dy * a.ay * sd, ez = dz * a.az * sd;
-        const float R2 = ex * ex + ey * ey + ez * ez;
-        const float ms = a.M[(size_t)(S - a.cell0) * a.KS];
-        const float thr = ms > 0.f ? log10f(a.tol * (float)frms * R2 / (ms * (float)sqrt(pbar))) : 30.f;
-        q = pmax;
-        for (int qq = ORD_QMIN; qq < pmax; ++qq)
-          if (y[qq - ORD_QMIN] <= thr) {
-            q = qq;
-            break;
-          }
+  const float lmt = log10f((float)fmax(*a.t.mtot, 1e-300));
+  const float sd = (float)(a.emax * ldexp(1.0, -a.t.batches[b].z));
+  for (int i = warp; i < ns; i += INF_WARPS) {
+    int q = a.p;
+    if (frms > 0.0) {
+      float f[ORD_NF];
+      int off, level;
+      tile_features(a.t, b, i, lane, f, off, level);
+      // layer 1: units lane and lane + 32
+      float h0 = bias[lane], h1 = bias[lane + 32];
+#pragma unroll
+      for (int k = 0; k < ORD_NF; ++k) {
+        const float x = bf16r(f[k]);
+        h0 = fmaf(w1t[k * ORD_NH + lane], x, h0);
+        h1 = fmaf(w1t[k * ORD_NH + lane + 32], x, h1);
       }
-      atomicMax(&s_q, q);
+      hs[warp][0][lane] = bf16r(fmaxf(h0, 0.f));
+      hs[warp][0][lane + 32] = bf16r(fmaxf(h1, 0.f));
+      __syncwarp();
+      float g0 = bias[ORD_NH + lane], g1 = bias[ORD_NH + lane + 32];
+#pragma unroll 8
+      for (int k = 0; k < ORD_NH; ++k) {
+        const float x = hs[warp][0][k];
+        g0 = fmaf(w2t[k * ORD_NH + lane], x, g0);
+        g1 = fmaf(w2t[k * ORD_NH + lane + 32], x, g1);
+      }
+      hs[warp][1][lane] = bf16r(fmaxf(g0, 0.f));
+      hs[warp][1][lane + 32] = bf16r(fmaxf(g1, 0.f));
+      __syncwarp();
+      float y = 0.f;
+      if (lane < ORD_NQ) {
+        y = bias[2 * ORD_NH + lane];
+        for (int k = 0; k < ORD_NH; ++k) y = fmaf(w3t[k * 16 + lane], hs[warp][1][k], y);
+      }
+      __syncwarp();
+      // budget of this tile's offset
+      const int dx = off % 7 - 3, dy = (off / 7) % 7 - 3, dz = off / 49 - 3;
+      const float ex = dx * a.t.ax * sd, ey = dy * a.t.ay * sd, ez = dz * a.t.az * sd;
+      const float R2 = ex * ex + ey * ey + ez * ez;
+      const float thr = log10f(a.tol * (float)frms * R2 / (float)sqrt(pbar)) - lmt;
+      const unsigned ok = __ballot_sync(0xffffffffu, lane < ORD_NQ && ORD_QMIN + lane < a.p && y <= thr);
+      q = ok ? ORD_QMIN + __ffs(ok) - 1 : a.p;
+      if (f[18] == 0.f) q = ORD_QMIN;  // no pair in the tile
     }
-    __syncthreads();
-    if (tid == 0) {
-      const int K = (s_q + 1) * (s_q + 1);
+    if (lane == 0) {
+      const int K = (q + 1) * (q + 1);
       a.slot_p16[base + i] = (uint8_t)((K + 15) & ~15);
     }
-    __syncthreads();
   }
 }
 
@@ -556,30 +646,28 @@ int order_judge_compare(const double *acc, const double *ref, const int64_t *tar
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
 }
 
-int order_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int cell0, int p,
-                        int KS, float *cf, cudaStream_t st, int64_t &launches) {
+int order_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int count2, int cell0,
+                        int p, int KS, float *cf, double *mtot, cudaStream_t st, int64_t &launches) {
   if (count <= 0) return FMM_OK;
-  k_cell_features<<<cdiv(count, 256), 256, 0, st>>>(M, pbeg, pend, first, count, cell0, p, KS, cf);
+  CUDA_TRY(cudaMemsetAsync(mtot, 0, sizeof(double), st));
+  k_cell_features<<<cdiv(count, 256), 256, 0, st>>>(M, pbeg, pend, first, count, count2, cell0, p, KS, cf, mtot);
   launches += 1;
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
 }
 
-int order_sample_pairs(const int4 *batches, const int *tlist, const int *src_tab, const int *slot_list,
-                       const int *tslot_list, const int *nslots, int nbm, const int *pbeg, const int *pend, int n,
-                       unsigned long long seed, int max_nt, int max_ns, int *pairs, cudaStream_t st,
-                       int64_t &launches) {
+int order_sample_tiles(const TileArgs &a, int nbm, int n, unsigned long long seed, int *tiles, float *feat,
+                       int *pairs, cudaStream_t st, int64_t &launches) {
   if (n <= 0 || nbm <= 0) return FMM_OK;
-  k_order_sample<<<cdiv(n, 256), 256, 0, st>>>(batches, tlist, src_tab, slot_list, tslot_list, nslots, nbm, pbeg,
-                                               pend, n, seed, max_nt, max_ns, reinterpret_cast<int4 *>(pairs));
+  k_order_sample_tiles<<<cdiv((int64_t)n * 32, 256), 256, 0, st>>>(a, nbm, n, seed, reinterpret_cast<int2 *>(tiles),
+                                                                   feat, reinterpret_cast<int4 *>(pairs));
   launches += 1;
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
 }
 
-int order_pair_features(const int *pairs, int n, const float *cf, int cell0, float ax, float ay, float az,
-                        float *feat, cudaStream_t st, int64_t &launches) {
+int order_tile_labels(const float *pair_labels, int n, const double *mtot, float *labels, float *feat,
+                      cudaStream_t st, int64_t &launches) {
   if (n <= 0) return FMM_OK;
-  k_pair_features<<<cdiv(n, 256), 256, 0, st>>>(reinterpret_cast<const int4 *>(pairs), n, cf, cell0, ax, ay, az,
-                                                feat);
+  k_tile_labels<<<cdiv(n, 128), 128, 0, st>>>(pair_labels, n, mtot, labels, feat);
   launches += 1;
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
 }
@@ -597,7 +685,7 @@ int order_probe_errors(const ProbeArgs &a, cudaStream_t st, int64_t &launches) {
 
 int order_infer(const InferArgs &a, int nbm, cudaStream_t st, int64_t &launches) {
   if (nbm <= 0) return FMM_OK;
-  k_order_infer<<<nbm, 128, 0, st>>>(a);
+  k_order_infer<<<nbm, 32 * INF_WARPS, 0, st>>>(a);
   launches += 1;
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
 }

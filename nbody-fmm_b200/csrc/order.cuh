@@ -1,14 +1,20 @@
-// Learned expansion order of each M2L pair (FMM_ORDER_LEARNED).
+// Learned expansion order of the M2L tiles (FMM_ORDER_LEARNED).
 //
-// A small MLP reads the features of an interaction-list pair (level, particle
-// counts, the source cell's multipole spectrum by degree, the target cell's
-// spread, the offset geometry) and predicts, for every order q in 4..12, the
-// base-10 logarithm of the pair's truncation error on the target particles
-// relative to the pair's monopole scale M_S sqrt(n_T) / R^2.  A pair takes the
-// lowest order whose predicted error fits its share of the error budget.
-// Training pairs and their errors come from the FMM itself: sampled M2L pairs
-// whose truncation error at every order is measured in FP64 against the
-// pair's direct sum.
+// An M2L tile is the unit of tensor-core work: up to 128 target cells of one
+// level and child class against their sources at one interaction offset, all
+// evaluated at one order.  A small MLP reads the tile's features (level,
+// offset geometry, the largest particle counts, the largest source multipole
+// norm of every degree relative to the total mass, the target cells' spread)
+// and predicts, for every order q in 4..12, the base-10 logarithm of
+//   z(q) = max over the tile's pairs of  e(q) / sqrt(n_T) * R^2 / M_tot,
+// e(q) the pair's truncation error on its target particles (L2 over them,
+// G = 1), R the distance of the cell centres and M_tot the total mass.  The
+// tile takes the lowest order with z(q) <= tol F_rms R^2 / (M_tot sqrt(P)),
+// which gives every pair the same share of the squared error budget
+// tol^2 F_rms^2 n (F_rms the RMS force of the previous pass, P the M2L pairs
+// per particle).  Training tiles come from the FMM itself: every pair of a
+// sampled tile has its truncation error at every order measured in FP64
+// against its direct sum.
 #pragma once
 #include "tree.cuh"
 
@@ -33,24 +39,32 @@ struct OrderGeom {
   double lo[3], ext[3], emax;
 };
 
-// Per-cell features of cells [first, first + count): log2(1 + n) and
-// log10(|M~_n| / |M~_0|) for n = 1..12 (|M~_n|^2 = sum over m of |M~_n^m|^2).
-int order_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int cell0, int p,
-                        int KS, float *cf, cudaStream_t st, int64_t &launches);
+// Per-cell features of cells [first, first + count): log2(1 + n),
+// log10(|M~_n| / |M~_0|) for n = 1..12 (|M~_n|^2 = sum over m of |M~_n^m|^2)
+// and log10 M~_0; the cells [first, first + count2) (one full level) also add
+// their M~_0 into *mtot (the total mass).
+int order_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int count2, int cell0,
+                        int p, int KS, float *cf, double *mtot, cudaStream_t st, int64_t &launches);
 
-// Samples n M2L pairs {T, S, offset slot, level} from the resolved M2L
-// tables; -1 entries where the draw found no pair or a cell above the caps.
-int order_sample_pairs(const int4 *batches, const int *tlist, const int *src_tab, const int *slot_list,
-                       const int *tslot_list, const int *nslots, int nbm, const int *pbeg, const int *pend, int n,
-                       unsigned long long seed, int max_nt, int max_ns, int *pairs, cudaStream_t st,
-                       int64_t &launches);
+// The resolved M2L tables and what the tile features read.
+struct TileArgs {
+  const int4 *batches;
+  const int *tlist, *src_tab, *slot_list, *tslot_list, *nslots;
+  const int *pbeg, *pend;
+  const float *cf;      // cell features
+  const double *mtot;   // device: total mass
+  int cell0;
+  float ax, ay, az;     // cell aspect (extent / largest extent)
+};
 
-// Features of the sampled pairs ([n][ORD_NF]).
-int order_pair_features(const int *pairs, int n, const float *cf, int cell0, float ax, float ay, float az,
-                        float *feat, cudaStream_t st, int64_t &launches);
+// Samples n tiles {batch, present-slot index} (-1 where the drawn batch has
+// no slot), their features ([n][ORD_NF]) and their pairs ([n][128] int4
+// {T, S, offset slot, level}, -1 rows where the tile has no pair).
+int order_sample_tiles(const TileArgs &a, int nbm, int n, unsigned long long seed, int *tiles, float *feat,
+                       int *pairs, cudaStream_t st, int64_t &launches);
 
-// FP64 truncation errors of the sampled pairs at orders 4..p ([n][ORD_NQ],
-// log10 of the error over the pair's monopole scale; orders above p = 0).
+// FP64 truncation errors of pairs at orders 4..p: log10(e(q) / sqrt(n_T) R^2)
+// per pair ([n][ORD_NQ]; -1e30 for rows without a pair; orders above p: 0).
 struct ProbeArgs {
   const int *pairs;
   int n;
@@ -65,24 +79,21 @@ struct ProbeArgs {
 };
 int order_probe_errors(const ProbeArgs &a, cudaStream_t st, int64_t &launches);
 
-// Hot path: the order of every present slot of every M2L batch (padded
-// width into slot_p16) from the MLP, with a row's budget
-// log10(tol * F_rms * R^2 / (M_S * sqrt(P))), F_rms the RMS force of the
-// previous pass (G = 1 units; <= 0: every slot at full order) and
-// P = (sum over M2L pairs of n_T) / n the M2L pairs per particle.
+// Tile labels: the largest pair label of each tile minus log10 M_tot
+// ([n][ORD_NQ]); tiles without a pair get zero features and labels.
+int order_tile_labels(const float *pair_labels, int n, const double *mtot, float *labels, float *feat,
+                      cudaStream_t st, int64_t &launches);
+
+// Hot path: the order of every present slot of every M2L batch from the MLP
+// (padded width into slot_p16).  F_rms <= 0 (no previous pass): full order.
 struct InferArgs {
-  const int4 *batches;
-  const int *tlist, *src_tab, *slot_list, *tslot_list, *nslots;
-  const int *pbeg, *pend;
-  const float *cf;       // cell features
-  const float *M;        // multipoles (M~_0 = source mass)
+  TileArgs t;
   const float *params;   // MLP parameters (FP32; weights rounded to BF16 on load)
   const double *frms;    // device: F_rms of the previous pass, G = 1 units
   const unsigned long long *nt_sum;  // device: sum over M2L pairs of n_T
   int64_t n;
-  int cell0, KS, p, dim;
+  int p;
   float tol;
-  float ax, ay, az;      // cell aspect (extent / largest extent)
   double emax;
   uint8_t *slot_p16;
 };

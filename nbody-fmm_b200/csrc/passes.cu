@@ -1151,7 +1151,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
       return FMM_ERR_OUT_OF_MEMORY;
     const bool geometric = tc && order.mode == FMM_ORDER_GEOMETRIC;
     const bool learned = tc && dim == 3 && order.mode == FMM_ORDER_LEARNED && order.params;
-    const bool collect = tc && dim == 3 && order.npairs > 0 && ops.tab64.ptr;
+    const bool collect = tc && dim == 3 && order.ntiles > 0 && ops.tab64.ptr;
     const bool var_order = geometric || learned;
     const float ax = (float)(g.ext[0] / emax), ay = (float)(g.ext[1] / emax),
                 az = (float)(dim == 3 ? g.ext[2] / emax : 0.0);
@@ -1162,11 +1162,26 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
                                        eb.order_p16.ptr);
       ws.launches += 1;
     }
+    TileArgs tla;
     if (learned || collect) {
-      if (!eb.cf.reserve((size_t)ncell * ORD_CF)) return FMM_ERR_OUT_OF_MEMORY;
-      int rc = order_cell_features(eb.M.ptr, ws.cell_pbeg, ws.cell_pend, t.level_off[2], ntl, cell0, p, KS, eb.cf.ptr,
-                                   st, ws.launches);
+      if (!eb.cf.reserve((size_t)ncell * ORD_CF) || !eb.frms.reserve(3)) return FMM_ERR_OUT_OF_MEMORY;
+      int rc = order_cell_features(eb.M.ptr, ws.cell_pbeg, ws.cell_pend, t.level_off[2], ntl, t.level_count[2], cell0,
+                                   p, KS, eb.cf.ptr, eb.frms.ptr + 2, st, ws.launches);
       if (rc) return rc;
+      tla.batches = c2.batches;
+      tla.tlist = tl_m2l;
+      tla.src_tab = eb.m2l_src.ptr;
+      tla.slot_list = eb.m2l_list.ptr;
+      tla.tslot_list = eb.m2l_tslot.ptr;
+      tla.nslots = eb.m2l_nslots.ptr;
+      tla.pbeg = ws.cell_pbeg;
+      tla.pend = ws.cell_pend;
+      tla.cf = eb.cf.ptr;
+      tla.mtot = eb.frms.ptr + 2;
+      tla.cell0 = cell0;
+      tla.ax = ax;
+      tla.ay = ay;
+      tla.az = az;
     }
     if (nbm > 0) {
       k_m2l_sources<<<nbm, 256, 0, st>>>(c2, tchunk, eb.m2l_src.ptr, eb.m2l_list.ptr, eb.m2l_nslots.ptr,
@@ -1176,46 +1191,26 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
       ws.launches += 1;
     }
     if (learned && nbm > 0) {
-      if (!eb.frms.reserve(2)) return FMM_ERR_OUT_OF_MEMORY;
       InferArgs ia;
-      ia.batches = c2.batches;
-      ia.tlist = tl_m2l;
-      ia.src_tab = eb.m2l_src.ptr;
-      ia.slot_list = eb.m2l_list.ptr;
-      ia.tslot_list = eb.m2l_tslot.ptr;
-      ia.nslots = eb.m2l_nslots.ptr;
-      ia.pbeg = ws.cell_pbeg;
-      ia.pend = ws.cell_pend;
-      ia.cf = eb.cf.ptr;
-      ia.M = eb.M.ptr;
+      ia.t = tla;
       ia.params = order.params;
       ia.frms = eb.frms.ptr;
       ia.nt_sum = ws.counters + 4;
       ia.n = n;
-      ia.cell0 = cell0;
-      ia.KS = KS;
       ia.p = p;
-      ia.dim = dim;
       ia.tol = order.tol;
-      ia.ax = ax;
-      ia.ay = ay;
-      ia.az = az;
       ia.emax = emax;
       ia.slot_p16 = eb.m2l_w.ptr;
       int rc = order_infer(ia, nbm, st, ws.launches);
       if (rc) return rc;
     }
     if (collect && nbm > 0) {
-      int rc = order_sample_pairs(c2.batches, tl_m2l, eb.m2l_src.ptr, eb.m2l_list.ptr, eb.m2l_tslot.ptr,
-                                  eb.m2l_nslots.ptr, nbm, ws.cell_pbeg, ws.cell_pend, order.npairs, order.seed,
-                                  1 << 30, 1 << 17, order.pairs, st, ws.launches);
-      if (!rc)
-        rc = order_pair_features(order.pairs, order.npairs, eb.cf.ptr, cell0, ax, ay, az, order.feat, st,
-                                 ws.launches);
+      int rc = order_sample_tiles(tla, nbm, order.ntiles, order.seed, order.tiles, order.feat, order.pairs, st,
+                                  ws.launches);
       if (!rc) {
         ProbeArgs pa;
         pa.pairs = order.pairs;
-        pa.n = order.npairs;
+        pa.n = order.ntiles * 128;
         pa.pos = d_pos_g;
         pa.mass = d_mass_g;
         pa.perm = t.d_perm;
@@ -1231,9 +1226,11 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
           pa.g.ext[k] = g.ext[k];
         }
         pa.g.emax = emax;
-        pa.labels = order.labels;
+        pa.labels = order.pair_labels;
         rc = order_probe_errors(pa, st, ws.launches);
       }
+      if (!rc) rc = order_tile_labels(order.pair_labels, order.ntiles, eb.frms.ptr + 2, order.labels, order.feat, st,
+                                      ws.launches);
       if (rc) return rc;
     }
     int rc;

@@ -292,11 +292,11 @@ class Context:
         _check(_lib.fmm_order_get_model(self._h, _p(out, ctypes.POINTER(ctypes.c_float)), out.size))
         return out
 
-    def order_collect(self, n, pos_ptr, mass_ptr, npairs, seed, feat_ptr, labels_ptr, stream=None):
+    def order_collect(self, n, pos_ptr, mass_ptr, ntiles, seed, feat_ptr, labels_ptr, stream=None):
         """One fixed-order evaluation that writes the features and FP64
-        truncation-error labels of npairs sampled M2L pairs into device
+        truncation-error labels of ntiles sampled M2L tiles into device
         buffers (fmm_order_collect)."""
-        _check(_lib.fmm_order_collect(self._h, n, pos_ptr, mass_ptr, npairs, seed, feat_ptr, labels_ptr, stream))
+        _check(_lib.fmm_order_collect(self._h, n, pos_ptr, mass_ptr, ntiles, seed, feat_ptr, labels_ptr, stream))
 
     def order_train(self, feat_ptr, labels_ptr, n, epochs, batch=8192, lr=1e-3):
         """Trains the loaded model in place on device data; returns the mean
