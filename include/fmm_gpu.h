@@ -110,7 +110,9 @@ typedef struct fmm_config {
                          as in the reference; -1 = automatic */
   int32_t order_mode; /* FMM_ORDER_*: expansion order of each M2L pair (tensor-core mode only) */
   int32_t order_margin; /* FMM_ORDER_GEOMETRIC: orders added to each reduced pair order */
-  float order_tol;      /* FMM_ORDER_LEARNED: relative L2 force budget of the reduced orders (default 5e-7) */
+  float order_tol;      /* FMM_ORDER_LEARNED: relative L2 force budget of the reduced orders (default 4e-6:
+                           the tile bound is conservative; on a 2^20 Plummer sphere at p = 12 it adds
+                           about 1e-7 to the FP32 error of fixed p) */
   int32_t judge_samples;/* FMM_ORDER_LEARNED: targets checked against the FP64 direct sum (0 = no check) */
   float judge_budget;   /* FMM_ORDER_LEARNED: relative L2 error above which the evaluation is redone at p */
   int32_t reserved[1];
@@ -135,6 +137,8 @@ typedef struct fmm_stats {
   int64_t direct_max;       /* the direct-pair threshold the pass used */
   double judge_rel_l2;      /* FMM_ORDER_LEARNED with judge_samples: the checked relative L2 error */
   int64_t order_fallbacks;  /* FMM_ORDER_LEARNED: 1 if the judge sent the evaluation back to fixed p */
+  int64_t m2l_width_sum;    /* FMM_M2L_TC: sum over the M2L tiles of their padded width (16 ceil(K_q / 16)) */
+  double reserved[7];
 } fmm_stats;
 
 typedef struct fmm_ctx fmm_ctx;

@@ -102,7 +102,7 @@ int fmm_config_default(fmm_config *cfg) {
   cfg->direct_max = -1;
   cfg->order_mode = FMM_ORDER_FIXED;
   cfg->order_margin = 1;
-  cfg->order_tol = 5e-7f;
+  cfg->order_tol = 4e-6f;
   cfg->judge_samples = 0;
   cfg->judge_budget = 1e-6f;
   return FMM_OK;
@@ -302,12 +302,13 @@ static int finish(fmm_ctx *c, cudaStream_t st) {
   unsigned int herr = 0;
   CUDA_TRY(cudaMemcpy(&herr, c->ws.dev_err, sizeof(herr), cudaMemcpyDeviceToHost));
   if (c->timing_pending) {
-    unsigned long long cnt[4] = {0, 0, 0, 0};  // [4] (sum of n_T) stays on the device
+    unsigned long long cnt[6] = {0, 0, 0, 0, 0, 0};
     CUDA_TRY(cudaMemcpy(cnt, c->ws.counters, sizeof(cnt), cudaMemcpyDeviceToHost));
     c->stats.m2l_pairs = (int64_t)cnt[0];
     c->stats.p2p_pairs = (int64_t)(cnt[1] + cnt[3]);
     c->stats.far_direct_pairs = (int64_t)cnt[3];
     c->stats.m2l_tiles = (int64_t)cnt[2];
+    c->stats.m2l_width_sum = (int64_t)cnt[5];
     float ms[5] = {0, 0, 0, 0, 0};
     for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], c->ev[i], c->ev[i + 1]);
     c->stats.ms_tree = ms[0];

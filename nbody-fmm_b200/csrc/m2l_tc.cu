@@ -246,6 +246,12 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
         s_n[buf] = n;
         s_b[buf] = b;
         if (n && a.mode == TC_M2L && a.tiles) atomicAdd(a.tiles, (unsigned long long)n);
+        if (n && a.mode == TC_M2L && a.widths) {
+          unsigned long long ws = 0;
+          const size_t tb = (size_t)b * TC_MAX_SLOTS;
+          for (int i = 0; i < n; ++i) ws += a.slot_p16 ? a.slot_p16[tb + i] : (unsigned long long)P16;
+          atomicAdd(a.widths, ws);
+        }
       }
       __syncthreads();  // also keeps s_grab until everyone has read it
       if (n) return tg;
@@ -333,16 +339,18 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
       else src = a.cparent[tg];
     }
     const float4 *xr = (const float4 *)(a.X + (size_t)(src >= 0 ? src - a.cell0 : 0) * a.KS);
+    const int lim = min(a.KS, (int)s_w[buf][i]);  // the slot's order needs its first w inputs
 #pragma unroll
-    for (int q = 0; q < P16 / 4; ++q) rv[q] = (src >= 0 && 4 * q < a.KS) ? xr[q] : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int q = 0; q < P16 / 4; ++q) rv[q] = (src >= 0 && 4 * q < lim) ? xr[q] : make_float4(0.f, 0.f, 0.f, 0.f);
   };
   // A operand of the next slot from the prefetched rows: two values per
   // conversion (cvt.rn.bf16x2.f32), the same round-to-nearest splits as
   // split3.  Columns K..KS-1 of a row are zero in memory and beyond KS the
   // prefetch is zero, so no masking is needed.
-  auto write_a = [&]() {
+  auto write_a = [&](int w) {
 #pragma unroll
     for (int kc = 0; kc < KC; ++kc) {
+      if (kc * 8 >= w) break;  // the MMAs of a slot of width w read only its first w columns
       const float v[8] = {rv[2 * kc].x, rv[2 * kc].y, rv[2 * kc].z, rv[2 * kc].w,
                           rv[2 * kc + 1].x, rv[2 * kc + 1].y, rv[2 * kc + 1].z, rv[2 * kc + 1].w};
       uint32_t h[4], m[4], l[4];
@@ -368,7 +376,7 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
   while (ok) {
     const int n = s_n[c];
     for (int j = 0; j < n; ++j, ++sidx) {
-      write_a();
+      write_a(s_w[c][j]);
       tc_fence_before();
       __syncthreads();
       tc_fence_after();

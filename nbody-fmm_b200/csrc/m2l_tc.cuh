@@ -30,6 +30,7 @@ struct TcArgs {
   int cell0, K, KS, P16;    // P16 = K rounded up to 16
   unsigned int *err;
   unsigned long long *tiles;  // M2L: number of (batch, slot) tiles contracted (nullable)
+  unsigned long long *widths; // M2L: sum of the tiles' padded widths (nullable)
 };
 
 // Width of the first output tile: one tile up to 128 columns, else two.

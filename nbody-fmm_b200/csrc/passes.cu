@@ -1246,6 +1246,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
       t2.X = eb.M.ptr;
       t2.Y = eb.L.ptr;
       t2.tiles = ws.counters + 2;
+      t2.widths = ws.counters + 5;
       t2.slot_p16 = var_order ? eb.m2l_w.ptr : nullptr;
       rc = tc_launch(t2, nbm, eb.tc_work.ptr + tc_k++, st, ws.launches);
     } else {

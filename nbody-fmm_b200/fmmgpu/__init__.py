@@ -73,7 +73,7 @@ class FmmStats(ctypes.Structure):
         ("ms_downward", ctypes.c_double), ("ms_p2p", ctypes.c_double), ("ms_total", ctypes.c_double),
         ("m2l_tiles", ctypes.c_int64), ("ms_far_direct", ctypes.c_double),
         ("far_direct_pairs", ctypes.c_int64), ("direct_max", ctypes.c_int64), ("judge_rel_l2", ctypes.c_double),
-        ("order_fallbacks", ctypes.c_int64),
+        ("order_fallbacks", ctypes.c_int64), ("m2l_width_sum", ctypes.c_int64), ("reserved", ctypes.c_double * 7),
     ]
 
 
@@ -156,7 +156,7 @@ class Context:
     """One FMM force evaluator on one GPU (fmm_create / fmm_destroy)."""
 
     def __init__(self, dim=3, p=8, leaf_cap=64, m2l_mode=FMM_M2L_FP32, eps2=0.0, G=1.0, device=0, direct_max=-1,
-                 order_mode=FMM_ORDER_FIXED, order_margin=1, order_tol=5e-7, judge_samples=0, judge_budget=1e-6,
+                 order_mode=FMM_ORDER_FIXED, order_margin=1, order_tol=4e-6, judge_samples=0, judge_budget=1e-6,
                  order_model=None):
         L = load_library()
         cfg = FmmConfig()
