@@ -21,8 +21,15 @@ value: N * K / (sum of the K per-step device times), inputs resident in HBM,
        written between steps (outside the event pair) to flush L2.  With N
        GPUs each rank runs its own replica (the single-system pass does not
        shard), value sums the particles of all ranks over the slowest rank.
-plain: the same workload, order and error through the plain FP32 GPU FMM
-       (SIMT contractions, FMM_M2L_FP32), timed the same way.
+order: the tensor-core tiles take the orders the learned MLP picks
+       (FMM_ORDER_LEARNED); the judge (512 targets against the FP64 direct
+       sum, budget 1e-6, fixed-order fallback) checks the first and then every
+       8th evaluation, inside the timed steps.  The first evaluation runs at
+       p (warm-up).
+tc_fixed_order, plain: the same workload and maximum order through the
+       tensor cores at fixed p, and through the plain FP32 GPU FMM (SIMT
+       contractions, FMM_M2L_FP32), timed the same way; speedup_vs_plain is
+       the headline against the latter at equal error.
 e2e:   the headline configuration through the public C ABI with pinned host
        buffers (fmm_evaluate: host-to-device copy of positions and masses,
        the pass, device-to-host copy of accelerations), wall clock per call.
@@ -225,7 +232,11 @@ def run_ours(args, world, rank, local):
     judge = (d_tg, r_acc.cpu().numpy(), r_pot.cpu().numpy())
 
     # headline: the chosen M2L mode
-    ctx = fmmgpu.Context(dim=3, p=p, leaf_cap=leaf, m2l_mode=mode, G=1.0, device=local, direct_max=args.direct_max)
+    learned = args.order == "learned" and mode == fmmgpu.FMM_M2L_TC
+    okw = dict(order_mode=fmmgpu.FMM_ORDER_LEARNED, judge_samples=args.judge, judge_budget=1e-6,
+               judge_every=args.judge_every) if learned else {}
+    ctx = fmmgpu.Context(dim=3, p=p, leaf_cap=leaf, m2l_mode=mode, G=1.0, device=local, direct_max=args.direct_max,
+                         **okw)
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
@@ -315,9 +326,17 @@ def run_ours(args, world, rank, local):
         "clocks": clocks,
     }
 
-    # the plain FP32 GPU FMM at the same order (same error)
-    if not args.no_plain and mode == fmmgpu.FMM_M2L_TC:
-        pc = fmmgpu.Context(dim=3, p=p, leaf_cap=leaf, m2l_mode=fmmgpu.FMM_M2L_FP32, G=1.0, device=local,
+    if learned:
+        line["order"] = {"mode": "learned (M2L tile orders from the MLP in fmmgpu/order_model.npy)",
+                         "judge_samples": args.judge, "judge_budget": 1e-6, "judge_every": args.judge_every,
+                         "fallbacks_in_timed_steps": int(sum(s["order_fallbacks"] for s in stats)),
+                         "judge_rel_l2_last": float(stats[-1]["judge_rel_l2"]),
+                         "m2l_width_mean": stats[-1]["m2l_width_sum"] / max(1, stats[-1]["m2l_tiles"])}
+
+    # comparisons at the same order: tensor cores at fixed p, and the plain
+    # FP32 GPU FMM (the method without tensor cores and learned orders)
+    def compare(m2l_mode, label):
+        pc = fmmgpu.Context(dim=3, p=p, leaf_cap=leaf, m2l_mode=m2l_mode, G=1.0, device=local,
                             direct_max=args.direct_max)
         psteps = max(3, args.steps // 2)
         pms, pst, _ = _timed(pc, n, d_pos, d_mass, d_acc, stream, flush, psteps, max(1, args.warmup), barrier)
@@ -328,8 +347,13 @@ def run_ours(args, world, rank, local):
             ptot = float(t.item())
         perr = _error(pc, n, d_pos, d_mass, d_acc, d_pot, stream, dev, judge)
         pc.close()
-        line["plain"] = {"m2l": "fp32", "value": n * psteps * world / (ptot / 1e3), "unit": UNIT, "steps": psteps,
-                         "ms_per_step": ptot / psteps, "error": perr, "phases_ms": _phases(pst)}
+        return {"m2l": label, "value": n * psteps * world / (ptot / 1e3), "unit": UNIT, "steps": psteps,
+                "ms_per_step": ptot / psteps, "error": perr, "phases_ms": _phases(pst)}
+
+    if not args.no_plain and mode == fmmgpu.FMM_M2L_TC:
+        if learned:
+            line["tc_fixed_order"] = compare(fmmgpu.FMM_M2L_TC, "tensor cores, fixed p")
+        line["plain"] = compare(fmmgpu.FMM_M2L_FP32, "fp32 SIMT, fixed p")
         line["speedup_vs_plain"] = value / line["plain"]["value"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(p, leaf)
@@ -429,6 +453,10 @@ def main():
     ap.add_argument("--leaf", type=int, default=64)
     ap.add_argument("--m2l", default="tc", choices=["fp32", "tc"])
     ap.add_argument("--direct-max", type=int, default=-1, help="-1: the library's automatic threshold")
+    ap.add_argument("--order", default="learned", choices=["learned", "fixed"],
+                    help="M2L tile orders (tensor-core mode): learned by the MLP, or fixed p")
+    ap.add_argument("--judge", type=int, default=512, help="learned orders: targets checked against FP64 direct")
+    ap.add_argument("--judge-every", type=int, default=8, help="learned orders: check every k-th evaluation")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

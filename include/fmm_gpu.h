@@ -66,7 +66,8 @@ enum {
    at p).  With
    judge_samples > 0 every learned-order evaluation is checked on that many
    targets against the FP64 direct sum and, if their relative L2 error
-   exceeds judge_budget, evaluated again at fixed p (fmm_stats.order_fallbacks). */
+   exceeds judge_budget, evaluated again at fixed p (fmm_stats.order_fallbacks);
+   judge_every > 1 checks every judge_every-th learned evaluation of a system. */
 enum {
   FMM_ORDER_FIXED = 0,
   FMM_ORDER_GEOMETRIC = 1,
@@ -110,12 +111,13 @@ typedef struct fmm_config {
                          as in the reference; -1 = automatic */
   int32_t order_mode; /* FMM_ORDER_*: expansion order of each M2L pair (tensor-core mode only) */
   int32_t order_margin; /* FMM_ORDER_GEOMETRIC: orders added to each reduced pair order */
-  float order_tol;      /* FMM_ORDER_LEARNED: relative L2 force budget of the reduced orders (default 4e-6:
-                           the tile bound is conservative; on a 2^20 Plummer sphere at p = 12 it adds
-                           about 1e-7 to the FP32 error of fixed p) */
+  float order_tol;      /* FMM_ORDER_LEARNED: relative L2 force budget of the reduced orders (default 2e-6:
+                           the tile bound is conservative, the orders it picks add a few 1e-7 to the
+                           error of fixed p on the seeded Plummer, mixture and uniform systems) */
   int32_t judge_samples;/* FMM_ORDER_LEARNED: targets checked against the FP64 direct sum (0 = no check) */
   float judge_budget;   /* FMM_ORDER_LEARNED: relative L2 error above which the evaluation is redone at p */
-  int32_t reserved[1];
+  int32_t judge_every;  /* FMM_ORDER_LEARNED: check every judge_every-th learned evaluation of a system
+                           (default 1: every one) */
 } fmm_config;
 
 typedef struct fmm_stats {

@@ -49,7 +49,7 @@ int build_op_tables(OpTables &ops, int dim, int p, int depth, const PassGeom &g,
 struct OrderOpts {
   int mode = 0;            // FMM_ORDER_*
   int margin = 1;          // FMM_ORDER_GEOMETRIC
-  float tol = 4e-6f;       // FMM_ORDER_LEARNED: relative error budget of the truncation
+  float tol = 2e-6f;       // FMM_ORDER_LEARNED: relative error budget of the truncation
   const float *params = nullptr;  // FMM_ORDER_LEARNED: MLP parameters
   // collection (ntiles = 0: none): sample `ntiles` M2L tiles, write their
   // features and FP64 error labels

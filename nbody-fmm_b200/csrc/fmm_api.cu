@@ -36,6 +36,7 @@ struct fmm_ctx {
   DevBuf<float> order_params;
   bool has_model = false;
   int64_t frms_n = -1;         // system size the cached F_rms belongs to
+  int64_t learned_evals = 0;   // learned evaluations of that system so far (judge cadence)
   DevBuf<int64_t> judge_tg;    // judge targets of (judge_n, judge_k)
   DevBuf<double> judge_ref, judge_sum;
   int64_t judge_n = -1, judge_k = -1;
@@ -62,7 +63,7 @@ static int check_cfg(const fmm_config *c) {
     return FMM_ERR_INVALID_ARGUMENT;
   if (c->order_mode == FMM_ORDER_LEARNED && c->dim != 3) return FMM_ERR_UNSUPPORTED;
   if (c->order_mode == FMM_ORDER_LEARNED && !(c->order_tol > 0.f)) return FMM_ERR_INVALID_ARGUMENT;
-  if (c->judge_samples < 0 || !(c->judge_budget > 0.f)) return FMM_ERR_INVALID_ARGUMENT;
+  if (c->judge_samples < 0 || !(c->judge_budget > 0.f) || c->judge_every < 1) return FMM_ERR_INVALID_ARGUMENT;
   if (c->order_mode != FMM_ORDER_FIXED && c->m2l_mode != FMM_M2L_TC)
     return FMM_ERR_UNSUPPORTED;  // per-pair orders live in the tensor-core kernel; the plain FMM is fixed-p
   if (c->order_margin < 0 || c->order_margin > FMM_MAX_P) return FMM_ERR_INVALID_ARGUMENT;
@@ -102,9 +103,10 @@ int fmm_config_default(fmm_config *cfg) {
   cfg->direct_max = -1;
   cfg->order_mode = FMM_ORDER_FIXED;
   cfg->order_margin = 1;
-  cfg->order_tol = 4e-6f;
+  cfg->order_tol = 2e-6f;
   cfg->judge_samples = 0;
   cfg->judge_budget = 1e-6f;
+  cfg->judge_every = 1;
   return FMM_OK;
 }
 
@@ -276,12 +278,13 @@ static int evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const dou
     if (c->frms_n != n) {  // a new system: its first evaluation runs at fixed p
       CUDA_TRY(cudaMemsetAsync(c->eb.frms.ptr, 0, 3 * sizeof(double), st));
       c->frms_n = n;
+      c->learned_evals = 0;
     }
   }
   int rc = pass(c, n, d_pos, d_mass, d_acc, d_pot, st, oo, false);
   if (rc) return rc;
   if (!learned) return FMM_OK;
-  if (c->cfg.judge_samples > 0) {
+  if (c->cfg.judge_samples > 0 && c->learned_evals++ % c->cfg.judge_every == 0) {
     double rel = 0.0;
     rc = judge(c, n, d_pos, d_mass, d_acc, st, rel);
     if (rc) return rc;

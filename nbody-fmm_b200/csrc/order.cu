@@ -524,6 +524,7 @@ __global__ void __launch_bounds__(32 * INF_WARPS) k_order_infer(InferArgs a) {
   __shared__ float w1t[ORD_NF * ORD_NH], w2t[ORD_NH * ORD_NH], w3t[ORD_NH * 16], bias[2 * ORD_NH + 16];
   __shared__ float hs[INF_WARPS][2][ORD_NH];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if ((int)blockIdx.y * INF_WARPS >= a.t.nslots[blockIdx.x]) return;  // nothing for this block
   for (int e = tid; e < ORD_NH * ORD_NF; e += blockDim.x) {
     const int j = e / ORD_NF, i = e % ORD_NF;
     w1t[i * ORD_NH + j] = bf16r(a.params[ORD_W1 + e]);
@@ -549,7 +550,7 @@ __global__ void __launch_bounds__(32 * INF_WARPS) k_order_infer(InferArgs a) {
   const double pbar = a.n > 0 ? (double)(*a.nt_sum) / (double)a.n : 1.0;
   const float lmt = log10f((float)fmax(*a.t.mtot, 1e-300));
   const float sd = (float)(a.emax * ldexp(1.0, -a.t.batches[b].z));
-  for (int i = warp; i < ns; i += INF_WARPS) {
+  for (int i = blockIdx.y * INF_WARPS + warp; i < ns; i += INF_WARPS * gridDim.y) {
     int q = a.p;
     if (frms > 0.0) {
       float f[ORD_NF];
@@ -685,7 +686,8 @@ int order_probe_errors(const ProbeArgs &a, cudaStream_t st, int64_t &launches) {
 
 int order_infer(const InferArgs &a, int nbm, cudaStream_t st, int64_t &launches) {
   if (nbm <= 0) return FMM_OK;
-  k_order_infer<<<nbm, 32 * INF_WARPS, 0, st>>>(a);
+  // blocks (batch, y) take every gridDim.y-th group of INF_WARPS slots
+  k_order_infer<<<dim3(nbm, 8), 32 * INF_WARPS, 0, st>>>(a);
   launches += 1;
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
 }

@@ -529,13 +529,13 @@ __device__ inline void two_sum(float a, float b, float &s, float &e) {
 
 // One pair: grad -= m d/|d|^3, phi += m/|d| (3D, leaf.cpp:118-142) or
 // grad -= m d/|d|^2, phi -= m log|d| (2D, leaf.cpp:81-95), r^2 -> r^2 + eps2.
-template <int DIM>
+template <int DIM, bool NEWTON = true>
 __device__ inline void pair_acc(float rx, float ry, float rz, float w, float eps2, float &ax, float &ay, float &az,
                                 float &ph) {
   if (DIM == 3) {
     const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2)));
     float inv = rsqrtf(r2);
-    inv = inv * fmaf(-0.5f * r2 * inv, inv, 1.5f);  // one Newton step
+    if (NEWTON) inv = inv * fmaf(-0.5f * r2 * inv, inv, 1.5f);  // one Newton step
     const float mi = w * inv;
     const float mi3 = mi * inv * inv;
     ax = fmaf(-rx, mi3, ax);
@@ -718,7 +718,7 @@ __device__ void direct_small(const DirectArgs &a, const float4 *off, int tb, int
     const float qx = q.x + s_shift[3 * si], qy = q.y + s_shift[3 * si + 1], qz = q.z + s_shift[3 * si + 2];
 #pragma unroll
     for (int k = 0; k < NT; ++k)
-      pair_acc<DIM>(tx[k] - qx, ty[k] - qy, tz[k] - qz, q.w, a.eps2, ax[k], ay[k], az[k], ph[k]);
+      pair_acc<DIM, false>(tx[k] - qx, ty[k] - qy, tz[k] - qz, q.w, a.eps2, ax[k], ay[k], az[k], ph[k]);
   }
 #pragma unroll
   for (int k = 0; k < NT; ++k) {
@@ -769,7 +769,7 @@ __device__ void direct_blocked(const DirectArgs &a, const float4 *off, int tb, i
         const float4 sq = stage[k];
 #pragma unroll
         for (int r = 0; r < R; ++r)
-          pair_acc<DIM>(tx[r] - sq.x, ty[r] - sq.y, tz[r] - sq.z, sq.w, a.eps2, ax[r], ay[r], az[r], ph[r]);
+          pair_acc<DIM, false>(tx[r] - sq.x, ty[r] - sq.y, tz[r] - sq.z, sq.w, a.eps2, ax[r], ay[r], az[r], ph[r]);
       }
       __syncwarp();
     }
