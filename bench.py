@@ -33,6 +33,8 @@ tc_fixed_order, plain: the same workload and maximum order through the
 e2e:   the headline configuration through the public C ABI with pinned host
        buffers (fmm_evaluate: host-to-device copy of positions and masses,
        the pass, device-to-host copy of accelerations), wall clock per call.
+autotune: before timing, fmm_autotune times the candidate direct-pair
+       thresholds on this input and keeps the fastest (setup, not timed).
 roofline: the dominant kernel by live-measured time, and both of the two
        largest: the tensor-core M2L (algorithmic FLOPs 2 K^2 per
        interaction-list pair, K = (p+1)^2, against the measured sustained
@@ -237,6 +239,13 @@ def run_ours(args, world, rank, local):
                judge_every=args.judge_every) if learned else {}
     ctx = fmmgpu.Context(dim=3, p=p, leaf_cap=leaf, m2l_mode=mode, G=1.0, device=local, direct_max=args.direct_max,
                          **okw)
+    tune = None
+    if args.autotune and args.direct_max < 0:
+        # the autotuner picks the direct-pair threshold on this input (setup, outside the timed steps)
+        t0 = time.perf_counter()
+        cands, best = ctx.autotune(n, d_pos.data_ptr(), d_mass.data_ptr(), stream=stream.cuda_stream)
+        tune = {"seconds": time.perf_counter() - t0, "chosen_direct_max": best["direct_max"],
+                "candidates": [[x["direct_max"], round(x["ms"], 3)] for x in cands]}
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
@@ -325,6 +334,8 @@ def run_ours(args, world, rank, local):
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
+    if tune:
+        line["autotune"] = tune
 
     if learned:
         line["order"] = {"mode": "learned (M2L tile orders from the MLP in fmmgpu/order_model.npy)",
@@ -338,6 +349,9 @@ def run_ours(args, world, rank, local):
     def compare(m2l_mode, label):
         pc = fmmgpu.Context(dim=3, p=p, leaf_cap=leaf, m2l_mode=m2l_mode, G=1.0, device=local,
                             direct_max=args.direct_max)
+        chosen = None
+        if args.autotune and args.direct_max < 0:  # tuned the same way as the headline
+            chosen = pc.autotune(n, d_pos.data_ptr(), d_mass.data_ptr(), stream=stream.cuda_stream)[1]["direct_max"]
         psteps = max(3, args.steps // 2)
         pms, pst, _ = _timed(pc, n, d_pos, d_mass, d_acc, stream, flush, psteps, max(1, args.warmup), barrier)
         ptot = float(sum(pms))
@@ -348,7 +362,7 @@ def run_ours(args, world, rank, local):
         perr = _error(pc, n, d_pos, d_mass, d_acc, d_pot, stream, dev, judge)
         pc.close()
         return {"m2l": label, "value": n * psteps * world / (ptot / 1e3), "unit": UNIT, "steps": psteps,
-                "ms_per_step": ptot / psteps, "error": perr, "phases_ms": _phases(pst)}
+                "ms_per_step": ptot / psteps, "error": perr, "phases_ms": _phases(pst), "direct_max": chosen}
 
     if not args.no_plain and mode == fmmgpu.FMM_M2L_TC:
         if learned:
@@ -453,6 +467,8 @@ def main():
     ap.add_argument("--leaf", type=int, default=64)
     ap.add_argument("--m2l", default="tc", choices=["fp32", "tc"])
     ap.add_argument("--direct-max", type=int, default=-1, help="-1: the library's automatic threshold")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the library's automatic direct-pair threshold")
     ap.add_argument("--order", default="learned", choices=["learned", "fixed"],
                     help="M2L tile orders (tensor-core mode): learned by the MLP, or fixed p")
     ap.add_argument("--judge", type=int, default=512, help="learned orders: targets checked against FP64 direct")

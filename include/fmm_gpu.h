@@ -169,6 +169,24 @@ FMM_API int fmm_evaluate_device(fmm_ctx *ctx, int64_t n, const double *d_pos, co
                         double *d_pot, void *stream);
 FMM_API int fmm_synchronize(fmm_ctx *ctx);
 
+/* Autotuner: times force evaluations of the given system (device buffers)
+   over candidate settings and keeps the fastest in the context: the
+   direct-pair threshold (K^2/200 .. K^2/12.5, K the expansion length) and,
+   with FMM_TUNE_LEAF, the leaf capacity in {16, 32, 64, 128} (which changes
+   the tree: the reference's algorithm at that threshold).  Learned orders
+   are tuned with them (every candidate is evaluated twice, the second timed).
+   result may be NULL.  Synchronous. */
+#define FMM_TUNE_LEAF 1
+typedef struct fmm_tune_result {
+  int32_t n_candidates;
+  int32_t best;            /* index of the chosen candidate */
+  int32_t leaf_cap[16];    /* candidates */
+  int32_t direct_max[16];
+  double ms[16];           /* device time of each candidate's timed evaluation */
+} fmm_tune_result;
+FMM_API int fmm_autotune(fmm_ctx *ctx, int64_t n, const double *d_pos, const double *d_mass, int32_t flags,
+                         fmm_tune_result *result, void *stream);
+
 /* FP64 O(N^2) direct sum on the GPU for `ntargets` target indices (all if
  * targets is NULL): replaces NaiveUpdate::update (naive_update.cpp:9-35)
  * when soft_mode is FMM_SOFT_NAIVE_REF; otherwise the Plummer form with

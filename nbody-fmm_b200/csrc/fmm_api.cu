@@ -341,6 +341,65 @@ int fmm_evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const double
   return evaluate_device(c, n, d_pos, d_mass, d_acc, d_pot, st);
 }
 
+int fmm_autotune(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass, int32_t flags,
+                 fmm_tune_result *result, void *stream) {
+  if (!c || n <= 0 || n > (int64_t)INT32_MAX || !d_pos || !d_mass) return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  const int dim = c->cfg.dim;
+  if (!c->d_acc.reserve((size_t)n * dim)) return FMM_ERR_OUT_OF_MEMORY;
+  const int K = dim == 3 ? (c->cfg.p + 1) * (c->cfg.p + 1) : 2 * c->cfg.p + 1;
+  const double base = (double)K * K / 25.0;
+  const double fac[5] = {0.125, 0.25, 0.5, 1.0, 2.0};
+  std::vector<int> leaves;
+  if (flags & FMM_TUNE_LEAF) leaves = {16, 32, 64, 128};
+  else leaves = {c->cfg.leaf_cap};
+  fmm_tune_result res;
+  memset(&res, 0, sizeof(res));
+  const fmm_config saved = c->cfg;
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  int rc = FMM_OK;
+  double best = 1e300;
+  for (int lc : leaves) {
+    for (double f : fac) {
+      if (res.n_candidates >= 16) break;
+      const int k = res.n_candidates++;
+      c->cfg.leaf_cap = lc;
+      c->cfg.direct_max = (int32_t)std::max(8.0, base * f);
+      res.leaf_cap[k] = lc;
+      res.direct_max[k] = c->cfg.direct_max;
+      const bool twice = c->cfg.order_mode == FMM_ORDER_LEARNED;
+      c->frms_n = -1;  // learned orders: start the system afresh
+      for (int r = 0; r < (twice ? 2 : 1) && !rc; ++r) rc = evaluate_device(c, n, d_pos, d_mass, c->d_acc.ptr, nullptr, st);
+      if (!rc) rc = finish(c, st);
+      if (!rc && cudaEventRecord(e0, st) != cudaSuccess) rc = FMM_ERR_CUDA;
+      if (!rc) rc = evaluate_device(c, n, d_pos, d_mass, c->d_acc.ptr, nullptr, st);
+      if (!rc && cudaEventRecord(e1, st) != cudaSuccess) rc = FMM_ERR_CUDA;
+      if (!rc) rc = finish(c, st);
+      float ms = 0.f;
+      if (!rc && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) rc = FMM_ERR_CUDA;
+      if (rc) break;
+      res.ms[k] = ms;
+      if (ms < best) {
+        best = ms;
+        res.best = k;
+      }
+    }
+    if (rc) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->cfg = saved;
+  if (rc) return rc;
+  c->cfg.leaf_cap = res.leaf_cap[res.best];
+  c->cfg.direct_max = res.direct_max[res.best];
+  c->frms_n = -1;
+  if (result) *result = res;
+  return FMM_OK;
+}
+
 int fmm_synchronize(fmm_ctx *c) {
   if (!c) return FMM_ERR_INVALID_ARGUMENT;
   CUDA_TRY(cudaSetDevice(c->cfg.device));

@@ -51,7 +51,7 @@ EXPORTED = (
     "fmm_evaluate_device", "fmm_synchronize", "fmm_direct", "fmm_direct_device", "fmm_integrate",
     "fmm_tree_build", "fmm_tree_depth", "fmm_tree_level_size", "fmm_tree_level_keys", "fmm_tree_leaves",
     "fmm_tree_pairs", "fmm_last_stats", "fmm_launch_count", "fmm_direct_noalloc", "fmm_order_set_model",
-    "fmm_order_get_model", "fmm_order_collect", "fmm_order_train", "fmm_order_forward_grad",
+    "fmm_order_get_model", "fmm_order_collect", "fmm_order_train", "fmm_order_forward_grad", "fmm_autotune",
 )
 
 
@@ -75,6 +75,14 @@ class FmmStats(ctypes.Structure):
         ("far_direct_pairs", ctypes.c_int64), ("direct_max", ctypes.c_int64), ("judge_rel_l2", ctypes.c_double),
         ("order_fallbacks", ctypes.c_int64), ("m2l_width_sum", ctypes.c_int64), ("reserved", ctypes.c_double * 7),
     ]
+
+
+class FmmTuneResult(ctypes.Structure):
+    _fields_ = [("n_candidates", ctypes.c_int32), ("best", ctypes.c_int32), ("leaf_cap", ctypes.c_int32 * 16),
+                ("direct_max", ctypes.c_int32 * 16), ("ms", ctypes.c_double * 16)]
+
+
+FMM_TUNE_LEAF = 1
 
 
 class FmmError(RuntimeError):
@@ -127,6 +135,7 @@ def load_library(path=LIB_PATH):
     L.fmm_order_collect.argtypes = [_vp, ctypes.c_int64, _vp, _vp, ctypes.c_int32, ctypes.c_uint64, _vp, _vp, _vp]
     L.fmm_order_train.argtypes = [_vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, _f]
     L.fmm_order_forward_grad.argtypes = [_vp, _vp, ctypes.c_int32, _vp, _vp, _vp, _vp, _vp]
+    L.fmm_autotune.argtypes = [_vp, ctypes.c_int64, _vp, _vp, ctypes.c_int32, ctypes.POINTER(FmmTuneResult), _vp]
     _lib = L
     return L
 
@@ -281,6 +290,18 @@ class Context:
 
     def launch_count(self):
         return int(_lib.fmm_launch_count(self._h))
+
+    def autotune(self, n, pos_ptr, mass_ptr, tune_leaf=False, stream=None):
+        """Times candidate direct-pair thresholds (and leaf capacities) on the
+        given system and keeps the fastest (fmm_autotune).  Returns the
+        candidates as a list of dicts and the chosen one."""
+        r = FmmTuneResult()
+        _check(_lib.fmm_autotune(self._h, n, pos_ptr, mass_ptr, FMM_TUNE_LEAF if tune_leaf else 0, ctypes.byref(r),
+                                 stream))
+        cands = [{"leaf_cap": r.leaf_cap[i], "direct_max": r.direct_max[i], "ms": r.ms[i]}
+                 for i in range(r.n_candidates)]
+        self.cfg.leaf_cap, self.cfg.direct_max = cands[r.best]["leaf_cap"], cands[r.best]["direct_max"]
+        return cands, cands[r.best]
 
     # ---- learned pair orders
     def set_order_model(self, params):
