@@ -169,6 +169,17 @@ FMM_API int fmm_evaluate_device(fmm_ctx *ctx, int64_t n, const double *d_pos, co
                         double *d_pot, void *stream);
 FMM_API int fmm_synchronize(fmm_ctx *ctx);
 
+/* Batched ensemble: nsys independent systems stored one after another in
+   the device arrays (system s = elements [offsets[s], offsets[s+1]) of
+   n x dim positions, masses, accelerations; offsets: host, nsys + 1 values
+   from 0).  Each system gets its own tree and force pass, as fmm_evaluate
+   would give it, at fixed p; the passes of different systems run
+   concurrently on a pool of `workers` streams (0: min(nsys, 8)), each fed
+   by its own host thread.  Synchronous; fmm_last_stats then holds the sums
+   of the counts and the wall time in ms_total. */
+FMM_API int fmm_evaluate_batched(fmm_ctx *ctx, int32_t nsys, const int64_t *offsets, const double *d_pos,
+                                 const double *d_mass, double *d_acc, double *d_pot, int32_t workers);
+
 /* Autotuner: times force evaluations of the given system (device buffers)
    over candidate settings and keeps the fastest in the context: the
    direct-pair threshold (K^2/200 .. K^2/12.5, K the expansion length) and,

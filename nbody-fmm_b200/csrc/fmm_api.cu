@@ -1,6 +1,9 @@
 // C ABI of libfmmgpu.so (declared in include/fmm_gpu.h).
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <thread>
 #include <cstring>
 #include <new>
 #include <string>
@@ -40,6 +43,7 @@ struct fmm_ctx {
   DevBuf<int64_t> judge_tg;    // judge targets of (judge_n, judge_k)
   DevBuf<double> judge_ref, judge_sum;
   int64_t judge_n = -1, judge_k = -1;
+  std::vector<fmm_ctx *> workers;  // batched ensemble: worker contexts (own stream and buffers)
   DevBuf<int> col_pairs, col_tiles;
   DevBuf<float> col_plabels;
   fmm_stats stats;
@@ -139,6 +143,8 @@ int fmm_create(const fmm_config *cfg, fmm_ctx **out) {
 
 int fmm_destroy(fmm_ctx *c) {
   if (!c) return FMM_ERR_INVALID_ARGUMENT;
+  for (fmm_ctx *w : c->workers) fmm_destroy(w);
+  c->workers.clear();
   cudaSetDevice(c->cfg.device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   c->ws.release_all();
@@ -339,6 +345,75 @@ int fmm_evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const double
   CUDA_TRY(cudaSetDevice(c->cfg.device));
   cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
   return evaluate_device(c, n, d_pos, d_mass, d_acc, d_pot, st);
+}
+
+int fmm_evaluate_batched(fmm_ctx *c, int32_t nsys, const int64_t *offsets, const double *d_pos, const double *d_mass,
+                         double *d_acc, double *d_pot, int32_t workers) {
+  if (!c || nsys < 0 || !offsets || workers < 0) return FMM_ERR_INVALID_ARGUMENT;
+  if (nsys == 0) return FMM_OK;
+  if (offsets[0] != 0) return FMM_ERR_INVALID_ARGUMENT;
+  for (int s = 0; s < nsys; ++s)
+    if (offsets[s + 1] < offsets[s] || offsets[s + 1] - offsets[s] > (int64_t)INT32_MAX) return FMM_ERR_INVALID_ARGUMENT;
+  if (offsets[nsys] > 0 && (!d_pos || !d_mass || !d_acc)) return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  const int W = std::max(1, std::min<int>(workers > 0 ? std::min(workers, 32) : 8, nsys));
+  while ((int)c->workers.size() < W) {
+    fmm_config wc = c->cfg;
+    wc.order_mode = FMM_ORDER_FIXED;  // a worker's next system is a new one: fixed p
+    wc.judge_samples = 0;
+    fmm_ctx *w = nullptr;
+    int rc = fmm_create(&wc, &w);
+    if (rc) return rc;
+    c->workers.push_back(w);
+  }
+  const int dim = c->cfg.dim;
+  std::atomic<int> next{0}, err{0};
+  std::vector<fmm_stats> st(W);
+  auto work = [&](int wi) {
+    fmm_ctx *w = c->workers[wi];
+    w->cfg.leaf_cap = c->cfg.leaf_cap;  // the parent's settings, as tuned
+    w->cfg.direct_max = c->cfg.direct_max;
+    memset(&st[wi], 0, sizeof(fmm_stats));
+    if (cudaSetDevice(w->cfg.device) != cudaSuccess) {
+      err = FMM_ERR_CUDA;
+      return;
+    }
+    while (!err) {
+      const int s = next++;
+      if (s >= nsys) break;
+      const int64_t off = offsets[s], n = offsets[s + 1] - off;
+      if (n == 0) continue;
+      int rc = evaluate_device(w, n, d_pos + off * dim, d_mass + off, d_acc + off * dim, d_pot ? d_pot + off : nullptr,
+                               w->stream);
+      if (!rc) rc = finish(w, w->stream);
+      if (rc) {
+        err = rc;
+        break;
+      }
+      st[wi].n_cells += w->stats.n_cells;
+      st[wi].m2l_pairs += w->stats.m2l_pairs;
+      st[wi].p2p_pairs += w->stats.p2p_pairs;
+      st[wi].far_direct_pairs += w->stats.far_direct_pairs;
+      st[wi].n_leaves += w->stats.n_leaves;
+    }
+  };
+  const auto t0 = std::chrono::steady_clock::now();
+  std::vector<std::thread> th;
+  for (int i = 1; i < W; ++i) th.emplace_back(work, i);
+  work(0);
+  for (auto &t : th) t.join();
+  const double wall = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  memset(&c->stats, 0, sizeof(c->stats));
+  for (const auto &x : st) {
+    c->stats.n_cells += x.n_cells;
+    c->stats.m2l_pairs += x.m2l_pairs;
+    c->stats.p2p_pairs += x.p2p_pairs;
+    c->stats.far_direct_pairs += x.far_direct_pairs;
+    c->stats.n_leaves += x.n_leaves;
+  }
+  c->stats.ms_total = wall;
+  c->timing_pending = false;
+  return err.load();
 }
 
 int fmm_autotune(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass, int32_t flags,

@@ -39,6 +39,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "m2l_tc.cuh"
 
@@ -501,20 +502,29 @@ static int tc_launch_p(const TcArgs &a, int nb, unsigned int *work, cudaStream_t
   // holds 512
   size_t sh = tc_dyn_smem(P16);
   sh = std::max(sh, P16 <= 128 ? (size_t)80 * 1024 : (size_t)120 * 1024);
-  static size_t attr = 0;
-  static int per_sm = 0;
-  if (attr < sh) {
-    if (cudaFuncSetAttribute(k_tc_translate<P16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) != cudaSuccess)
-      return FMM_ERR_CUDA;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tc_translate<P16>, TC_M, sh) != cudaSuccess ||
-        per_sm < 1)
-      return FMM_ERR_CUDA;
-    attr = sh;
-  }
+  // the shared-memory opt-in is per function and device
+  static std::mutex mu;
+  static size_t attr[64] = {};
+  static int per_sm_dev[64] = {};
   int dev = 0, nsm = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64 ||
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return FMM_ERR_CUDA;
+  int per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (attr[dev] < sh) {
+      if (cudaFuncSetAttribute(k_tc_translate<P16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) !=
+          cudaSuccess)
+        return FMM_ERR_CUDA;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_dev[dev], k_tc_translate<P16>, TC_M, sh) !=
+              cudaSuccess ||
+          per_sm_dev[dev] < 1)
+        return FMM_ERR_CUDA;
+      attr[dev] = sh;
+    }
+    per_sm = per_sm_dev[dev];
+  }
   const int grid = std::min(nb, per_sm * nsm);
   k_tc_translate<P16><<<grid, TC_M, sh, st>>>(a, nb, work);
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;

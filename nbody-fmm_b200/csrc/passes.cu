@@ -12,6 +12,7 @@
 // the same kernel.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "expansions.cuh"
@@ -25,9 +26,14 @@ __constant__ float c_rec1[FMM_MAX_P + 1][FMM_MAX_P + 1];  // (2l-1)/(l^2-m^2)
 __constant__ float c_rec2[FMM_MAX_P + 1][FMM_MAX_P + 1];  // 1/(l^2-m^2)
 
 void upload_class_tables() {
-  static bool done = false;
-  if (done) return;
-  done = true;
+  // __constant__ memory is per device: upload once for every device used
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done[dev]) return;
+  done[dev] = true;
   static int h[2][8][189] = {};
   for (int dim = 2; dim <= 3; ++dim)
   for (int c = 0; c < (1 << dim); ++c) {
@@ -251,9 +257,14 @@ static int launch_contract(const ContractArgs &a, int nb, cudaStream_t st, int64
   int stages = contract_smem(a.K, a.KS, a.KP, 2) <= 200 * 1024 ? 2 : 1;
   size_t sh = contract_smem(a.K, a.KS, a.KP, stages);
   if (sh > 227 * 1024) return FMM_ERR_UNSUPPORTED;
-  static size_t attr_set[8][3] = {};
+  // the shared-memory opt-in is per function and device
+  static std::mutex mu;
+  static size_t attr_set[64][8][3] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return FMM_ERR_CUDA;
+  std::lock_guard<std::mutex> lk(mu);
   auto set_attr = [&](auto kern) { return cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh); };
-  if (attr_set[J][stages] < sh) {
+  if (attr_set[dev][J][stages] < sh) {
     cudaError_t e = cudaSuccess;
     switch (J) {
       case 1: e = stages == 2 ? set_attr(k_contract<1, 2>) : set_attr(k_contract<1, 1>); break;
@@ -265,7 +276,7 @@ static int launch_contract(const ContractArgs &a, int nb, cudaStream_t st, int64
       default: return FMM_ERR_UNSUPPORTED;
     }
     if (e != cudaSuccess) return FMM_ERR_CUDA;
-    attr_set[J][stages] = sh;
+    attr_set[dev][J][stages] = sh;
   }
   switch (J) {
     case 1: launch_contract_j<1>(a, nb, stages, sh, st); break;

@@ -52,6 +52,7 @@ EXPORTED = (
     "fmm_tree_build", "fmm_tree_depth", "fmm_tree_level_size", "fmm_tree_level_keys", "fmm_tree_leaves",
     "fmm_tree_pairs", "fmm_last_stats", "fmm_launch_count", "fmm_direct_noalloc", "fmm_order_set_model",
     "fmm_order_get_model", "fmm_order_collect", "fmm_order_train", "fmm_order_forward_grad", "fmm_autotune",
+    "fmm_evaluate_batched",
 )
 
 
@@ -136,6 +137,7 @@ def load_library(path=LIB_PATH):
     L.fmm_order_train.argtypes = [_vp, _vp, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_float, _f]
     L.fmm_order_forward_grad.argtypes = [_vp, _vp, ctypes.c_int32, _vp, _vp, _vp, _vp, _vp]
     L.fmm_autotune.argtypes = [_vp, ctypes.c_int64, _vp, _vp, ctypes.c_int32, ctypes.POINTER(FmmTuneResult), _vp]
+    L.fmm_evaluate_batched.argtypes = [_vp, ctypes.c_int32, _i64, _vp, _vp, _vp, _vp, ctypes.c_int32]
     _lib = L
     return L
 
@@ -290,6 +292,13 @@ class Context:
 
     def launch_count(self):
         return int(_lib.fmm_launch_count(self._h))
+
+    def evaluate_batched(self, offsets, pos_ptr, mass_ptr, acc_ptr, pot_ptr=None, workers=0):
+        """Independent systems stored one after another in device arrays
+        (fmm_evaluate_batched); offsets: nsys + 1 int64 values from 0."""
+        offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+        _check(_lib.fmm_evaluate_batched(self._h, len(offsets) - 1, _p(offsets, _i64), pos_ptr, mass_ptr, acc_ptr,
+                                         pot_ptr, workers))
 
     def autotune(self, n, pos_ptr, mass_ptr, tune_leaf=False, stream=None):
         """Times candidate direct-pair thresholds (and leaf capacities) on the
