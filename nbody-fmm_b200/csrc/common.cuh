@@ -20,6 +20,11 @@ namespace fmm {
 // [Re(n,0), Re(n,1), Im(n,1), ..., Re(n,n), Im(n,n)] start at n*n, so an
 // expansion holds (p+1)^2 floats (the same indexing as the reference's
 // PowerSet<3>, power_set3D.cpp:50-63).
+// Interaction-list pairs whose cells are not well separated for the box's
+// aspect ratio (sum of the cells' radii over the distance of their centres
+// above this) are summed directly instead of by M2L.
+static constexpr double FMM_RHO_MAX = 0.9;
+
 __host__ __device__ inline int re_idx(int n, int m) { return n * n + (m ? 2 * m - 1 : 0); }
 __host__ __device__ inline int im_idx(int n, int m) { return n * n + 2 * m; }
 

@@ -31,6 +31,7 @@ struct ExpBuffers {
   DevBuf<uint16_t> tc_img;
   DevBuf<unsigned int> tc_work;  // zeroed work counters of the tensor-core launches
   DevBuf<uint8_t> order_p16;     // per M2L operator slot: padded width of its pair order
+  DevBuf<uint8_t> fdirect;       // per offset (dx+3) + 7(dy+3) + 49(dz+3): not well separated (direct)
   DevBuf<uint8_t> m2l_w;         // per M2L batch and present slot: padded width of its order
   DevBuf<float> cf;              // learned orders: per-cell features (ORD_CF floats per cell)
   DevBuf<double> frms;           // learned orders: [0] F_rms of the previous pass (G = 1), [1] scratch,

@@ -169,6 +169,7 @@ int fmm_destroy(fmm_ctx *c) {
   c->eb.tc_img.release();
   c->eb.tc_work.release();
   c->eb.order_p16.release();
+  c->eb.fdirect.release();
   c->eb.m2l_w.release();
   c->eb.cf.release();
   c->eb.frms.release();

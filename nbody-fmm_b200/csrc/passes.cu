@@ -94,6 +94,7 @@ struct ContractArgs {
   const float *tab;
   const int *cparent, *cchild, *ccoll, *cpbeg, *cpend;
   long long direct_max;  // M2L skips pairs with n_t * n_s <= direct_max (summed directly instead)
+  const uint8_t *fdirect;  // M2L: per offset (dx+3) + 7(dy+3) + 49(dz+3): not well separated, summed directly
   const int *src_tab;    // M2L: [batch][slot][CT_TGT] source cells resolved ahead (or null)
   const int *slot_list;  // M2L: [batch][slot index] present slots, nslots_tab[batch] of them
   const int *nslots_tab;
@@ -110,6 +111,7 @@ __device__ inline int contract_source(const ContractArgs &a, int tgt, int s, int
     int P = a.cparent[tgt];
     int Q = a.ccoll[(int64_t)P * ns + ((e >> 9) & 31)];
     if (Q < 0) return -1;
+    if (a.fdirect && a.fdirect[e & 511]) return -1;  // not well separated: direct far field
     int src = a.cchild[(int64_t)Q * nc + ((e >> 14) & 7)];
     if (src >= 0 && a.direct_max > 0) {
       long long nt = a.cpend[tgt] - a.cpbeg[tgt], nsrc = a.cpend[src] - a.cpbeg[src];
@@ -698,6 +700,8 @@ struct DirectArgs {
   const uint64_t *ckey;
   float eps2;
   long long direct_max;
+  const uint8_t *fdirect;  // per offset: not well separated, always summed directly
+  int any_fdirect;
   float4 *far;
   unsigned long long *pair_count;
 };
@@ -825,7 +829,7 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   const float4 *off = a.off[lv];
   const float hx = a.h[lv][0], hy = a.h[lv][1], hz = a.h[lv][2];
   const int tb = a.pbeg[T], nt = a.pend[T] - tb;
-  if ((long long)nt > a.direct_max) return;
+  if ((long long)nt > a.direct_max && !a.any_fdirect) return;
   int *s_pb = s_pb_all[wib];
   float *s_shift = s_shift_all[wib];
   int *s_pref = s_pref_all[wib];
@@ -858,7 +862,8 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
     const int ddy = 2 * ((dl / 3) % 3 - 1) + ((k >> 1) & 1) - ((cls >> 1) & 1);
     const int ddz = DIM == 3 ? 2 * (dl / 9 - 1) + ((k >> 2) & 1) - ((cls >> 2) & 1) : 0;
     const bool adj = ddx >= -1 && ddx <= 1 && ddy >= -1 && ddy <= 1 && ddz >= -1 && ddz <= 1;
-    if (q >= 0 && (adj || (long long)nt * nsv[r] > a.direct_max)) q = -1;
+    const bool fd = a.any_fdirect && !adj && a.fdirect[(ddx + 3) + 7 * (ddy + 3) + (DIM == 3 ? 49 * (ddz + 3) : 0)];
+    if (q >= 0 && (adj || ((long long)nt * nsv[r] > a.direct_max && !fd))) q = -1;
     const unsigned mask = __ballot_sync(0xffffffffu, q >= 0);
     const int pos = nsrc + __popc(mask & ((1u << lane) - 1u));
     int x = q >= 0 ? nsv[r] : 0;  // inclusive scan of the kept counts
@@ -957,6 +962,23 @@ __global__ void k_class_hist(const uint64_t *keys, int n, uint32_t *hist) {
   if (h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
 }
 
+// ------------------------------------------------------------ separation
+// Offset o = (dx+3) + 7(dy+3) + 49(dz+3) (cells of the box with extents ex):
+// the two cells' radii summed over the distance of their centres exceeds
+// FMM_RHO_MAX, so their multipole expansion may not converge.
+__host__ __device__ inline bool offset_not_well_separated(int o, int dim, double ex, double ey, double ez) {
+  if (dim == 2 && o >= 49) return false;  // 2D offsets: (dx+3) + 7(dy+3)
+  const int dx = o % 7 - 3, dy = (o / 7) % 7 - 3, dz = dim == 3 ? o / 49 - 3 : 0;
+  const double diag2 = ex * ex + ey * ey + (dim == 3 ? ez * ez : 0.0);
+  const double dist2 = dx * ex * dx * ex + dy * ey * dy * ey + (dim == 3 ? dz * ez * dz * ez : 0.0);
+  return dist2 > 0.0 && sqrt(diag2) > FMM_RHO_MAX * sqrt(dist2);
+}
+
+__global__ void k_fdirect_table(int dim, double ex, double ey, double ez, uint8_t *out) {
+  const int o = threadIdx.x;
+  if (o < 343) out[o] = offset_not_well_separated(o, dim, ex, ey, ez) ? 1 : 0;
+}
+
 // ------------------------------------------------------------ pair orders
 // FMM_ORDER_GEOMETRIC: for every M2L operator slot (offset D of source from
 // target, in cell sizes), the order whose truncation bound rho^(q+1),
@@ -1022,6 +1044,18 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   }
   const double emax = g.emax > 0 ? g.emax : 1.0;
   const double sD = std::ldexp(emax, -D);
+  // offsets whose cells are not well separated for this box (summed
+  // directly): flags on the device, and on the host whether there are any
+  // (the same FP64 arithmetic, IEEE square roots, so both agree)
+  int any_fdirect = 0;
+  for (int o = 0; o < 343; ++o)
+    if (offset_not_well_separated(o, dim, g.ext[0], g.ext[1], g.ext[2])) {
+      const int dd[3] = {o % 7 - 3, (o / 7) % 7 - 3, dim == 3 ? o / 49 - 3 : 0};
+      if (std::abs(dd[0]) > 1 || std::abs(dd[1]) > 1 || std::abs(dd[2]) > 1) any_fdirect = 1;
+    }
+  if (!eb.fdirect.reserve(343)) return FMM_ERR_OUT_OF_MEMORY;
+  k_fdirect_table<<<1, 352, 0, st>>>(dim, g.ext[0], g.ext[1], g.ext[2], eb.fdirect.ptr);
+  ws.launches += 1;
   const float inv_sD = (float)(1.0 / sD);
 
   // class-grouped target lists of levels >= 2: every cell (for L2L) and the
@@ -1096,6 +1130,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   ca.cpbeg = ws.cell_pbeg;
   ca.cpend = ws.cell_pend;
   ca.direct_max = direct_max;
+  ca.fdirect = any_fdirect ? eb.fdirect.ptr : nullptr;
   ca.src_tab = nullptr;
   ca.slot_list = nullptr;
   ca.nslots_tab = nullptr;
@@ -1301,7 +1336,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   if (ev) cudaEventRecord(ev[4], st);
   // direct far field, all levels >= 2 (they have interaction lists) in one
   // launch, coarse levels first so that their long warps start early
-  if (direct_max > 0 && D >= 2) {
+  if ((direct_max > 0 || any_fdirect) && D >= 2) {
     if (D + 1 > DF_MAX_LEVELS) return FMM_ERR_UNSUPPORTED;
     if (D > 2) {
       if (!eb.lvl_off.reserve((size_t)n * (D - 2))) return FMM_ERR_OUT_OF_MEMORY;
@@ -1319,6 +1354,8 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     da.ckey = ws.cell_key;
     da.eps2 = (float)eps2;
     da.direct_max = direct_max;
+    da.fdirect = eb.fdirect.ptr;
+    da.any_fdirect = any_fdirect;
     da.far = ws.far;
     da.pair_count = ws.counters + 3;
     da.nlev = 0;

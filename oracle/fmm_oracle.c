@@ -569,6 +569,26 @@ int orc_fmm(int dim, int64_t n, const double *pos, const double *mass, unsigned 
   return orc_fmm_ex(dim, n, pos, mass, p_, threshold, centre_mode, 0.0, 0, grad, pot);
 }
 
+/* With geometric centres, an interaction-list pair whose cells are not well
+ * separated for the box's aspect ratio -- the sum of the two cells' radii
+ * over the distance of their centres above FMM_RHO_MAX -- is summed directly,
+ * as on the GPU.  The lists (node_i.cpp:39-43) count offsets in cells of the
+ * rectangular bounding box (tree.cpp:20-30), so along a short axis a pair two
+ * cells apart can have a divergent expansion. */
+#define ORC_RHO_MAX 0.9
+static int orc_not_well_separated(int dim, uint64_t kt, uint64_t ks, const double *ext) {
+  uint32_t qt[3] = {0, 0, 0}, qs[3] = {0, 0, 0};
+  orc_morton_decode(kt, dim, qt);
+  orc_morton_decode(ks, dim, qs);
+  double diag = 0.0, dist = 0.0;
+  for (int a = 0; a < dim; ++a) {
+    const double dd = ((double)qs[a] - (double)qt[a]) * ext[a];
+    diag += ext[a] * ext[a];
+    dist += dd * dd;
+  }
+  return dist <= 0.0 || sqrt(diag) > ORC_RHO_MAX * sqrt(dist);
+}
+
 int orc_fmm_ex(int dim, int64_t n, const double *pos, const double *mass, unsigned p_, unsigned threshold,
                int centre_mode, double eps2, int64_t direct_max, double *grad, double *pot) {
   orc_tree *t = orc_tree_build(dim, n, pos, threshold);
@@ -652,7 +672,8 @@ int orc_fmm_ex(int dim, int64_t n, const double *pos, const double *mass, unsign
     for (int64_t i = 0; i < t->ncell[d]; ++i)
       for (int64_t k = t->il_off[d][i]; k < t->il_off[d][i + 1]; ++k) {
         int64_t s = t->il_idx[d][k];
-        if (direct_max > 0 && (pe[d][i] - pb[d][i]) * (pe[d][s] - pb[d][s]) <= direct_max) {
+        if ((direct_max > 0 && (pe[d][i] - pb[d][i]) * (pe[d][s] - pb[d][s]) <= direct_max) ||
+            (centre_mode == 0 && orc_not_well_separated(dim, t->keys[d][i], t->keys[d][s], ext))) {
           for (int64_t a = pb[d][i]; a < pe[d][i]; ++a) {
             int64_t pi = t->perm[a];
             for (int64_t b = pb[d][s]; b < pe[d][s]; ++b) {

@@ -178,3 +178,17 @@ def test_reference_own_tests_pass():
     for b in bins:
         r = subprocess.run([os.path.join(d, b)], capture_output=True, timeout=120)
         assert r.returncode == 0, (b, r.stderr[-500:])
+
+
+def test_oracle_converges_on_an_elongated_box(oracle):
+    """Interaction pairs that are not well separated for the box's aspect
+    ratio are summed directly, so the FMM error falls as p rises even when
+    the bounding box is far from cubic."""
+    from fmmgpu import workloads
+
+    pos, m = workloads.plummer(1457, seed=1138)
+    ext = pos.max(0) - pos.min(0)
+    assert ext.max() / ext.min() > 1.5
+    ref = oracle.direct(pos, m)
+    errs = [rel_l2(oracle.fmm(pos, m, p, 64), ref) for p in (4, 8, 12)]
+    assert errs[0] > errs[1] > errs[2] and errs[2] < 2e-6, errs
