@@ -33,6 +33,8 @@ struct ExpBuffers {
   DevBuf<uint8_t> order_p16;     // per M2L operator slot: padded width of its pair order
   DevBuf<uint8_t> fdirect;       // per offset (dx+3) + 7(dy+3) + 49(dz+3): not well separated (direct)
   DevBuf<uint8_t> m2l_w;         // per M2L batch and present slot: padded width of its order
+  DevBuf<int> m2l_split;         // variable orders: [4][batch][189] (lo slot, lo op, hi slot, hi op) + counts
+  DevBuf<uint8_t> m2l_split_w;   // [2][batch][189] widths of the lo / hi lists
   DevBuf<float> cf;              // learned orders: per-cell features (ORD_CF floats per cell)
   DevBuf<double> frms;           // learned orders: [0] F_rms of the previous pass (G = 1), [1] scratch,
                                  // [2] total mass  // BF16 split operator images for the tensor-core M2L  // particle offsets from their level-d ancestor (direct far field)

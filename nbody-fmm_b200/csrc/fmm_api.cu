@@ -170,6 +170,8 @@ int fmm_destroy(fmm_ctx *c) {
   c->eb.tc_work.release();
   c->eb.order_p16.release();
   c->eb.fdirect.release();
+  c->eb.m2l_split.release();
+  c->eb.m2l_split_w.release();
   c->eb.m2l_w.release();
   c->eb.cf.release();
   c->eb.frms.release();

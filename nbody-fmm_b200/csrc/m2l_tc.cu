@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
   uint16_t *Bs = As + 3 * ASPLIT;   // 2 buffers
   __shared__ __align__(8) uint64_t s_full[2], s_mma[2], s_done;
   __shared__ uint32_t s_tmem;
-  __shared__ int s_slot[2][TC_MAX_SLOTS], s_op[2][TC_MAX_SLOTS];
+  __shared__ short s_slot[2][TC_MAX_SLOTS], s_op[2][TC_MAX_SLOTS];  // 16-bit: two 96-wide CTAs fit an SM
   __shared__ uint8_t s_w[2][TC_MAX_SLOTS];  // padded width of each slot's order
   __shared__ int s_n[2], s_b[2];
   __shared__ int s_grab;
@@ -231,14 +231,14 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
         n = a.nslots[b];
         const size_t tb = (size_t)b * TC_MAX_SLOTS;
         for (int i = tid; i < n; i += TC_M) {
-          s_slot[buf][i] = a.slot_list[tb + i];
-          s_op[buf][i] = a.tslot_list[tb + i];
+          s_slot[buf][i] = (short)a.slot_list[tb + i];
+          s_op[buf][i] = (short)a.tslot_list[tb + i];
           s_w[buf][i] = a.slot_p16 ? a.slot_p16[tb + i] : (uint8_t)P16;
         }
       } else {
         if (tid == 0) {
           s_slot[buf][0] = 0;
-          s_op[buf][0] = a.op_base + bt.w;
+          s_op[buf][0] = (short)(a.op_base + bt.w);
           s_w[buf][0] = (uint8_t)P16;
         }
         n = bt.y > 0 ? 1 : 0;
@@ -291,6 +291,7 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
   // slot of padded width w < P16 needs only the first w rows (k) of each
   // tile, a contiguous prefix, and no second tile when w <= N0; an unneeded
   // copy completes its barrier without data.
+  const int IMG = a.img_p16 ? a.img_p16 : P16;  // operator images: N0 equals this kernel's first tile
   auto load_tile = [&](long long g) {
     const int buf = g < t_nxt ? c : c ^ 1;
     const int i = (int)((g - (g < t_nxt ? t_cur : t_nxt)) / TILES), t = (int)(g % TILES);
@@ -302,7 +303,7 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
     }
     const uint32_t bytes = (uint32_t)(w * (j ? N1 : N0) * 2);
     const uint16_t *src =
-        a.bimg + (size_t)s_op[buf][i] * 3 * P16 * P16 + (size_t)s * P16 * P16 + (j ? (size_t)P16 * N0 : 0);
+        a.bimg + (size_t)s_op[buf][i] * 3 * IMG * IMG + (size_t)s * IMG * IMG + (j ? (size_t)IMG * N0 : 0);
     bulk_load(Bs + (g & 1) * BTILE, src, bytes, &s_full[g & 1]);
   };
   // the MMAs of operator copy g for a slot of width w: B split s against A
@@ -527,6 +528,61 @@ static int tc_launch_p(const TcArgs &a, int nb, unsigned int *work, cudaStream_t
   }
   const int grid = std::min(nb, per_sm * nsm);
   k_tc_translate<P16><<<grid, TC_M, sh, st>>>(a, nb, work);
+  return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
+}
+
+__global__ void k_tc_split(const int *slot_list, const int *tslot_list, const uint8_t *slot_p16, const int *nslots,
+                           int wsplit, int *lo_slot, int *lo_tslot, uint8_t *lo_w, int *lo_n, int *hi_slot,
+                           int *hi_tslot, uint8_t *hi_w, int *hi_n) {
+  const size_t base = (size_t)blockIdx.x * TC_MAX_SLOTS;
+  const int n = nslots[blockIdx.x];
+  __shared__ int s_lo, s_hi;
+  if (threadIdx.x == 0) s_lo = s_hi = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  // warps take 32 slots at a time, in order, so the compacted lists keep the order
+  for (int i0 = 0; i0 < n; i0 += 32) {
+    if (threadIdx.x < 32) {
+      const int i = i0 + lane;
+      const bool ok = i < n;
+      const int w = ok ? slot_p16[base + i] : 0;
+      const bool lo = ok && w <= wsplit, hi = ok && w > wsplit;
+      const unsigned ml = __ballot_sync(0xffffffffu, lo), mh = __ballot_sync(0xffffffffu, hi);
+      const unsigned below = (1u << lane) - 1u;
+      if (lo) {
+        const int at = s_lo + __popc(ml & below);
+        lo_slot[base + at] = slot_list[base + i];
+        lo_tslot[base + at] = tslot_list[base + i];
+        lo_w[base + at] = (uint8_t)w;
+      }
+      if (hi) {
+        const int at = s_hi + __popc(mh & below);
+        hi_slot[base + at] = slot_list[base + i];
+        hi_tslot[base + at] = tslot_list[base + i];
+        hi_w[base + at] = (uint8_t)w;
+      }
+      __syncwarp();
+      if (lane == 0) {
+        s_lo += __popc(ml);
+        s_hi += __popc(mh);
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    lo_n[blockIdx.x] = s_lo;
+    hi_n[blockIdx.x] = s_hi;
+  }
+}
+
+int tc_split_slots(const int *slot_list, const int *tslot_list, const uint8_t *slot_p16, const int *nslots, int nbm,
+                   int wsplit, int *lo_slot, int *lo_tslot, uint8_t *lo_w, int *lo_n, int *hi_slot, int *hi_tslot,
+                   uint8_t *hi_w, int *hi_n, cudaStream_t st, int64_t &launches) {
+  if (nbm <= 0) return FMM_OK;
+  k_tc_split<<<nbm, 32, 0, st>>>(slot_list, tslot_list, slot_p16, nslots, wsplit, lo_slot, lo_tslot, lo_w, lo_n,
+                                 hi_slot, hi_tslot, hi_w, hi_n);
+  launches += 1;
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
 }
 

@@ -28,6 +28,8 @@ struct TcArgs {
   float *Y;                 // target expansions (accumulated into)
   const uint16_t *bimg;     // BF16 split operator images, 3 * P16^2 per table slot
   int cell0, K, KS, P16;    // P16 = K rounded up to 16
+  int img_p16;              // padded width the operator images were built for (0: P16); a narrower
+                            // kernel reads the first output tile of wider images (same first-tile width)
   unsigned int *err;
   unsigned long long *tiles;  // M2L: number of (batch, slot) tiles contracted (nullable)
   unsigned long long *widths; // M2L: sum of the tiles' padded widths (nullable)
@@ -42,6 +44,12 @@ int tc_build_images(const float *tab, int n_slots, int K, int KP, int P16, uint1
 // Launches one translation pass over nb batches; `work` is a zeroed device
 // counter the persistent CTAs take batches from.
 int tc_launch(const TcArgs &a, int nb, unsigned int *work, cudaStream_t st, int64_t &launches);
+
+// Splits the present slots of every M2L batch by padded width: slots with
+// w <= wsplit into (lo_*), the others into (hi_*), each [batch][189] with counts.
+int tc_split_slots(const int *slot_list, const int *tslot_list, const uint8_t *slot_p16, const int *nslots, int nbm,
+                   int wsplit, int *lo_slot, int *lo_tslot, uint8_t *lo_w, int *lo_n, int *hi_slot, int *hi_tslot,
+                   uint8_t *hi_w, int *hi_n, cudaStream_t st, int64_t &launches);
 
 // Work counters per pass (one per launch).
 static constexpr int TC_MAX_LAUNCHES = 80;

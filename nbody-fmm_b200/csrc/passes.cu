@@ -1037,7 +1037,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   if (tc && D >= 2) {
     if (!eb.tc_img.reserve((size_t)ops.n_slots * 3 * P16 * P16) || !eb.tc_work.reserve(TC_MAX_LAUNCHES))
       return FMM_ERR_OUT_OF_MEMORY;
-    if (2 * D + 1 > TC_MAX_LAUNCHES) return FMM_ERR_UNSUPPORTED;
+    if (2 * D + 2 > TC_MAX_LAUNCHES) return FMM_ERR_UNSUPPORTED;
     CUDA_TRY(cudaMemsetAsync(eb.tc_work.ptr, 0, TC_MAX_LAUNCHES * sizeof(unsigned int), st));
     int rc = tc_build_images(ops.tab.ptr, ops.n_slots, ops.K, ops.KP, P16, eb.tc_img.ptr, st, ws.launches);
     if (rc) return rc;
@@ -1294,7 +1294,38 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
       t2.tiles = ws.counters + 2;
       t2.widths = ws.counters + 5;
       t2.slot_p16 = var_order ? eb.m2l_w.ptr : nullptr;
-      rc = tc_launch(t2, nbm, eb.tc_work.ptr + tc_k++, st, ws.launches);
+      if (var_order && P16 == 176 && nbm > 0) {
+        // narrow tiles (w <= 96) in a 96-wide kernel (two CTAs per SM, reading the first output
+        // tile of the 176-wide images), the others in the 176-wide kernel; both add into L
+        const size_t ns = (size_t)nbm * 189;
+        if (!eb.m2l_split.reserve(4 * ns + 2 * (size_t)nbm) || !eb.m2l_split_w.reserve(2 * ns))
+          return FMM_ERR_OUT_OF_MEMORY;
+        int *lo_s = eb.m2l_split.ptr, *lo_t = lo_s + ns, *hi_s = lo_t + ns, *hi_t = hi_s + ns;
+        int *lo_n = hi_t + ns, *hi_n = lo_n + nbm;
+        uint8_t *lo_w = eb.m2l_split_w.ptr, *hi_w = lo_w + ns;
+        rc = tc_split_slots(eb.m2l_list.ptr, eb.m2l_tslot.ptr, eb.m2l_w.ptr, eb.m2l_nslots.ptr, nbm, 96, lo_s, lo_t,
+                            lo_w, lo_n, hi_s, hi_t, hi_w, hi_n, st, ws.launches);
+        if (!rc) {
+          TcArgs lo = t2;
+          lo.P16 = 96;
+          lo.img_p16 = 176;
+          lo.slot_list = lo_s;
+          lo.tslot_list = lo_t;
+          lo.slot_p16 = lo_w;
+          lo.nslots = lo_n;
+          rc = tc_launch(lo, nbm, eb.tc_work.ptr + tc_k++, st, ws.launches);
+        }
+        if (!rc) {
+          TcArgs hi = t2;
+          hi.slot_list = hi_s;
+          hi.tslot_list = hi_t;
+          hi.slot_p16 = hi_w;
+          hi.nslots = hi_n;
+          rc = tc_launch(hi, nbm, eb.tc_work.ptr + tc_k++, st, ws.launches);
+        }
+      } else {
+        rc = tc_launch(t2, nbm, eb.tc_work.ptr + tc_k++, st, ws.launches);
+      }
     } else {
       c2.src_tab = eb.m2l_src.ptr;
       c2.slot_list = eb.m2l_list.ptr;
