@@ -896,7 +896,7 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
     case 8: direct_small<8, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
     default: break;
   }
-  // larger T: the register blocking R in 1..4 that minimises the busiest lane's work
+  // larger T: the register blocking R in 1..4 that minimises the busiest lane's work (largest R on ties)
   int bestR = 1, bestG = 1;
   float best = 1e30f;
 #pragma unroll
@@ -904,7 +904,7 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
     int G;
     float c;
     blocked_shape(nt, R, G, c);
-    if (c < best) {
+    if (c <= best) {  // ties: the larger R reuses each staged source for more targets
       best = c;
       bestR = R;
       bestG = G;
