@@ -27,6 +27,10 @@ struct ExpBuffers {
   DevBuf<int4> batches;
   DevBuf<uint32_t> cls_count;
   DevBuf<float4> lvl_off;
+  DevBuf<uint8_t> lact;    // L2L shortcut: [0, ncell) cells with M2L contributions, [ncell, 2 ncell) cells needing L
+  DevBuf<int4> batches2;   // L2L shortcut: batches of the cells that need L2L
+  DevBuf<int> esrc;        // L2L shortcut: per leaf, the cell whose local expansion its particles evaluate
+  DevBuf<uint8_t> elev;    //   and that cell's level
   DevBuf<int> m2l_src, m2l_list, m2l_nslots, m2l_tslot;  // per M2L batch: resolved sources and present slots
   DevBuf<uint16_t> tc_img;
   DevBuf<unsigned int> tc_work;  // zeroed work counters of the tensor-core launches

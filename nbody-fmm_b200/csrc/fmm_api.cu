@@ -171,6 +171,10 @@ int fmm_destroy(fmm_ctx *c) {
   c->eb.order_p16.release();
   c->eb.fdirect.release();
   c->eb.m2l_split.release();
+  c->eb.lact.release();
+  c->eb.batches2.release();
+  c->eb.esrc.release();
+  c->eb.elev.release();
   c->eb.m2l_split_w.release();
   c->eb.m2l_w.release();
   c->eb.cf.release();

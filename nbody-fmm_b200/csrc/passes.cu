@@ -300,7 +300,7 @@ static int launch_contract(const ContractArgs &a, int nb, cudaStream_t st, int64
 // pair_count set it also counts the (target, source) pairs.
 __global__ void k_m2l_sources(ContractArgs a, int tchunk, int *src_tab, int *slot_list, int *nslots_tab,
                               int *tslot_list, unsigned long long *pair_count, const uint8_t *order_p16,
-                              uint8_t *slot_p16, unsigned long long *nt_sum) {
+                              uint8_t *slot_p16, unsigned long long *nt_sum, uint8_t *lact, int cell0) {
   __shared__ int s_flag[189];
   __shared__ int s_tgt[128];
   __shared__ int s_cnt;
@@ -327,6 +327,7 @@ __global__ void k_m2l_sources(ContractArgs a, int tchunk, int *src_tab, int *slo
       s_flag[slot] = 1;
       ++cnt;
       ntc += (unsigned long long)(a.cpend[s_tgt[t]] - a.cpbeg[s_tgt[t]]);
+      if (lact) lact[s_tgt[t] - cell0] = 1;
     }
   }
   if (pair_count && cnt) atomicAdd(&s_cnt, cnt);
@@ -426,12 +427,32 @@ __device__ inline float2 lget(const float *Lr, int n, int m) {
   return make_float2(-Lr[re_idx(n, 1)], Lr[im_idx(n, 1)]);
 }
 
+// With `esrc` set, the expansion evaluated for the particles of a leaf is
+// that of the leaf's deepest ancestor-or-self on a path to a cell with M2L
+// contributions (esrc[leaf] = that cell, elev its level, -1: none, far field
+// zero): below it the local expansion only moves by L2L, which is exact, so
+// evaluating it there gives the same field without the L2L chain.  Offsets
+// of the particles from level-d centres: `part` at the leaf level,
+// lvl_off[(d - 2) n + i] above.
 __global__ void k_l2p3d(const float4 *part, const int *leaf_of, int64_t n, int cell0, float inv_s, int p, int KS,
-                        const float *L, float4 *far) {
+                        const float *L, float4 *far, const int *esrc, const uint8_t *elev, int leaf_first, int D,
+                        const float4 *lvl_off, float inv_s0) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float4 q = part[i];
-  const float *Lr = L + (size_t)(leaf_of[i] - cell0) * KS;
+  int src = leaf_of[i];
+  if (esrc) {
+    const int lf = src - leaf_first;
+    src = esrc[lf];
+    if (src < 0) {
+      far[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      return;
+    }
+    const int lev = elev[lf];
+    if (lev < D) q = lvl_off[(size_t)(lev - 2) * n + i];
+    inv_s = ldexpf(inv_s0, lev);
+  }
+  const float *Lr = L + (size_t)(src - cell0) * KS;
   const float x = q.x * inv_s, y = q.y * inv_s, z = q.z * inv_s, r2 = x * x + y * y + z * z;
   float gx = 0.f, gy = 0.f, gz = 0.f, ph = 0.f;
   float dre = 1.f, dim_ = 0.f;
@@ -962,6 +983,44 @@ __global__ void k_class_hist(const uint64_t *keys, int n, uint32_t *hist) {
   if (h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
 }
 
+// ------------------------------------------------------------ L2L shortcut
+// Marks every ancestor-or-self at levels >= 2 of the cells with M2L
+// contributions (lact): the cells whose local expansion is needed below.
+__global__ void k_needs_l(const uint8_t *lact, int first2, int count, const int *parent, int cell0, uint8_t *needs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  int c = first2 + i;
+  if (!lact[c - cell0]) return;
+  while (c >= first2 && !needs[c - cell0]) {  // stops where another walk already passed
+    needs[c - cell0] = 1;
+    c = parent[c];
+  }
+}
+
+// Per leaf: its deepest ancestor-or-self with a needed local expansion.
+__global__ void k_leaf_esrc(int leaf_first, int nleaves, int D, int first2, const int *parent, const uint8_t *needs,
+                            int cell0, int *esrc, uint8_t *elev) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nleaves) return;
+  int c = leaf_first + i, lev = D;
+  while (c >= first2 && !needs[c - cell0]) {
+    c = parent[c];
+    --lev;
+  }
+  esrc[i] = c >= first2 ? c : -1;
+  elev[i] = (uint8_t)(c >= first2 ? lev : 0);
+}
+
+// Sort keys of the cells of one level that need L2L: (level, class), else 255.
+__global__ void k_l2l_keys(const uint64_t *ckey, const uint8_t *needs, int first, int count, int level, int dim,
+                           int cell0, uint64_t *keys, uint32_t *vals, int out_off) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int g = first + i;
+  keys[out_off + i] = needs[g - cell0] ? (((uint64_t)level << dim) | (ckey[g] & ((1u << dim) - 1))) : 255u;
+  vals[out_off + i] = (uint32_t)g;
+}
+
 // ------------------------------------------------------------ separation
 // Offset o = (dx+3) + 7(dy+3) + 49(dz+3) (cells of the box with extents ex):
 // the two cells' radii summed over the distance of their centres exceeds
@@ -1182,6 +1241,13 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     if (rc) return rc;
   }
   if (ev) cudaEventRecord(ev[2], st);
+  // L2L shortcut (3D): only the cells on a path to M2L contributions get
+  // local expansions; L2P reads the deepest such ancestor of each leaf
+  const bool shortcut = dim == 3 && D >= 3;
+  if (shortcut) {
+    if (!eb.lact.reserve(2 * (size_t)ncell)) return FMM_ERR_OUT_OF_MEMORY;
+    CUDA_TRY(cudaMemsetAsync(eb.lact.ptr, 0, 2 * (size_t)ncell, st));
+  }
   // M2L, all levels in one launch
   if (D >= 2) {
     ContractArgs c2 = ca;
@@ -1233,7 +1299,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
       k_m2l_sources<<<nbm, 256, 0, st>>>(c2, tchunk, eb.m2l_src.ptr, eb.m2l_list.ptr, eb.m2l_nslots.ptr,
                                          tc ? eb.m2l_tslot.ptr : nullptr, tc ? ws.counters : nullptr,
                                          geometric ? eb.order_p16.ptr : nullptr, geometric ? eb.m2l_w.ptr : nullptr,
-                                         ws.counters + 4);
+                                         ws.counters + 4, shortcut ? eb.lact.ptr : nullptr, cell0);
       ws.launches += 1;
     }
     if (learned && nbm > 0) {
@@ -1335,32 +1401,90 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     if (rc) return rc;
   }
   if (ev) cudaEventRecord(ev[3], st);
-  // L2L, top-down
+  // particle offsets from their ancestors' centres, levels 2..D-1 (L2P
+  // shortcut and direct far field)
+  const bool need_lvl_off = D > 2 && (shortcut || direct_max > 0 || any_fdirect);
+  if (need_lvl_off) {
+    if (!eb.lvl_off.reserve((size_t)n * (D - 2))) return FMM_ERR_OUT_OF_MEMORY;
+    auto lo_kern = dim == 3 ? k_level_offsets<3> : k_level_offsets<2>;
+    lo_kern<<<cdiv(n, TPB), TPB, 0, st>>>(d_pos_g, d_mass_g, t.d_perm, ws.leaf_of, ws.cell_key, n, D, 2, D - 1,
+                                          g.lo[0], g.lo[1], g.lo[2], g.ext[0], g.ext[1], g.ext[2], eb.lvl_off.ptr);
+    ws.launches += 1;
+  }
+  // L2L, top-down: every cell of levels >= 3, or with the shortcut only the
+  // cells that need a local expansion (their own class-grouped list)
+  const int *tl2 = tl;
+  const int4 *b2 = eb.batches.ptr;
+  std::vector<int> l2_b0(lvl_b0), l2_b1(lvl_b1);
+  uint8_t *needs = shortcut ? eb.lact.ptr + ncell : nullptr;
+  if (shortcut) {
+    const int first2 = t.level_off[2];
+    k_needs_l<<<cdiv(ntl, TPB), TPB, 0, st>>>(eb.lact.ptr, first2, ntl, ws.cell_parent, cell0, needs);
+    const int nl3 = t.level_off[D] + t.level_count[D] - t.level_off[3];
+    for (int d = 3; d <= D; ++d)
+      k_l2l_keys<<<cdiv(t.level_count[d], TPB), TPB, 0, st>>>(ws.cell_key, needs, t.level_off[d], t.level_count[d], d,
+                                                              dim, cell0, eb.ckey.ptr, eb.cval.ptr,
+                                                              t.level_off[d] - t.level_off[3]);
+    ws.launches += D - 1;
+    uint64_t *kk = eb.ckey.ptr, *kk2 = eb.ckey_alt.ptr;
+    uint32_t *vv = eb.cval.ptr, *vv2 = eb.cval2.ptr;
+    radix_sort(ws, kk, vv, kk2, vv2, nl3, 8, st);
+    CUDA_TRY(cudaMemsetAsync(eb.cls_count.ptr, 0, 256 * sizeof(uint32_t), st));
+    k_class_hist<<<std::min(cdiv(nl3, TPB), 148 * 4), TPB, 0, st>>>(kk, nl3, eb.cls_count.ptr);
+    ws.launches += 1;
+    uint32_t hc[256];
+    CUDA_TRY(cudaMemcpyAsync(hc, eb.cls_count.ptr, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<int4> hb2;
+    int off = 0;
+    const int ncls = 1 << dim;
+    for (int d = 3; d <= D; ++d) {
+      l2_b0[d] = (int)hb2.size();
+      for (int c = 0; c < ncls; ++c) {
+        const int cnt = (int)hc[(d << dim) | c];
+        for (int s0 = 0; s0 < cnt; s0 += tchunk) hb2.push_back(make_int4(off + s0, std::min(tchunk, cnt - s0), d, c));
+        off += cnt;
+      }
+      l2_b1[d] = (int)hb2.size();
+    }
+    if (!eb.batches2.reserve(hb2.size() + 1)) return FMM_ERR_OUT_OF_MEMORY;
+    if (!hb2.empty())
+      CUDA_TRY(cudaMemcpyAsync(eb.batches2.ptr, hb2.data(), hb2.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+    tl2 = (const int *)vv;
+    b2 = eb.batches2.ptr;
+    if (!eb.esrc.reserve((size_t)t.level_count[D]) || !eb.elev.reserve((size_t)t.level_count[D]))
+      return FMM_ERR_OUT_OF_MEMORY;
+    k_leaf_esrc<<<cdiv(t.level_count[D], TPB), TPB, 0, st>>>(t.level_off[D], t.level_count[D], D, first2,
+                                                              ws.cell_parent, needs, cell0, eb.esrc.ptr, eb.elev.ptr);
+    ws.launches += 2;
+  }
   for (int d = 3; d <= D && tc; ++d) {
     TcArgs t2 = ta;
     t2.mode = TC_L2L;
-    t2.batches = eb.batches.ptr + lvl_b0[d];
-    t2.tlist = tl;
+    t2.batches = b2 + l2_b0[d];
+    t2.tlist = tl2;
     t2.op_base = ops.off_l2l;
     t2.X = eb.L.ptr;
     t2.Y = eb.L.ptr;
-    int rc = tc_launch(t2, lvl_b1[d] - lvl_b0[d], eb.tc_work.ptr + tc_k++, st, ws.launches);
+    int rc = tc_launch(t2, l2_b1[d] - l2_b0[d], eb.tc_work.ptr + tc_k++, st, ws.launches);
     if (rc) return rc;
   }
   for (int d = 3; d <= D && !tc; ++d) {
     ContractArgs c2 = ca;
     c2.mode = MODE_L2L;
     c2.slot_base = ops.off_l2l;
-    c2.tlist = tl;
+    c2.tlist = tl2;
     c2.X = eb.L.ptr;
     c2.Y = eb.L.ptr;
-    c2.batches = eb.batches.ptr + lvl_b0[d];
-    int rc = launch_contract(c2, lvl_b1[d] - lvl_b0[d], st, ws.launches);
+    c2.batches = b2 + l2_b0[d];
+    int rc = launch_contract(c2, l2_b1[d] - l2_b0[d], st, ws.launches);
     if (rc) return rc;
   }
   // L2P
   if (dim == 3)
-    k_l2p3d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far);
+    k_l2p3d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far,
+                                          shortcut ? eb.esrc.ptr : nullptr, shortcut ? eb.elev.ptr : nullptr,
+                                          t.level_off[D], D, eb.lvl_off.ptr, (float)(1.0 / emax));
   else
     k_l2p2d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far);
   ws.launches += 1;
@@ -1369,13 +1493,6 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   // launch, coarse levels first so that their long warps start early
   if ((direct_max > 0 || any_fdirect) && D >= 2) {
     if (D + 1 > DF_MAX_LEVELS) return FMM_ERR_UNSUPPORTED;
-    if (D > 2) {
-      if (!eb.lvl_off.reserve((size_t)n * (D - 2))) return FMM_ERR_OUT_OF_MEMORY;
-      auto lo_kern = dim == 3 ? k_level_offsets<3> : k_level_offsets<2>;
-      lo_kern<<<cdiv(n, TPB), TPB, 0, st>>>(d_pos_g, d_mass_g, t.d_perm, ws.leaf_of, ws.cell_key, n, D, 2, D - 1,
-                                            g.lo[0], g.lo[1], g.lo[2], g.ext[0], g.ext[1], g.ext[2], eb.lvl_off.ptr);
-      ws.launches += 1;
-    }
     DirectArgs da;
     da.pbeg = ws.cell_pbeg;
     da.pend = ws.cell_pend;
