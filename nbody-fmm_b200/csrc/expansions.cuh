@@ -26,13 +26,16 @@ struct ExpBuffers {
   DevBuf<uint32_t> cval, cval2;
   DevBuf<int4> batches;
   DevBuf<uint32_t> cls_count;
-  DevBuf<float4> lvl_off;
-  DevBuf<uint8_t> lact;    // L2L shortcut: [0, ncell) cells with M2L contributions, [ncell, 2 ncell) cells needing L
-  DevBuf<int4> batches2;   // L2L shortcut: batches of the cells that need L2L
+  DevBuf<float4> lvl_off;  // particle offsets from their level-d ancestor's centre, levels 2..D-1
+  DevBuf<uint8_t> lact;    // shortcuts, per cell: [0, ncell) M2L contributions, [ncell, 2 ncell) needs L,
+                           // [2 ncell, 3 ncell) M2L source, [3 ncell, 4 ncell) how M is formed
+  DevBuf<uint64_t> ukey;   // shortcuts: sort keys (two sorts, key and alternate each)
+  DevBuf<uint32_t> uval;
+  DevBuf<int4> batches2;   // shortcuts: batches of the cells that need L2L, then of the M2M rows
   DevBuf<int> esrc;        // L2L shortcut: per leaf, the cell whose local expansion its particles evaluate
   DevBuf<uint8_t> elev;    //   and that cell's level
   DevBuf<int> m2l_src, m2l_list, m2l_nslots, m2l_tslot;  // per M2L batch: resolved sources and present slots
-  DevBuf<uint16_t> tc_img;
+  DevBuf<uint16_t> tc_img;       // BF16 split operator images for the tensor-core translations
   DevBuf<unsigned int> tc_work;  // zeroed work counters of the tensor-core launches
   DevBuf<uint8_t> order_p16;     // per M2L operator slot: padded width of its pair order
   DevBuf<uint8_t> fdirect;       // per offset (dx+3) + 7(dy+3) + 49(dz+3): not well separated (direct)
@@ -41,7 +44,7 @@ struct ExpBuffers {
   DevBuf<uint8_t> m2l_split_w;   // [2][batch][189] widths of the lo / hi lists
   DevBuf<float> cf;              // learned orders: per-cell features (ORD_CF floats per cell)
   DevBuf<double> frms;           // learned orders: [0] F_rms of the previous pass (G = 1), [1] scratch,
-                                 // [2] total mass  // BF16 split operator images for the tensor-core M2L  // particle offsets from their level-d ancestor (direct far field)
+                                 // [2] total mass
 };
 
 // Per-pass parameters.

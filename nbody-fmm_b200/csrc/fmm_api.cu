@@ -175,6 +175,8 @@ int fmm_destroy(fmm_ctx *c) {
   c->eb.batches2.release();
   c->eb.esrc.release();
   c->eb.elev.release();
+  c->eb.ukey.release();
+  c->eb.uval.release();
   c->eb.m2l_split_w.release();
   c->eb.m2l_w.release();
   c->eb.cf.release();

@@ -18,8 +18,8 @@ namespace fmm {
 __device__ inline float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
 // ---------------------------------------------------------------- features
-__global__ void k_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int count2,
-                                int cell0, int p, int KS, float *cf, double *mtot) {
+__global__ void k_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int cell0,
+                                int p, int KS, float *cf) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const int c = first + i;
@@ -38,7 +38,22 @@ __global__ void k_cell_features(const float *M, const int *pbeg, const int *pend
   }
   o[13] = m0 > 0.f ? log10f(m0) : -30.f;
   o[14] = o[15] = 0.f;
-  if (i < count2) atomicAdd(mtot, (double)m[0]);
+}
+
+__global__ void k_mass_total(const float4 *part, int64_t n, double *mtot) {
+  __shared__ double s[8];
+  double v = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v += (double)part[i].w;
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s[w];
+    atomicAdd(mtot, t);
+  }
 }
 
 __device__ inline unsigned long long splitmix(unsigned long long x) {
@@ -647,11 +662,16 @@ int order_judge_compare(const double *acc, const double *ref, const int64_t *tar
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
 }
 
-int order_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int count2, int cell0,
-                        int p, int KS, float *cf, double *mtot, cudaStream_t st, int64_t &launches) {
-  if (count <= 0) return FMM_OK;
+int order_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int cell0, int p,
+                        int KS, float *cf, const float4 *part, int64_t n, double *mtot, cudaStream_t st,
+                        int64_t &launches) {
   CUDA_TRY(cudaMemsetAsync(mtot, 0, sizeof(double), st));
-  k_cell_features<<<cdiv(count, 256), 256, 0, st>>>(M, pbeg, pend, first, count, count2, cell0, p, KS, cf, mtot);
+  if (n > 0) {
+    k_mass_total<<<std::max(1, std::min(cdiv(n, 256), 148 * 2)), 256, 0, st>>>(part, n, mtot);
+    launches += 1;
+  }
+  if (count <= 0) return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
+  k_cell_features<<<cdiv(count, 256), 256, 0, st>>>(M, pbeg, pend, first, count, cell0, p, KS, cf);
   launches += 1;
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
 }

@@ -297,10 +297,12 @@ static int launch_contract(const ContractArgs &a, int nb, cudaStream_t st, int64
 // the contraction (the lookups are chains of dependent loads, cheap when
 // thousands are in flight) and lists, per batch, the slots with at least one
 // source.  One block per batch of up to `tchunk` (64 or 128) targets; with
-// pair_count set it also counts the (target, source) pairs.
+// pair_count set it also counts the (target, source) pairs, with lact / msrc
+// set it flags the targets with a source and the sources.
 __global__ void k_m2l_sources(ContractArgs a, int tchunk, int *src_tab, int *slot_list, int *nslots_tab,
                               int *tslot_list, unsigned long long *pair_count, const uint8_t *order_p16,
-                              uint8_t *slot_p16, unsigned long long *nt_sum, uint8_t *lact, int cell0) {
+                              uint8_t *slot_p16, unsigned long long *nt_sum, uint8_t *lact, uint8_t *msrc,
+                              int cell0) {
   __shared__ int s_flag[189];
   __shared__ int s_tgt[128];
   __shared__ int s_cnt;
@@ -328,6 +330,7 @@ __global__ void k_m2l_sources(ContractArgs a, int tchunk, int *src_tab, int *slo
       ++cnt;
       ntc += (unsigned long long)(a.cpend[s_tgt[t]] - a.cpbeg[s_tgt[t]]);
       if (lact) lact[s_tgt[t] - cell0] = 1;
+      if (msrc) msrc[src - cell0] = 1;
     }
   }
   if (pair_count && cnt) atomicAdd(&s_cnt, cnt);
@@ -983,6 +986,123 @@ __global__ void k_class_hist(const uint64_t *keys, int n, uint32_t *hist) {
   if (h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
 }
 
+// ------------------------------------------------------------ M shortcut
+// Multipoles are formed only for the cells M2L reads (its sources) and for
+// its targets (their spectrum is a feature of the learned orders), plus what
+// M2M needs to form those.  A needed cell with at most P2M_DIRECT_MAX
+// particles, or a leaf, takes its multipole straight from its particles
+// (mode 1); a larger one sums its children by M2M (mode 2), which makes all
+// of them needed.  mode 0: not formed.
+static constexpr int P2M_DIRECT_MAX = 64;
+
+__global__ void k_m_mode(const uint8_t *lact, const uint8_t *msrc, int first2, int leaf_first, int count,
+                         const int *parent, const int *pbeg, const int *pend, int cell0, int tmax, uint8_t *mode) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int c = first2 + i;
+  int a = c;
+  bool req = lact[a - cell0] || msrc[a - cell0];
+  while (!req) {  // needed through a chain of M2M ancestors
+    const int P = parent[a];
+    if (P < first2 || pend[P] - pbeg[P] <= tmax) break;
+    a = P;
+    req = lact[a - cell0] || msrc[a - cell0];
+  }
+  mode[c - cell0] = !req ? 0 : (c >= leaf_first || pend[c] - pbeg[c] <= tmax) ? 1 : 2;
+}
+
+// Sort keys of the M2M rows of one level: with child_rows (tensor-core
+// M2M, rows are children) the children of mode-2 cells by (level, class),
+// else (CUDA-core M2M, rows are parents) the mode-2 cells by (level, 0);
+// 255 for the rest.
+__global__ void k_m2m_keys(const uint64_t *ckey, const uint8_t *mode, const int *parent, int first, int count,
+                           int level, int dim, int cell0, int child_rows, uint64_t *keys, uint32_t *vals, int out_off) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int g = first + i;
+  const bool on = child_rows ? mode[parent[g] - cell0] == 2 : mode[g - cell0] == 2;
+  const uint64_t cls = child_rows ? (ckey[g] & ((1u << dim) - 1)) : 0u;
+  keys[out_off + i] = on ? (((uint64_t)level << dim) | cls) : 255u;
+  vals[out_off + i] = (uint32_t)g;
+}
+
+struct P2MCellArgs {
+  int nlev;                          // levels 2 .. nlev + 1
+  int first[DF_MAX_LEVELS + 1];      // first cell of each level; first[nlev]: end
+  const float4 *off[DF_MAX_LEVELS];  // particle offsets from the level's cell centres, mass in w
+  float inv_s[DF_MAX_LEVELS];        // 2^level / emax
+  const int *pbeg, *pend;
+  const uint8_t *mode;
+  int cell0, p, KS;
+  float *M;
+};
+
+// P2M of the mode-1 cells of every level: one warp per cell, lanes over its
+// particles (32 at a time), every coefficient summed by a warp reduction as
+// wide as the particles present, collected in shared memory and stored as
+// one row (no atomics; the padding columns are written as zeros).
+__global__ void __launch_bounds__(256) k_p2m_cells(P2MCellArgs a) {
+  __shared__ float s_row[8][FMM_MAX_P * FMM_MAX_P + 2 * FMM_MAX_P + 4];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t c64 = (int64_t)a.first[0] + (int64_t)blockIdx.x * 8 + warp;
+  if (c64 >= a.first[a.nlev]) return;
+  const int c = (int)c64;
+  if (a.mode[c - a.cell0] != 1) return;
+  int k = 0;
+  while (k + 1 < a.nlev && c >= a.first[k + 1]) ++k;
+  float *s = s_row[warp];
+  for (int j = lane; j < a.KS; j += 32) s[j] = 0.f;
+  __syncwarp();
+  const int pb = a.pbeg[c], pe = a.pend[c], p = a.p;
+  const float4 *off = a.off[k];
+  const float inv_s = a.inv_s[k];
+  for (int j0 = pb; j0 < pe; j0 += 32) {
+    const int cnt = min(32, pe - j0);
+    int width = 1;
+    while (width < cnt) width <<= 1;
+    const float4 q = lane < cnt ? off[j0 + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float x = q.x * inv_s, y = q.y * inv_s, z = q.z * inv_s, r2 = x * x + y * y + z * z, w = q.w;
+    auto wsum = [&](float v) {
+      for (int o = width >> 1; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      return v;
+    };
+    float dre = 1.f, dim_ = 0.f;
+    for (int m = 0; m <= p; ++m) {
+      if (m > 0) {
+        const float h = -0.5f / m;
+        const float nre = h * (x * dre - y * dim_), nim = h * (x * dim_ + y * dre);
+        dre = nre;
+        dim_ = nim;
+      }
+      float p1re = dre, p1im = dim_, p2re = 0.f, p2im = 0.f;
+      for (int l = m; l <= p; ++l) {
+        float cre, cim;
+        if (l == m) {
+          cre = dre;
+          cim = dim_;
+        } else {
+          const float a1 = c_rec1[l][m] * z, a2 = c_rec2[l][m] * r2;
+          cre = a1 * p1re - a2 * p2re;
+          cim = a1 * p1im - a2 * p2im;
+          p2re = p1re;
+          p2im = p1im;
+          p1re = cre;
+          p1im = cim;
+        }
+        const float vr = wsum(w * cre);
+        if (lane == 0) s[re_idx(l, m)] += vr;
+        if (m > 0) {
+          const float vi = wsum(-w * cim);
+          if (lane == 0) s[im_idx(l, m)] += vi;
+        }
+      }
+    }
+  }
+  __syncwarp();
+  float *row = a.M + (size_t)(c - a.cell0) * a.KS;
+  for (int j = lane; j < a.KS; j += 32) row[j] = s[j];
+}
+
 // ------------------------------------------------------------ L2L shortcut
 // Marks every ancestor-or-self at levels >= 2 of the cells with M2L
 // contributions (lact): the cells whose local expansion is needed below.
@@ -1212,61 +1332,39 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   ta.P16 = P16;
   ta.err = ws.dev_err;
 
-  if (ev) cudaEventRecord(ev[1], st);
-  // P2M
-  if (dim == 3) k_p2m3d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.M.ptr);
-  else k_p2m2d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.M.ptr);
-  ws.launches += 1;
-  // M2M, bottom-up
-  for (int d = D - 1; d >= 2 && tc; --d) {  // children of level d + 1 by class
-    TcArgs t2 = ta;
-    t2.mode = TC_M2M;
-    t2.batches = eb.batches.ptr + lvl_b0[d + 1];
-    t2.tlist = tl;
-    t2.op_base = ops.off_m2m;
-    t2.X = eb.M.ptr;
-    t2.Y = eb.M.ptr;
-    int rc = tc_launch(t2, lvl_b1[d + 1] - lvl_b0[d + 1], eb.tc_work.ptr + tc_k++, st, ws.launches);
-    if (rc) return rc;
-  }
-  for (int d = D - 1; d >= 2 && !tc; --d) {
-    ca.mode = MODE_M2M;
-    ca.slot_base = ops.off_m2m;
-    ca.tlist = nullptr;
-    ca.X = eb.M.ptr;
-    ca.Y = eb.M.ptr;
-    ContractArgs c2 = ca;
-    c2.batches = eb.batches.ptr + m2m_b0[d];
-    int rc = launch_contract(c2, m2m_b1[d] - m2m_b0[d], st, ws.launches);
-    if (rc) return rc;
-  }
-  if (ev) cudaEventRecord(ev[2], st);
-  // L2L shortcut (3D): only the cells on a path to M2L contributions get
-  // local expansions; L2P reads the deepest such ancestor of each leaf
+  // 3D shortcuts: local expansions only on paths to cells with M2L
+  // contributions (L2P from each leaf's deepest such ancestor), multipoles
+  // only for what M2L reads (P2M straight into small cells, M2M above them)
   const bool shortcut = dim == 3 && D >= 3;
+  uint8_t *lact = nullptr, *needs = nullptr, *msrc = nullptr, *mmode = nullptr;
   if (shortcut) {
-    if (!eb.lact.reserve(2 * (size_t)ncell)) return FMM_ERR_OUT_OF_MEMORY;
-    CUDA_TRY(cudaMemsetAsync(eb.lact.ptr, 0, 2 * (size_t)ncell, st));
+    if (!eb.lact.reserve(4 * (size_t)ncell)) return FMM_ERR_OUT_OF_MEMORY;
+    CUDA_TRY(cudaMemsetAsync(eb.lact.ptr, 0, 4 * (size_t)ncell, st));
+    lact = eb.lact.ptr;
+    needs = lact + ncell;
+    msrc = lact + 2 * (size_t)ncell;
+    mmode = lact + 3 * (size_t)ncell;
   }
-  // M2L, all levels in one launch
+  // M2L plan, all levels: the source of every (slot, target) of each batch
+  // and, with variable orders, the geometric widths
+  ContractArgs cm = ca;
+  cm.mode = MODE_M2L;
+  cm.slot_base = 0;
+  cm.tlist = tl_m2l;
+  cm.X = eb.M.ptr;
+  cm.Y = eb.L.ptr;
+  cm.batches = eb.batches.ptr + m2l_b0[2];
+  const int nbm = D >= 2 ? m2l_b1[D] - m2l_b0[2] : 0;
+  const bool geometric = tc && order.mode == FMM_ORDER_GEOMETRIC;
+  const bool learned = tc && dim == 3 && order.mode == FMM_ORDER_LEARNED && order.params;
+  const bool collect = tc && dim == 3 && order.ntiles > 0 && ops.tab64.ptr;
+  const bool var_order = geometric || learned;
+  const float ax = (float)(g.ext[0] / emax), ay = (float)(g.ext[1] / emax),
+              az = (float)(dim == 3 ? g.ext[2] / emax : 0.0);
   if (D >= 2) {
-    ContractArgs c2 = ca;
-    c2.mode = MODE_M2L;
-    c2.slot_base = 0;
-    c2.tlist = tl_m2l;
-    c2.X = eb.M.ptr;
-    c2.Y = eb.L.ptr;
-    c2.batches = eb.batches.ptr + m2l_b0[2];
-    const int nbm = m2l_b1[D] - m2l_b0[2];
     if (!eb.m2l_src.reserve((size_t)nbm * 189 * tchunk) || !eb.m2l_list.reserve((size_t)nbm * 189) ||
         !eb.m2l_nslots.reserve(nbm) || !eb.m2l_tslot.reserve((size_t)nbm * 189))
       return FMM_ERR_OUT_OF_MEMORY;
-    const bool geometric = tc && order.mode == FMM_ORDER_GEOMETRIC;
-    const bool learned = tc && dim == 3 && order.mode == FMM_ORDER_LEARNED && order.params;
-    const bool collect = tc && dim == 3 && order.ntiles > 0 && ops.tab64.ptr;
-    const bool var_order = geometric || learned;
-    const float ax = (float)(g.ext[0] / emax), ay = (float)(g.ext[1] / emax),
-                az = (float)(dim == 3 ? g.ext[2] / emax : 0.0);
     if (var_order && !eb.m2l_w.reserve((size_t)nbm * 189)) return FMM_ERR_OUT_OF_MEMORY;
     if (geometric) {
       if (!eb.order_p16.reserve(ops.n_m2l)) return FMM_ERR_OUT_OF_MEMORY;
@@ -1274,13 +1372,160 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
                                        eb.order_p16.ptr);
       ws.launches += 1;
     }
+    if (nbm > 0) {
+      k_m2l_sources<<<nbm, 256, 0, st>>>(cm, tchunk, eb.m2l_src.ptr, eb.m2l_list.ptr, eb.m2l_nslots.ptr,
+                                         tc ? eb.m2l_tslot.ptr : nullptr, tc ? ws.counters : nullptr,
+                                         geometric ? eb.order_p16.ptr : nullptr, geometric ? eb.m2l_w.ptr : nullptr,
+                                         ws.counters + 4, lact, msrc, cell0);
+      ws.launches += 1;
+    }
+  }
+  // particle offsets from their ancestors' centres, levels 2..D-1 (P2M and
+  // L2P shortcuts, direct far field)
+  const bool need_lvl_off = D > 2 && (shortcut || direct_max > 0 || any_fdirect);
+  if (need_lvl_off) {
+    if (!eb.lvl_off.reserve((size_t)n * (D - 2))) return FMM_ERR_OUT_OF_MEMORY;
+    auto lo_kern = dim == 3 ? k_level_offsets<3> : k_level_offsets<2>;
+    lo_kern<<<cdiv(n, TPB), TPB, 0, st>>>(d_pos_g, d_mass_g, t.d_perm, ws.leaf_of, ws.cell_key, n, D, 2, D - 1,
+                                          g.lo[0], g.lo[1], g.lo[2], g.ext[0], g.ext[1], g.ext[2], eb.lvl_off.ptr);
+    ws.launches += 1;
+  }
+  // shortcut lists: the cells that need L2L and the M2M rows, each grouped
+  // by (level, class), from one histogram read-back
+  const int *tl2 = tl, *tlm = nullptr;
+  const int4 *b2 = eb.batches.ptr;
+  std::vector<int> l2_b0(lvl_b0), l2_b1(lvl_b1), um_b0(D + 2, 0), um_b1(D + 2, 0);
+  if (shortcut) {
+    const int first2 = t.level_off[2], leaf_first = t.level_off[D];
+    k_needs_l<<<cdiv(ntl, TPB), TPB, 0, st>>>(lact, first2, ntl, ws.cell_parent, cell0, needs);
+    k_m_mode<<<cdiv(ntl, TPB), TPB, 0, st>>>(lact, msrc, first2, leaf_first, ntl, ws.cell_parent, ws.cell_pbeg,
+                                             ws.cell_pend, cell0, P2M_DIRECT_MAX, mmode);
+    ws.launches += 2;
+    // L2L rows: levels 3..D; M2M rows: children at levels 3..D (tensor
+    // cores) or the mode-2 parents at levels 2..D-1
+    const int l3 = t.level_off[3], nl3 = t.level_off[D] + t.level_count[D] - l3;
+    const int m_lo = tc ? 3 : 2, m_hi = tc ? D : D - 1;
+    const int m_first = t.level_off[m_lo], nm = t.level_off[m_hi] + t.level_count[m_hi] - m_first;
+    if (!eb.ukey.reserve(4 * (size_t)ntl) || !eb.uval.reserve(4 * (size_t)ntl)) return FMM_ERR_OUT_OF_MEMORY;
+    for (int d = 3; d <= D; ++d)
+      k_l2l_keys<<<cdiv(t.level_count[d], TPB), TPB, 0, st>>>(ws.cell_key, needs, t.level_off[d], t.level_count[d], d,
+                                                              dim, cell0, eb.ukey.ptr, eb.uval.ptr, t.level_off[d] - l3);
+    for (int d = m_lo; d <= m_hi; ++d)
+      k_m2m_keys<<<cdiv(t.level_count[d], TPB), TPB, 0, st>>>(ws.cell_key, mmode, ws.cell_parent, t.level_off[d],
+                                                              t.level_count[d], d, dim, cell0, tc ? 1 : 0,
+                                                              eb.ukey.ptr + 2 * (size_t)ntl,
+                                                              eb.uval.ptr + 2 * (size_t)ntl, t.level_off[d] - m_first);
+    ws.launches += (D - 2) + (m_hi - m_lo + 1);
+    uint64_t *kk = eb.ukey.ptr, *kk2 = eb.ukey.ptr + ntl;
+    uint32_t *vv = eb.uval.ptr, *vv2 = eb.uval.ptr + ntl;
+    radix_sort(ws, kk, vv, kk2, vv2, nl3, 8, st);
+    uint64_t *mk = eb.ukey.ptr + 2 * (size_t)ntl, *mk2 = eb.ukey.ptr + 3 * (size_t)ntl;
+    uint32_t *mv = eb.uval.ptr + 2 * (size_t)ntl, *mv2 = eb.uval.ptr + 3 * (size_t)ntl;
+    radix_sort(ws, mk, mv, mk2, mv2, nm, 8, st);
+    CUDA_TRY(cudaMemsetAsync(eb.cls_count.ptr, 0, 512 * sizeof(uint32_t), st));
+    k_class_hist<<<std::max(1, std::min(cdiv(nl3, TPB), 148 * 4)), TPB, 0, st>>>(kk, nl3, eb.cls_count.ptr);
+    k_class_hist<<<std::max(1, std::min(cdiv(nm, TPB), 148 * 4)), TPB, 0, st>>>(mk, nm, eb.cls_count.ptr + 256);
+    ws.launches += 2;
+    uint32_t hc[512];
+    CUDA_TRY(cudaMemcpyAsync(hc, eb.cls_count.ptr, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    std::vector<int4> hb2;
+    const int ncls = 1 << dim;
+    int off = 0;
+    for (int d = 3; d <= D; ++d) {
+      l2_b0[d] = (int)hb2.size();
+      for (int c = 0; c < ncls; ++c) {
+        const int cnt = (int)hc[(d << dim) | c];
+        for (int s0 = 0; s0 < cnt; s0 += tchunk) hb2.push_back(make_int4(off + s0, std::min(tchunk, cnt - s0), d, c));
+        off += cnt;
+      }
+      l2_b1[d] = (int)hb2.size();
+    }
+    off = 0;
+    for (int d = m_lo; d <= m_hi; ++d) {
+      um_b0[d] = (int)hb2.size();
+      for (int c = 0; c < (tc ? ncls : 1); ++c) {
+        const int cnt = (int)hc[256 + ((d << dim) | c)];
+        for (int s0 = 0; s0 < cnt; s0 += tchunk)
+          hb2.push_back(make_int4(off + s0, std::min(tchunk, cnt - s0), d, tc ? c : -1));
+        off += cnt;
+      }
+      um_b1[d] = (int)hb2.size();
+    }
+    if (!eb.batches2.reserve(hb2.size() + 1)) return FMM_ERR_OUT_OF_MEMORY;
+    if (!hb2.empty())
+      CUDA_TRY(cudaMemcpyAsync(eb.batches2.ptr, hb2.data(), hb2.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+    tl2 = (const int *)vv;
+    tlm = (const int *)mv;
+    b2 = eb.batches2.ptr;
+    if (!eb.esrc.reserve((size_t)t.level_count[D]) || !eb.elev.reserve((size_t)t.level_count[D]))
+      return FMM_ERR_OUT_OF_MEMORY;
+    k_leaf_esrc<<<cdiv(t.level_count[D], TPB), TPB, 0, st>>>(leaf_first, t.level_count[D], D, first2, ws.cell_parent,
+                                                              needs, cell0, eb.esrc.ptr, eb.elev.ptr);
+    ws.launches += 1;
+  }
+
+  if (ev) cudaEventRecord(ev[1], st);
+  // P2M
+  if (shortcut) {
+    if (D - 1 > DF_MAX_LEVELS) return FMM_ERR_UNSUPPORTED;
+    P2MCellArgs pm;
+    pm.nlev = D - 1;
+    for (int d = 2; d <= D; ++d) {
+      pm.first[d - 2] = t.level_off[d];
+      pm.off[d - 2] = d == D ? ws.part : eb.lvl_off.ptr + (size_t)(d - 2) * n;
+      pm.inv_s[d - 2] = (float)(std::ldexp(1.0, d) / emax);
+    }
+    pm.first[D - 1] = t.level_off[D] + t.level_count[D];
+    pm.pbeg = ws.cell_pbeg;
+    pm.pend = ws.cell_pend;
+    pm.mode = mmode;
+    pm.cell0 = cell0;
+    pm.p = p;
+    pm.KS = KS;
+    pm.M = eb.M.ptr;
+    k_p2m_cells<<<cdiv(ntl, 8), 256, 0, st>>>(pm);
+  } else if (dim == 3) {
+    k_p2m3d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.M.ptr);
+  } else {
+    k_p2m2d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.M.ptr);
+  }
+  ws.launches += 1;
+  // M2M, bottom-up
+  for (int d = D - 1; d >= 2 && tc; --d) {  // children of level d + 1 by class
+    TcArgs t2 = ta;
+    t2.mode = TC_M2M;
+    t2.batches = shortcut ? b2 + um_b0[d + 1] : eb.batches.ptr + lvl_b0[d + 1];
+    t2.tlist = shortcut ? tlm : tl;
+    t2.op_base = ops.off_m2m;
+    t2.X = eb.M.ptr;
+    t2.Y = eb.M.ptr;
+    const int nb = shortcut ? um_b1[d + 1] - um_b0[d + 1] : lvl_b1[d + 1] - lvl_b0[d + 1];
+    int rc = tc_launch(t2, nb, eb.tc_work.ptr + tc_k++, st, ws.launches);
+    if (rc) return rc;
+  }
+  for (int d = D - 1; d >= 2 && !tc; --d) {  // cells of level d gather their children
+    ContractArgs c2 = ca;
+    c2.mode = MODE_M2M;
+    c2.slot_base = ops.off_m2m;
+    c2.tlist = shortcut ? tlm : nullptr;
+    c2.X = eb.M.ptr;
+    c2.Y = eb.M.ptr;
+    c2.batches = shortcut ? b2 + um_b0[d] : eb.batches.ptr + m2m_b0[d];
+    const int nb = shortcut ? um_b1[d] - um_b0[d] : m2m_b1[d] - m2m_b0[d];
+    int rc = launch_contract(c2, nb, st, ws.launches);
+    if (rc) return rc;
+  }
+  if (ev) cudaEventRecord(ev[2], st);
+  // M2L, all levels in one launch
+  if (D >= 2) {
     TileArgs tla;
     if (learned || collect) {
       if (!eb.cf.reserve((size_t)ncell * ORD_CF) || !eb.frms.reserve(3)) return FMM_ERR_OUT_OF_MEMORY;
-      int rc = order_cell_features(eb.M.ptr, ws.cell_pbeg, ws.cell_pend, t.level_off[2], ntl, t.level_count[2], cell0,
-                                   p, KS, eb.cf.ptr, eb.frms.ptr + 2, st, ws.launches);
+      int rc = order_cell_features(eb.M.ptr, ws.cell_pbeg, ws.cell_pend, t.level_off[2], ntl, cell0, p, KS, eb.cf.ptr,
+                                   ws.part, n, eb.frms.ptr + 2, st, ws.launches);
       if (rc) return rc;
-      tla.batches = c2.batches;
+      tla.batches = cm.batches;
       tla.tlist = tl_m2l;
       tla.src_tab = eb.m2l_src.ptr;
       tla.slot_list = eb.m2l_list.ptr;
@@ -1294,13 +1539,6 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
       tla.ax = ax;
       tla.ay = ay;
       tla.az = az;
-    }
-    if (nbm > 0) {
-      k_m2l_sources<<<nbm, 256, 0, st>>>(c2, tchunk, eb.m2l_src.ptr, eb.m2l_list.ptr, eb.m2l_nslots.ptr,
-                                         tc ? eb.m2l_tslot.ptr : nullptr, tc ? ws.counters : nullptr,
-                                         geometric ? eb.order_p16.ptr : nullptr, geometric ? eb.m2l_w.ptr : nullptr,
-                                         ws.counters + 4, shortcut ? eb.lact.ptr : nullptr, cell0);
-      ws.launches += 1;
     }
     if (learned && nbm > 0) {
       InferArgs ia;
@@ -1349,7 +1587,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     if (tc) {
       TcArgs t2 = ta;
       t2.mode = TC_M2L;
-      t2.batches = c2.batches;
+      t2.batches = cm.batches;
       t2.tlist = tl_m2l;
       t2.src_tab = eb.m2l_src.ptr;
       t2.slot_list = eb.m2l_list.ptr;
@@ -1393,71 +1631,16 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
         rc = tc_launch(t2, nbm, eb.tc_work.ptr + tc_k++, st, ws.launches);
       }
     } else {
-      c2.src_tab = eb.m2l_src.ptr;
-      c2.slot_list = eb.m2l_list.ptr;
-      c2.nslots_tab = eb.m2l_nslots.ptr;
-      rc = launch_contract(c2, nbm, st, ws.launches);
+      cm.src_tab = eb.m2l_src.ptr;
+      cm.slot_list = eb.m2l_list.ptr;
+      cm.nslots_tab = eb.m2l_nslots.ptr;
+      rc = launch_contract(cm, nbm, st, ws.launches);
     }
     if (rc) return rc;
   }
   if (ev) cudaEventRecord(ev[3], st);
-  // particle offsets from their ancestors' centres, levels 2..D-1 (L2P
-  // shortcut and direct far field)
-  const bool need_lvl_off = D > 2 && (shortcut || direct_max > 0 || any_fdirect);
-  if (need_lvl_off) {
-    if (!eb.lvl_off.reserve((size_t)n * (D - 2))) return FMM_ERR_OUT_OF_MEMORY;
-    auto lo_kern = dim == 3 ? k_level_offsets<3> : k_level_offsets<2>;
-    lo_kern<<<cdiv(n, TPB), TPB, 0, st>>>(d_pos_g, d_mass_g, t.d_perm, ws.leaf_of, ws.cell_key, n, D, 2, D - 1,
-                                          g.lo[0], g.lo[1], g.lo[2], g.ext[0], g.ext[1], g.ext[2], eb.lvl_off.ptr);
-    ws.launches += 1;
-  }
   // L2L, top-down: every cell of levels >= 3, or with the shortcut only the
   // cells that need a local expansion (their own class-grouped list)
-  const int *tl2 = tl;
-  const int4 *b2 = eb.batches.ptr;
-  std::vector<int> l2_b0(lvl_b0), l2_b1(lvl_b1);
-  uint8_t *needs = shortcut ? eb.lact.ptr + ncell : nullptr;
-  if (shortcut) {
-    const int first2 = t.level_off[2];
-    k_needs_l<<<cdiv(ntl, TPB), TPB, 0, st>>>(eb.lact.ptr, first2, ntl, ws.cell_parent, cell0, needs);
-    const int nl3 = t.level_off[D] + t.level_count[D] - t.level_off[3];
-    for (int d = 3; d <= D; ++d)
-      k_l2l_keys<<<cdiv(t.level_count[d], TPB), TPB, 0, st>>>(ws.cell_key, needs, t.level_off[d], t.level_count[d], d,
-                                                              dim, cell0, eb.ckey.ptr, eb.cval.ptr,
-                                                              t.level_off[d] - t.level_off[3]);
-    ws.launches += D - 1;
-    uint64_t *kk = eb.ckey.ptr, *kk2 = eb.ckey_alt.ptr;
-    uint32_t *vv = eb.cval.ptr, *vv2 = eb.cval2.ptr;
-    radix_sort(ws, kk, vv, kk2, vv2, nl3, 8, st);
-    CUDA_TRY(cudaMemsetAsync(eb.cls_count.ptr, 0, 256 * sizeof(uint32_t), st));
-    k_class_hist<<<std::min(cdiv(nl3, TPB), 148 * 4), TPB, 0, st>>>(kk, nl3, eb.cls_count.ptr);
-    ws.launches += 1;
-    uint32_t hc[256];
-    CUDA_TRY(cudaMemcpyAsync(hc, eb.cls_count.ptr, sizeof(hc), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
-    std::vector<int4> hb2;
-    int off = 0;
-    const int ncls = 1 << dim;
-    for (int d = 3; d <= D; ++d) {
-      l2_b0[d] = (int)hb2.size();
-      for (int c = 0; c < ncls; ++c) {
-        const int cnt = (int)hc[(d << dim) | c];
-        for (int s0 = 0; s0 < cnt; s0 += tchunk) hb2.push_back(make_int4(off + s0, std::min(tchunk, cnt - s0), d, c));
-        off += cnt;
-      }
-      l2_b1[d] = (int)hb2.size();
-    }
-    if (!eb.batches2.reserve(hb2.size() + 1)) return FMM_ERR_OUT_OF_MEMORY;
-    if (!hb2.empty())
-      CUDA_TRY(cudaMemcpyAsync(eb.batches2.ptr, hb2.data(), hb2.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
-    tl2 = (const int *)vv;
-    b2 = eb.batches2.ptr;
-    if (!eb.esrc.reserve((size_t)t.level_count[D]) || !eb.elev.reserve((size_t)t.level_count[D]))
-      return FMM_ERR_OUT_OF_MEMORY;
-    k_leaf_esrc<<<cdiv(t.level_count[D], TPB), TPB, 0, st>>>(t.level_off[D], t.level_count[D], D, first2,
-                                                              ws.cell_parent, needs, cell0, eb.esrc.ptr, eb.elev.ptr);
-    ws.launches += 2;
-  }
   for (int d = 3; d <= D && tc; ++d) {
     TcArgs t2 = ta;
     t2.mode = TC_L2L;
