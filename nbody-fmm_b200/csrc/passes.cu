@@ -566,12 +566,21 @@ __device__ inline void two_sum(float a, float b, float &s, float &e) {
 
 // One pair: grad -= m d/|d|^3, phi += m/|d| (3D, leaf.cpp:118-142) or
 // grad -= m d/|d|^2, phi -= m log|d| (2D, leaf.cpp:81-95), r^2 -> r^2 + eps2.
+// 1/sqrt(x) by the SFU (PTX rsqrt.approx.ftz.f32, relative error below
+// 2^-22.9), without the subnormal-input handling of rsqrtf: the r^2 of
+// distinct particles here is far above the FP32 subnormal range.
+__device__ __forceinline__ float rsqrt_sfu(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 template <int DIM, bool NEWTON = true>
 __device__ inline void pair_acc(float rx, float ry, float rz, float w, float eps2, float &ax, float &ay, float &az,
                                 float &ph) {
   if (DIM == 3) {
     const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps2)));
-    float inv = rsqrtf(r2);
+    float inv = rsqrt_sfu(r2);
     if (NEWTON) inv = inv * fmaf(-0.5f * r2 * inv, inv, 1.5f);  // one Newton step
     const float mi = w * inv;
     const float mi3 = mi * inv * inv;
@@ -736,6 +745,24 @@ struct DirectArgs {
 // Small T (NT <= 8 targets): every lane holds all targets and takes every
 // 32nd particle of the concatenated sources; larger T: register-blocked
 // target groups over sources staged through shared memory.
+// The source cells of a target concatenated: cell si holds positions
+// [s_pref[si], s_pref[si + 1]) (every cell non-empty, so at most 32 cells
+// overlap 32 consecutive positions).  For the chunk f0 .. f0 + 31, given the
+// cell si0 holding f0, returns the cell holding f0 + lane (lanes past the end
+// get the last cell; the caller masks them) and moves si0 to the cell holding
+// f0 + 32: one shared load per lane, the cell starts inside the chunk as the
+// bits of a warp-wide OR, and a population count.
+__device__ inline int chunk_cell(const int *s_pref, int nsrc, int f0, int &si0, int lane) {
+  const int c = si0 + lane;
+  const int rel = c < nsrc ? s_pref[c] - f0 : 32;  // lane 0: <= 0
+  const unsigned bit = rel < 32 ? 1u << max(rel, 0) : 0u;
+  const unsigned starts = __reduce_or_sync(0xffffffffu, bit);
+  const int si = si0 + __popc(starts & (0xffffffffu >> (31 - lane))) - 1;
+  const int last = __shfl_sync(0xffffffffu, si, 31);
+  si0 = s_pref[last + 1] <= f0 + 32 ? last + 1 : last;
+  return si;
+}
+
 template <int NT, int DIM>
 __device__ void direct_small(const DirectArgs &a, const float4 *off, int tb, int nt, const int *s_pb,
                              const float *s_shift, const int *s_pref, int nsrc, int lane) {
@@ -749,15 +776,18 @@ __device__ void direct_small(const DirectArgs &a, const float4 *off, int tb, int
     ax[k] = ay[k] = az[k] = ph[k] = 0.f;
   }
   const int total = s_pref[nsrc];
-  int si = 0;
-  for (int f = lane; f < total; f += 32) {
-    while (f >= s_pref[si + 1]) ++si;
-    const int j = s_pb[si] + (f - s_pref[si]);
-    const float4 q = off[j];
-    const float qx = q.x + s_shift[3 * si], qy = q.y + s_shift[3 * si + 1], qz = q.z + s_shift[3 * si + 2];
+  int si0 = 0;
+  for (int f0 = 0; f0 < total; f0 += 32) {
+    const int f = f0 + lane;
+    const int si = chunk_cell(s_pref, nsrc, f0, si0, lane);
+    if (f < total) {
+      const int j = s_pb[si] + (f - s_pref[si]);
+      const float4 q = off[j];
+      const float qx = q.x + s_shift[3 * si], qy = q.y + s_shift[3 * si + 1], qz = q.z + s_shift[3 * si + 2];
 #pragma unroll
-    for (int k = 0; k < NT; ++k)
-      pair_acc<DIM, false>(tx[k] - qx, ty[k] - qy, tz[k] - qz, q.w, a.eps2, ax[k], ay[k], az[k], ph[k]);
+      for (int k = 0; k < NT; ++k)
+        pair_acc<DIM, false>(tx[k] - qx, ty[k] - qy, tz[k] - qz, q.w, a.eps2, ax[k], ay[k], az[k], ph[k]);
+    }
   }
 #pragma unroll
   for (int k = 0; k < NT; ++k) {
@@ -792,12 +822,12 @@ __device__ void direct_blocked(const DirectArgs &a, const float4 *off, int tb, i
       tz[r] = t.z;
       ax[r] = ay[r] = az[r] = ph[r] = 0.f;
     }
-    int si = 0;
+    int si0 = 0;
     for (int f0 = 0; f0 < total; f0 += 32) {
       const int f = f0 + lane;
+      const int si = chunk_cell(s_pref, nsrc, f0, si0, lane);
       float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
       if (f < total) {
-        while (f >= s_pref[si + 1]) ++si;
         const float4 qq = off[s_pb[si] + (f - s_pref[si])];
         q = make_float4(qq.x + s_shift[3 * si], qq.y + s_shift[3 * si + 1], qq.z + s_shift[3 * si + 2], qq.w);
       }
@@ -862,16 +892,23 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   const int *pc = a.coll + (int64_t)P * NS;
   int nsrc = 0, ptotal = 0;
   if (lane == 0) s_pref[0] = 0;
-  // all candidate loads in flight at once: colleague, child, then counts
+  // the existing colleagues, compacted (slot positions in s_pb, which is
+  // rewritten below only after the last read), then the children of those
+  // only: all candidate loads in flight at once, child then counts
   const int Qlane = lane < NS ? pc[lane] : -1;
-  int qv[NR], nsv[NR], pbv[NR];
+  const unsigned qmask = __ballot_sync(0xffffffffu, Qlane >= 0);
+  if (Qlane >= 0) s_pb[__popc(qmask & ((1u << lane) - 1u))] = lane;
+  __syncwarp();
+  const int ncand = __popc(qmask) * NC;
+  int qv[NR], nsv[NR], pbv[NR], dlv[NR];
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
     const int cand = r * 32 + lane;
-    const int dl = cand / NC;
-    const int Q = __shfl_sync(0xffffffffu, Qlane, dl < NS ? dl : 0);
-    qv[r] = (cand < NCAND && Q >= 0) ? a.child[(int64_t)Q * NC + (cand % NC)] : -1;
+    dlv[r] = cand < ncand ? s_pb[cand / NC] : 0;
+    const int Q = __shfl_sync(0xffffffffu, Qlane, dlv[r]);
+    qv[r] = cand < ncand ? a.child[(int64_t)Q * NC + (cand % NC)] : -1;
   }
+  __syncwarp();
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
     pbv[r] = qv[r] >= 0 ? a.pbeg[qv[r]] : 0;
@@ -879,8 +916,9 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   }
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
+    if (r * 32 >= ncand) break;  // warp-uniform
     const int cand = r * 32 + lane;
-    const int dl = cand / NC, k = cand % NC;
+    const int dl = dlv[r], k = cand % NC;
     int q = qv[r];
     const int ddx = 2 * (dl % 3 - 1) + (k & 1) - (cls & 1);
     const int ddy = 2 * ((dl / 3) % 3 - 1) + ((k >> 1) & 1) - ((cls >> 1) & 1);
