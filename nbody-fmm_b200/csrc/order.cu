@@ -19,10 +19,11 @@ __device__ inline float bf16r(float x) { return __bfloat162float(__float2bfloat1
 
 // ---------------------------------------------------------------- features
 __global__ void k_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int cell0,
-                                int p, int KS, float *cf) {
+                                int p, int KS, const uint8_t *mode, float *cf) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const int c = first + i;
+  if (mode && !mode[c - cell0]) return;
   const float *m = M + (size_t)(c - cell0) * KS;
   float *o = cf + (size_t)(c - cell0) * ORD_CF;
   const float m0 = fabsf(m[0]);
@@ -663,15 +664,15 @@ int order_judge_compare(const double *acc, const double *ref, const int64_t *tar
 }
 
 int order_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int cell0, int p,
-                        int KS, float *cf, const float4 *part, int64_t n, double *mtot, cudaStream_t st,
-                        int64_t &launches) {
+                        int KS, const uint8_t *mode, float *cf, const float4 *part, int64_t n, double *mtot,
+                        cudaStream_t st, int64_t &launches) {
   CUDA_TRY(cudaMemsetAsync(mtot, 0, sizeof(double), st));
   if (n > 0) {
     k_mass_total<<<std::max(1, std::min(cdiv(n, 256), 148 * 2)), 256, 0, st>>>(part, n, mtot);
     launches += 1;
   }
   if (count <= 0) return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
-  k_cell_features<<<cdiv(count, 256), 256, 0, st>>>(M, pbeg, pend, first, count, cell0, p, KS, cf);
+  k_cell_features<<<cdiv(count, 256), 256, 0, st>>>(M, pbeg, pend, first, count, cell0, p, KS, mode, cf);
   launches += 1;
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
 }

@@ -41,11 +41,12 @@ struct OrderGeom {
 
 // Per-cell features of cells [first, first + count): log2(1 + n),
 // log10(|M~_n| / |M~_0|) for n = 1..12 (|M~_n|^2 = sum over m of |M~_n^m|^2)
-// and log10 M~_0 (cells whose multipole was not formed read as empty); and
-// the total mass of the n particles `part` (mass in w) into *mtot.
+// and log10 M~_0; with `mode` set only for the cells whose multipole was
+// formed (mode != 0), the others are left as they are.  Also the total mass
+// of the n particles `part` (mass in w) into *mtot.
 int order_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int cell0, int p,
-                        int KS, float *cf, const float4 *part, int64_t n, double *mtot, cudaStream_t st,
-                        int64_t &launches);
+                        int KS, const uint8_t *mode, float *cf, const float4 *part, int64_t n, double *mtot,
+                        cudaStream_t st, int64_t &launches);
 
 // The resolved M2L tables and what the tile features read.
 struct TileArgs {

@@ -1049,6 +1049,18 @@ __global__ void k_m_mode(const uint8_t *lact, const uint8_t *msrc, int first2, i
   mode[c - cell0] = !req ? 0 : (c >= leaf_first || pend[c] - pbeg[c] <= tmax) ? 1 : 2;
 }
 
+// Zeroes the rows (KS floats, KS a multiple of 4) of the cells
+// [first, first + count) whose flag equals `want`.
+__global__ void k_zero_rows(const uint8_t *flag, uint8_t want, int first, int count, int cell0, int KS, float *X) {
+  const int per = KS >> 2;
+  const int64_t nvec = (int64_t)count * per;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nvec; e += (int64_t)gridDim.x * blockDim.x) {
+    const int c = first + (int)(e / per);
+    if (flag[c - cell0] == want)
+      reinterpret_cast<float4 *>(X + (size_t)(c - cell0) * KS)[e % per] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+}
+
 // Sort keys of the M2M rows of one level: with child_rows (tensor-core
 // M2M, rows are children) the children of mode-2 cells by (level, class),
 // else (CUDA-core M2M, rows are parents) the mode-2 cells by (level, 0);
@@ -1244,8 +1256,15 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   const int ncell = t.n_cells, cell0 = t.cell0;
   const int TPB = 256;
   if (!eb.M.reserve((size_t)ncell * KS) || !eb.L.reserve((size_t)ncell * KS)) return FMM_ERR_OUT_OF_MEMORY;
-  CUDA_TRY(cudaMemsetAsync(eb.M.ptr, 0, sizeof(float) * (size_t)ncell * KS, st));
-  CUDA_TRY(cudaMemsetAsync(eb.L.ptr, 0, sizeof(float) * (size_t)ncell * KS, st));
+  // 3D shortcuts: local expansions only on paths to cells with M2L
+  // contributions (L2P from each leaf's deepest such ancestor), multipoles
+  // only for what M2L reads (P2M straight into small cells, M2M above them);
+  // only the rows that are summed into start at zero
+  const bool shortcut = dim == 3 && D >= 3;
+  if (!shortcut) {
+    CUDA_TRY(cudaMemsetAsync(eb.M.ptr, 0, sizeof(float) * (size_t)ncell * KS, st));
+    CUDA_TRY(cudaMemsetAsync(eb.L.ptr, 0, sizeof(float) * (size_t)ncell * KS, st));
+  }
   // tensor-core translations: 128-target batches, BF16 split operator images
   const int P16 = (ops.K + 15) & ~15;
   const bool tc = m2l_mode == FMM_M2L_TC && P16 <= TC_MAX_P16;
@@ -1370,10 +1389,6 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   ta.P16 = P16;
   ta.err = ws.dev_err;
 
-  // 3D shortcuts: local expansions only on paths to cells with M2L
-  // contributions (L2P from each leaf's deepest such ancestor), multipoles
-  // only for what M2L reads (P2M straight into small cells, M2M above them)
-  const bool shortcut = dim == 3 && D >= 3;
   uint8_t *lact = nullptr, *needs = nullptr, *msrc = nullptr, *mmode = nullptr;
   if (shortcut) {
     if (!eb.lact.reserve(4 * (size_t)ncell)) return FMM_ERR_OUT_OF_MEMORY;
@@ -1500,7 +1515,12 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
       return FMM_ERR_OUT_OF_MEMORY;
     k_leaf_esrc<<<cdiv(t.level_count[D], TPB), TPB, 0, st>>>(leaf_first, t.level_count[D], D, first2, ws.cell_parent,
                                                               needs, cell0, eb.esrc.ptr, eb.elev.ptr);
-    ws.launches += 1;
+    // rows summed into: M of the M2M cells, L of the cells that need L
+    const int64_t nvec = (int64_t)ntl * (KS / 4);
+    const int zgrid = std::max(1, std::min(cdiv(nvec, TPB), 148 * 16));
+    k_zero_rows<<<zgrid, TPB, 0, st>>>(mmode, 2, first2, ntl, cell0, KS, eb.M.ptr);
+    k_zero_rows<<<zgrid, TPB, 0, st>>>(needs, 1, first2, ntl, cell0, KS, eb.L.ptr);
+    ws.launches += 3;
   }
 
   if (ev) cudaEventRecord(ev[1], st);
@@ -1560,8 +1580,8 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     TileArgs tla;
     if (learned || collect) {
       if (!eb.cf.reserve((size_t)ncell * ORD_CF) || !eb.frms.reserve(3)) return FMM_ERR_OUT_OF_MEMORY;
-      int rc = order_cell_features(eb.M.ptr, ws.cell_pbeg, ws.cell_pend, t.level_off[2], ntl, cell0, p, KS, eb.cf.ptr,
-                                   ws.part, n, eb.frms.ptr + 2, st, ws.launches);
+      int rc = order_cell_features(eb.M.ptr, ws.cell_pbeg, ws.cell_pend, t.level_off[2], ntl, cell0, p, KS, mmode,
+                                   eb.cf.ptr, ws.part, n, eb.frms.ptr + 2, st, ws.launches);
       if (rc) return rc;
       tla.batches = cm.batches;
       tla.tlist = tl_m2l;
