@@ -64,9 +64,12 @@ REF_SAMPLE_N = 512           # particles per reference process per step (about 2
 BASELINE_SAMPLE_N = 2048     # single-thread CPU baseline sample (about 20 s at p = 12)
 
 
-def workload_desc(n, p, leaf, m2l, direct_max=None):
+def workload_desc(n, p, leaf, m2l, direct_max=None, mixture=False):
+    inputs = (f"3D clustered mixture N={n} (32 Plummer spheres, scale radii log-uniform in [0.01, 0.1], "
+              f"centres uniform in [0,1]^3, equal mass per sphere, seed 5)" if mixture
+              else f"3D Plummer sphere N={n} (a=1, r<=20, seed 2)")
     return {
-        "workload": f"3D Plummer sphere N={n} (a=1, r<=20, seed 2), p={p}, leaf capacity {leaf}, "
+        "workload": f"{inputs}, p={p}, leaf capacity {leaf}, "
                     f"one force evaluation (tree build + all FMM passes) per step",
         "n": n, "p": p, "leaf_cap": leaf, "m2l": m2l, "direct_max": direct_max, "positions": "f64",
         "forces": "f32", "l2": "256 MiB buffer written between steps (outside the timed events)",
@@ -204,8 +207,10 @@ def run_ours(args, world, rank, local):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     n, p, leaf = args.n, args.p, args.leaf
+    mixture = args.workload == "mixture"
+    tune_leaf = mixture  # the mixture's configuration leaves the leaf capacity open
     mode = fmmgpu.FMM_M2L_TC if args.m2l == "tc" else fmmgpu.FMM_M2L_FP32
-    pos, mass = workloads.plummer(n, seed=2)
+    pos, mass = workloads.plummer_mixture(n, seed=5) if mixture else workloads.plummer(n, seed=2)
     d_pos = torch.from_numpy(pos).to(dev)
     d_mass = torch.from_numpy(mass).to(dev)
     d_acc = torch.empty((n, 3), dtype=torch.float64, device=dev)
@@ -221,9 +226,9 @@ def run_ours(args, world, rank, local):
             torch.distributed.barrier()
         torch.cuda.synchronize(dev)
 
-    # the judge: FP64 direct sum on 4096 sampled targets
+    # the judge: FP64 direct sum on 4096 sampled targets (8192 on the mixture)
     rng = np.random.default_rng(7)
-    tg = np.sort(rng.choice(n, size=min(4096, n), replace=False)).astype(np.int64)
+    tg = np.sort(rng.choice(n, size=min(8192 if mixture else 4096, n), replace=False)).astype(np.int64)
     d_tg = torch.from_numpy(tg).to(dev)
     r_acc = torch.empty((len(tg), 3), dtype=torch.float64, device=dev)
     r_pot = torch.empty((len(tg),), dtype=torch.float64, device=dev)
@@ -243,9 +248,12 @@ def run_ours(args, world, rank, local):
     if args.autotune and args.direct_max < 0:
         # the autotuner picks the direct-pair threshold on this input (setup, outside the timed steps)
         t0 = time.perf_counter()
-        cands, best = ctx.autotune(n, d_pos.data_ptr(), d_mass.data_ptr(), stream=stream.cuda_stream)
+        cands, best = ctx.autotune(n, d_pos.data_ptr(), d_mass.data_ptr(), tune_leaf=tune_leaf,
+                                   stream=stream.cuda_stream)
         tune = {"seconds": time.perf_counter() - t0, "chosen_direct_max": best["direct_max"],
-                "candidates": [[x["direct_max"], round(x["ms"], 3)] for x in cands]}
+                "chosen_leaf_cap": best["leaf_cap"],
+                "candidates": [[x["leaf_cap"], x["direct_max"], round(x["ms"], 3)] for x in cands]}
+        leaf = best["leaf_cap"]
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
@@ -323,8 +331,9 @@ def run_ours(args, world, rank, local):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded Plummer sphere)", "impl": "fmmgpu",
-        "config": workload_desc(n, p, leaf, args.m2l, s_last.get("direct_max")),
+        "dtype": "f32", "data": f"synthetic (seeded {'Plummer mixture' if mixture else 'Plummer sphere'})",
+        "impl": "fmmgpu",
+        "config": workload_desc(n, p, leaf, args.m2l, s_last.get("direct_max"), mixture),
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(n * 3 * 8 + n * 8),
                 "d2h_bytes_per_step": int(n * 3 * 8)},
         "roofline": roof, "rooflines": roofs, "error": err, "phases_ms": ph,
@@ -347,11 +356,13 @@ def run_ours(args, world, rank, local):
     # comparisons at the same order: tensor cores at fixed p, and the plain
     # FP32 GPU FMM (the method without tensor cores and learned orders)
     def compare(m2l_mode, label):
-        pc = fmmgpu.Context(dim=3, p=p, leaf_cap=leaf, m2l_mode=m2l_mode, G=1.0, device=local,
+        pc = fmmgpu.Context(dim=3, p=p, leaf_cap=args.leaf, m2l_mode=m2l_mode, G=1.0, device=local,
                             direct_max=args.direct_max)
         chosen = None
         if args.autotune and args.direct_max < 0:  # tuned the same way as the headline
-            chosen = pc.autotune(n, d_pos.data_ptr(), d_mass.data_ptr(), stream=stream.cuda_stream)[1]["direct_max"]
+            b = pc.autotune(n, d_pos.data_ptr(), d_mass.data_ptr(), tune_leaf=tune_leaf,
+                            stream=stream.cuda_stream)[1]
+            chosen = {"direct_max": b["direct_max"], "leaf_cap": b["leaf_cap"]}
         psteps = max(3, args.steps // 2)
         pms, pst, _ = _timed(pc, n, d_pos, d_mass, d_acc, stream, flush, psteps, max(1, args.warmup), barrier)
         ptot = float(sum(pms))
@@ -362,7 +373,7 @@ def run_ours(args, world, rank, local):
         perr = _error(pc, n, d_pos, d_mass, d_acc, d_pot, stream, dev, judge)
         pc.close()
         return {"m2l": label, "value": n * psteps * world / (ptot / 1e3), "unit": UNIT, "steps": psteps,
-                "ms_per_step": ptot / psteps, "error": perr, "phases_ms": _phases(pst), "direct_max": chosen}
+                "ms_per_step": ptot / psteps, "error": perr, "phases_ms": _phases(pst), "tuned": chosen}
 
     if not args.no_plain and mode == fmmgpu.FMM_M2L_TC:
         if learned:
@@ -370,7 +381,7 @@ def run_ours(args, world, rank, local):
         line["plain"] = compare(fmmgpu.FMM_M2L_FP32, "fp32 SIMT, fixed p")
         line["speedup_vs_plain"] = value / line["plain"]["value"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(p, leaf)
+        line["cpu_baseline"] = cpu_baseline(p, leaf, mixture)
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:
@@ -462,27 +473,30 @@ def load_traffic():
 
 # ------------------------------------------------------------- reference
 def _ref_worker(args):
-    n, p, leaf, seed = args
+    n, p, leaf, seed = args[:4]
+    mixture = len(args) > 4 and args[4]
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     sys.path.insert(0, os.path.join(ROOT, "nbody-fmm_b200"))
     from oracle import RefLib
     from fmmgpu import workloads
 
     R = RefLib()
-    pos, m = workloads.plummer(n, seed=seed)
+    pos, m = workloads.plummer_mixture(n, seed=seed) if mixture else workloads.plummer(n, seed=seed)
     t0 = time.perf_counter()
     R.fmm(pos, m, p, leaf)
     return time.perf_counter() - t0
 
 
-def cpu_baseline(p, leaf):
+def cpu_baseline(p, leaf, mixture=False):
     """The reference FMM::update, single thread, on a bounded sample."""
+    seed = 5 if mixture else 2
     try:
-        dt = _ref_worker((BASELINE_SAMPLE_N, p, leaf, 2))
+        dt = _ref_worker((BASELINE_SAMPLE_N, p, leaf, seed, mixture))
     except Exception as e:  # reference build missing
         return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"unavailable: {e}"}
+    inputs = "Plummer mixture" if mixture else "Plummer"
     return {"value": BASELINE_SAMPLE_N / dt, "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": f"reference FMM::update (oracle/_ref, g++ -O2), Plummer N={BASELINE_SAMPLE_N} seed 2, "
+            "sample": f"reference FMM::update (oracle/_ref, g++ -O2), {inputs} N={BASELINE_SAMPLE_N} seed {seed}, "
                       f"p={p}, leaf capacity {leaf}, 1 thread, {dt:.1f} s"}
 
 
@@ -494,22 +508,25 @@ def run_reference(args, world, rank):
     cores = os.cpu_count() or 1
     ctx = mp.get_context("spawn")
     n, p, leaf = REF_SAMPLE_N, args.p, args.leaf
+    mixture = args.workload == "mixture"
     with ctx.Pool(cores) as pool:
         for _ in range(args.warmup):
-            pool.map(_ref_worker, [(n, p, leaf, 2 + i) for i in range(cores)])
+            pool.map(_ref_worker, [(n, p, leaf, 2 + i, mixture) for i in range(cores)])
         step_s = []
         for _ in range(args.steps):
-            ts = pool.map(_ref_worker, [(n, p, leaf, 2 + i) for i in range(cores)])
+            ts = pool.map(_ref_worker, [(n, p, leaf, 2 + i, mixture) for i in range(cores)])
             step_s.append(max(ts))
     total = sum(step_s)
     value = n * cores * args.steps / total
-    sample = (f"reference FMM::update (oracle/_ref, g++ -O2) on {cores} processes x Plummer N={n} (seeds 2..), "
+    inputs = "Plummer mixture" if mixture else "Plummer"
+    sample = (f"reference FMM::update (oracle/_ref, g++ -O2) on {cores} processes x {inputs} N={n} (seeds 2..), "
               f"p={p}, leaf capacity {leaf}, one process per host core; step = slowest process")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Plummer sphere)", "impl": "reference",
-        "config": workload_desc(args.n, p, leaf, "reference (CPU)"),
+        "vs_baseline": None, "dtype": "f64",
+        "data": f"synthetic (seeded {'Plummer mixture' if mixture else 'Plummer sphere'})", "impl": "reference",
+        "config": workload_desc(args.n, p, leaf, "reference (CPU)", mixture=mixture),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -522,7 +539,10 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=1 << 20)
+    ap.add_argument("--workload", default="plummer", choices=["plummer", "mixture"],
+                    help="plummer: the 2^20 Plummer sphere (default); mixture: the 16M clustered mixture of the "
+                         "learned-order configuration, leaf capacity tuned with the threshold")
+    ap.add_argument("--n", type=int, default=None, help="particles (default 2^20, mixture 2^24)")
     ap.add_argument("--p", type=int, default=12)
     ap.add_argument("--leaf", type=int, default=64)
     ap.add_argument("--m2l", default="tc", choices=["fp32", "tc"])
@@ -538,6 +558,8 @@ def main():
     ap.add_argument("--ensemble", action="store_true", help="the batched-ensemble configuration instead")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
+    if args.n is None:
+        args.n = 1 << 24 if args.workload == "mixture" else 1 << 20
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)

@@ -182,11 +182,13 @@ FMM_API int fmm_evaluate_batched(fmm_ctx *ctx, int32_t nsys, const int64_t *offs
 
 /* Autotuner: times force evaluations of the given system (device buffers)
    over candidate settings and keeps the fastest in the context: the
-   direct-pair threshold (K^2/200 .. K^2/12.5, K the expansion length) and,
-   with FMM_TUNE_LEAF, the leaf capacity in {16, 32, 64, 128} (which changes
-   the tree: the reference's algorithm at that threshold).  Learned orders
-   are tuned with them (every candidate is evaluated twice, the second timed).
-   result may be NULL.  Synchronous. */
+   direct-pair threshold (K^2/200 .. K^2/12.5, K the expansion length; five
+   candidates) or, with FMM_TUNE_LEAF, a coordinate search: the leaf
+   capacity in {32, 64, 128, 256} (which changes the tree: the reference's
+   algorithm at that threshold) at the threshold K^2/25, then the thresholds
+   K^2/100, K^2/50 and K^2/12.5 at the best capacity (seven candidates).
+   Learned orders are tuned with them (every candidate is evaluated twice,
+   the second timed).  result may be NULL.  Synchronous. */
 #define FMM_TUNE_LEAF 1
 typedef struct fmm_tune_result {
   int32_t n_candidates;

@@ -434,10 +434,6 @@ int fmm_autotune(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mas
   if (!c->d_acc.reserve((size_t)n * dim)) return FMM_ERR_OUT_OF_MEMORY;
   const int K = dim == 3 ? (c->cfg.p + 1) * (c->cfg.p + 1) : 2 * c->cfg.p + 1;
   const double base = (double)K * K / 25.0;
-  const double fac[5] = {0.125, 0.25, 0.5, 1.0, 2.0};
-  std::vector<int> leaves;
-  if (flags & FMM_TUNE_LEAF) leaves = {16, 32, 64, 128};
-  else leaves = {c->cfg.leaf_cap};
   fmm_tune_result res;
   memset(&res, 0, sizeof(res));
   const fmm_config saved = c->cfg;
@@ -446,32 +442,38 @@ int fmm_autotune(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mas
   CUDA_TRY(cudaEventCreate(&e1));
   int rc = FMM_OK;
   double best = 1e300;
-  for (int lc : leaves) {
-    for (double f : fac) {
-      if (res.n_candidates >= 16) break;
-      const int k = res.n_candidates++;
-      c->cfg.leaf_cap = lc;
-      c->cfg.direct_max = (int32_t)std::max(8.0, base * f);
-      res.leaf_cap[k] = lc;
-      res.direct_max[k] = c->cfg.direct_max;
-      const bool twice = c->cfg.order_mode == FMM_ORDER_LEARNED;
-      c->frms_n = -1;  // learned orders: start the system afresh
-      for (int r = 0; r < (twice ? 2 : 1) && !rc; ++r) rc = evaluate_device(c, n, d_pos, d_mass, c->d_acc.ptr, nullptr, st);
-      if (!rc) rc = finish(c, st);
-      if (!rc && cudaEventRecord(e0, st) != cudaSuccess) rc = FMM_ERR_CUDA;
-      if (!rc) rc = evaluate_device(c, n, d_pos, d_mass, c->d_acc.ptr, nullptr, st);
-      if (!rc && cudaEventRecord(e1, st) != cudaSuccess) rc = FMM_ERR_CUDA;
-      if (!rc) rc = finish(c, st);
-      float ms = 0.f;
-      if (!rc && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) rc = FMM_ERR_CUDA;
-      if (rc) break;
-      res.ms[k] = ms;
-      if (ms < best) {
-        best = ms;
-        res.best = k;
-      }
+  auto trial = [&](int lc, double f) {
+    if (rc || res.n_candidates >= 16) return;
+    const int k = res.n_candidates++;
+    c->cfg.leaf_cap = lc;
+    c->cfg.direct_max = (int32_t)std::max(8.0, base * f);
+    res.leaf_cap[k] = lc;
+    res.direct_max[k] = c->cfg.direct_max;
+    const bool twice = c->cfg.order_mode == FMM_ORDER_LEARNED;
+    c->frms_n = -1;  // learned orders: start the system afresh
+    for (int r = 0; r < (twice ? 2 : 1) && !rc; ++r) rc = evaluate_device(c, n, d_pos, d_mass, c->d_acc.ptr, nullptr, st);
+    if (!rc) rc = finish(c, st);
+    if (!rc && cudaEventRecord(e0, st) != cudaSuccess) rc = FMM_ERR_CUDA;
+    if (!rc) rc = evaluate_device(c, n, d_pos, d_mass, c->d_acc.ptr, nullptr, st);
+    if (!rc && cudaEventRecord(e1, st) != cudaSuccess) rc = FMM_ERR_CUDA;
+    if (!rc) rc = finish(c, st);
+    float ms = 0.f;
+    if (!rc && cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) rc = FMM_ERR_CUDA;
+    if (rc) return;
+    res.ms[k] = ms;
+    if (ms < best) {
+      best = ms;
+      res.best = k;
     }
-    if (rc) break;
+  };
+  // coordinate search: the leaf capacity at the default threshold, then the
+  // threshold at the best capacity
+  if (flags & FMM_TUNE_LEAF) {
+    for (int lc : {32, 64, 128, 256}) trial(lc, 1.0);
+    const int lc = res.leaf_cap[res.best];
+    for (double f : {0.25, 0.5, 2.0}) trial(lc, f);
+  } else {
+    for (double f : {0.125, 0.25, 0.5, 1.0, 2.0}) trial(c->cfg.leaf_cap, f);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

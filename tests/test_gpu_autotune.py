@@ -43,6 +43,11 @@ def test_autotune_with_leaf_capacities():
     torch.cuda.synchronize()
     with fmmgpu.Context(dim=3, p=6, leaf_cap=64, G=1.0, m2l_mode=fmmgpu.FMM_M2L_TC) as c:
         cands, best = c.autotune(n, d_pos.data_ptr(), d_m.data_ptr(), tune_leaf=True)
-        assert len(cands) == 16 and {x["leaf_cap"] for x in cands} == {16, 32, 64, 128}
+        # coordinate search: four capacities at one threshold, then three
+        # more thresholds at the best capacity
+        assert len(cands) == 7 and [x["leaf_cap"] for x in cands[:4]] == [32, 64, 128, 256]
+        assert len({x["direct_max"] for x in cands[:4]}) == 1
+        assert {x["leaf_cap"] for x in cands[4:]} == {cands[int(np.argmin([x["ms"] for x in cands[:4]]))]["leaf_cap"]}
+        assert best["ms"] == min(x["ms"] for x in cands)
         a = c.evaluate(pos, m)
         assert np.all(np.isfinite(a))
