@@ -742,16 +742,20 @@ struct DirectArgs {
 // One warp per level-d target cell T with n_T <= direct_max: the sources are
 // the cells S of T's interaction list (node_i.cpp:39-43) with
 // n_T * n_S <= direct_max, exactly the pairs the M2L contraction skips.
-// Small T (NT <= 8 targets): every lane holds all targets and takes every
+// Small T (NT <= 7 targets): every lane holds all targets and takes every
 // 32nd particle of the concatenated sources; larger T: register-blocked
 // target groups over sources staged through shared memory.
-// The source cells of a target concatenated: cell si holds positions
-// [s_pref[si], s_pref[si + 1]) (every cell non-empty, so at most 32 cells
-// overlap 32 consecutive positions).  For the chunk f0 .. f0 + 31, given the
-// cell si0 holding f0, returns the cell holding f0 + lane (lanes past the end
-// get the last cell; the caller masks them) and moves si0 to the cell holding
-// f0 + 32: one shared load per lane, the cell starts inside the chunk as the
-// bits of a warp-wide OR, and a population count.
+//
+// Per kept source cell si the warp keeps s_pref[si] (its first position in
+// the concatenation; every cell non-empty) and s_cell[si] = (shift c_S - c_T,
+// index delta): the particle at concatenated position f of cell si is
+// off[f + delta].
+
+// For the chunk f0 .. f0 + 31, given the cell si0 holding f0, returns the
+// cell holding f0 + lane (lanes past the end get the last cell; the caller
+// masks them) and moves si0 to the cell holding f0 + 32: one shared load per
+// lane, the cell starts inside the chunk as the bits of a warp-wide OR, and a
+// population count (at most 32 cells overlap 32 consecutive positions).
 __device__ inline int chunk_cell(const int *s_pref, int nsrc, int f0, int &si0, int lane) {
   const int c = si0 + lane;
   const int rel = c < nsrc ? s_pref[c] - f0 : 32;  // lane 0: <= 0
@@ -763,9 +767,17 @@ __device__ inline int chunk_cell(const int *s_pref, int nsrc, int f0, int &si0, 
   return si;
 }
 
+// The source particle at concatenated position f of cell si, shifted into
+// the target's frame.
+__device__ inline float4 shifted_source(const float4 *off, const float4 *s_cell, int f, int si) {
+  const float4 cd = s_cell[si];
+  const float4 q = off[f + __float_as_int(cd.w)];
+  return make_float4(q.x + cd.x, q.y + cd.y, q.z + cd.z, q.w);
+}
+
 template <int NT, int DIM>
-__device__ void direct_small(const DirectArgs &a, const float4 *off, int tb, int nt, const int *s_pb,
-                             const float *s_shift, const int *s_pref, int nsrc, int lane) {
+__device__ void direct_small(const DirectArgs &a, const float4 *off, int tb, int nt, const float4 *s_cell,
+                             const int *s_pref, int nsrc, int lane) {
   float tx[NT], ty[NT], tz[NT], ax[NT], ay[NT], az[NT], ph[NT];
 #pragma unroll
   for (int k = 0; k < NT; ++k) {
@@ -781,12 +793,10 @@ __device__ void direct_small(const DirectArgs &a, const float4 *off, int tb, int
     const int f = f0 + lane;
     const int si = chunk_cell(s_pref, nsrc, f0, si0, lane);
     if (f < total) {
-      const int j = s_pb[si] + (f - s_pref[si]);
-      const float4 q = off[j];
-      const float qx = q.x + s_shift[3 * si], qy = q.y + s_shift[3 * si + 1], qz = q.z + s_shift[3 * si + 2];
+      const float4 q = shifted_source(off, s_cell, f, si);
 #pragma unroll
       for (int k = 0; k < NT; ++k)
-        pair_acc<DIM, false>(tx[k] - qx, ty[k] - qy, tz[k] - qz, q.w, a.eps2, ax[k], ay[k], az[k], ph[k]);
+        pair_acc<DIM, false>(tx[k] - q.x, ty[k] - q.y, tz[k] - q.z, q.w, a.eps2, ax[k], ay[k], az[k], ph[k]);
     }
   }
 #pragma unroll
@@ -806,8 +816,8 @@ __device__ void direct_small(const DirectArgs &a, const float4 *off, int tb, int
 // chunks of 32 staged through shared memory; ceil(nt / R) target groups of
 // Gl lanes, 32 / Gl groups per round.
 template <int R, int DIM>
-__device__ void direct_blocked(const DirectArgs &a, const float4 *off, int tb, int nt, int Gl, const int *s_pb,
-                               const float *s_shift, const int *s_pref, int nsrc, int lane, float4 *stage) {
+__device__ void direct_blocked(const DirectArgs &a, const float4 *off, int tb, int nt, int Gl, const float4 *s_cell,
+                               const int *s_pref, int nsrc, int lane, float4 *stage) {
   const int groups = (nt + R - 1) / R, gpr = 32 / Gl;
   const int total = s_pref[nsrc];
   for (int g0 = 0; g0 < groups; g0 += gpr) {
@@ -826,12 +836,7 @@ __device__ void direct_blocked(const DirectArgs &a, const float4 *off, int tb, i
     for (int f0 = 0; f0 < total; f0 += 32) {
       const int f = f0 + lane;
       const int si = chunk_cell(s_pref, nsrc, f0, si0, lane);
-      float4 q = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (f < total) {
-        const float4 qq = off[s_pb[si] + (f - s_pref[si])];
-        q = make_float4(qq.x + s_shift[3 * si], qq.y + s_shift[3 * si + 1], qq.z + s_shift[3 * si + 2], qq.w);
-      }
-      stage[lane] = q;
+      stage[lane] = f < total ? shifted_source(off, s_cell, f, si) : make_float4(0.f, 0.f, 0.f, 0.f);
       __syncwarp();
       const int cnt = min(32, total - f0);
       for (int k = sub; k < cnt; k += Gl) {
@@ -870,43 +875,47 @@ __device__ inline void blocked_shape(int nt, int R, int &Gl, float &cost) {
 template <int DIM>
 __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   constexpr int NS = DIM == 3 ? 27 : 9, NC = 1 << DIM, NCAND = NS * NC, NR = (NCAND + 31) / 32;
-  __shared__ int s_pb_all[8][189];
-  __shared__ float s_shift_all[8][3 * 189];
+  __shared__ float4 s_cell_all[8][189];
   __shared__ int s_pref_all[8][190];
   __shared__ float4 s_stage_all[8][32];
+  __shared__ int s_dir_all[8][32];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int wl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (wl >= a.w0[a.nlev]) return;
-  int lv = 0;
-  while (wl >= a.w0[lv + 1]) ++lv;
+  int lv = a.nlev - 1;  // deep levels, which hold most of the warps, first
+  while (wl < a.w0[lv]) --lv;
   const int T = a.first[lv] + (wl - a.w0[lv]);
-  const float4 *off = a.off[lv];
-  const float hx = a.h[lv][0], hy = a.h[lv][1], hz = a.h[lv][2];
   const int tb = a.pbeg[T], nt = a.pend[T] - tb;
   if ((long long)nt > a.direct_max && !a.any_fdirect) return;
-  int *s_pb = s_pb_all[wib];
-  float *s_shift = s_shift_all[wib];
+  const float4 *off = a.off[lv];
+  float4 *s_cell = s_cell_all[wib];
   int *s_pref = s_pref_all[wib];
   const int P = a.parent[T];
   const int cls = (int)(a.ckey[T] & (uint64_t)(NC - 1));
-  const int *pc = a.coll + (int64_t)P * NS;
+  // kept sources have n_S <= ns_max (n_T n_S <= direct_max)
+  const int ns_max = (int)min(a.direct_max, (long long)0x7fffffff) / max(nt, 1);
   int nsrc = 0, ptotal = 0;
   if (lane == 0) s_pref[0] = 0;
-  // the existing colleagues, compacted (slot positions in s_pb, which is
-  // rewritten below only after the last read), then the children of those
-  // only: all candidate loads in flight at once, child then counts
-  const int Qlane = lane < NS ? pc[lane] : -1;
+  // the existing colleagues, compacted, with their directions packed as
+  // (dx+1) | (dy+1) << 2 | (dz+1) << 4 | slot << 8 in s_dir; then the
+  // children of those only, all candidate loads in flight at once, child
+  // then counts
+  int *s_dir = s_dir_all[wib];
+  const int Qlane = lane < NS ? a.coll[(size_t)P * NS + lane] : -1;
   const unsigned qmask = __ballot_sync(0xffffffffu, Qlane >= 0);
-  if (Qlane >= 0) s_pb[__popc(qmask & ((1u << lane) - 1u))] = lane;
+  if (Qlane >= 0)
+    s_dir[__popc(qmask & ((1u << lane) - 1u))] = (lane % 3) | (((lane / 3) % 3) << 2) | ((lane / 9) << 4) | (lane << 8);
   __syncwarp();
   const int ncand = __popc(qmask) * NC;
-  int qv[NR], nsv[NR], pbv[NR], dlv[NR];
+  int qv[NR], nsv[NR], pbv[NR];
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
-    const int cand = r * 32 + lane;
-    dlv[r] = cand < ncand ? s_pb[cand / NC] : 0;
-    const int Q = __shfl_sync(0xffffffffu, Qlane, dlv[r]);
-    qv[r] = cand < ncand ? a.child[(int64_t)Q * NC + (cand % NC)] : -1;
+    qv[r] = -1;
+    if (r * 32 < ncand) {  // warp-uniform
+      const int cand = r * 32 + lane;
+      const int Q = __shfl_sync(0xffffffffu, Qlane, cand < ncand ? s_dir[cand / NC] >> 8 : 0);
+      if (cand < ncand) qv[r] = a.child[(size_t)Q * NC + (cand % NC)];
+    }
   }
   __syncwarp();
 #pragma unroll
@@ -914,18 +923,19 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
     pbv[r] = qv[r] >= 0 ? a.pbeg[qv[r]] : 0;
     nsv[r] = qv[r] >= 0 ? a.pend[qv[r]] - pbv[r] : 0;
   }
+  const float hx = a.h[lv][0], hy = a.h[lv][1], hz = a.h[lv][2];
 #pragma unroll
   for (int r = 0; r < NR; ++r) {
     if (r * 32 >= ncand) break;  // warp-uniform
     const int cand = r * 32 + lane;
-    const int dl = dlv[r], k = cand % NC;
+    const int k = cand % NC, d = cand < ncand ? s_dir[cand / NC] : 0;
     int q = qv[r];
-    const int ddx = 2 * (dl % 3 - 1) + (k & 1) - (cls & 1);
-    const int ddy = 2 * ((dl / 3) % 3 - 1) + ((k >> 1) & 1) - ((cls >> 1) & 1);
-    const int ddz = DIM == 3 ? 2 * (dl / 9 - 1) + ((k >> 2) & 1) - ((cls >> 2) & 1) : 0;
+    const int ddx = 2 * ((d & 3) - 1) + (k & 1) - (cls & 1);
+    const int ddy = 2 * (((d >> 2) & 3) - 1) + ((k >> 1) & 1) - ((cls >> 1) & 1);
+    const int ddz = DIM == 3 ? 2 * (((d >> 4) & 3) - 1) + ((k >> 2) & 1) - ((cls >> 2) & 1) : 0;
     const bool adj = ddx >= -1 && ddx <= 1 && ddy >= -1 && ddy <= 1 && ddz >= -1 && ddz <= 1;
     const bool fd = a.any_fdirect && !adj && a.fdirect[(ddx + 3) + 7 * (ddy + 3) + (DIM == 3 ? 49 * (ddz + 3) : 0)];
-    if (q >= 0 && (adj || ((long long)nt * nsv[r] > a.direct_max && !fd))) q = -1;
+    if (q >= 0 && (adj || (nsv[r] > ns_max && !fd))) q = -1;
     const unsigned mask = __ballot_sync(0xffffffffu, q >= 0);
     const int pos = nsrc + __popc(mask & ((1u << lane) - 1u));
     int x = q >= 0 ? nsv[r] : 0;  // inclusive scan of the kept counts
@@ -935,10 +945,8 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
       if (lane >= o) x += y;
     }
     if (q >= 0) {
-      s_pb[pos] = pbv[r];
-      s_shift[3 * pos] = ddx * hx;  // c_S - c_T
-      s_shift[3 * pos + 1] = ddy * hy;
-      s_shift[3 * pos + 2] = ddz * hz;
+      // c_S - c_T, and the delta from concatenated position to particle index
+      s_cell[pos] = make_float4(ddx * hx, ddy * hy, ddz * hz, __int_as_float(pbv[r] - (ptotal + x - nsv[r])));
       s_pref[pos + 1] = ptotal + x;
     }
     ptotal += __shfl_sync(0xffffffffu, x, 31);
@@ -948,14 +956,13 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   if (nsrc == 0) return;
   if (lane == 0 && a.pair_count) atomicAdd(a.pair_count, (unsigned long long)((long long)nt * ptotal));
   switch (nt) {
-    case 1: direct_small<1, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
-    case 2: direct_small<2, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
-    case 3: direct_small<3, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
-    case 4: direct_small<4, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
-    case 5: direct_small<5, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
-    case 6: direct_small<6, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
-    case 7: direct_small<7, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
-    case 8: direct_small<8, DIM>(a, off, tb, nt, s_pb, s_shift, s_pref, nsrc, lane); return;
+    case 1: direct_small<1, DIM>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
+    case 2: direct_small<2, DIM>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
+    case 3: direct_small<3, DIM>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
+    case 4: direct_small<4, DIM>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
+    case 5: direct_small<5, DIM>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
+    case 6: direct_small<6, DIM>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
+    case 7: direct_small<7, DIM>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
     default: break;
   }
   // larger T: the register blocking R in 1..4 that minimises the busiest lane's work (largest R on ties)
@@ -974,10 +981,10 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   }
   float4 *stage = s_stage_all[wib];
   switch (bestR) {
-    case 1: direct_blocked<1, DIM>(a, off, tb, nt, bestG, s_pb, s_shift, s_pref, nsrc, lane, stage); break;
-    case 2: direct_blocked<2, DIM>(a, off, tb, nt, bestG, s_pb, s_shift, s_pref, nsrc, lane, stage); break;
-    case 3: direct_blocked<3, DIM>(a, off, tb, nt, bestG, s_pb, s_shift, s_pref, nsrc, lane, stage); break;
-    default: direct_blocked<4, DIM>(a, off, tb, nt, bestG, s_pb, s_shift, s_pref, nsrc, lane, stage); break;
+    case 1: direct_blocked<1, DIM>(a, off, tb, nt, bestG, s_cell, s_pref, nsrc, lane, stage); break;
+    case 2: direct_blocked<2, DIM>(a, off, tb, nt, bestG, s_cell, s_pref, nsrc, lane, stage); break;
+    case 3: direct_blocked<3, DIM>(a, off, tb, nt, bestG, s_cell, s_pref, nsrc, lane, stage); break;
+    default: direct_blocked<4, DIM>(a, off, tb, nt, bestG, s_cell, s_pref, nsrc, lane, stage); break;
   }
 }
 
