@@ -1,5 +1,6 @@
 // Expansion passes (P2M, M2M, M2L, L2L, L2P) and the near field.
 #pragma once
+#include <algorithm>
 #include "order.cuh"
 #include "tree.cuh"
 
@@ -18,6 +19,36 @@ struct OpTables {
   DevBuf<double> tab64;     // FP64 copy of the 3D M2L operators (training-pair probe only)
 };
 
+// Page-locked host staging (batch tables uploaded every pass): the copies
+// from it are asynchronous, so the buffer is rewritten only after a stream
+// synchronisation, which every pass makes before building its tables.
+template <class T>
+struct HostPinned {
+  T *ptr = nullptr;
+  size_t cap = 0;
+  bool reserve(size_t n, cudaStream_t st) {
+    if (n <= cap) return true;
+    if (ptr) {
+      cudaStreamSynchronize(st);
+      cudaFreeHost(ptr);
+    }
+    ptr = nullptr;
+    cap = 0;
+    size_t want = std::max(n, (size_t)4096);
+    if (cudaHostAlloc((void **)&ptr, want * sizeof(T), cudaHostAllocDefault) != cudaSuccess) {
+      ptr = nullptr;
+      return false;
+    }
+    cap = want;
+    return true;
+  }
+  void release() {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    cap = 0;
+  }
+};
+
 struct ExpBuffers {
   DevBuf<float> M, L;  // n_cells * KS each (indexed by absolute cell - cell0)
   DevBuf<int> tlist;      // class-grouped cells of levels >= 2 (L2L targets)
@@ -32,6 +63,7 @@ struct ExpBuffers {
   DevBuf<uint64_t> ukey;   // shortcuts: sort keys (two sorts, key and alternate each)
   DevBuf<uint32_t> uval;
   DevBuf<int4> batches2;   // shortcuts: batches of the cells that need L2L, then of the M2M rows
+  HostPinned<int4> hbatches, hbatches2;  // their host staging
   DevBuf<int> esrc;        // L2L shortcut: per leaf, the cell whose local expansion its particles evaluate
   DevBuf<uint8_t> elev;    //   and that cell's level
   DevBuf<int> m2l_src, m2l_list, m2l_nslots, m2l_tslot;  // per M2L batch: resolved sources and present slots

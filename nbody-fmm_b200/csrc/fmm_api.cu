@@ -176,6 +176,8 @@ int fmm_destroy(fmm_ctx *c) {
   c->eb.esrc.release();
   c->eb.elev.release();
   c->eb.ukey.release();
+  c->eb.hbatches.release();
+  c->eb.hbatches2.release();
   c->eb.uval.release();
   c->eb.m2l_split_w.release();
   c->eb.m2l_w.release();

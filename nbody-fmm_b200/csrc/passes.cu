@@ -1056,15 +1056,29 @@ __global__ void k_m_mode(const uint8_t *lact, const uint8_t *msrc, int first2, i
   mode[c - cell0] = !req ? 0 : (c >= leaf_first || pend[c] - pbeg[c] <= tmax) ? 1 : 2;
 }
 
-// Zeroes the rows (KS floats, KS a multiple of 4) of the cells
-// [first, first + count) whose flag equals `want`.
-__global__ void k_zero_rows(const uint8_t *flag, uint8_t want, int first, int count, int cell0, int KS, float *X) {
-  const int per = KS >> 2;
-  const int64_t nvec = (int64_t)count * per;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nvec; e += (int64_t)gridDim.x * blockDim.x) {
-    const int c = first + (int)(e / per);
-    if (flag[c - cell0] == want)
-      reinterpret_cast<float4 *>(X + (size_t)(c - cell0) * KS)[e % per] = make_float4(0.f, 0.f, 0.f, 0.f);
+// Zeroes the rows (KS floats, KS a multiple of 4) of X of the cells
+// [first, first + count) with fx[c] == wx, and those of Y with fy[c] == wy:
+// a warp reads the flags of 32 cells at once and stores each flagged row
+// with all its lanes.
+__global__ void k_zero_rows(const uint8_t *fx, uint8_t wx, float *X, const uint8_t *fy, uint8_t wy, float *Y,
+                            int first, int count, int cell0, int KS) {
+  const int lane = threadIdx.x & 31;
+  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t i0 = w0 * 32; i0 < count; i0 += nw * 32) {
+    const int64_t i = i0 + lane;
+    const int c = first + (int)i;
+    const bool in = i < count;
+    unsigned mx = __ballot_sync(0xffffffffu, in && fx[c - cell0] == wx);
+    unsigned my = __ballot_sync(0xffffffffu, in && fy[c - cell0] == wy);
+    while (mx | my) {
+      const bool isx = mx != 0;
+      unsigned &m = isx ? mx : my;
+      const int b = __ffs(m) - 1;
+      m &= m - 1;
+      float4 *row = reinterpret_cast<float4 *>((isx ? X : Y) + (size_t)(first + (int)i0 + b - cell0) * KS);
+      for (int q = lane; q < (KS >> 2); q += 32) row[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
   }
 }
 
@@ -1267,8 +1281,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   // contributions (L2P from each leaf's deepest such ancestor), multipoles
   // only for what M2L reads (P2M straight into small cells, M2M above them);
   // only the rows that are summed into start at zero
-  const bool shortcut = dim == 3 && D >= 3;
-  if (!shortcut) {
+  if (!(t.dim == 3 && D >= 3)) {
     CUDA_TRY(cudaMemsetAsync(eb.M.ptr, 0, sizeof(float) * (size_t)ncell * KS, st));
     CUDA_TRY(cudaMemsetAsync(eb.L.ptr, 0, sizeof(float) * (size_t)ncell * KS, st));
   }
@@ -1301,12 +1314,15 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   ws.launches += 1;
   const float inv_sD = (float)(1.0 / sD);
 
-  // class-grouped target lists of levels >= 2: every cell (for L2L) and the
-  // cells with possible M2L pairs (for M2L)
-  std::vector<int4> hb;
+  // class-grouped target lists of levels >= 2: the cells with possible M2L
+  // pairs (for M2L) and, without the shortcuts (which build their own lists
+  // below), every cell (for M2M and L2L) and consecutive M2M parents
+  const bool shortcut = dim == 3 && D >= 3;
   std::vector<int> lvl_b0(D + 2, 0), lvl_b1(D + 2, 0), m2l_b0(D + 2, 0), m2l_b1(D + 2, 0);
+  std::vector<int> m2m_b0(D + 1, 0), m2m_b1(D + 1, 0);
   int ntl = 0;
   const int *tl = nullptr, *tl_m2l = nullptr;
+  size_t nhb = 0;
   if (D >= 2) {
     ntl = t.level_off[D] + t.level_count[D] - t.level_off[2];
     if (!eb.tlist.reserve(ntl) || !eb.tlist_m2l.reserve(ntl) || !eb.cls_count.reserve(512) ||
@@ -1319,49 +1335,60 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
           t.level_off[d], t.level_count[d], d, dim, eb.ckey.ptr, eb.ckey_m2l.ptr, eb.cval.ptr,
           t.level_off[d] - t.level_off[2]);
     ws.launches += D - 1;
-    CUDA_TRY(cudaMemcpyAsync(eb.cval2.ptr, eb.cval.ptr, sizeof(uint32_t) * ntl, cudaMemcpyDeviceToDevice, st));
-    uint64_t *kk = eb.ckey.ptr, *kk2 = eb.ckey_alt.ptr;
-    uint32_t *vv = eb.cval.ptr, *vv2 = (uint32_t *)eb.tlist.ptr;
-    radix_sort(ws, kk, vv, kk2, vv2, ntl, 8, st);  // sorted (keys, cells) end in (kk, vv)
-    tl = (const int *)vv;
     CUDA_TRY(cudaMemsetAsync(eb.cls_count.ptr, 0, 512 * sizeof(uint32_t), st));
-    k_class_hist<<<std::min(cdiv(ntl, TPB), 148 * 4), TPB, 0, st>>>(kk, ntl, eb.cls_count.ptr);
+    uint64_t *kk = eb.ckey.ptr, *kk2 = eb.ckey_alt.ptr;
+    uint32_t *mv = eb.cval.ptr, *mv2 = (uint32_t *)eb.tlist_m2l.ptr;
+    if (!shortcut) {
+      CUDA_TRY(cudaMemcpyAsync(eb.cval2.ptr, eb.cval.ptr, sizeof(uint32_t) * ntl, cudaMemcpyDeviceToDevice, st));
+      uint32_t *vv = eb.cval.ptr, *vv2 = (uint32_t *)eb.tlist.ptr;
+      radix_sort(ws, kk, vv, kk2, vv2, ntl, 8, st);  // sorted (keys, cells) end in (kk, vv)
+      tl = (const int *)vv;
+      k_class_hist<<<std::min(cdiv(ntl, TPB), 148 * 4), TPB, 0, st>>>(kk, ntl, eb.cls_count.ptr);
+      ws.launches += 1;
+      mv = eb.cval2.ptr;
+    }
     uint64_t *mk = eb.ckey_m2l.ptr, *mk2 = (kk == eb.ckey.ptr) ? eb.ckey_alt.ptr : eb.ckey.ptr;
-    uint32_t *mv = eb.cval2.ptr, *mv2 = (uint32_t *)eb.tlist_m2l.ptr;
     radix_sort(ws, mk, mv, mk2, mv2, ntl, 8, st);
     tl_m2l = (const int *)mv;
     k_class_hist<<<std::min(cdiv(ntl, TPB), 148 * 4), TPB, 0, st>>>(mk, ntl, eb.cls_count.ptr + 256);
-    ws.launches += 2;
+    ws.launches += 1;
     uint32_t hc[512];
     CUDA_TRY(cudaMemcpyAsync(hc, eb.cls_count.ptr, sizeof(hc), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     const int ncls = 1 << dim;
-    for (int pass = 0; pass < 2; ++pass) {
+    // batch count, then the table written straight into pinned staging
+    size_t cnt_b = 0;
+    for (int pass = shortcut ? 1 : 0; pass < 2; ++pass)
+      for (int d = 2; d <= D; ++d)
+        for (int c = 0; c < ncls; ++c) cnt_b += ((size_t)hc[256 * pass + ((d << dim) | c)] + tchunk - 1) / tchunk;
+    if (!shortcut)
+      for (int d = D - 1; d >= 2; --d) cnt_b += ((size_t)t.level_count[d] + tchunk - 1) / tchunk;
+    if (!eb.hbatches.reserve(cnt_b + 1, st)) return FMM_ERR_OUT_OF_MEMORY;
+    int4 *hb = eb.hbatches.ptr;
+    for (int pass = shortcut ? 1 : 0; pass < 2; ++pass) {
       const uint32_t *h = hc + 256 * pass;
-      const int chunk = tchunk;
       int off = 0;
       for (int d = 2; d <= D; ++d) {
-        (pass ? m2l_b0 : lvl_b0)[d] = (int)hb.size();
+        (pass ? m2l_b0 : lvl_b0)[d] = (int)nhb;
         for (int c = 0; c < ncls; ++c) {
-          int cnt = (int)h[(d << dim) | c];
-          for (int s0 = 0; s0 < cnt; s0 += chunk) hb.push_back(make_int4(off + s0, std::min(chunk, cnt - s0), d, c));
+          const int cnt = (int)h[(d << dim) | c];
+          for (int s0 = 0; s0 < cnt; s0 += tchunk) hb[nhb++] = make_int4(off + s0, std::min(tchunk, cnt - s0), d, c);
           off += cnt;
         }
-        (pass ? m2l_b1 : lvl_b1)[d] = (int)hb.size();
+        (pass ? m2l_b1 : lvl_b1)[d] = (int)nhb;
       }
     }
+    // M2M batches (levels D-1 .. 2, consecutive cells)
+    for (int d = D - 1; d >= 2 && !shortcut; --d) {
+      m2m_b0[d] = (int)nhb;
+      for (int s = 0; s < t.level_count[d]; s += tchunk)
+        hb[nhb++] = make_int4(t.level_off[d] + s, std::min(tchunk, t.level_count[d] - s), d, -1);
+      m2m_b1[d] = (int)nhb;
+    }
   }
-  // M2M batches (levels D-1 .. 2, consecutive cells)
-  std::vector<int> m2m_b0(D + 1, 0), m2m_b1(D + 1, 0);
-  for (int d = D - 1; d >= 2; --d) {
-    m2m_b0[d] = (int)hb.size();
-    for (int s = 0; s < t.level_count[d]; s += tchunk)
-      hb.push_back(make_int4(t.level_off[d] + s, std::min(tchunk, t.level_count[d] - s), d, -1));
-    m2m_b1[d] = (int)hb.size();
-  }
-  if (!eb.batches.reserve(hb.size() + 1)) return FMM_ERR_OUT_OF_MEMORY;
-  if (!hb.empty())
-    CUDA_TRY(cudaMemcpyAsync(eb.batches.ptr, hb.data(), hb.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+  if (!eb.batches.reserve(nhb + 1)) return FMM_ERR_OUT_OF_MEMORY;
+  if (nhb)
+    CUDA_TRY(cudaMemcpyAsync(eb.batches.ptr, eb.hbatches.ptr, nhb * sizeof(int4), cudaMemcpyHostToDevice, st));
 
   ContractArgs ca;
   ca.batches = eb.batches.ptr;
@@ -1489,32 +1516,38 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     uint32_t hc[512];
     CUDA_TRY(cudaMemcpyAsync(hc, eb.cls_count.ptr, sizeof(hc), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
-    std::vector<int4> hb2;
     const int ncls = 1 << dim;
+    size_t cnt_b = 0, nb2 = 0;
+    for (int d = 3; d <= D; ++d)
+      for (int c = 0; c < ncls; ++c) cnt_b += ((size_t)hc[(d << dim) | c] + tchunk - 1) / tchunk;
+    for (int d = m_lo; d <= m_hi; ++d)
+      for (int c = 0; c < (tc ? ncls : 1); ++c) cnt_b += ((size_t)hc[256 + ((d << dim) | c)] + tchunk - 1) / tchunk;
+    if (!eb.hbatches2.reserve(cnt_b + 1, st)) return FMM_ERR_OUT_OF_MEMORY;
+    int4 *hb2 = eb.hbatches2.ptr;
     int off = 0;
     for (int d = 3; d <= D; ++d) {
-      l2_b0[d] = (int)hb2.size();
+      l2_b0[d] = (int)nb2;
       for (int c = 0; c < ncls; ++c) {
         const int cnt = (int)hc[(d << dim) | c];
-        for (int s0 = 0; s0 < cnt; s0 += tchunk) hb2.push_back(make_int4(off + s0, std::min(tchunk, cnt - s0), d, c));
+        for (int s0 = 0; s0 < cnt; s0 += tchunk) hb2[nb2++] = make_int4(off + s0, std::min(tchunk, cnt - s0), d, c);
         off += cnt;
       }
-      l2_b1[d] = (int)hb2.size();
+      l2_b1[d] = (int)nb2;
     }
     off = 0;
     for (int d = m_lo; d <= m_hi; ++d) {
-      um_b0[d] = (int)hb2.size();
+      um_b0[d] = (int)nb2;
       for (int c = 0; c < (tc ? ncls : 1); ++c) {
         const int cnt = (int)hc[256 + ((d << dim) | c)];
         for (int s0 = 0; s0 < cnt; s0 += tchunk)
-          hb2.push_back(make_int4(off + s0, std::min(tchunk, cnt - s0), d, tc ? c : -1));
+          hb2[nb2++] = make_int4(off + s0, std::min(tchunk, cnt - s0), d, tc ? c : -1);
         off += cnt;
       }
-      um_b1[d] = (int)hb2.size();
+      um_b1[d] = (int)nb2;
     }
-    if (!eb.batches2.reserve(hb2.size() + 1)) return FMM_ERR_OUT_OF_MEMORY;
-    if (!hb2.empty())
-      CUDA_TRY(cudaMemcpyAsync(eb.batches2.ptr, hb2.data(), hb2.size() * sizeof(int4), cudaMemcpyHostToDevice, st));
+    if (!eb.batches2.reserve(nb2 + 1)) return FMM_ERR_OUT_OF_MEMORY;
+    if (nb2)
+      CUDA_TRY(cudaMemcpyAsync(eb.batches2.ptr, hb2, nb2 * sizeof(int4), cudaMemcpyHostToDevice, st));
     tl2 = (const int *)vv;
     tlm = (const int *)mv;
     b2 = eb.batches2.ptr;
@@ -1523,11 +1556,9 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     k_leaf_esrc<<<cdiv(t.level_count[D], TPB), TPB, 0, st>>>(leaf_first, t.level_count[D], D, first2, ws.cell_parent,
                                                               needs, cell0, eb.esrc.ptr, eb.elev.ptr);
     // rows summed into: M of the M2M cells, L of the cells that need L
-    const int64_t nvec = (int64_t)ntl * (KS / 4);
-    const int zgrid = std::max(1, std::min(cdiv(nvec, TPB), 148 * 16));
-    k_zero_rows<<<zgrid, TPB, 0, st>>>(mmode, 2, first2, ntl, cell0, KS, eb.M.ptr);
-    k_zero_rows<<<zgrid, TPB, 0, st>>>(needs, 1, first2, ntl, cell0, KS, eb.L.ptr);
-    ws.launches += 3;
+    k_zero_rows<<<std::max(1, std::min(cdiv((int64_t)ntl, TPB), 148 * 32)), TPB, 0, st>>>(
+        mmode, 2, eb.M.ptr, needs, 1, eb.L.ptr, first2, ntl, cell0, KS);
+    ws.launches += 2;
   }
 
   if (ev) cudaEventRecord(ev[1], st);

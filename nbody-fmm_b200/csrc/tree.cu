@@ -336,26 +336,24 @@ __global__ void k_make_parents(uint64_t *ckey, int *cpbeg, int *cpend, int *cpar
 // two dependent loads and no key decoding.
 __global__ void k_colleagues(const uint64_t *ckey, const int *cparent, const int *cchild, int *ccoll, int base,
                              int count, int dim) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= count) return;
-  c += base;
+  // blocks of 8 cells x ns slots, one thread per (cell, slot): consecutive
+  // threads write consecutive slots
   const int nc = 1 << dim, ns = dim == 3 ? 27 : 9;
+  const int ci = blockIdx.x * 8 + (int)threadIdx.x / ns, s = (int)threadIdx.x % ns;
+  if (ci >= count) return;
+  const int c = base + ci;
   const int b = (int)(ckey[c] & (uint64_t)(nc - 1));
-  const int *pc = ccoll + (int64_t)cparent[c] * ns;
-  int *out = ccoll + (int64_t)c * ns;
-  for (int s = 0; s < ns; ++s) {
-    int pslot = 0, child = 0, mul = 1;
-    for (int a = 0; a < dim; ++a) {
-      const int delta = (s / mul) % 3 - 1;
-      const int v = ((b >> a) & 1) + delta;  // in [-1, 2]
-      const int e = (v + 2) / 2 - 1;        // floor(v / 2)
-      pslot += (e + 1) * mul;
-      child |= (v - 2 * e) << a;
-      mul *= 3;
-    }
-    const int Q = pc[pslot];
-    out[s] = Q >= 0 ? cchild[(int64_t)Q * nc + child] : -1;
+  int pslot = 0, child = 0, mul = 1;
+  for (int a = 0; a < dim; ++a) {
+    const int delta = (s / mul) % 3 - 1;
+    const int v = ((b >> a) & 1) + delta;  // in [-1, 2]
+    const int f = (v + 2) / 2 - 1;        // floor(v / 2)
+    pslot += (f + 1) * mul;
+    child |= (v - 2 * f) << a;
+    mul *= 3;
   }
+  const int Q = ccoll[(int64_t)cparent[c] * ns + pslot];
+  ccoll[(int64_t)c * ns + s] = Q >= 0 ? cchild[(int64_t)Q * nc + child] : -1;
 }
 
 __global__ void k_root_colleague(int *ccoll, int root, int dim) {
@@ -513,8 +511,8 @@ int build_tree(Workspace &ws, TreeState &t, const double *d_pos, const double *d
   k_root_colleague<<<1, 32, 0, st>>>(ws.cell_coll, lbase[0], dim);
   ws.launches += 2;
   for (int d = 1; d <= D; ++d) {
-    k_colleagues<<<cdiv(t.level_count[d], TPB), TPB, 0, st>>>(ws.cell_key, ws.cell_parent, ws.cell_child,
-                                                              ws.cell_coll, lbase[d], t.level_count[d], dim);
+    k_colleagues<<<cdiv(t.level_count[d], 8), 8 * ns, 0, st>>>(ws.cell_key, ws.cell_parent, ws.cell_child,
+                                                                ws.cell_coll, lbase[d], t.level_count[d], dim);
     ws.launches += 1;
   }
   // particles in leaf order
