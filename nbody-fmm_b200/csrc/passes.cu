@@ -437,6 +437,7 @@ __device__ inline float2 lget(const float *Lr, int n, int m) {
 // evaluating it there gives the same field without the L2L chain.  Offsets
 // of the particles from level-d centres: `part` at the leaf level,
 // lvl_off[(d - 2) n + i] above.
+template <bool POT>
 __global__ void k_l2p3d(const float4 *part, const int *leaf_of, int64_t n, int cell0, float inv_s, int p, int KS,
                         const float *L, float4 *far, const int *esrc, const uint8_t *elev, int leaf_first, int D,
                         const float4 *lvl_off, float inv_s0) {
@@ -482,8 +483,10 @@ __global__ void k_l2p3d(const float4 *part, const int *leaf_of, int64_t n, int c
         p1re = cre;
         p1im = cim;
       }
-      float2 Lv = lget(Lr, l, m);
-      ph += wm * (Lv.x * cre - Lv.y * cim);
+      if (POT) {
+        const float2 Lv = lget(Lr, l, m);
+        ph += wm * (Lv.x * cre - Lv.y * cim);
+      }
       if (l < p) {
         float2 A = lget(Lr, l + 1, m), Lm = lget(Lr, l + 1, m - 1), Lp = lget(Lr, l + 1, m + 1);
         gz += wm * (A.x * cre - A.y * cim);
@@ -575,7 +578,7 @@ __device__ __forceinline__ float rsqrt_sfu(float x) {
   return y;
 }
 
-template <int DIM, bool NEWTON = true>
+template <int DIM, bool NEWTON = true, bool POT = true>
 __device__ inline void pair_acc(float rx, float ry, float rz, float w, float eps2, float &ax, float &ay, float &az,
                                 float &ph) {
   if (DIM == 3) {
@@ -587,13 +590,13 @@ __device__ inline void pair_acc(float rx, float ry, float rz, float w, float eps
     ax = fmaf(-rx, mi3, ax);
     ay = fmaf(-ry, mi3, ay);
     az = fmaf(-rz, mi3, az);
-    ph += mi;
+    if (POT) ph += mi;
   } else {
     const float r2 = fmaf(rx, rx, fmaf(ry, ry, eps2));
     const float f = w / r2;
     ax = fmaf(-rx, f, ax);
     ay = fmaf(-ry, f, ay);
-    ph = fmaf(-0.5f * w, logf(r2), ph);
+    if (POT) ph = fmaf(-0.5f * w, logf(r2), ph);
   }
 }
 
@@ -624,7 +627,7 @@ struct P2PArgs {
 // of the leaf size.  Offsets are hi + lo FP32 pairs, the shift is hi + lo
 // from FP64, and (t_hi - shift_hi) is formed error-free (TwoSum), so each
 // difference is rounded once, relative to itself, whatever the separation.
-template <int DIM>
+template <int DIM, bool POT>
 __global__ void k_p2p(P2PArgs a) {
   constexpr int NS = DIM == 3 ? 27 : 9;
   const int lane = threadIdx.x & 31;
@@ -666,7 +669,7 @@ __global__ void k_p2p(P2PArgs a) {
         const float rx = (tx - q.x) + (ex - ql.x);
         const float ry = (ty - q.y) + (ey - ql.y);
         const float rz = (tz - q.z) + (ez - ql.z);
-        pair_acc<DIM>(rx, ry, rz, q.w, a.eps2, ax, ay, az, ph);
+        pair_acc<DIM, true, POT>(rx, ry, rz, q.w, a.eps2, ax, ay, az, ph);
       }
     }
     for (int o = 1; o < Gl; o <<= 1) {
@@ -775,7 +778,7 @@ __device__ inline float4 shifted_source(const float4 *off, const float4 *s_cell,
   return make_float4(q.x + cd.x, q.y + cd.y, q.z + cd.z, q.w);
 }
 
-template <int NT, int DIM>
+template <int NT, int DIM, bool POT>
 __device__ void direct_small(const DirectArgs &a, const float4 *off, int tb, int nt, const float4 *s_cell,
                              const int *s_pref, int nsrc, int lane) {
   float tx[NT], ty[NT], tz[NT], ax[NT], ay[NT], az[NT], ph[NT];
@@ -796,7 +799,7 @@ __device__ void direct_small(const DirectArgs &a, const float4 *off, int tb, int
       const float4 q = shifted_source(off, s_cell, f, si);
 #pragma unroll
       for (int k = 0; k < NT; ++k)
-        pair_acc<DIM, false>(tx[k] - q.x, ty[k] - q.y, tz[k] - q.z, q.w, a.eps2, ax[k], ay[k], az[k], ph[k]);
+        pair_acc<DIM, false, POT>(tx[k] - q.x, ty[k] - q.y, tz[k] - q.z, q.w, a.eps2, ax[k], ay[k], az[k], ph[k]);
     }
   }
 #pragma unroll
@@ -815,7 +818,7 @@ __device__ void direct_small(const DirectArgs &a, const float4 *off, int tb, int
 // Larger T: each lane holds R targets and takes every Gl-th source of the
 // chunks of 32 staged through shared memory; ceil(nt / R) target groups of
 // Gl lanes, 32 / Gl groups per round.
-template <int R, int DIM>
+template <int R, int DIM, bool POT>
 __device__ void direct_blocked(const DirectArgs &a, const float4 *off, int tb, int nt, int Gl, const float4 *s_cell,
                                const int *s_pref, int nsrc, int lane, float4 *stage) {
   const int groups = (nt + R - 1) / R, gpr = 32 / Gl;
@@ -843,7 +846,7 @@ __device__ void direct_blocked(const DirectArgs &a, const float4 *off, int tb, i
         const float4 sq = stage[k];
 #pragma unroll
         for (int r = 0; r < R; ++r)
-          pair_acc<DIM, false>(tx[r] - sq.x, ty[r] - sq.y, tz[r] - sq.z, sq.w, a.eps2, ax[r], ay[r], az[r], ph[r]);
+          pair_acc<DIM, false, POT>(tx[r] - sq.x, ty[r] - sq.y, tz[r] - sq.z, sq.w, a.eps2, ax[r], ay[r], az[r], ph[r]);
       }
       __syncwarp();
     }
@@ -872,7 +875,7 @@ __device__ inline void blocked_shape(int nt, int R, int &Gl, float &cost) {
   cost = (float)(rounds * R) / (float)Gl;
 }
 
-template <int DIM>
+template <int DIM, bool POT>
 __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   constexpr int NS = DIM == 3 ? 27 : 9, NC = 1 << DIM, NCAND = NS * NC, NR = (NCAND + 31) / 32;
   __shared__ float4 s_cell_all[8][189];
@@ -956,13 +959,13 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   if (nsrc == 0) return;
   if (lane == 0 && a.pair_count) atomicAdd(a.pair_count, (unsigned long long)((long long)nt * ptotal));
   switch (nt) {
-    case 1: direct_small<1, DIM>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
-    case 2: direct_small<2, DIM>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
-    case 3: direct_small<3, DIM>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
-    case 4: direct_small<4, DIM>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
-    case 5: direct_small<5, DIM>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
-    case 6: direct_small<6, DIM>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
-    case 7: direct_small<7, DIM>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
+    case 1: direct_small<1, DIM, POT>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
+    case 2: direct_small<2, DIM, POT>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
+    case 3: direct_small<3, DIM, POT>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
+    case 4: direct_small<4, DIM, POT>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
+    case 5: direct_small<5, DIM, POT>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
+    case 6: direct_small<6, DIM, POT>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
+    case 7: direct_small<7, DIM, POT>(a, off, tb, nt, s_cell, s_pref, nsrc, lane); return;
     default: break;
   }
   // larger T: the register blocking R in 1..4 that minimises the busiest lane's work (largest R on ties)
@@ -981,10 +984,10 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   }
   float4 *stage = s_stage_all[wib];
   switch (bestR) {
-    case 1: direct_blocked<1, DIM>(a, off, tb, nt, bestG, s_cell, s_pref, nsrc, lane, stage); break;
-    case 2: direct_blocked<2, DIM>(a, off, tb, nt, bestG, s_cell, s_pref, nsrc, lane, stage); break;
-    case 3: direct_blocked<3, DIM>(a, off, tb, nt, bestG, s_cell, s_pref, nsrc, lane, stage); break;
-    default: direct_blocked<4, DIM>(a, off, tb, nt, bestG, s_cell, s_pref, nsrc, lane, stage); break;
+    case 1: direct_blocked<1, DIM, POT>(a, off, tb, nt, bestG, s_cell, s_pref, nsrc, lane, stage); break;
+    case 2: direct_blocked<2, DIM, POT>(a, off, tb, nt, bestG, s_cell, s_pref, nsrc, lane, stage); break;
+    case 3: direct_blocked<3, DIM, POT>(a, off, tb, nt, bestG, s_cell, s_pref, nsrc, lane, stage); break;
+    default: direct_blocked<4, DIM, POT>(a, off, tb, nt, bestG, s_cell, s_pref, nsrc, lane, stage); break;
   }
 }
 
@@ -1274,6 +1277,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
                    const OrderOpts &order, cudaStream_t st, fmm_stats &stats, cudaEvent_t *ev) {
   const int dim = t.dim, D = t.depth, KS = ops.KS;
   const int64_t n = t.n;
+  const bool want_pot = d_pot != nullptr;  // the potential is summed only when it is asked for
   const int ncell = t.n_cells, cell0 = t.cell0;
   const int TPB = 256;
   if (!eb.M.reserve((size_t)ncell * KS) || !eb.L.reserve((size_t)ncell * KS)) return FMM_ERR_OUT_OF_MEMORY;
@@ -1761,7 +1765,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   }
   // L2P
   if (dim == 3)
-    k_l2p3d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far,
+    (want_pot ? k_l2p3d<true> : k_l2p3d<false>)<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far,
                                           shortcut ? eb.esrc.ptr : nullptr, shortcut ? eb.elev.ptr : nullptr,
                                           t.level_off[D], D, eb.lvl_off.ptr, (float)(1.0 / emax));
   else
@@ -1799,8 +1803,14 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
       nw += t.level_count[d];
     }
     da.w0[da.nlev] = (int)nw;
-    if (dim == 3) k_direct_far<3><<<cdiv(nw * 32, TPB), TPB, 0, st>>>(da);
-    else k_direct_far<2><<<cdiv(nw * 32, TPB), TPB, 0, st>>>(da);
+    const int64_t grid = cdiv(nw * 32, TPB);
+    if (dim == 3) {
+      if (want_pot) k_direct_far<3, true><<<grid, TPB, 0, st>>>(da);
+      else k_direct_far<3, false><<<grid, TPB, 0, st>>>(da);
+    } else {
+      if (want_pot) k_direct_far<2, true><<<grid, TPB, 0, st>>>(da);
+      else k_direct_far<2, false><<<grid, TPB, 0, st>>>(da);
+    }
     ws.launches += 1;
   }
   if (ev) cudaEventRecord(ev[6], st);
@@ -1831,8 +1841,14 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   pa.pot = d_pot;
   pa.err = ws.dev_err;
   pa.pair_count = ws.counters + 1;
-  if (dim == 3) k_p2p<3><<<cdiv((int64_t)pa.nleaves * 32, TPB), TPB, 0, st>>>(pa);
-  else k_p2p<2><<<cdiv((int64_t)pa.nleaves * 32, TPB), TPB, 0, st>>>(pa);
+  const int pgrid = cdiv((int64_t)pa.nleaves * 32, TPB);
+  if (dim == 3) {
+    if (want_pot) k_p2p<3, true><<<pgrid, TPB, 0, st>>>(pa);
+    else k_p2p<3, false><<<pgrid, TPB, 0, st>>>(pa);
+  } else {
+    if (want_pot) k_p2p<2, true><<<pgrid, TPB, 0, st>>>(pa);
+    else k_p2p<2, false><<<pgrid, TPB, 0, st>>>(pa);
+  }
   ws.launches += 1;
   if (ev) cudaEventRecord(ev[5], st);
   stats.n_cells = ncell;
