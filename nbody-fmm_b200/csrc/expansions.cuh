@@ -62,6 +62,7 @@ struct ExpBuffers {
                            // [2 ncell, 3 ncell) M2L source, [3 ncell, 4 ncell) how M is formed
   DevBuf<uint64_t> ukey;   // shortcuts: sort keys (two sorts, key and alternate each)
   DevBuf<uint32_t> uval;
+  DevBuf<int> p2m_list;    // shortcuts: the cells whose multipole comes straight from their particles, then their count
   DevBuf<int4> batches2;   // shortcuts: batches of the cells that need L2L, then of the M2M rows
   HostPinned<int4> hbatches, hbatches2;  // their host staging
   DevBuf<int> esrc;        // L2L shortcut: per leaf, the cell whose local expansion its particles evaluate

@@ -176,6 +176,7 @@ int fmm_destroy(fmm_ctx *c) {
   c->eb.esrc.release();
   c->eb.elev.release();
   c->eb.ukey.release();
+  c->eb.p2m_list.release();
   c->eb.hbatches.release();
   c->eb.hbatches2.release();
   c->eb.uval.release();

@@ -1044,19 +1044,31 @@ __global__ void k_class_hist(const uint64_t *keys, int n, uint32_t *hist) {
 static constexpr int P2M_DIRECT_MAX = 64;
 
 __global__ void k_m_mode(const uint8_t *lact, const uint8_t *msrc, int first2, int leaf_first, int count,
-                         const int *parent, const int *pbeg, const int *pend, int cell0, int tmax, uint8_t *mode) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
+                         const int *parent, const int *pbeg, const int *pend, int cell0, int tmax, uint8_t *mode,
+                         int *list1, unsigned *count1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31;
   const int c = first2 + i;
-  int a = c;
-  bool req = lact[a - cell0] || msrc[a - cell0];
-  while (!req) {  // needed through a chain of M2M ancestors
-    const int P = parent[a];
-    if (P < first2 || pend[P] - pbeg[P] <= tmax) break;
-    a = P;
-    req = lact[a - cell0] || msrc[a - cell0];
+  int md = 0;
+  if (i < count) {
+    int a = c;
+    bool req = lact[a - cell0] || msrc[a - cell0];
+    while (!req) {  // needed through a chain of M2M ancestors
+      const int P = parent[a];
+      if (P < first2 || pend[P] - pbeg[P] <= tmax) break;
+      a = P;
+      req = lact[a - cell0] || msrc[a - cell0];
+    }
+    md = !req ? 0 : (c >= leaf_first || pend[c] - pbeg[c] <= tmax) ? 1 : 2;
+    mode[c - cell0] = (uint8_t)md;
   }
-  mode[c - cell0] = !req ? 0 : (c >= leaf_first || pend[c] - pbeg[c] <= tmax) ? 1 : 2;
+  // the mode-1 cells, appended a warp at a time (ascending within a warp)
+  const unsigned m1 = __ballot_sync(0xffffffffu, md == 1);
+  if (m1) {
+    unsigned at = 0;
+    if (lane == 0) at = atomicAdd(count1, (unsigned)__popc(m1));
+    at = __shfl_sync(0xffffffffu, at, 0);
+    if (md == 1) list1[at + __popc(m1 & ((1u << lane) - 1u))] = c;
+  }
 }
 
 // Zeroes the rows (KS floats, KS a multiple of 4) of X of the cells
@@ -1100,81 +1112,153 @@ __global__ void k_m2m_keys(const uint64_t *ckey, const uint8_t *mode, const int 
   vals[out_off + i] = (uint32_t)g;
 }
 
-struct P2MCellArgs {
+struct P2MListArgs {
   int nlev;                          // levels 2 .. nlev + 1
   int first[DF_MAX_LEVELS + 1];      // first cell of each level; first[nlev]: end
   const float4 *off[DF_MAX_LEVELS];  // particle offsets from the level's cell centres, mass in w
   float inv_s[DF_MAX_LEVELS];        // 2^level / emax
   const int *pbeg, *pend;
-  const uint8_t *mode;
-  int cell0, p, KS;
+  const int *list;                   // the mode-1 cells
+  const unsigned *count;             // their number
+  int cell0, p, K, KS;
+  int rs;                            // shared-memory row stride: K rounded up to odd
   float *M;
 };
+static constexpr int P2M_WARPS = 4, P2M_KC = (FMM_MAX_P * FMM_MAX_P + 2 * FMM_MAX_P + 4 + 31) / 32;
 
-// P2M of the mode-1 cells of every level: one warp per cell, lanes over its
-// particles (32 at a time), every coefficient summed by a warp reduction as
-// wide as the particles present, collected in shared memory and stored as
-// one row (no atomics; the padding columns are written as zeros).
-__global__ void __launch_bounds__(256) k_p2m_cells(P2MCellArgs a) {
-  __shared__ float s_row[8][FMM_MAX_P * FMM_MAX_P + 2 * FMM_MAX_P + 4];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t c64 = (int64_t)a.first[0] + (int64_t)blockIdx.x * 8 + warp;
-  if (c64 >= a.first[a.nlev]) return;
-  const int c = (int)c64;
-  if (a.mode[c - a.cell0] != 1) return;
-  int k = 0;
-  while (k + 1 < a.nlev && c >= a.first[k + 1]) ++k;
-  float *s = s_row[warp];
-  for (int j = lane; j < a.KS; j += 32) s[j] = 0.f;
-  __syncwarp();
-  const int pb = a.pbeg[c], pe = a.pend[c], p = a.p;
-  const float4 *off = a.off[k];
-  const float inv_s = a.inv_s[k];
-  for (int j0 = pb; j0 < pe; j0 += 32) {
-    const int cnt = min(32, pe - j0);
-    int width = 1;
-    while (width < cnt) width <<= 1;
-    const float4 q = lane < cnt ? off[j0 + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float x = q.x * inv_s, y = q.y * inv_s, z = q.z * inv_s, r2 = x * x + y * y + z * z, w = q.w;
-    auto wsum = [&](float v) {
-      for (int o = width >> 1; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-      return v;
-    };
-    float dre = 1.f, dim_ = 0.f;
-    for (int m = 0; m <= p; ++m) {
-      if (m > 0) {
-        const float h = -0.5f / m;
-        const float nre = h * (x * dre - y * dim_), nim = h * (x * dim_ + y * dre);
-        dre = nre;
-        dim_ = nim;
+// One particle's contributions w R~_l^m (real parts, then -imaginary parts
+// as the layout stores them) into a shared-memory row.
+__device__ inline void p2m_row(float x, float y, float z, float w, int p, float *row) {
+  const float r2 = x * x + y * y + z * z;
+  float dre = 1.f, dim_ = 0.f;
+  for (int m = 0; m <= p; ++m) {
+    if (m > 0) {
+      const float h = -0.5f / m;
+      const float nre = h * (x * dre - y * dim_), nim = h * (x * dim_ + y * dre);
+      dre = nre;
+      dim_ = nim;
+    }
+    float p1re = dre, p1im = dim_, p2re = 0.f, p2im = 0.f;
+    for (int l = m; l <= p; ++l) {
+      float cre, cim;
+      if (l == m) {
+        cre = dre;
+        cim = dim_;
+      } else {
+        const float a1 = c_rec1[l][m] * z, a2 = c_rec2[l][m] * r2;
+        cre = a1 * p1re - a2 * p2re;
+        cim = a1 * p1im - a2 * p2im;
+        p2re = p1re;
+        p2im = p1im;
+        p1re = cre;
+        p1im = cim;
       }
-      float p1re = dre, p1im = dim_, p2re = 0.f, p2im = 0.f;
-      for (int l = m; l <= p; ++l) {
-        float cre, cim;
-        if (l == m) {
-          cre = dre;
-          cim = dim_;
-        } else {
-          const float a1 = c_rec1[l][m] * z, a2 = c_rec2[l][m] * r2;
-          cre = a1 * p1re - a2 * p2re;
-          cim = a1 * p1im - a2 * p2im;
-          p2re = p1re;
-          p2im = p1im;
-          p1re = cre;
-          p1im = cim;
-        }
-        const float vr = wsum(w * cre);
-        if (lane == 0) s[re_idx(l, m)] += vr;
-        if (m > 0) {
-          const float vi = wsum(-w * cim);
-          if (lane == 0) s[im_idx(l, m)] += vi;
-        }
-      }
+      row[re_idx(l, m)] = w * cre;
+      if (m > 0) row[im_idx(l, m)] = -w * cim;
     }
   }
-  __syncwarp();
-  float *row = a.M + (size_t)(c - a.cell0) * a.KS;
-  for (int j = lane; j < a.KS; j += 32) row[j] = s[j];
+}
+
+// P2M of the mode-1 cells (their own particles at their own level, no M2M).
+// Persistent warps take the list 32 (8 or 16 for short lists) cells at a
+// time.  Consecutive cells of
+// at most 32 particles share 32-particle chunks; a larger cell takes chunks
+// of its own with a running sum.  In a chunk each lane writes the
+// contributions of one particle as a row of a shared-memory tile (odd
+// stride: conflict-free), then the lanes sum each cell's rows column by
+// column, in particle order, and store the cell's row once, padding
+// columns zero (no atomics, no reductions across lanes).
+__global__ void __launch_bounds__(32 * P2M_WARPS) k_p2m_list(P2MListArgs a) {
+  extern __shared__ float s_tile[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  float *S = s_tile + (size_t)wib * 32 * a.rs;
+  const unsigned total = *a.count;
+  // cells per group: 32, or fewer when the list is short, so that the warps
+  // share the work evenly
+  const unsigned nw = (unsigned)gridDim.x * P2M_WARPS;
+  const unsigned G = total >= nw * 128u ? 32u : total >= nw * 32u ? 16u : 8u;
+  for (unsigned g0 = ((unsigned)blockIdx.x * P2M_WARPS + wib) * G; g0 < total; g0 += nw * G) {
+    const int gcount = (int)min(G, total - g0);
+    const bool has = lane < gcount;
+    const int c = has ? a.list[g0 + lane] : 0;
+    int pb = 0, n = 0, lv = 0;
+    if (has) {
+      pb = a.pbeg[c];
+      n = a.pend[c] - pb;
+      while (lv + 1 < a.nlev && c >= a.first[lv + 1]) ++lv;
+    }
+    // inclusive prefix of the sizes of the cells of at most 32 particles
+    int P = has && n <= 32 ? n : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, P, o);
+      if (lane >= o) P += y;
+    }
+    const unsigned bigmask = __ballot_sync(0xffffffffu, has && n > 32);
+    int j = 0;
+    while (j < gcount) {  // warp-uniform
+      const int nj = __shfl_sync(0xffffffffu, n, j);
+      if (nj > 32) {  // a large cell: chunks of 32 with a running sum
+        const int cb = __shfl_sync(0xffffffffu, c, j), pbj = __shfl_sync(0xffffffffu, pb, j);
+        const int lvj = __shfl_sync(0xffffffffu, lv, j);
+        const float4 *off = a.off[lvj];
+        const float inv_s = a.inv_s[lvj];
+        float acc[P2M_KC];
+#pragma unroll
+        for (int t = 0; t < P2M_KC; ++t) acc[t] = 0.f;
+        for (int e0 = 0; e0 < nj; e0 += 32) {
+          const int cnt = min(32, nj - e0);
+          const float4 q = lane < cnt ? off[pbj + e0 + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+          p2m_row(q.x * inv_s, q.y * inv_s, q.z * inv_s, q.w, a.p, S + lane * a.rs);
+          __syncwarp();
+#pragma unroll
+          for (int t = 0; t < P2M_KC; ++t) {
+            const int col = lane + 32 * t;
+            if (col < a.K)
+              for (int r = 0; r < cnt; ++r) acc[t] += S[r * a.rs + col];
+          }
+          __syncwarp();
+        }
+        float *mrow = a.M + (size_t)(cb - a.cell0) * a.KS;
+#pragma unroll
+        for (int t = 0; t < P2M_KC; ++t) {
+          const int col = lane + 32 * t;
+          if (col < a.KS) mrow[col] = col < a.K ? acc[t] : 0.f;
+        }
+        ++j;
+        continue;
+      }
+      // a chunk of consecutive small cells j .. j1 (up to the next large cell)
+      const int start = j > 0 ? __shfl_sync(0xffffffffu, P, j - 1) : 0;
+      const unsigned after = bigmask & ~(0xffffffffu >> (31 - j));  // large cells after j
+      const int jb = after ? __ffs(after) - 1 : gcount;
+      const unsigned fit = __ballot_sync(0xffffffffu, lane >= j && lane < jb && P - start <= 32);
+      const int j1 = 31 - __clz(fit);
+      const int used = __shfl_sync(0xffffffffu, P, j1) - start;
+      const int rel = lane >= j && lane <= j1 ? P - n - start : 32;  // each cell's first row
+      const unsigned starts = __reduce_or_sync(0xffffffffu, rel < 32 ? 1u << rel : 0u);
+      const int myk = j + __popc(starts & (0xffffffffu >> (31 - lane))) - 1;
+      const int s0 = __shfl_sync(0xffffffffu, P - n, myk) - start;
+      const int mpb = __shfl_sync(0xffffffffu, pb, myk), mlv = __shfl_sync(0xffffffffu, lv, myk);
+      const float4 q = lane < used ? a.off[mlv][mpb + lane - s0] : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float inv_s = a.inv_s[mlv];
+      p2m_row(q.x * inv_s, q.y * inv_s, q.z * inv_s, q.w, a.p, S + lane * a.rs);
+      __syncwarp();
+      for (int k = j; k <= j1; ++k) {
+        const int r0 = __shfl_sync(0xffffffffu, P - n, k) - start, nk = __shfl_sync(0xffffffffu, n, k);
+        const int ck = __shfl_sync(0xffffffffu, c, k);
+        float *mrow = a.M + (size_t)(ck - a.cell0) * a.KS;
+        for (int col = lane; col < a.KS; col += 32) {
+          float v = 0.f;
+          if (col < a.K)
+            for (int r = r0; r < r0 + nk; ++r) v += S[r * a.rs + col];
+          mrow[col] = v;
+        }
+      }
+      __syncwarp();
+      j = j1 + 1;
+    }
+  }
 }
 
 // ------------------------------------------------------------ L2L shortcut
@@ -1489,8 +1573,11 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   if (shortcut) {
     const int first2 = t.level_off[2], leaf_first = t.level_off[D];
     k_needs_l<<<cdiv(ntl, TPB), TPB, 0, st>>>(lact, first2, ntl, ws.cell_parent, cell0, needs);
+    if (!eb.p2m_list.reserve((size_t)ntl + 1)) return FMM_ERR_OUT_OF_MEMORY;
+    CUDA_TRY(cudaMemsetAsync(eb.p2m_list.ptr + ntl, 0, sizeof(int), st));
     k_m_mode<<<cdiv(ntl, TPB), TPB, 0, st>>>(lact, msrc, first2, leaf_first, ntl, ws.cell_parent, ws.cell_pbeg,
-                                             ws.cell_pend, cell0, P2M_DIRECT_MAX, mmode);
+                                             ws.cell_pend, cell0, P2M_DIRECT_MAX, mmode, eb.p2m_list.ptr,
+                                             reinterpret_cast<unsigned *>(eb.p2m_list.ptr + ntl));
     ws.launches += 2;
     // L2L rows: levels 3..D; M2M rows: children at levels 3..D (tensor
     // cores) or the mode-2 parents at levels 2..D-1
@@ -1569,7 +1656,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   // P2M
   if (shortcut) {
     if (D - 1 > DF_MAX_LEVELS) return FMM_ERR_UNSUPPORTED;
-    P2MCellArgs pm;
+    P2MListArgs pm;
     pm.nlev = D - 1;
     for (int d = 2; d <= D; ++d) {
       pm.first[d - 2] = t.level_off[d];
@@ -1579,12 +1666,27 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     pm.first[D - 1] = t.level_off[D] + t.level_count[D];
     pm.pbeg = ws.cell_pbeg;
     pm.pend = ws.cell_pend;
-    pm.mode = mmode;
+    pm.list = eb.p2m_list.ptr;
+    pm.count = reinterpret_cast<const unsigned *>(eb.p2m_list.ptr + ntl);
     pm.cell0 = cell0;
     pm.p = p;
+    pm.K = ops.K;
     pm.KS = KS;
+    pm.rs = ops.K | 1;
     pm.M = eb.M.ptr;
-    k_p2m_cells<<<cdiv(ntl, 8), 256, 0, st>>>(pm);
+    const size_t psh = sizeof(float) * (size_t)P2M_WARPS * 32 * pm.rs;
+    {
+      static std::mutex mu;
+      static size_t attr[64] = {};
+      int dev = 0;
+      if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return FMM_ERR_CUDA;
+      std::lock_guard<std::mutex> lk(mu);
+      if (attr[dev] < psh) {
+        CUDA_TRY(cudaFuncSetAttribute(k_p2m_list, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psh));
+        attr[dev] = psh;
+      }
+    }
+    k_p2m_list<<<148 * 2, 32 * P2M_WARPS, psh, st>>>(pm);
   } else if (dim == 3) {
     k_p2m3d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.M.ptr);
   } else {
