@@ -515,8 +515,12 @@ static int tc_launch_p(const TcArgs &a, int nb, unsigned int *work, cudaStream_t
   {
     std::lock_guard<std::mutex> lk(mu);
     if (attr[dev] < sh) {
+      // the largest shared-memory carveout, so that two CTAs of the narrow
+      // kernels fit one SM
       if (cudaFuncSetAttribute(k_tc_translate<P16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh) !=
-          cudaSuccess)
+              cudaSuccess ||
+          cudaFuncSetAttribute(k_tc_translate<P16>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               cudaSharedmemCarveoutMaxShared) != cudaSuccess)
         return FMM_ERR_CUDA;
       if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_dev[dev], k_tc_translate<P16>, TC_M, sh) !=
               cudaSuccess ||

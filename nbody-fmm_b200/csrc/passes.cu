@@ -1683,6 +1683,8 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
       std::lock_guard<std::mutex> lk(mu);
       if (attr[dev] < psh) {
         CUDA_TRY(cudaFuncSetAttribute(k_p2m_list, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psh));
+        CUDA_TRY(cudaFuncSetAttribute(k_p2m_list, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      cudaSharedmemCarveoutMaxShared));
         attr[dev] = psh;
       }
     }
