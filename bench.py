@@ -350,7 +350,8 @@ def run_ours(args, world, rank, local):
         line["order"] = {"mode": "learned (M2L tile orders from the MLP in fmmgpu/order_model.npy)",
                          "judge_samples": args.judge, "judge_budget": 1e-6, "judge_every": args.judge_every,
                          "fallbacks_in_timed_steps": int(sum(s["order_fallbacks"] for s in stats)),
-                         "judge_rel_l2_last": float(stats[-1]["judge_rel_l2"]),
+                         "judged_in_timed_steps": int(sum(1 for s in stats if s["judge_rel_l2"] > 0)),
+                         "judge_rel_l2_max": float(max([s["judge_rel_l2"] for s in stats] + [0.0])),
                          "m2l_width_mean": stats[-1]["m2l_width_sum"] / max(1, stats[-1]["m2l_tiles"])}
 
     # comparisons at the same order: tensor cores at fixed p, and the plain
