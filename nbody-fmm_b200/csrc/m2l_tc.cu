@@ -330,16 +330,17 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
     mma_commit(&s_mma[g & 1]);
   };
 
-  // source row of target `tg` for slot i of metadata buffer `buf`
+  // source cell of target `tg` for slot i of metadata buffer `buf`, and its
+  // row.  The source index of a slot is loaded one slot ahead of its row,
+  // so that only the row load is left in the window of the MMAs.
   float4 rv[P16 / 4];
-  auto fetch = [&](int buf, int i, int tg) {
-    int src = -1;
-    if (tg >= 0) {
-      const int sl = s_slot[buf][i];
-      if (a.mode == TC_M2L) src = a.src_tab[((size_t)s_b[buf] * TC_MAX_SLOTS + sl) * TC_M + tid];
-      else if (a.mode == TC_M2M) src = tg;
-      else src = a.cparent[tg];
-    }
+  auto src_of = [&](int buf, int i, int tg) -> int {
+    if (tg < 0) return -1;
+    if (a.mode == TC_M2L) return a.src_tab[((size_t)s_b[buf] * TC_MAX_SLOTS + s_slot[buf][i]) * TC_M + tid];
+    if (a.mode == TC_M2M) return tg;
+    return a.cparent[tg];
+  };
+  auto fetch = [&](int buf, int i, int src) {
     const float4 *xr = (const float4 *)(a.X + (size_t)(src >= 0 ? src - a.cell0 : 0) * a.KS);
     const int lim = min(a.KS, (int)s_w[buf][i]);  // the slot's order needs its first w inputs
 #pragma unroll
@@ -373,7 +374,16 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
     load_tile(1);  // every slot has three or more copies
     nl = 2;
   }
-  fetch(0, 0, tg_cur);
+  fetch(0, 0, src_of(0, 0, tg_cur));
+  int src_nx = -1;    // the source index of the next slot to fetch ...
+  bool pre = false;   // ... when it was loaded ahead
+  if (s_n[0] > 1) {
+    src_nx = src_of(0, 1, tg_cur);
+    pre = true;
+  } else if (s_n[1]) {
+    src_nx = src_of(1, 0, tg_nxt);
+    pre = true;
+  }
   bool ok = true;
   while (ok) {
     const int n = s_n[c];
@@ -383,8 +393,24 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
       __syncthreads();
       tc_fence_after();
       // rows of the next slot, in flight during the MMAs
-      if (j + 1 < n) fetch(c, j + 1, tg_cur);
-      else if (s_n[c ^ 1]) fetch(c ^ 1, 0, tg_nxt);
+      if (j + 1 < n) {
+        fetch(c, j + 1, pre ? src_nx : src_of(c, j + 1, tg_cur));
+        pre = false;
+        if (j + 2 < n) {
+          src_nx = src_of(c, j + 2, tg_cur);
+          pre = true;
+        } else if (s_n[c ^ 1]) {
+          src_nx = src_of(c ^ 1, 0, tg_nxt);
+          pre = true;
+        }
+      } else if (s_n[c ^ 1]) {
+        fetch(c ^ 1, 0, pre ? src_nx : src_of(c ^ 1, 0, tg_nxt));
+        pre = false;
+        if (s_n[c ^ 1] > 1) {  // the batch after next is not loaded yet
+          src_nx = src_of(c ^ 1, 1, tg_nxt);
+          pre = true;
+        }
+      }
       if (tid == 0) {
         for (int t = 0; t < TILES && ok; ++t) {
           const long long g = t_cur + (long long)j * TILES + t;
@@ -530,6 +556,11 @@ static int tc_launch_p(const TcArgs &a, int nb, unsigned int *work, cudaStream_t
     }
     per_sm = per_sm_dev[dev];
   }
+  // a CTA of the kernels up to 128 wide holds 256 TMEM columns and under
+  // half the shared memory, so two share an SM: launch two per SM whatever
+  // the occupancy query says (the CTAs take work from a counter, so a CTA
+  // that cannot start at once only finds less work)
+  if (P16 <= 128) per_sm = std::max(per_sm, 2);
   const int grid = std::min(nb, per_sm * nsm);
   k_tc_translate<P16><<<grid, TC_M, sh, st>>>(a, nb, work);
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
