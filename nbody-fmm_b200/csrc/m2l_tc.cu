@@ -209,14 +209,17 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
 
   const int tid = threadIdx.x, warp = tid >> 5;
 
-  // Takes the next batch with at least one slot into metadata buffer `buf`
-  // (s_n[buf] = 0 when the work is exhausted); returns this thread's target.
+  // Takes the next work item with at least one slot into metadata buffer
+  // `buf` (s_n[buf] = 0 when the work is exhausted); returns this thread's
+  // target.  An item is a batch, or for M2L a run of up to chunk_slots of
+  // its present slots (item = batch * chunks + run).
+  const int chunks = a.mode == TC_M2L ? (TC_MAX_SLOTS + a.chunk_slots - 1) / a.chunk_slots : 1;
   auto load_meta = [&](int buf) -> int {
     while (true) {
       if (tid == 0) s_grab = (int)atomicAdd(work, 1u);
       __syncthreads();
-      const int b = s_grab;
-      if (b >= nb) {
+      const int item = s_grab;
+      if (item >= nb * chunks) {
         if (tid == 0) {
           s_n[buf] = 0;
           s_b[buf] = -1;
@@ -224,12 +227,13 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
         __syncthreads();
         return -1;
       }
+      const int b = item / chunks, s0 = (item % chunks) * a.chunk_slots;
       const int4 bt = a.batches[b];
       const int tg = tid < bt.y ? (a.tlist ? a.tlist[bt.x + tid] : bt.x + tid) : -1;
       int n = 0;
       if (a.mode == TC_M2L) {
-        n = a.nslots[b];
-        const size_t tb = (size_t)b * TC_MAX_SLOTS;
+        n = max(0, min(a.chunk_slots, a.nslots[b] - s0));
+        const size_t tb = (size_t)b * TC_MAX_SLOTS + s0;
         for (int i = tid; i < n; i += TC_M) {
           s_slot[buf][i] = (short)a.slot_list[tb + i];
           s_op[buf][i] = (short)a.tslot_list[tb + i];
@@ -249,7 +253,7 @@ __global__ void __launch_bounds__(TC_M, 1) k_tc_translate(TcArgs a, int nb, unsi
         if (n && a.mode == TC_M2L && a.tiles) atomicAdd(a.tiles, (unsigned long long)n);
         if (n && a.mode == TC_M2L && a.widths) {
           unsigned long long ws = 0;
-          const size_t tb = (size_t)b * TC_MAX_SLOTS;
+          const size_t tb = (size_t)b * TC_MAX_SLOTS + s0;
           for (int i = 0; i < n; ++i) ws += a.slot_p16 ? a.slot_p16[tb + i] : (unsigned long long)P16;
           atomicAdd(a.widths, ws);
         }
@@ -561,8 +565,14 @@ static int tc_launch_p(const TcArgs &a, int nb, unsigned int *work, cudaStream_t
   // the occupancy query says (the CTAs take work from a counter, so a CTA
   // that cannot start at once only finds less work)
   if (P16 <= 128) per_sm = std::max(per_sm, 2);
-  const int grid = std::min(nb, per_sm * nsm);
-  k_tc_translate<P16><<<grid, TC_M, sh, st>>>(a, nb, work);
+  // M2L with fewer than four batches per CTA: runs of 24 slots as work items,
+  // so that the CTAs finish together
+  TcArgs b = a;
+  b.chunk_slots = TC_MAX_SLOTS;
+  if (a.mode == TC_M2L && nb < 4 * per_sm * nsm) b.chunk_slots = 24;
+  const int chunks = a.mode == TC_M2L ? (TC_MAX_SLOTS + b.chunk_slots - 1) / b.chunk_slots : 1;
+  const int grid = std::min(nb * chunks, per_sm * nsm);
+  k_tc_translate<P16><<<grid, TC_M, sh, st>>>(b, nb, work);
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
 }
 
