@@ -138,6 +138,19 @@ def test_fmm_hybrid_matches_oracle(oracle, gen, n, p, T, dm):
     assert s["m2l_pairs"] < s0["m2l_pairs"] and s["p2p_pairs"] > s0["p2p_pairs"]
 
 
+@pytest.mark.parametrize("n,p,T,mode", [(30000, 8, 256, fmmgpu.FMM_M2L_FP32), (20000, 12, 128, fmmgpu.FMM_M2L_TC)])
+def test_fmm_large_leaves_match_oracle(oracle, n, p, T, mode):
+    """Leaf capacities the autotuner may choose (128, 256) on a clustered
+    input: leaves of up to 130 particles take their multipoles in several
+    32-particle chunks, and the few M2L batches of a small tree are split
+    into runs of slots on the tensor cores."""
+    pos, m = workloads.plummer_mixture(n, seed=13)
+    with fmmgpu.Context(dim=3, p=p, leaf_cap=T, G=1.0, direct_max=256, m2l_mode=mode) as c:
+        a, ph = c.evaluate(pos, m, want_pot=True)
+    g, po = oracle.fmm(pos, m, p, T, want_pot=True, direct_max=256)
+    _check_parity(a, ph, g, po)
+
+
 def test_fmm_near_field_matches_reference():
     """p = 0: the far field's gradient vanishes and what remains is the
     reference's near-field sum (leaf.cpp:118-142), checked on its fixture."""
