@@ -51,7 +51,8 @@ enum {
   FMM_ERR_TIMEOUT = -7,
   FMM_ERR_NO_DEVICE = -8,
   FMM_ERR_INTERNAL = -9,
-  FMM_ERR_TOO_LARGE = -10         /* request larger than fmm_direct_noalloc's fixed scratch */
+  FMM_ERR_TOO_LARGE = -10,        /* request larger than fmm_direct_noalloc's fixed scratch */
+  FMM_ERR_IO = -11                /* a frame file could not be written */
 };
 
 /* Order of each M2L pair (FMM_M2L_TC).  FIXED: every pair at p.  GEOMETRIC:
@@ -253,6 +254,40 @@ FMM_API int fmm_tree_pairs(fmm_ctx *ctx, int32_t level, int32_t kind, int64_t *c
 FMM_API int fmm_direct_noalloc(int32_t dim, int64_t n, const double *d_pos, const double *d_mass, int64_t ntargets,
                                const int64_t *d_targets, int32_t soft_mode, double eps2, double G, double *d_acc,
                                double *d_pot, void *stream);
+
+/* Frame output: replaces HDF5Exporter (io/hdf5_exporter.cpp:10-128) for a
+ * simulation loop that writes a frame per step (main.cpp:85-91).  Each
+ * frame holds the reference's datasets, the order and shapes of
+ * write_frame (hdf5_exporter.cpp:24-44, 70-73): position, velocity and
+ * acceleration as n x 3 FP64 (2D padded with z = 0) and weight as n FP64,
+ * stored one after another, little-endian, in `<dir>/<base>_<step:05>.bin`
+ * (the reference: `.h5` datasets; libhdf5 is not used).  After every frame
+ * `<dir>/<base>.xmf` is rewritten as the reference's temporal collection
+ * (hdf5_exporter.cpp:83-128), its data items pointing into the .bin files
+ * (Format="Binary", Seek = byte offset of each dataset), so ParaView reads
+ * the series as it reads the reference's.  fmm_frames_open creates `dir`
+ * (like the constructor, hdf5_exporter.cpp:10-13); a frame of n = 0 is
+ * skipped (hdf5_exporter.cpp:22).
+ *
+ * fmm_frames_write takes host arrays (n x dim positions, velocities and
+ * accelerations, n masses; acc may be NULL: zeros) and writes the frame
+ * before it returns.  fmm_frames_write_device takes device arrays: it
+ * enqueues their copy into page-locked staging on `stream`, after the work
+ * already queued there, and returns; a writer thread writes the file when
+ * the copy has completed, so the copy and the file writing overlap the
+ * caller's next steps.  Two frames can be in flight; a third call waits
+ * for the oldest.  Frames are written in call order.  fmm_frames_flush
+ * waits for every frame in flight and returns the first error met
+ * (FMM_ERR_IO, FMM_ERR_CUDA); fmm_frames_close flushes and frees. */
+typedef struct fmm_frames fmm_frames;
+FMM_API int fmm_frames_open(const char *dir, const char *base, int32_t dim, fmm_frames **out);
+FMM_API int fmm_frames_write(fmm_frames *f, int64_t n, const double *pos, const double *vel, const double *acc,
+                             const double *mass, int32_t step, double time);
+FMM_API int fmm_frames_write_device(fmm_frames *f, int64_t n, const double *d_pos, const double *d_vel,
+                                    const double *d_acc, const double *d_mass, int32_t step, double time,
+                                    void *stream);
+FMM_API int fmm_frames_flush(fmm_frames *f);
+FMM_API int fmm_frames_close(fmm_frames *f);
 
 /* Statistics of the last force pass (per-phase device times, sizes). */
 FMM_API int fmm_last_stats(fmm_ctx *ctx, fmm_stats *out);

@@ -88,6 +88,7 @@ const char *fmm_strerror(int code) {
     case FMM_ERR_TIMEOUT: return "device wait timed out";
     case FMM_ERR_NO_DEVICE: return "no CUDA device";
     case FMM_ERR_TOO_LARGE: return "more targets than fmm_direct_noalloc's fixed scratch holds (FMM_NOALLOC_MAX_TARGETS)";
+    case FMM_ERR_IO: return "a frame file could not be written";
     default: return "internal error";
   }
 }

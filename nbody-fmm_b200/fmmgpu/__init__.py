@@ -29,6 +29,7 @@ FMM_ERR_UNSUPPORTED = -6
 FMM_ERR_TIMEOUT = -7
 FMM_ERR_NO_DEVICE = -8
 FMM_ERR_TOO_LARGE = -10
+FMM_ERR_IO = -11
 FMM_NOALLOC_MAX_TARGETS = 262144
 
 FMM_M2L_FP32 = 0
@@ -52,7 +53,8 @@ EXPORTED = (
     "fmm_tree_build", "fmm_tree_depth", "fmm_tree_level_size", "fmm_tree_level_keys", "fmm_tree_leaves",
     "fmm_tree_pairs", "fmm_last_stats", "fmm_launch_count", "fmm_direct_noalloc", "fmm_order_set_model",
     "fmm_order_get_model", "fmm_order_collect", "fmm_order_train", "fmm_order_forward_grad", "fmm_autotune",
-    "fmm_evaluate_batched",
+    "fmm_evaluate_batched", "fmm_frames_open", "fmm_frames_write", "fmm_frames_write_device", "fmm_frames_flush",
+    "fmm_frames_close",
 )
 
 
@@ -138,6 +140,12 @@ def load_library(path=LIB_PATH):
     L.fmm_order_forward_grad.argtypes = [_vp, _vp, ctypes.c_int32, _vp, _vp, _vp, _vp, _vp]
     L.fmm_autotune.argtypes = [_vp, ctypes.c_int64, _vp, _vp, ctypes.c_int32, ctypes.POINTER(FmmTuneResult), _vp]
     L.fmm_evaluate_batched.argtypes = [_vp, ctypes.c_int32, _i64, _vp, _vp, _vp, _vp, ctypes.c_int32]
+    L.fmm_frames_open.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(_vp)]
+    L.fmm_frames_write.argtypes = [_vp, ctypes.c_int64, _d, _d, _d, _d, ctypes.c_int32, ctypes.c_double]
+    L.fmm_frames_write_device.argtypes = [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, ctypes.c_int32, ctypes.c_double,
+                                          _vp]
+    L.fmm_frames_flush.argtypes = [_vp]
+    L.fmm_frames_close.argtypes = [_vp]
     _lib = L
     return L
 
@@ -149,6 +157,47 @@ def _check(rc):
 
 def _p(a, t=_d):
     return None if a is None else a.ctypes.data_as(t)
+
+
+class Frames:
+    """Frame output of a simulation loop (fmm_frames_*): per step the
+    reference exporter's datasets (position, velocity, acceleration as
+    n x 3 FP64, 2D padded with z = 0; weight as n) in `<dir>/<base>_<step:05>.bin`
+    and the XDMF time-series index `<dir>/<base>.xmf`, rewritten per frame."""
+
+    def __init__(self, directory, base="particles", dim=3):
+        L = load_library()
+        self._h = _vp()
+        _check(L.fmm_frames_open(os.fsencode(directory), base.encode(), dim, ctypes.byref(self._h)))
+        self.dim = dim
+
+    def write(self, pos, vel, mass, step, time, acc=None):
+        """A frame from host arrays (n x dim, n x dim, n; acc optional),
+        written before the call returns."""
+        pos = np.ascontiguousarray(pos, dtype=np.float64)
+        vel = np.ascontiguousarray(vel, dtype=np.float64)
+        mass = np.ascontiguousarray(mass, dtype=np.float64)
+        acc = None if acc is None else np.ascontiguousarray(acc, dtype=np.float64)
+        _check(_lib.fmm_frames_write(self._h, len(mass), _p(pos), _p(vel), _p(acc), _p(mass), step, time))
+
+    def write_device(self, n, pos_ptr, vel_ptr, mass_ptr, step, time, acc_ptr=None, stream=None):
+        """A frame from device arrays: their copy is enqueued on `stream`
+        (an int handle) and the file is written by a writer thread."""
+        _check(_lib.fmm_frames_write_device(self._h, n, pos_ptr, vel_ptr, acc_ptr, mass_ptr, step, time, stream))
+
+    def flush(self):
+        _check(_lib.fmm_frames_flush(self._h))
+
+    def close(self):
+        if self._h:
+            h, self._h = self._h, _vp()
+            _check(_lib.fmm_frames_close(h))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def direct_noalloc(dim, n, pos_ptr, mass_ptr, acc_ptr, pot_ptr=None, ntargets=0, targets_ptr=None,

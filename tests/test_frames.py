@@ -1,0 +1,112 @@
+"""Frame output (fmm_frames_*), the counterpart of the reference's
+HDF5Exporter (io/hdf5_exporter.cpp): the datasets of write_frame and the
+XDMF temporal index of write_xdmf_metadata, here with the datasets as raw
+little-endian FP64 in one .bin per frame.  CPU tests write from host
+arrays; the GPU test writes from device arrays through the asynchronous
+path and expects the same bytes."""
+import os
+
+import numpy as np
+import pytest
+
+import fmmgpu
+
+
+def expected_index(frames):
+    """The reference's index text (hdf5_exporter.cpp:88-127) for frames
+    [(time, file, n)], with each data item pointing into the frame's .bin
+    (Format="Binary", Seek = byte offset of the dataset)."""
+    out = ['<?xml version="1.0" ?>\n', '<!DOCTYPE Xdmf SYSTEM "Xdmf.dtd" []>\n', '<Xdmf Version="2.0">\n',
+           ' <Domain>\n', '  <Grid Name="TimeSeries" GridType="Collection" CollectionType="Temporal">\n']
+
+    def item(dims, seek, f):
+        return [f'       <DataItem Dimensions="{dims}" NumberType="Float" Precision="8" Format="Binary" '
+                f'Endian="Little" Seek="{seek}">\n', f'         {f}\n', '       </DataItem>\n']
+
+    for t, (time, f, n) in enumerate(frames):
+        out += [f'   <Grid Name="Step_{t}" GridType="Uniform">\n', f'     <Time Value="{time:g}"/>\n',
+                f'     <Topology TopologyType="Polyvertex" NumberOfElements="{n}"/>\n',
+                '     <Geometry GeometryType="XYZ">\n', *item(f"{n} 3", 0, f), '     </Geometry>\n',
+                '     <Attribute Name="Velocity" AttributeType="Vector" Center="Node">\n', *item(f"{n} 3", 24 * n, f),
+                '     </Attribute>\n',
+                '     <Attribute Name="Acceleration" AttributeType="Vector" Center="Node">\n',
+                *item(f"{n} 3", 48 * n, f), '     </Attribute>\n',
+                '     <Attribute Name="Weight" AttributeType="Scalar" Center="Node">\n', *item(f"{n}", 72 * n, f),
+                '     </Attribute>\n', '   </Grid>\n']
+    out += ['  </Grid>\n', ' </Domain>\n', '</Xdmf>\n']
+    return "".join(out)
+
+
+def read_frame(path, n):
+    a = np.fromfile(path, dtype="<f8")
+    assert a.size == 10 * n
+    return a[:3 * n].reshape(n, 3), a[3 * n:6 * n].reshape(n, 3), a[6 * n:9 * n].reshape(n, 3), a[9 * n:]
+
+
+def pad3(x):
+    return np.hstack([x, np.zeros((len(x), 3 - x.shape[1]))]) if x.shape[1] < 3 else x
+
+
+def system(n, dim, seed):
+    rng = np.random.default_rng(seed)
+    return rng.normal(size=(n, dim)), rng.normal(size=(n, dim)), rng.normal(size=(n, dim)), rng.uniform(1, 2, n)
+
+
+@pytest.mark.parametrize("dim", [3, 2])
+def test_frames_hold_the_reference_datasets_and_index(tmp_path, dim):
+    d = tmp_path / "out"
+    frames, want = [], []
+    with fmmgpu.Frames(str(d), "particles", dim=dim) as fr:
+        for step, (n, time) in enumerate([(1000, 0.0), (1000, 0.001), (0, 0.002), (700, 1e-05)]):
+            pos, vel, acc, m = system(n, dim, step)
+            fr.write(pos, vel, m, step, time, acc=None if step == 1 else acc)
+            if n == 0:  # an empty frame is skipped (hdf5_exporter.cpp:22)
+                assert not (d / f"particles_{step:05d}.bin").exists()
+                continue
+            name = f"particles_{step:05d}.bin"
+            frames.append((time, name, n))
+            want.append((name, n, pad3(pos), pad3(vel), np.zeros((n, 3)) if step == 1 else pad3(acc), m))
+            # the index is rewritten after every frame
+            assert (d / "particles.xmf").read_text() == expected_index(frames)
+    for name, n, pos, vel, acc, m in want:
+        p, v, a, w = read_frame(d / name, n)
+        np.testing.assert_array_equal(p, pos)
+        np.testing.assert_array_equal(v, vel)
+        np.testing.assert_array_equal(a, acc)
+        np.testing.assert_array_equal(w, m)
+
+
+def test_frames_errors(tmp_path):
+    with pytest.raises(fmmgpu.FmmError) as e:
+        fmmgpu.Frames(str(tmp_path), dim=4)
+    assert e.value.code == fmmgpu.FMM_ERR_INVALID_ARGUMENT
+    blocker = tmp_path / "file"
+    blocker.write_text("x")
+    with pytest.raises(fmmgpu.FmmError) as e:
+        fmmgpu.Frames(str(blocker / "sub"))
+    assert e.value.code == fmmgpu.FMM_ERR_IO
+
+
+@pytest.mark.gpu
+def test_device_frames_match_host_frames(tmp_path):
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    n, dim = 5000, 3
+    systems = [system(n, dim, s) for s in range(4)]
+    with fmmgpu.Frames(str(tmp_path / "host"), dim=dim) as fh:
+        for step, (pos, vel, acc, m) in enumerate(systems):
+            fh.write(pos, vel, m, step, 0.5 * step, acc=acc)
+    st = torch.cuda.Stream(dev)
+    with fmmgpu.Frames(str(tmp_path / "dev"), dim=dim) as fd:
+        keep = []
+        for step, (pos, vel, acc, m) in enumerate(systems):
+            t = [torch.from_numpy(x).to(dev) for x in (pos, vel, acc, m)]
+            torch.cuda.synchronize()
+            keep.append(t)  # device arrays stay alive until their copy has run
+            fd.write_device(n, t[0].data_ptr(), t[1].data_ptr(), t[3].data_ptr(), step, 0.5 * step,
+                            acc_ptr=t[2].data_ptr(), stream=st.cuda_stream)
+        fd.flush()
+    for step in range(4):
+        name = f"particles_{step:05d}.bin"
+        assert (tmp_path / "dev" / name).read_bytes() == (tmp_path / "host" / name).read_bytes()
+    assert (tmp_path / "dev" / "particles.xmf").read_text() == (tmp_path / "host" / "particles.xmf").read_text()
