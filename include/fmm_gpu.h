@@ -271,14 +271,19 @@ FMM_API int fmm_direct_noalloc(int32_t dim, int64_t n, const double *d_pos, cons
  *
  * fmm_frames_write takes host arrays (n x dim positions, velocities and
  * accelerations, n masses; acc may be NULL: zeros) and writes the frame
- * before it returns.  fmm_frames_write_device takes device arrays: it
- * enqueues their copy into page-locked staging on `stream`, after the work
- * already queued there, and returns; a writer thread writes the file when
- * the copy has completed, so the copy and the file writing overlap the
- * caller's next steps.  Two frames can be in flight; a third call waits
- * for the oldest.  Frames are written in call order.  fmm_frames_flush
- * waits for every frame in flight and returns the first error met
- * (FMM_ERR_IO, FMM_ERR_CUDA); fmm_frames_close flushes and frees. */
+ * before it returns.  fmm_frames_write_device takes device arrays on the
+ * current device: it enqueues a device-to-device snapshot of them on
+ * `stream`, after the work already queued there, and returns; work queued
+ * on `stream` afterwards may change the arrays at once.  The snapshot is
+ * copied to page-locked staging on a stream of the writer's own, and a
+ * writer thread writes the file when that copy has completed, so the host
+ * copy and the file writing overlap the caller's next steps.  Two frames
+ * can be in flight (two snapshots of 80 bytes per particle on the device,
+ * two staging buffers on the host); a third call waits for the oldest.
+ * Frames are written in call order; all device frames of a writer come
+ * from one device.  fmm_frames_flush waits for every frame in flight and
+ * returns the first error met (FMM_ERR_IO, FMM_ERR_CUDA); fmm_frames_close
+ * flushes and frees. */
 typedef struct fmm_frames fmm_frames;
 FMM_API int fmm_frames_open(const char *dir, const char *base, int32_t dim, fmm_frames **out);
 FMM_API int fmm_frames_write(fmm_frames *f, int64_t n, const double *pos, const double *vel, const double *acc,

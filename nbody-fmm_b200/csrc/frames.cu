@@ -3,10 +3,12 @@
 // with the datasets stored as raw little-endian FP64 in one file per frame
 // (XDMF "Binary" data items with byte offsets) instead of HDF5.
 //
-// Frames from device arrays are copied into page-locked staging on the
-// caller's stream and written by a writer thread once the copy's event has
-// completed, so the copy and the file writing overlap the caller's next
-// steps.  Two staging slots; frames are written in call order.
+// Frames from device arrays: a device-to-device snapshot on the caller's
+// stream (microseconds), then the copy of the snapshot into page-locked
+// staging on a copy stream of this writer, and the file written by a writer
+// thread once that copy has completed.  The caller's next steps may change
+// its arrays at once; the host copy and the file writing overlap them.  Two
+// slots; frames are written in call order.
 #include <cuda_runtime.h>
 #include <sys/stat.h>
 
@@ -36,9 +38,9 @@ struct fmm_frames {
 
   struct Slot {
     double *buf = nullptr;  // page-locked: positions, velocities, accelerations (n x dim each), masses
+    double *dbuf = nullptr; // the device snapshot, same layout
     size_t cap = 0;         // doubles
-    cudaEvent_t done = nullptr;
-    int device = 0;
+    cudaEvent_t snap = nullptr, done = nullptr;
     bool busy = false;
     bool has_acc = true;
     int64_t n = 0;
@@ -47,6 +49,8 @@ struct fmm_frames {
   };
   Slot slots[2];
   int next_slot = 0;
+  int device = -1;             // the device of the device frames (set by the first)
+  cudaStream_t copy = nullptr; // the host copies of the snapshots
 
   std::mutex mu;
   std::condition_variable cv;
@@ -155,7 +159,7 @@ void writer_loop(fmm_frames *f) {
     fmm_frames::Slot &sl = f->slots[s];
     lk.unlock();
     int rc = FMM_OK;
-    if (cudaSetDevice(sl.device) != cudaSuccess || cudaEventSynchronize(sl.done) != cudaSuccess) rc = FMM_ERR_CUDA;
+    if (cudaSetDevice(f->device) != cudaSuccess || cudaEventSynchronize(sl.done) != cudaSuccess) rc = FMM_ERR_CUDA;
     if (rc == FMM_OK) {
       const size_t nd = (size_t)sl.n * f->dim;
       rc = write_frame(f, sl.n, sl.buf, sl.buf + nd, sl.has_acc ? sl.buf + 2 * nd : nullptr, sl.buf + 3 * nd, sl.step,
@@ -215,6 +219,14 @@ int fmm_frames_write_device(fmm_frames *f, int64_t n, const double *d_pos, const
   if (cudaGetDevice(&dev) != cudaSuccess) return FMM_ERR_CUDA;
   cudaStream_t st = (cudaStream_t)stream;
   std::unique_lock<std::mutex> lk(f->mu);
+  if (f->device >= 0 && f->device != dev) return FMM_ERR_INVALID_ARGUMENT;  // one device per writer
+  if (!f->copy) {
+    if (cudaStreamCreateWithFlags(&f->copy, cudaStreamNonBlocking) != cudaSuccess) {
+      f->copy = nullptr;
+      return FMM_ERR_CUDA;
+    }
+    f->device = dev;
+  }
   const int s = f->next_slot;
   fmm_frames::Slot &sl = f->slots[s];
   f->cv.wait(lk, [&] { return !sl.busy; });  // at most two frames in flight
@@ -222,30 +234,36 @@ int fmm_frames_write_device(fmm_frames *f, int64_t n, const double *d_pos, const
   const size_t nd = (size_t)n * f->dim, need = 3 * nd + (size_t)n;
   if (sl.cap < need) {
     if (sl.buf) cudaFreeHost(sl.buf);
+    if (sl.dbuf) cudaFree(sl.dbuf);
     sl.buf = nullptr;
+    sl.dbuf = nullptr;
     sl.cap = 0;
     if (cudaHostAlloc((void **)&sl.buf, need * sizeof(double), cudaHostAllocDefault) != cudaSuccess) {
       sl.buf = nullptr;
       return FMM_ERR_OUT_OF_MEMORY;
     }
+    if (cudaMalloc((void **)&sl.dbuf, need * sizeof(double)) != cudaSuccess) {
+      sl.dbuf = nullptr;
+      return FMM_ERR_OUT_OF_MEMORY;
+    }
     sl.cap = need;
   }
-  if (sl.done && sl.device != dev) {
-    cudaEventDestroy(sl.done);
-    sl.done = nullptr;
-  }
-  if (!sl.done && cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess) {
-    sl.done = nullptr;
+  if ((!sl.snap && cudaEventCreateWithFlags(&sl.snap, cudaEventDisableTiming) != cudaSuccess) ||
+      (!sl.done && cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess))
     return FMM_ERR_CUDA;
-  }
-  sl.device = dev;
   const size_t vb = nd * sizeof(double);
-  if (cudaMemcpyAsync(sl.buf, d_pos, vb, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-      cudaMemcpyAsync(sl.buf + nd, d_vel, vb, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-      (d_acc && cudaMemcpyAsync(sl.buf + 2 * nd, d_acc, vb, cudaMemcpyDeviceToHost, st) != cudaSuccess) ||
-      cudaMemcpyAsync(sl.buf + 3 * nd, d_mass, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st) !=
+  // the snapshot, ordered after the caller's work on `stream`
+  if (cudaMemcpyAsync(sl.dbuf, d_pos, vb, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(sl.dbuf + nd, d_vel, vb, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+      (d_acc && cudaMemcpyAsync(sl.dbuf + 2 * nd, d_acc, vb, cudaMemcpyDeviceToDevice, st) != cudaSuccess) ||
+      cudaMemcpyAsync(sl.dbuf + 3 * nd, d_mass, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st) !=
           cudaSuccess ||
-      cudaEventRecord(sl.done, st) != cudaSuccess)
+      cudaEventRecord(sl.snap, st) != cudaSuccess)
+    return FMM_ERR_CUDA;
+  // its host copy on the writer's stream
+  if (cudaStreamWaitEvent(f->copy, sl.snap, 0) != cudaSuccess ||
+      cudaMemcpyAsync(sl.buf, sl.dbuf, need * sizeof(double), cudaMemcpyDeviceToHost, f->copy) != cudaSuccess ||
+      cudaEventRecord(sl.done, f->copy) != cudaSuccess)
     return FMM_ERR_CUDA;
   sl.busy = true;
   sl.has_acc = d_acc != nullptr;
@@ -276,10 +294,14 @@ int fmm_frames_close(fmm_frames *f) {
     f->cv.notify_all();
   }
   f->writer.join();
+  if (f->device >= 0) cudaSetDevice(f->device);
   for (auto &sl : f->slots) {
     if (sl.buf) cudaFreeHost(sl.buf);
+    if (sl.dbuf) cudaFree(sl.dbuf);
+    if (sl.snap) cudaEventDestroy(sl.snap);
     if (sl.done) cudaEventDestroy(sl.done);
   }
+  if (f->copy) cudaStreamDestroy(f->copy);
   delete f;
   return rc;
 }
