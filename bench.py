@@ -48,6 +48,7 @@ cpu_baseline: the reference itself (compiled from its sources into
 import argparse
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -389,6 +390,67 @@ def run_ours(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_frames(args, world, rank, local):
+    """Frame output around the force pass: per-step device time of a loop
+    of passes on the 2^20 Plummer sphere (tensor cores, fixed p) without
+    frames and with a device frame (fmm_frames_write_device) every
+    `frames_every` steps into a temporary directory, the final flush
+    included; and the host path's write rate."""
+    import tempfile
+
+    import torch
+
+    import fmmgpu
+    from fmmgpu import workloads
+
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.n
+    pos, mass = workloads.plummer(n, seed=2)
+    d_pos = torch.from_numpy(pos).to(dev)
+    d_mass = torch.from_numpy(mass).to(dev)
+    d_vel = torch.zeros_like(d_pos)
+    d_acc = torch.empty_like(d_pos)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    sp = stream.cuda_stream
+    ctx = fmmgpu.Context(dim=3, p=args.p, leaf_cap=args.leaf, G=1.0, device=local, m2l_mode=fmmgpu.FMM_M2L_TC)
+    out = tempfile.mkdtemp()
+
+    def loop(steps, frames):
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for s in range(steps):
+            ctx.evaluate_device(n, d_pos.data_ptr(), d_mass.data_ptr(), d_acc.data_ptr(), None, sp)
+            if frames is not None and s % args.frames_every == 0:
+                frames.write_device(n, d_pos.data_ptr(), d_vel.data_ptr(), d_mass.data_ptr(), s, 1e-3 * s,
+                                    acc_ptr=d_acc.data_ptr(), stream=sp)
+        ctx.synchronize()
+        if frames is not None:
+            frames.flush()
+        return (time.perf_counter() - t0) / steps * 1e3
+
+    loop(args.warmup, None)
+    plain = loop(args.steps, None)
+    with fmmgpu.Frames(os.path.join(out, "device")) as fr:
+        loop(args.warmup, fr)
+        framed = loop(args.steps, fr)
+    acc = d_acc.cpu().numpy()
+    vel = np.zeros_like(pos)
+    with fmmgpu.Frames(os.path.join(out, "host")) as fh:
+        t0 = time.perf_counter()
+        for s in range(3):
+            fh.write(pos, vel, mass, s, 1e-3 * s, acc=acc)
+        host_ms = (time.perf_counter() - t0) / 3 * 1e3
+    ctx.close()
+    shutil.rmtree(out, ignore_errors=True)
+    print(json.dumps({"mode": "frames", "n": n, "frame_bytes": 80 * n, "frames_every": args.frames_every,
+                      "steps": args.steps, "ms_per_step_without_frames": plain, "ms_per_step_with_frames": framed,
+                      "host_write_ms_per_frame": host_ms, "host_write_GBps": 80 * n / host_ms / 1e6}), flush=True)
+
+
 def run_ensemble(args, world, rank, local):
     """The batched-ensemble configuration: 256 independent Plummer spheres,
     N per system log-uniform in [1024, 65536] (seed 4), p = 8, leaf 64, all
@@ -557,6 +619,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ensemble", action="store_true", help="the batched-ensemble configuration instead")
+    ap.add_argument("--frames-every", type=int, default=0,
+                    help="measure frame output instead: a device frame every K steps of the pass loop")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
     if args.n is None:
@@ -566,6 +630,8 @@ def main():
         run_reference(args, world, rank)
     elif args.ensemble:
         run_ensemble(args, world, rank, local)
+    elif args.frames_every > 0:
+        run_frames(args, world, rank, local)
     else:
         run_ours(args, world, rank, local)
 
