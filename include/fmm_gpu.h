@@ -294,6 +294,17 @@ FMM_API int fmm_frames_write_device(fmm_frames *f, int64_t n, const double *d_po
 FMM_API int fmm_frames_flush(fmm_frames *f);
 FMM_API int fmm_frames_close(fmm_frames *f);
 
+/* The reference's simulation loop (main.cpp:85-91: write a frame, then
+ * integrate a step) with the state on the device: as fmm_integrate, and
+ * before each step s = 0, every, 2 every, ... a frame of the state through
+ * fmm_frames_write_device (step number step0 + s, time t0 + s dt; the
+ * acceleration of the last force evaluation, zeros before the first step).
+ * The frames overlap the following steps; the call flushes them before it
+ * returns. */
+FMM_API int fmm_integrate_frames(fmm_ctx *ctx, int32_t method, double dt, int32_t steps, int64_t n, double *pos,
+                                 double *vel, const double *mass, double *acc_out, fmm_frames *frames, int32_t every,
+                                 int32_t step0, double t0);
+
 /* Statistics of the last force pass (per-phase device times, sizes). */
 FMM_API int fmm_last_stats(fmm_ctx *ctx, fmm_stats *out);
 

@@ -558,10 +558,14 @@ int fmm_direct(fmm_ctx *c, int64_t n, const double *pos, const double *mass, int
   return FMM_OK;
 }
 
-int fmm_integrate(fmm_ctx *c, int32_t method, double dt, int32_t steps, int64_t n, double *pos, double *vel,
-                  const double *mass, double *acc_out) {
+// The integrator loop, optionally with a device frame of the state before
+// every `every`-th step (the reference's driver: main.cpp:85-91).
+static int integrate(fmm_ctx *c, int32_t method, double dt, int32_t steps, int64_t n, double *pos, double *vel,
+                     const double *mass, double *acc_out, fmm_frames *frames, int32_t every, int32_t step0,
+                     double t0) {
   if (!c || n < 0 || steps < 0 || (n > 0 && (!pos || !vel || !mass))) return FMM_ERR_INVALID_ARGUMENT;
   if (method != FMM_INT_SYMPLECTIC_EULER && method != FMM_INT_RK4) return FMM_ERR_INVALID_ARGUMENT;
+  if (frames && (every < 1 || step0 < 0)) return FMM_ERR_INVALID_ARGUMENT;
   if (n == 0 || steps == 0) return FMM_OK;
   CUDA_TRY(cudaSetDevice(c->cfg.device));
   const int dim = c->cfg.dim;
@@ -573,6 +577,10 @@ int fmm_integrate(fmm_ctx *c, int32_t method, double dt, int32_t steps, int64_t 
   double *x = c->d_pos.ptr, *v = c->d_vel.ptr, *a = c->d_acc.ptr;
   cudaStream_t st = c->stream;
   for (int s = 0; s < steps; ++s) {
+    if (frames && s % every == 0) {  // no acceleration before the first step: zeros
+      rc = fmm_frames_write_device(frames, n, x, v, s ? a : nullptr, c->d_mass.ptr, step0 + s, t0 + s * dt, st);
+      if (rc) return rc;
+    }
     if (method == FMM_INT_SYMPLECTIC_EULER) {
       rc = evaluate_device(c, n, x, c->d_mass.ptr, a, nullptr, st);
       if (rc) return rc;
@@ -601,7 +609,19 @@ int fmm_integrate(fmm_ctx *c, int32_t method, double dt, int32_t steps, int64_t 
   CUDA_TRY(cudaMemcpyAsync(vel, v, sizeof(double) * nd, cudaMemcpyDeviceToHost, st));
   if (acc_out) CUDA_TRY(cudaMemcpyAsync(acc_out, a, sizeof(double) * nd, cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
-  return FMM_OK;
+  return frames ? fmm_frames_flush(frames) : FMM_OK;
+}
+
+int fmm_integrate(fmm_ctx *c, int32_t method, double dt, int32_t steps, int64_t n, double *pos, double *vel,
+                  const double *mass, double *acc_out) {
+  return integrate(c, method, dt, steps, n, pos, vel, mass, acc_out, nullptr, 1, 0, 0.0);
+}
+
+int fmm_integrate_frames(fmm_ctx *c, int32_t method, double dt, int32_t steps, int64_t n, double *pos, double *vel,
+                         const double *mass, double *acc_out, fmm_frames *frames, int32_t every, int32_t step0,
+                         double t0) {
+  if (!frames) return FMM_ERR_INVALID_ARGUMENT;
+  return integrate(c, method, dt, steps, n, pos, vel, mass, acc_out, frames, every, step0, t0);
 }
 
 // ------------------------------------------------------------ tree export

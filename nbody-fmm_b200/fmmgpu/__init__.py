@@ -54,7 +54,7 @@ EXPORTED = (
     "fmm_tree_pairs", "fmm_last_stats", "fmm_launch_count", "fmm_direct_noalloc", "fmm_order_set_model",
     "fmm_order_get_model", "fmm_order_collect", "fmm_order_train", "fmm_order_forward_grad", "fmm_autotune",
     "fmm_evaluate_batched", "fmm_frames_open", "fmm_frames_write", "fmm_frames_write_device", "fmm_frames_flush",
-    "fmm_frames_close",
+    "fmm_frames_close", "fmm_integrate_frames",
 )
 
 
@@ -146,6 +146,8 @@ def load_library(path=LIB_PATH):
                                           _vp]
     L.fmm_frames_flush.argtypes = [_vp]
     L.fmm_frames_close.argtypes = [_vp]
+    L.fmm_integrate_frames.argtypes = [_vp, ctypes.c_int32, ctypes.c_double, ctypes.c_int32, ctypes.c_int64, _d, _d,
+                                       _d, _d, _vp, ctypes.c_int32, ctypes.c_int32, ctypes.c_double]
     _lib = L
     return L
 
@@ -292,13 +294,19 @@ class Context:
         _check(_lib.fmm_direct_device(self._h, n, pos_ptr, mass_ptr, ntargets, targets_ptr, soft_mode, acc_ptr,
                                       pot_ptr, stream))
 
-    def integrate(self, method, dt, steps, pos, vel, mass):
-        """Advances (pos, vel) by `steps` steps; returns new pos, vel and the last acc."""
+    def integrate(self, method, dt, steps, pos, vel, mass, frames=None, every=1, step0=0, t0=0.0):
+        """Advances (pos, vel) by `steps` steps; returns new pos, vel and the
+        last acc.  With `frames` (a Frames), a frame of the state is written
+        before every `every`-th step (fmm_integrate_frames)."""
         pos, mass = self._arrays(pos, mass)
         pos = pos.copy()
         vel = np.array(vel, dtype=np.float64, order="C", copy=True)
         acc = np.zeros_like(pos)
-        _check(_lib.fmm_integrate(self._h, method, dt, steps, pos.shape[0], _p(pos), _p(vel), _p(mass), _p(acc)))
+        if frames is None:
+            _check(_lib.fmm_integrate(self._h, method, dt, steps, pos.shape[0], _p(pos), _p(vel), _p(mass), _p(acc)))
+        else:
+            _check(_lib.fmm_integrate_frames(self._h, method, dt, steps, pos.shape[0], _p(pos), _p(vel), _p(mass),
+                                             _p(acc), frames._h, every, step0, t0))
         return pos, vel, acc
 
     def tree(self, pos, with_pairs=True):

@@ -2,8 +2,9 @@
 HDF5Exporter (io/hdf5_exporter.cpp): the datasets of write_frame and the
 XDMF temporal index of write_xdmf_metadata, here with the datasets as raw
 little-endian FP64 in one .bin per frame.  CPU tests write from host
-arrays; the GPU test writes from device arrays through the asynchronous
-path and expects the same bytes."""
+arrays; the GPU tests write from device arrays through the asynchronous
+path and expect the same bytes, and check the integrator loop's frames
+against the states of plain integrator runs."""
 import os
 
 import numpy as np
@@ -110,3 +111,30 @@ def test_device_frames_match_host_frames(tmp_path):
         name = f"particles_{step:05d}.bin"
         assert (tmp_path / "dev" / name).read_bytes() == (tmp_path / "host" / name).read_bytes()
     assert (tmp_path / "dev" / "particles.xmf").read_text() == (tmp_path / "host" / "particles.xmf").read_text()
+
+
+@pytest.mark.gpu
+def test_integrate_frames_writes_the_state_before_each_step(tmp_path):
+    """The reference's loop (main.cpp:85-91): frame k is the state after k
+    steps, with the acceleration of the last force evaluation (zeros before
+    the first step); checked against plain fmm_integrate runs of k steps."""
+    from fmmgpu import workloads
+
+    n, dt, steps = 2000, 1e-3, 3
+    pos0, m = workloads.plummer(n, seed=8)
+    vel0 = np.zeros_like(pos0)
+    with fmmgpu.Context(dim=3, p=8, leaf_cap=64, G=1.0) as c:
+        with fmmgpu.Frames(str(tmp_path), dim=3) as fr:
+            c.integrate(fmmgpu.FMM_INT_SYMPLECTIC_EULER, dt, steps, pos0, vel0, m, frames=fr, every=1, step0=10,
+                        t0=0.5)
+        want = [(pos0, vel0, np.zeros_like(pos0))]
+        for k in range(1, steps):
+            want.append(c.integrate(fmmgpu.FMM_INT_SYMPLECTIC_EULER, dt, k, pos0, vel0, m))
+    for k, (wp, wv, wa) in enumerate(want):
+        p, v, a, w = read_frame(tmp_path / f"particles_{10 + k:05d}.bin", n)
+        np.testing.assert_allclose(p, wp, rtol=1e-6, atol=1e-12)
+        np.testing.assert_allclose(v, wv, rtol=1e-6, atol=1e-9)
+        np.testing.assert_allclose(a, wa, rtol=1e-6, atol=1e-6 * np.abs(wa).max() + 1e-300)
+        np.testing.assert_array_equal(w, m)
+    idx = (tmp_path / "particles.xmf").read_text()
+    assert idx == expected_index([(0.5 + k * dt, f"particles_{10 + k:05d}.bin", n) for k in range(steps)])
