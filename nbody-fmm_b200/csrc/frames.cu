@@ -119,7 +119,7 @@ int write_index(const fmm_frames *f) {
 // (hdf5_exporter.cpp:29-44), then the weights; then the index.  The caller
 // holds no lock; only the writer thread or a synchronous write (after a
 // flush) runs this, so frames stay in order.
-int write_frame(fmm_frames *f, int64_t n, const double *pos, const double *vel, const double *acc,
+int write_frame_unguarded(fmm_frames *f, int64_t n, const double *pos, const double *vel, const double *acc,
                 const double *mass, int step, double time) {
   if (n <= 0) return FMM_OK;  // hdf5_exporter.cpp:22
   const int dim = f->dim;
@@ -146,6 +146,20 @@ int write_frame(fmm_frames *f, int64_t n, const double *pos, const double *vel, 
   f->names.push_back(name);
   f->counts.push_back(n);
   return write_index(f);
+}
+
+// The same with allocation failures (strings, buffers, the frame lists)
+// turned into a status: nothing may throw across the C ABI or out of the
+// writer thread.
+int write_frame(fmm_frames *f, int64_t n, const double *pos, const double *vel, const double *acc,
+                const double *mass, int step, double time) {
+  try {
+    return write_frame_unguarded(f, n, pos, vel, acc, mass, step, time);
+  } catch (const std::bad_alloc &) {
+    return FMM_ERR_OUT_OF_MEMORY;
+  } catch (...) {
+    return FMM_ERR_INTERNAL;
+  }
 }
 
 void writer_loop(fmm_frames *f) {
@@ -188,10 +202,10 @@ int fmm_frames_open(const char *dir, const char *base, int32_t dim, fmm_frames *
   if (mkdir(dir, 0755) != 0 && errno != EEXIST) return FMM_ERR_IO;  // hdf5_exporter.cpp:12
   fmm_frames *f = new (std::nothrow) fmm_frames;
   if (!f) return FMM_ERR_OUT_OF_MEMORY;
-  f->dir = dir;
-  f->base = base;
-  f->dim = dim;
   try {
+    f->dir = dir;
+    f->base = base;
+    f->dim = dim;
     f->writer = std::thread(writer_loop, f);
   } catch (...) {
     delete f;
