@@ -78,6 +78,34 @@ def workload_desc(n, p, leaf, m2l, direct_max=None, mixture=False):
     }
 
 
+def max_over_ranks(x, world, dev):
+    """The largest x over the ranks (the slowest rank's time); x on one rank."""
+    if world <= 1:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def min_over_ranks(x, world, dev):
+    """The smallest x over the ranks (the slowest rank's rate); x on one rank."""
+    if world <= 1:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MIN)
+    return float(t.item())
+
+
+def job_rate(particles_per_rank, steps, world, seconds):
+    """Whole-job particles/s: the particles of every rank's steps over the
+    slowest rank's time."""
+    return particles_per_rank * steps * world / seconds
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -260,12 +288,8 @@ def run_ours(args, world, rank, local):
     time.sleep(0.3)
     step_ms, stats, launches = _timed(ctx, n, d_pos, d_mass, d_acc, stream, flush, args.steps, args.warmup, barrier)
     clocks = sampler.stop()
-    total_ms = float(sum(step_ms))
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = n * args.steps * world / (total_ms / 1e3)
+    total_ms = max_over_ranks(float(sum(step_ms)), world, dev)
+    value = job_rate(n, args.steps, world, total_ms / 1e3)
     err = _error(ctx, n, d_pos, d_mass, d_acc, d_pot, stream, dev, judge)
 
     # end to end through the C ABI with pinned host buffers
@@ -282,11 +306,7 @@ def run_ours(args, world, rank, local):
         t0 = time.perf_counter()
         ctx.evaluate(hp, hm, out=ha)
         e2e_s += time.perf_counter() - t0
-    e2e_val = n * e2e_steps * world / e2e_s
-    if world > 1:
-        t = torch.tensor([e2e_val / world], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MIN)
-        e2e_val = float(t.item()) * world
+    e2e_val = min_over_ranks(job_rate(n, e2e_steps, 1, e2e_s), world, dev) * world
     ctx.close()
 
     # rooflines of the two largest kernels, from the live event timings
@@ -367,14 +387,10 @@ def run_ours(args, world, rank, local):
             chosen = {"direct_max": b["direct_max"], "leaf_cap": b["leaf_cap"]}
         psteps = max(3, args.steps // 2)
         pms, pst, _ = _timed(pc, n, d_pos, d_mass, d_acc, stream, flush, psteps, max(1, args.warmup), barrier)
-        ptot = float(sum(pms))
-        if world > 1:
-            t = torch.tensor([ptot], dtype=torch.float64, device=dev)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ptot = float(t.item())
+        ptot = max_over_ranks(float(sum(pms)), world, dev)
         perr = _error(pc, n, d_pos, d_mass, d_acc, d_pot, stream, dev, judge)
         pc.close()
-        return {"m2l": label, "value": n * psteps * world / (ptot / 1e3), "unit": UNIT, "steps": psteps,
+        return {"m2l": label, "value": job_rate(n, psteps, world, ptot / 1e3), "unit": UNIT, "steps": psteps,
                 "ms_per_step": ptot / psteps, "error": perr, "phases_ms": _phases(pst), "tuned": chosen}
 
     if not args.no_plain and mode == fmmgpu.FMM_M2L_TC:
