@@ -3,8 +3,9 @@
 // Include this header in the reference's own build (its src/ directory on
 // the include path) and link libfmmgpu.so:
 //
-//   GpuFMM          replaces FMM          (src/system_updaters/FMM.cpp:9-12)
-//   GpuNaiveUpdate  replaces NaiveUpdate  (src/system_updaters/naive_update.cpp:9-35)
+//   GpuFMM            replaces FMM           (src/system_updaters/FMM.cpp:9-12)
+//   GpuNaiveUpdate    replaces NaiveUpdate   (src/system_updaters/naive_update.cpp:9-35)
+//   GpuFrameExporter  replaces HDF5Exporter  (src/io/hdf5_exporter.cpp:10-128)
 //
 // Both derive from the reference's SystemUpdateMethod
 // (system_update_method.hpp:24-31), so QuadratureMethod::integrate and the
@@ -130,4 +131,41 @@ class GpuNaiveUpdate : public SystemUpdateMethod {
  private:
   fmm_b200::ContextCache cache_;
   std::vector<double> pos_, mass_, grad_;
+};
+
+// Frame output with HDF5Exporter's interface (hdf5_exporter.hpp:20-49): the
+// same datasets per step and the same XDMF time series, the datasets stored
+// as raw FP64 in one .bin per step (fmm_frames_*: no libhdf5).  The writer
+// opens at the first frame, which fixes the dimension.
+class GpuFrameExporter {
+ public:
+  explicit GpuFrameExporter(const std::string &dir = "output", const std::string &base = "particles")
+      : dir_(dir), base_(base) {}
+  GpuFrameExporter(const GpuFrameExporter &) = delete;
+  GpuFrameExporter &operator=(const GpuFrameExporter &) = delete;
+  ~GpuFrameExporter() {
+    if (f_) fmm_frames_close(f_);
+  }
+  void write_frame(const std::vector<Particle> &particles, int step, double time) {
+    if (particles.empty()) return;  // hdf5_exporter.cpp:22
+    const int dim = fmm_b200::pack(particles, pos_, mass_);
+    if (!f_) fmm_b200::check(fmm_frames_open(dir_.c_str(), base_.c_str(), dim, &f_), "fmm_frames_open");
+    vel_.resize(pos_.size());
+    acc_.resize(pos_.size());
+    for (size_t i = 0; i < particles.size(); ++i) {
+      const Tensor &v = particles[i].get_velocity(), &a = particles[i].get_acceleration();
+      for (int d = 0; d < dim; ++d) {
+        vel_[i * dim + d] = v[d];
+        acc_[i * dim + d] = a[d];
+      }
+    }
+    fmm_b200::check(fmm_frames_write(f_, (int64_t)particles.size(), pos_.data(), vel_.data(), acc_.data(),
+                                     mass_.data(), step, time),
+                    "fmm_frames_write");
+  }
+
+ private:
+  std::string dir_, base_;
+  fmm_frames *f_ = nullptr;
+  std::vector<double> pos_, vel_, acc_, mass_;
 };

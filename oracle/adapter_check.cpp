@@ -2,11 +2,13 @@
 // nbody-fmm_b200/cpp/gpu_fmm.hpp plugged into the reference's classes
 // (Particle, SystemUpdateMethod, SyplecticEuler, NaiveUpdate), compiled
 // against the reference's headers and objects.  TEST INFRASTRUCTURE: built
-// by oracle/Makefile into _ref/adapter_check, run by tests/test_gpu_adapter.py.
-// Exit status 0 = every check passed.
+// by oracle/Makefile into _ref/adapter_check, run by tests/test_gpu_adapter.py
+// (GPU checks) and tests/test_frames.py (`adapter_check frames <dir>`: the
+// frame exporter alone, no GPU).  Exit status 0 = every check passed.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 #include "gpu_fmm.hpp"
@@ -74,7 +76,46 @@ static void fmm_vs_naive_3d() {
   CHECK(std::sqrt(num / den) < 1e-12, "GpuNaiveUpdate vs NaiveUpdate: rel L2 %.3e", std::sqrt(num / den));
 }
 
-int main() {
+// The reference driver's frame loop (main.cpp:85-91) with GpuFrameExporter
+// in place of HDF5Exporter: three frames of 3D particles whose velocities
+// and accelerations are set; each .bin holds position, velocity,
+// acceleration (n x 3) and weight (n) as the particles have them.
+static void frames(const char *dir) {
+  std::vector<Particle> ps = make3d(50);
+  {
+    GpuFrameExporter ex(dir, "particles");
+    for (int step = 0; step < 3; ++step) {
+      for (size_t i = 0; i < ps.size(); ++i) {
+        Tensor g(3);
+        for (int d = 0; d < 3; ++d) g[d] = 0.01 * (double)(i + d + step);
+        ps[i].compute_new_accelaration(g);
+      }
+      ex.write_frame(ps, step, 0.5 * step);
+      const std::string path = std::string(dir) + "/particles_0000" + std::to_string(step) + ".bin";
+      std::FILE *fp = std::fopen(path.c_str(), "rb");
+      CHECK(fp != nullptr, "frames: %s missing", path.c_str());
+      if (!fp) continue;
+      const size_t n = ps.size();
+      std::vector<double> buf(10 * n);
+      CHECK(std::fread(buf.data(), sizeof(double), buf.size(), fp) == buf.size(), "frames: %s short", path.c_str());
+      std::fclose(fp);
+      for (size_t i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) {
+          CHECK(buf[3 * i + d] == ps[i].get_position()[d], "frames: position %zu %d", i, d);
+          CHECK(buf[3 * n + 3 * i + d] == ps[i].get_velocity()[d], "frames: velocity %zu %d", i, d);
+          CHECK(buf[6 * n + 3 * i + d] == ps[i].get_acceleration()[d], "frames: acceleration %zu %d", i, d);
+        }
+      for (size_t i = 0; i < n; ++i) CHECK(buf[9 * n + i] == ps[i].get_weight(), "frames: weight %zu", i);
+    }
+  }
+}
+
+int main(int argc, char **argv) {
+  if (argc == 3 && std::string(argv[1]) == "frames") {
+    frames(argv[2]);
+    std::fprintf(stderr, "%d failure(s)\n", failures);
+    return failures ? 1 : 0;
+  }
   two_bodies();
   fmm_vs_naive_3d();
   std::fprintf(stderr, "%d failure(s)\n", failures);

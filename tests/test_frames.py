@@ -6,9 +6,11 @@ arrays; the GPU tests write from device arrays through the asynchronous
 path and expect the same bytes, and check the integrator loop's frames
 against the states of plain integrator runs."""
 import os
+import subprocess
 
 import numpy as np
 import pytest
+from conftest import ROOT
 
 import fmmgpu
 
@@ -86,6 +88,20 @@ def test_frames_errors(tmp_path):
     with pytest.raises(fmmgpu.FmmError) as e:
         fmmgpu.Frames(str(blocker / "sub"))
     assert e.value.code == fmmgpu.FMM_ERR_IO
+
+
+def test_exporter_drop_in_for_the_reference_driver(tmp_path):
+    """GpuFrameExporter (nbody-fmm_b200/cpp/gpu_fmm.hpp), HDF5Exporter's
+    interface, compiled against the reference's Particle: three frames of
+    the reference's own particles, datasets checked by the program itself
+    (oracle/adapter_check.cpp), the index here."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "adapter_check")
+    if not os.path.exists(exe):
+        pytest.skip("the reference is not built here (oracle/_ref)")
+    r = subprocess.run([exe, "frames", str(tmp_path)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr[-2000:]
+    want = [(0.5 * k, f"particles_{k:05d}.bin", 50) for k in range(3)]
+    assert (tmp_path / "particles.xmf").read_text() == expected_index(want)
 
 
 @pytest.mark.gpu
