@@ -62,7 +62,7 @@ sys.path.insert(0, os.path.join(ROOT, "nbody-fmm_b200"))
 METRIC = "3D FMM particles/s at 1e-6 rel force err: learned+TC vs plain GPU FMM"
 UNIT = "particles/s"
 REF_SAMPLE_N = 512           # particles per reference process per step (about 2 s at p = 12)
-BASELINE_SAMPLE_N = 2048     # single-thread CPU baseline sample (about 20 s at p = 12)
+CPU_SAMPLE_N = 2048     # single-thread CPU baseline sample (about 20 s at p = 12)
 
 
 def workload_desc(n, p, leaf, m2l, direct_max=None, mixture=False):
@@ -570,12 +570,12 @@ def cpu_baseline(p, leaf, mixture=False):
     """The reference FMM::update, single thread, on a bounded sample."""
     seed = 5 if mixture else 2
     try:
-        dt = _ref_worker((BASELINE_SAMPLE_N, p, leaf, seed, mixture))
+        dt = _ref_worker((CPU_SAMPLE_N, p, leaf, seed, mixture))
     except Exception as e:  # reference build missing
         return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"unavailable: {e}"}
     inputs = "Plummer mixture" if mixture else "Plummer"
-    return {"value": BASELINE_SAMPLE_N / dt, "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": f"reference FMM::update (oracle/_ref, g++ -O2), {inputs} N={BASELINE_SAMPLE_N} seed {seed}, "
+    return {"value": CPU_SAMPLE_N / dt, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"reference FMM::update (oracle/_ref, g++ -O2), {inputs} N={CPU_SAMPLE_N} seed {seed}, "
                       f"p={p}, leaf capacity {leaf}, 1 thread, {dt:.1f} s"}
 
 

@@ -3,8 +3,8 @@ reference fixtures.  Tolerances:
   - tree build: bit-exact (depth, leaf keys, membership order, lists);
   - FP64 direct sum: 1e-12 relative to the CPU FP64 sum;
   - FMM in FP32 mode vs the FP64 oracle FMM with the same p, leaf capacity
-    and direct-pair rule: relative L2 force error <= 1e-6 (the north-star
-    bar); largest per-particle error <= 2e-5 of the RMS acceleration;
+    and direct-pair rule: relative L2 force error <= 1e-6 (the bar for the
+    FP32 mode); largest per-particle error <= 2e-5 of the RMS acceleration;
   - FMM vs FP64 direct sum: within 1.5x the oracle's own truncation error
     plus 1e-6.
 """
