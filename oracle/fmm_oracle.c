@@ -737,3 +737,231 @@ int orc_fmm_ex(int dim, int64_t n, const double *pos, const double *mass, unsign
   orc_tree_free(t);
   return 0;
 }
+
+/* ------------------------------------------------------- adaptive targets */
+/* M2P: the multipole M (centre c) evaluated at a point r = x - c, through
+ * the order-0 and order-1 local coefficients at x (M2L to the point, then
+ * L2P at offset zero); g and phi accumulate. */
+static void m2p_3d(int p, const cplx *M, const double *r, double *g, double *phi, cplx *S, cplx *Lw, cplx *R) {
+  irregular_s(p + 1, r, S);
+  for (int q = 0; q < 3; ++q) Lw[q] = 0;
+  for (int k = 0; k <= 1; ++k)
+    for (int l = 0; l <= k; ++l) {
+      cplx s = 0;
+      for (int n = 0; n <= p; ++n)
+        for (int m = -n; m <= n; ++m) s += hget(M, n, m) * hget(S, n + k, m - l);
+      Lw[hidx(k, l)] = ((k + l) & 1) ? -s : s;
+    }
+  const double zero[3] = {0, 0, 0};
+  l2p_3d(1, Lw, zero, g, phi, R);
+}
+
+/* An FMM whose targets stop descending at small cells, the adaptive form
+ * of the uniform-depth tree of orc_tree_build (3D, geometric centres).
+ *
+ * Every cell of the uniform tree stays a source.  A target cell is active
+ * if it is the root or its parent is active and holds more than `aleaf`
+ * particles; an active cell with at most `aleaf` particles, or at depth D,
+ * is an adaptive leaf.  A particle of an adaptive leaf B at level d gets the
+ * interaction lists of B and of its ancestors (M2L into active cells, L2L
+ * down active cells, L2P from B) and, directly, the particles of B's
+ * colleagues at level d.  Those pairs, at all deeper levels and in the leaf
+ * level's near field, are exactly what the uniform FMM sums below level d.
+ * A colleague cell C is summed particle by particle when
+ * n_B n_C <= w_direct_max or C is at depth D; otherwise its children are
+ * taken in its place: a child too close to B (touching it, or its radius
+ * over its distance from B's box above 0.75) again as a colleague, a child
+ * farther away through its multipole evaluated at B's particles (M2P; the
+ * W list of the adaptive FMM), or directly when n_B n_child <= w_direct_max.
+ * Interaction-list pairs follow orc_fmm_ex's rules (direct_max, separation).
+ */
+int orc_fmm_adaptive(int dim, int64_t n, const double *pos, const double *mass, unsigned p_, unsigned threshold,
+                     unsigned aleaf, double eps2, int64_t direct_max, int64_t w_direct_max, double *grad,
+                     double *pot) {
+  if (dim != 3) return -2;
+  orc_tree *t = orc_tree_build(dim, n, pos, threshold);
+  if (!t) return -1;
+  const int p = (int)p_, D = t->depth;
+  const int K = (p + 1) * (p + 2) / 2, KW = (2 * p + 2) * (2 * p + 3) / 2;
+  cplx *work = (cplx *)malloc(sizeof(cplx) * KW), *work2 = (cplx *)malloc(sizeof(cplx) * KW);
+  cplx Lw[3];
+  double ext[3];
+  for (int a = 0; a < 3; ++a) ext[a] = t->hi[a] - t->lo[a];
+  double **cen = (double **)calloc(D + 1, sizeof(double *));
+  cplx **M = (cplx **)calloc(D + 1, sizeof(cplx *)), **Lx = (cplx **)calloc(D + 1, sizeof(cplx *));
+  int64_t **pb = (int64_t **)calloc(D + 1, sizeof(int64_t *)), **pe = (int64_t **)calloc(D + 1, sizeof(int64_t *));
+  int64_t **par = (int64_t **)calloc(D + 1, sizeof(int64_t *));
+  char **act = (char **)calloc(D + 1, sizeof(char *)), **leaf = (char **)calloc(D + 1, sizeof(char *));
+  for (int d = 0; d <= D; ++d) {
+    const int64_t m = t->ncell[d];
+    cen[d] = (double *)calloc(m * 3, sizeof(double));
+    M[d] = (cplx *)calloc(m * K, sizeof(cplx));
+    Lx[d] = (cplx *)calloc(m * K, sizeof(cplx));
+    pb[d] = (int64_t *)malloc(sizeof(int64_t) * m);
+    pe[d] = (int64_t *)malloc(sizeof(int64_t) * m);
+    par[d] = (int64_t *)malloc(sizeof(int64_t) * m);
+    act[d] = (char *)calloc(m, 1);
+    leaf[d] = (char *)calloc(m, 1);
+  }
+  for (int d = D; d >= 0; --d)
+    for (int64_t i = 0; i < t->ncell[d]; ++i) {
+      if (d == D) { pb[d][i] = t->leaf_start[i]; pe[d][i] = t->leaf_start[i + 1]; }
+      else {
+        pb[d][i] = pb[d + 1][t->cbeg[d][i]];
+        pe[d][i] = pe[d + 1][t->cend[d][i] - 1];
+        for (int64_t ch = t->cbeg[d][i]; ch < t->cend[d][i]; ++ch) par[d + 1][ch] = i;
+      }
+    }
+  par[0][0] = -1;
+  /* geometric centres, P2M at depth D, M2M up */
+  for (int d = D; d >= 0; --d)
+    for (int64_t i = 0; i < t->ncell[d]; ++i) {
+      double *c = cen[d] + 3 * i;
+      uint32_t q[3] = {0, 0, 0};
+      orc_morton_decode(t->keys[d][i], 3, q);
+      for (int a = 0; a < 3; ++a) c[a] = t->lo[a] + (q[a] + 0.5) * (ext[a] / (double)((uint64_t)1 << d));
+      cplx *Mi = M[d] + (int64_t)K * i;
+      if (d == D) {
+        for (int64_t k = pb[d][i]; k < pe[d][i]; ++k) {
+          const int64_t j = t->perm[k];
+          double r[3] = {pos[3 * j] - c[0], pos[3 * j + 1] - c[1], pos[3 * j + 2] - c[2]};
+          regular_s(p, r, work);
+          for (int qq = 0; qq < K; ++qq) Mi[qq] += mass[j] * conj(work[qq]);
+        }
+      } else {
+        for (int64_t ch = t->cbeg[d][i]; ch < t->cend[d][i]; ++ch) {
+          double tv[3];
+          for (int a = 0; a < 3; ++a) tv[a] = cen[d + 1][3 * ch + a] - c[a];
+          m2m_3d(p, M[d + 1] + (int64_t)K * ch, tv, Mi, work);
+        }
+      }
+    }
+  /* active target cells and adaptive leaves */
+  for (int d = 0; d <= D; ++d)
+    for (int64_t i = 0; i < t->ncell[d]; ++i) {
+      const int64_t cnt = pe[d][i] - pb[d][i];
+      act[d][i] = d == 0 ? 1 : (act[d - 1][par[d][i]] && !leaf[d - 1][par[d][i]]);
+      leaf[d][i] = act[d][i] && (cnt <= (int64_t)aleaf || d == D);
+    }
+  double *fd = (double *)calloc((size_t)n * 4, sizeof(double));
+  /* interaction lists of the active targets: M2L, or direct (orc_fmm_ex's rules) */
+  for (int d = 0; d <= D; ++d)
+    for (int64_t i = 0; i < t->ncell[d]; ++i) {
+      if (!act[d][i]) continue;
+      for (int64_t k = t->il_off[d][i]; k < t->il_off[d][i + 1]; ++k) {
+        const int64_t s = t->il_idx[d][k];
+        if ((direct_max > 0 && (pe[d][i] - pb[d][i]) * (pe[d][s] - pb[d][s]) <= direct_max) ||
+            orc_not_well_separated(3, t->keys[d][i], t->keys[d][s], ext)) {
+          for (int64_t a = pb[d][i]; a < pe[d][i]; ++a) {
+            const int64_t pi = t->perm[a];
+            for (int64_t b = pb[d][s]; b < pe[d][s]; ++b) {
+              const int64_t pj = t->perm[b];
+              pair_kernel(3, pos + pi * 3, pos + pj * 3, mass[pj], eps2, fd + 4 * pi, fd + 4 * pi + 3);
+            }
+          }
+          continue;
+        }
+        double r[3];
+        for (int a = 0; a < 3; ++a) r[a] = cen[d][3 * i + a] - cen[d][3 * s + a];
+        m2l_3d(p, M[d] + (int64_t)K * s, r, Lx[d] + (int64_t)K * i, work);
+      }
+    }
+  /* L2L down the active cells */
+  for (int d = 0; d < D; ++d)
+    for (int64_t i = 0; i < t->ncell[d]; ++i) {
+      if (!act[d][i] || leaf[d][i]) continue;
+      for (int64_t ch = t->cbeg[d][i]; ch < t->cend[d][i]; ++ch) {
+        double tv[3];
+        for (int a = 0; a < 3; ++a) tv[a] = cen[d + 1][3 * ch + a] - cen[d][3 * i + a];
+        l2l_3d(p, Lx[d] + (int64_t)K * i, tv, Lx[d + 1] + (int64_t)K * ch, work);
+      }
+    }
+  /* adaptive leaves: L2P, then the colleagues' particles (with the W list) */
+  int64_t cap = 1024, top = 0;
+  int64_t *stk = (int64_t *)malloc(sizeof(int64_t) * 2 * cap);
+  for (int d = 0; d <= D; ++d)
+    for (int64_t b = 0; b < t->ncell[d]; ++b) {
+      if (!leaf[d][b]) continue;
+      const int64_t nB = pe[d][b] - pb[d][b];
+      const double *cb = cen[d] + 3 * b;
+      double hb[3];
+      for (int a = 0; a < 3; ++a) hb[a] = 0.5 * ext[a] / (double)((uint64_t)1 << d);
+      for (int64_t k = pb[d][b]; k < pe[d][b]; ++k) {
+        const int64_t pi = t->perm[k];
+        double u[3] = {pos[3 * pi] - cb[0], pos[3 * pi + 1] - cb[1], pos[3 * pi + 2] - cb[2]};
+        double *g = fd + 4 * pi;
+        l2p_3d(p, Lx[d] + (int64_t)K * b, u, g, g + 3, work);
+        for (int64_t kk = pb[d][b]; kk < pe[d][b]; ++kk) {  /* the leaf itself */
+          const int64_t pj = t->perm[kk];
+          if (pj != pi) pair_kernel(3, pos + pi * 3, pos + pj * 3, mass[pj], eps2, g, g + 3);
+        }
+      }
+      top = 0;
+      for (int64_t k = t->nb_off[d][b]; k < t->nb_off[d][b + 1]; ++k) {
+        stk[2 * top] = d;
+        stk[2 * top + 1] = t->nb_idx[d][k];
+        ++top;
+      }
+      while (top > 0) {
+        --top;
+        const int e = (int)stk[2 * top];
+        const int64_t C = stk[2 * top + 1];
+        const int64_t nC = pe[e][C] - pb[e][C];
+        if (e == D || nB * nC <= w_direct_max) {
+          for (int64_t k = pb[d][b]; k < pe[d][b]; ++k) {
+            const int64_t pi = t->perm[k];
+            for (int64_t kk = pb[e][C]; kk < pe[e][C]; ++kk) {
+              const int64_t pj = t->perm[kk];
+              pair_kernel(3, pos + pi * 3, pos + pj * 3, mass[pj], eps2, fd + 4 * pi, fd + 4 * pi + 3);
+            }
+          }
+          continue;
+        }
+        for (int64_t ch = t->cbeg[e][C]; ch < t->cend[e][C]; ++ch) {
+          const double *cc = cen[e + 1] + 3 * ch;
+          double dist2 = 0.0, rad2 = 0.0;
+          for (int a = 0; a < 3; ++a) {
+            const double hc = 0.5 * ext[a] / (double)((uint64_t)1 << (e + 1));
+            const double gap = fabs(cc[a] - cb[a]) - hb[a];
+            if (gap > 0) dist2 += gap * gap;
+            rad2 += hc * hc;
+          }
+          const int64_t nc = pe[e + 1][ch] - pb[e + 1][ch];
+          if (dist2 <= 0.0 || rad2 > 0.75 * 0.75 * dist2) {  /* too close: a colleague again */
+            if (top + 1 > cap) {
+              cap *= 2;
+              stk = (int64_t *)realloc(stk, sizeof(int64_t) * 2 * cap);
+            }
+            stk[2 * top] = e + 1;
+            stk[2 * top + 1] = ch;
+            ++top;
+          } else if (nB * nc <= w_direct_max) {
+            for (int64_t k = pb[d][b]; k < pe[d][b]; ++k) {
+              const int64_t pi = t->perm[k];
+              for (int64_t kk = pb[e + 1][ch]; kk < pe[e + 1][ch]; ++kk) {
+                const int64_t pj = t->perm[kk];
+                pair_kernel(3, pos + pi * 3, pos + pj * 3, mass[pj], eps2, fd + 4 * pi, fd + 4 * pi + 3);
+              }
+            }
+          } else {
+            for (int64_t k = pb[d][b]; k < pe[d][b]; ++k) {
+              const int64_t pi = t->perm[k];
+              double r[3] = {pos[3 * pi] - cc[0], pos[3 * pi + 1] - cc[1], pos[3 * pi + 2] - cc[2]};
+              m2p_3d(p, M[e + 1] + (int64_t)K * ch, r, fd + 4 * pi, fd + 4 * pi + 3, work, Lw, work2);
+            }
+          }
+        }
+      }
+    }
+  for (int64_t i = 0; i < n; ++i) {
+    for (int a = 0; a < 3; ++a) grad[3 * i + a] = fd[4 * i + a];
+    if (pot) pot[i] = fd[4 * i + 3];
+  }
+  free(stk);
+  for (int d = 0; d <= D; ++d) {
+    free(cen[d]); free(M[d]); free(Lx[d]); free(pb[d]); free(pe[d]); free(par[d]); free(act[d]); free(leaf[d]);
+  }
+  free(cen); free(M); free(Lx); free(pb); free(pe); free(par); free(act); free(leaf); free(work); free(work2); free(fd);
+  orc_tree_free(t);
+  return 0;
+}

@@ -57,6 +57,8 @@ class Oracle:
         L.orc_fmm.argtypes = [ctypes.c_int, ctypes.c_int64, _d, _d, ctypes.c_uint, ctypes.c_uint, ctypes.c_int, _d, _d]
         L.orc_fmm_ex.argtypes = [ctypes.c_int, ctypes.c_int64, _d, _d, ctypes.c_uint, ctypes.c_uint, ctypes.c_int,
                                  ctypes.c_double, ctypes.c_int64, _d, _d]
+        L.orc_fmm_adaptive.argtypes = [ctypes.c_int, ctypes.c_int64, _d, _d, ctypes.c_uint, ctypes.c_uint,
+                                       ctypes.c_uint, ctypes.c_double, ctypes.c_int64, ctypes.c_int64, _d, _d]
         for f in ("orc_regular_scaled", "orc_irregular_scaled", "orc_regular_racah", "orc_irregular_racah"):
             getattr(L, f).argtypes = [ctypes.c_uint, _d, _d]
         L.orc_p2m_3d.argtypes = [ctypes.c_uint, ctypes.c_int64, _d, _d, _d, _d]
@@ -140,6 +142,24 @@ class Oracle:
                                _p(g, _d), _p(pot, _d))
         if rc != 0:
             raise ValueError("orc_fmm failed")
+        return (g, pot) if want_pot else g
+
+    def fmm_adaptive(self, pos, mass, p, threshold, aleaf=None, want_pot=False, eps2=0.0, direct_max=0,
+                     w_direct_max=0):
+        """FMM with adaptive targets on the uniform tree (3D): targets stop at
+        cells of at most `aleaf` (default: threshold) particles and sum their
+        colleagues' particles directly, larger colleagues through their
+        children's multipoles where far enough (orc_fmm_adaptive)."""
+        pos = _f64(pos)
+        mass = _f64(mass)
+        n, dim = pos.shape
+        g = np.zeros((n, dim))
+        pot = np.zeros(n) if want_pot else None
+        rc = self.L.orc_fmm_adaptive(dim, n, _p(pos, _d), _p(mass, _d), p, threshold,
+                                     threshold if aleaf is None else aleaf, eps2, direct_max, w_direct_max,
+                                     _p(g, _d), _p(pot, _d))
+        if rc != 0:
+            raise ValueError("orc_fmm_adaptive failed")
         return (g, pot) if want_pot else g
 
     # ---- harmonics

@@ -192,3 +192,31 @@ def test_oracle_converges_on_an_elongated_box(oracle):
     ref = oracle.direct(pos, m)
     errs = [rel_l2(oracle.fmm(pos, m, p, 64), ref) for p in (4, 8, 12)]
     assert errs[0] > errs[1] > errs[2] and errs[2] < 2e-6, errs
+
+
+@pytest.mark.parametrize("gen,n,T", [("plummer", 3000, 16), ("plummer_mixture", 4000, 16), ("uniform3d", 2000, 8)])
+def test_adaptive_targets_partition_the_pairs_exactly(oracle, gen, n, T):
+    """orc_fmm_adaptive with every interaction-list pair and every W-list
+    child summed directly is the direct sum: the adaptive leaves' lists and
+    colleague sums cover every pair exactly once."""
+    pos, m = workloads.WORKLOADS[gen](n, seed=3)
+    d, pd = oracle.direct(pos, m, want_pot=True)
+    big = 10 ** 18
+    g, pg = oracle.fmm_adaptive(pos, m, 4, T, direct_max=big, w_direct_max=big, want_pot=True)
+    assert rel_l2(g, d) < 1e-12 and rel_l2(pg, pd) < 1e-12
+
+
+@pytest.mark.parametrize("gen,n,T", [("plummer", 3000, 16), ("plummer_mixture", 4000, 16)])
+def test_adaptive_targets_converge_like_the_uniform_fmm(oracle, gen, n, T):
+    """Adaptive targets (multipoles of far W-list children included) converge
+    with p, as accurately as the uniform-depth FMM with the same
+    direct-pair rule."""
+    pos, m = workloads.WORKLOADS[gen](n, seed=3)
+    d = oracle.direct(pos, m)
+    errs = []
+    for p in (4, 8, 12):
+        ga = oracle.fmm_adaptive(pos, m, p, T, direct_max=256, w_direct_max=256)
+        gu = oracle.fmm(pos, m, p, T, direct_max=256)
+        errs.append(rel_l2(ga, d))
+        assert errs[-1] < 1.5 * rel_l2(gu, d) + 1e-7, (p, errs[-1], rel_l2(gu, d))
+    assert errs[0] > errs[1] > errs[2]
