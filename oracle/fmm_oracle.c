@@ -547,6 +547,33 @@ static void l2l_2d(int p, const cplx *b, cplx z, cplx *out) {
   }
 }
 
+static void l2p_2d(int p, const cplx *b, cplx u, double *g, double *phi) {
+  cplx dphi = 0, up = 1, phic = b[0];
+  for (int q = 1; q <= p; ++q) {
+    dphi += (double)q * b[q] * up;
+    up *= u;
+    phic += b[q] * up;
+  }
+  g[0] -= creal(dphi);
+  g[1] += cimag(dphi);
+  *phi -= creal(phic);
+}
+
+/* M2P: the outer expansion w(z) = a_0 log z - sum_k a_k/(k z^k) at z = x - c,
+ * w'(z) = a_0/z + sum_k a_k/z^{k+1}; grad and phi as in L2P. */
+static void m2p_2d(int p, const cplx *a, cplx z, double *g, double *phi) {
+  const cplx iz = 1.0 / z;
+  cplx w = a[0] * clog(z), dw = a[0] * iz, izk = 1;
+  for (int k = 1; k <= p; ++k) {
+    izk *= iz;
+    w -= a[k] * izk / (double)k;
+    dw += a[k] * izk * iz;
+  }
+  g[0] -= creal(dw);
+  g[1] += cimag(dw);
+  *phi -= creal(w);
+}
+
 /* ------------------------------------------------------------ FMM driver */
 /* Tree::compute_accelerations, tree.cpp:93-111: P2M/M2M bottom-up, M2L over
  * every interaction list, L2L top-down, then per leaf L2P + P2P over the leaf
@@ -708,16 +735,7 @@ int orc_fmm_ex(int dim, int64_t n, const double *pos, const double *mass, unsign
         double u[3] = {pos[3 * pi] - c[0], pos[3 * pi + 1] - c[1], pos[3 * pi + 2] - c[2]};
         l2p_3d(p, Li, u, g, &ph, work);
       } else {
-        cplx u = (pos[2 * pi] - c[0]) + I * (pos[2 * pi + 1] - c[1]);
-        cplx dphi = 0, up = 1, phic = Li[0];
-        for (int q = 1; q <= p; ++q) {
-          dphi += (double)q * Li[q] * up;
-          up *= u;
-          phic += Li[q] * up;
-        }
-        g[0] -= creal(dphi);
-        g[1] += cimag(dphi);
-        ph -= creal(phic);
+        l2p_2d(p, Li, (pos[2 * pi] - c[0]) + I * (pos[2 * pi + 1] - c[1]), g, &ph);
       }
       /* near field: the leaf itself then its neighbours */
       for (int64_t nb = -1; nb < t->nb_off[D][i + 1] - t->nb_off[D][i]; ++nb) {
@@ -757,7 +775,7 @@ static void m2p_3d(int p, const cplx *M, const double *r, double *g, double *phi
 }
 
 /* An FMM whose targets stop descending at small cells, the adaptive form
- * of the uniform-depth tree of orc_tree_build (3D, geometric centres).
+ * of the uniform-depth tree of orc_tree_build (3D and 2D, geometric centres).
  *
  * Every cell of the uniform tree stays a source.  A target cell is active
  * if it is the root or its parent is active and holds more than `aleaf`
@@ -778,15 +796,15 @@ static void m2p_3d(int p, const cplx *M, const double *r, double *g, double *phi
 int orc_fmm_adaptive(int dim, int64_t n, const double *pos, const double *mass, unsigned p_, unsigned threshold,
                      unsigned aleaf, double eps2, int64_t direct_max, int64_t w_direct_max, double *grad,
                      double *pot) {
-  if (dim != 3) return -2;
+  if (dim != 2 && dim != 3) return -2;
   orc_tree *t = orc_tree_build(dim, n, pos, threshold);
   if (!t) return -1;
   const int p = (int)p_, D = t->depth;
-  const int K = (p + 1) * (p + 2) / 2, KW = (2 * p + 2) * (2 * p + 3) / 2;
+  const int K = dim == 3 ? (p + 1) * (p + 2) / 2 : p + 1, KW = (2 * p + 2) * (2 * p + 3) / 2;
   cplx *work = (cplx *)malloc(sizeof(cplx) * KW), *work2 = (cplx *)malloc(sizeof(cplx) * KW);
   cplx Lw[3];
-  double ext[3];
-  for (int a = 0; a < 3; ++a) ext[a] = t->hi[a] - t->lo[a];
+  double ext[3] = {0, 0, 0};
+  for (int a = 0; a < dim; ++a) ext[a] = t->hi[a] - t->lo[a];
   double **cen = (double **)calloc(D + 1, sizeof(double *));
   cplx **M = (cplx **)calloc(D + 1, sizeof(cplx *)), **Lx = (cplx **)calloc(D + 1, sizeof(cplx *));
   int64_t **pb = (int64_t **)calloc(D + 1, sizeof(int64_t *)), **pe = (int64_t **)calloc(D + 1, sizeof(int64_t *));
@@ -818,21 +836,27 @@ int orc_fmm_adaptive(int dim, int64_t n, const double *pos, const double *mass, 
     for (int64_t i = 0; i < t->ncell[d]; ++i) {
       double *c = cen[d] + 3 * i;
       uint32_t q[3] = {0, 0, 0};
-      orc_morton_decode(t->keys[d][i], 3, q);
-      for (int a = 0; a < 3; ++a) c[a] = t->lo[a] + (q[a] + 0.5) * (ext[a] / (double)((uint64_t)1 << d));
+      orc_morton_decode(t->keys[d][i], dim, q);
+      for (int a = 0; a < dim; ++a) c[a] = t->lo[a] + (q[a] + 0.5) * (ext[a] / (double)((uint64_t)1 << d));
       cplx *Mi = M[d] + (int64_t)K * i;
       if (d == D) {
         for (int64_t k = pb[d][i]; k < pe[d][i]; ++k) {
           const int64_t j = t->perm[k];
-          double r[3] = {pos[3 * j] - c[0], pos[3 * j + 1] - c[1], pos[3 * j + 2] - c[2]};
-          regular_s(p, r, work);
-          for (int qq = 0; qq < K; ++qq) Mi[qq] += mass[j] * conj(work[qq]);
+          if (dim == 3) {
+            double r[3] = {pos[3 * j] - c[0], pos[3 * j + 1] - c[1], pos[3 * j + 2] - c[2]};
+            regular_s(p, r, work);
+            for (int qq = 0; qq < K; ++qq) Mi[qq] += mass[j] * conj(work[qq]);
+          } else {
+            cplx zz = (pos[2 * j] - c[0]) + I * (pos[2 * j + 1] - c[1]), zp = 1;
+            for (int qq = 0; qq <= p; ++qq) { Mi[qq] += mass[j] * zp; zp *= zz; }
+          }
         }
       } else {
         for (int64_t ch = t->cbeg[d][i]; ch < t->cend[d][i]; ++ch) {
-          double tv[3];
-          for (int a = 0; a < 3; ++a) tv[a] = cen[d + 1][3 * ch + a] - c[a];
-          m2m_3d(p, M[d + 1] + (int64_t)K * ch, tv, Mi, work);
+          double tv[3] = {0, 0, 0};
+          for (int a = 0; a < dim; ++a) tv[a] = cen[d + 1][3 * ch + a] - c[a];
+          if (dim == 3) m2m_3d(p, M[d + 1] + (int64_t)K * ch, tv, Mi, work);
+          else m2m_2d(p, M[d + 1] + (int64_t)K * ch, tv[0] + I * tv[1], Mi);
         }
       }
     }
@@ -851,19 +875,20 @@ int orc_fmm_adaptive(int dim, int64_t n, const double *pos, const double *mass, 
       for (int64_t k = t->il_off[d][i]; k < t->il_off[d][i + 1]; ++k) {
         const int64_t s = t->il_idx[d][k];
         if ((direct_max > 0 && (pe[d][i] - pb[d][i]) * (pe[d][s] - pb[d][s]) <= direct_max) ||
-            orc_not_well_separated(3, t->keys[d][i], t->keys[d][s], ext)) {
+            orc_not_well_separated(dim, t->keys[d][i], t->keys[d][s], ext)) {
           for (int64_t a = pb[d][i]; a < pe[d][i]; ++a) {
             const int64_t pi = t->perm[a];
             for (int64_t b = pb[d][s]; b < pe[d][s]; ++b) {
               const int64_t pj = t->perm[b];
-              pair_kernel(3, pos + pi * 3, pos + pj * 3, mass[pj], eps2, fd + 4 * pi, fd + 4 * pi + 3);
+              pair_kernel(dim, pos + pi * dim, pos + pj * dim, mass[pj], eps2, fd + 4 * pi, fd + 4 * pi + 3);
             }
           }
           continue;
         }
-        double r[3];
-        for (int a = 0; a < 3; ++a) r[a] = cen[d][3 * i + a] - cen[d][3 * s + a];
-        m2l_3d(p, M[d] + (int64_t)K * s, r, Lx[d] + (int64_t)K * i, work);
+        double r[3] = {0, 0, 0};
+        for (int a = 0; a < dim; ++a) r[a] = cen[d][3 * i + a] - cen[d][3 * s + a];
+        if (dim == 3) m2l_3d(p, M[d] + (int64_t)K * s, r, Lx[d] + (int64_t)K * i, work);
+        else m2l_2d(p, M[d] + (int64_t)K * s, r[0] + I * r[1], Lx[d] + (int64_t)K * i);
       }
     }
   /* L2L down the active cells */
@@ -871,9 +896,10 @@ int orc_fmm_adaptive(int dim, int64_t n, const double *pos, const double *mass, 
     for (int64_t i = 0; i < t->ncell[d]; ++i) {
       if (!act[d][i] || leaf[d][i]) continue;
       for (int64_t ch = t->cbeg[d][i]; ch < t->cend[d][i]; ++ch) {
-        double tv[3];
-        for (int a = 0; a < 3; ++a) tv[a] = cen[d + 1][3 * ch + a] - cen[d][3 * i + a];
-        l2l_3d(p, Lx[d] + (int64_t)K * i, tv, Lx[d + 1] + (int64_t)K * ch, work);
+        double tv[3] = {0, 0, 0};
+        for (int a = 0; a < dim; ++a) tv[a] = cen[d + 1][3 * ch + a] - cen[d][3 * i + a];
+        if (dim == 3) l2l_3d(p, Lx[d] + (int64_t)K * i, tv, Lx[d + 1] + (int64_t)K * ch, work);
+        else l2l_2d(p, Lx[d] + (int64_t)K * i, tv[0] + I * tv[1], Lx[d + 1] + (int64_t)K * ch);
       }
     }
   /* adaptive leaves: L2P, then the colleagues' particles (with the W list) */
@@ -884,16 +910,20 @@ int orc_fmm_adaptive(int dim, int64_t n, const double *pos, const double *mass, 
       if (!leaf[d][b]) continue;
       const int64_t nB = pe[d][b] - pb[d][b];
       const double *cb = cen[d] + 3 * b;
-      double hb[3];
-      for (int a = 0; a < 3; ++a) hb[a] = 0.5 * ext[a] / (double)((uint64_t)1 << d);
+      double hb[3] = {0, 0, 0};
+      for (int a = 0; a < dim; ++a) hb[a] = 0.5 * ext[a] / (double)((uint64_t)1 << d);
       for (int64_t k = pb[d][b]; k < pe[d][b]; ++k) {
         const int64_t pi = t->perm[k];
-        double u[3] = {pos[3 * pi] - cb[0], pos[3 * pi + 1] - cb[1], pos[3 * pi + 2] - cb[2]};
         double *g = fd + 4 * pi;
-        l2p_3d(p, Lx[d] + (int64_t)K * b, u, g, g + 3, work);
+        if (dim == 3) {
+          double u[3] = {pos[3 * pi] - cb[0], pos[3 * pi + 1] - cb[1], pos[3 * pi + 2] - cb[2]};
+          l2p_3d(p, Lx[d] + (int64_t)K * b, u, g, g + 3, work);
+        } else {
+          l2p_2d(p, Lx[d] + (int64_t)K * b, (pos[2 * pi] - cb[0]) + I * (pos[2 * pi + 1] - cb[1]), g, g + 3);
+        }
         for (int64_t kk = pb[d][b]; kk < pe[d][b]; ++kk) {  /* the leaf itself */
           const int64_t pj = t->perm[kk];
-          if (pj != pi) pair_kernel(3, pos + pi * 3, pos + pj * 3, mass[pj], eps2, g, g + 3);
+          if (pj != pi) pair_kernel(dim, pos + pi * dim, pos + pj * dim, mass[pj], eps2, g, g + 3);
         }
       }
       top = 0;
@@ -912,7 +942,7 @@ int orc_fmm_adaptive(int dim, int64_t n, const double *pos, const double *mass, 
             const int64_t pi = t->perm[k];
             for (int64_t kk = pb[e][C]; kk < pe[e][C]; ++kk) {
               const int64_t pj = t->perm[kk];
-              pair_kernel(3, pos + pi * 3, pos + pj * 3, mass[pj], eps2, fd + 4 * pi, fd + 4 * pi + 3);
+              pair_kernel(dim, pos + pi * dim, pos + pj * dim, mass[pj], eps2, fd + 4 * pi, fd + 4 * pi + 3);
             }
           }
           continue;
@@ -920,7 +950,7 @@ int orc_fmm_adaptive(int dim, int64_t n, const double *pos, const double *mass, 
         for (int64_t ch = t->cbeg[e][C]; ch < t->cend[e][C]; ++ch) {
           const double *cc = cen[e + 1] + 3 * ch;
           double dist2 = 0.0, rad2 = 0.0;
-          for (int a = 0; a < 3; ++a) {
+          for (int a = 0; a < dim; ++a) {
             const double hc = 0.5 * ext[a] / (double)((uint64_t)1 << (e + 1));
             const double gap = fabs(cc[a] - cb[a]) - hb[a];
             if (gap > 0) dist2 += gap * gap;
@@ -940,21 +970,27 @@ int orc_fmm_adaptive(int dim, int64_t n, const double *pos, const double *mass, 
               const int64_t pi = t->perm[k];
               for (int64_t kk = pb[e + 1][ch]; kk < pe[e + 1][ch]; ++kk) {
                 const int64_t pj = t->perm[kk];
-                pair_kernel(3, pos + pi * 3, pos + pj * 3, mass[pj], eps2, fd + 4 * pi, fd + 4 * pi + 3);
+                pair_kernel(dim, pos + pi * dim, pos + pj * dim, mass[pj], eps2, fd + 4 * pi, fd + 4 * pi + 3);
               }
             }
           } else {
             for (int64_t k = pb[d][b]; k < pe[d][b]; ++k) {
               const int64_t pi = t->perm[k];
-              double r[3] = {pos[3 * pi] - cc[0], pos[3 * pi + 1] - cc[1], pos[3 * pi + 2] - cc[2]};
-              m2p_3d(p, M[e + 1] + (int64_t)K * ch, r, fd + 4 * pi, fd + 4 * pi + 3, work, Lw, work2);
+              double *g = fd + 4 * pi;
+              if (dim == 3) {
+                double r[3] = {pos[3 * pi] - cc[0], pos[3 * pi + 1] - cc[1], pos[3 * pi + 2] - cc[2]};
+                m2p_3d(p, M[e + 1] + (int64_t)K * ch, r, g, g + 3, work, Lw, work2);
+              } else {
+                m2p_2d(p, M[e + 1] + (int64_t)K * ch, (pos[2 * pi] - cc[0]) + I * (pos[2 * pi + 1] - cc[1]), g,
+                       g + 3);
+              }
             }
           }
         }
       }
     }
   for (int64_t i = 0; i < n; ++i) {
-    for (int a = 0; a < 3; ++a) grad[3 * i + a] = fd[4 * i + a];
+    for (int a = 0; a < dim; ++a) grad[dim * i + a] = fd[4 * i + a];
     if (pot) pot[i] = fd[4 * i + 3];
   }
   free(stk);

@@ -60,7 +60,7 @@ int orc_fmm(int dim, int64_t n, const double *pos, const double *mass, unsigned 
  * instead of by M2L (0 = none, as the reference). */
 int orc_fmm_ex(int dim, int64_t n, const double *pos, const double *mass, unsigned p, unsigned threshold,
                int centre_mode, double eps2, int64_t direct_max, double *grad, double *pot);
-/* Adaptive targets on the uniform tree (3D, geometric centres): targets stop
+/* Adaptive targets on the uniform tree (3D and 2D, geometric centres): targets stop
  * descending at cells of at most `aleaf` particles, whose particles then sum
  * their colleagues' particles directly (with the W list for large ones). */
 int orc_fmm_adaptive(int dim, int64_t n, const double *pos, const double *mass, unsigned p, unsigned threshold,

@@ -146,7 +146,7 @@ class Oracle:
 
     def fmm_adaptive(self, pos, mass, p, threshold, aleaf=None, want_pot=False, eps2=0.0, direct_max=0,
                      w_direct_max=0):
-        """FMM with adaptive targets on the uniform tree (3D): targets stop at
+        """FMM with adaptive targets on the uniform tree (3D and 2D): targets stop at
         cells of at most `aleaf` (default: threshold) particles and sum their
         colleagues' particles directly, larger colleagues through their
         children's multipoles where far enough (orc_fmm_adaptive)."""

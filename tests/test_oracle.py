@@ -194,7 +194,8 @@ def test_oracle_converges_on_an_elongated_box(oracle):
     assert errs[0] > errs[1] > errs[2] and errs[2] < 2e-6, errs
 
 
-@pytest.mark.parametrize("gen,n,T", [("plummer", 3000, 16), ("plummer_mixture", 4000, 16), ("uniform3d", 2000, 8)])
+@pytest.mark.parametrize("gen,n,T", [("plummer", 3000, 16), ("plummer_mixture", 4000, 16), ("uniform3d", 2000, 8),
+                                     ("disk_clumps2d", 3000, 16), ("disk2d", 2000, 8)])
 def test_adaptive_targets_partition_the_pairs_exactly(oracle, gen, n, T):
     """orc_fmm_adaptive with every interaction-list pair and every W-list
     child summed directly is the direct sum: the adaptive leaves' lists and
@@ -206,7 +207,7 @@ def test_adaptive_targets_partition_the_pairs_exactly(oracle, gen, n, T):
     assert rel_l2(g, d) < 1e-12 and rel_l2(pg, pd) < 1e-12
 
 
-@pytest.mark.parametrize("gen,n,T", [("plummer", 3000, 16), ("plummer_mixture", 4000, 16)])
+@pytest.mark.parametrize("gen,n,T", [("plummer", 3000, 16), ("plummer_mixture", 4000, 16), ("disk_clumps2d", 4000, 16)])
 def test_adaptive_targets_converge_like_the_uniform_fmm(oracle, gen, n, T):
     """Adaptive targets (multipoles of far W-list children included) converge
     with p, as accurately as the uniform-depth FMM with the same
@@ -220,3 +221,20 @@ def test_adaptive_targets_converge_like_the_uniform_fmm(oracle, gen, n, T):
         errs.append(rel_l2(ga, d))
         assert errs[-1] < 1.5 * rel_l2(gu, d) + 1e-7, (p, errs[-1], rel_l2(gu, d))
     assert errs[0] > errs[1] > errs[2]
+
+
+@pytest.mark.parametrize("gen", ["plummer", "disk_clumps2d"])
+def test_adaptive_w_list_multipoles_converge(oracle, gen):
+    """Every far W-list child evaluated through its multipole (M2P,
+    w_direct_max = 0) converges with p and stays within a few times the
+    error with every W-list child summed directly."""
+    pos, m = workloads.WORKLOADS[gen](4000, seed=3)
+    d = oracle.direct(pos, m)
+    errs = []
+    for p in (4, 8, 16):
+        gw = oracle.fmm_adaptive(pos, m, p, 16, direct_max=256, w_direct_max=0)
+        gd = oracle.fmm_adaptive(pos, m, p, 16, direct_max=256, w_direct_max=10 ** 18)
+        errs.append(rel_l2(gw, d))
+        assert rel_l2(gw, gd) > 0  # the multipoles were used
+        assert errs[-1] < 5 * rel_l2(gd, d) + 1e-9, (p, errs[-1], rel_l2(gd, d))
+    assert errs[0] > 10 * errs[1] > 100 * errs[2]
