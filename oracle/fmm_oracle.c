@@ -774,6 +774,36 @@ static void m2p_3d(int p, const cplx *M, const double *r, double *g, double *phi
   l2p_3d(1, Lw, zero, g, phi, R);
 }
 
+/* Particle range [pb, pe) in leaf order and parent index of every cell
+ * (the root's parent is -1); arrays of t->ncell[d] entries per level. */
+static void cell_ranges(const orc_tree *t, int64_t **pb, int64_t **pe, int64_t **par) {
+  const int D = t->depth;
+  for (int d = D; d >= 0; --d)
+    for (int64_t i = 0; i < t->ncell[d]; ++i) {
+      if (d == D) { pb[d][i] = t->leaf_start[i]; pe[d][i] = t->leaf_start[i + 1]; }
+      else {
+        pb[d][i] = pb[d + 1][t->cbeg[d][i]];
+        pe[d][i] = pe[d + 1][t->cend[d][i] - 1];
+        for (int64_t ch = t->cbeg[d][i]; ch < t->cend[d][i]; ++ch) par[d + 1][ch] = i;
+      }
+    }
+  par[0][0] = -1;
+}
+
+/* Active target cells and adaptive leaves, top down: the root is active; a
+ * cell is active if its parent is active and not an adaptive leaf; an active
+ * cell with at most `aleaf` particles, or at depth D, is an adaptive leaf. */
+static void adaptive_flags(const orc_tree *t, int64_t **pb, int64_t **pe, int64_t **par, unsigned aleaf, char **act,
+                           char **leaf) {
+  const int D = t->depth;
+  for (int d = 0; d <= D; ++d)
+    for (int64_t i = 0; i < t->ncell[d]; ++i) {
+      const int64_t cnt = pe[d][i] - pb[d][i];
+      act[d][i] = d == 0 ? 1 : (act[d - 1][par[d][i]] && !leaf[d - 1][par[d][i]]);
+      leaf[d][i] = act[d][i] && (cnt <= (int64_t)aleaf || d == D);
+    }
+}
+
 /* An FMM whose targets stop descending at small cells, the adaptive form
  * of the uniform-depth tree of orc_tree_build (3D and 2D, geometric centres).
  *
@@ -821,16 +851,7 @@ int orc_fmm_adaptive(int dim, int64_t n, const double *pos, const double *mass, 
     act[d] = (char *)calloc(m, 1);
     leaf[d] = (char *)calloc(m, 1);
   }
-  for (int d = D; d >= 0; --d)
-    for (int64_t i = 0; i < t->ncell[d]; ++i) {
-      if (d == D) { pb[d][i] = t->leaf_start[i]; pe[d][i] = t->leaf_start[i + 1]; }
-      else {
-        pb[d][i] = pb[d + 1][t->cbeg[d][i]];
-        pe[d][i] = pe[d + 1][t->cend[d][i] - 1];
-        for (int64_t ch = t->cbeg[d][i]; ch < t->cend[d][i]; ++ch) par[d + 1][ch] = i;
-      }
-    }
-  par[0][0] = -1;
+  cell_ranges(t, pb, pe, par);
   /* geometric centres, P2M at depth D, M2M up */
   for (int d = D; d >= 0; --d)
     for (int64_t i = 0; i < t->ncell[d]; ++i) {
@@ -860,13 +881,7 @@ int orc_fmm_adaptive(int dim, int64_t n, const double *pos, const double *mass, 
         }
       }
     }
-  /* active target cells and adaptive leaves */
-  for (int d = 0; d <= D; ++d)
-    for (int64_t i = 0; i < t->ncell[d]; ++i) {
-      const int64_t cnt = pe[d][i] - pb[d][i];
-      act[d][i] = d == 0 ? 1 : (act[d - 1][par[d][i]] && !leaf[d - 1][par[d][i]]);
-      leaf[d][i] = act[d][i] && (cnt <= (int64_t)aleaf || d == D);
-    }
+  adaptive_flags(t, pb, pe, par, aleaf, act, leaf);
   double *fd = (double *)calloc((size_t)n * 4, sizeof(double));
   /* interaction lists of the active targets: M2L, or direct (orc_fmm_ex's rules) */
   for (int d = 0; d <= D; ++d)
@@ -1000,4 +1015,39 @@ int orc_fmm_adaptive(int dim, int64_t n, const double *pos, const double *mass, 
   free(cen); free(M); free(Lx); free(pb); free(pe); free(par); free(act); free(leaf); free(work); free(work2); free(fd);
   orc_tree_free(t);
   return 0;
+}
+
+/* The flags of orc_fmm_adaptive for every cell, level by level in the order
+ * of orc_tree_level_keys: bit 0 active target, bit 1 adaptive leaf.  Returns
+ * the number of cells (writing nothing when it exceeds cap), or -1. */
+int64_t orc_adaptive_flags(int dim, int64_t n, const double *pos, unsigned threshold, unsigned aleaf, int64_t cap,
+                           uint8_t *flags) {
+  orc_tree *t = orc_tree_build(dim, n, pos, threshold);
+  if (!t) return -1;
+  const int D = t->depth;
+  int64_t total = 0;
+  for (int d = 0; d <= D; ++d) total += t->ncell[d];
+  if (total <= cap && flags) {
+    const size_t nlev = (size_t)(D < 0 ? 0 : D) + 1;
+    int64_t **pb = (int64_t **)calloc(nlev, sizeof(int64_t *)), **pe = (int64_t **)calloc(nlev, sizeof(int64_t *));
+    int64_t **par = (int64_t **)calloc(nlev, sizeof(int64_t *));
+    char **act = (char **)calloc(nlev, sizeof(char *)), **leaf = (char **)calloc(nlev, sizeof(char *));
+    for (int d = 0; d <= D; ++d) {
+      const int64_t m = t->ncell[d];
+      pb[d] = (int64_t *)malloc(sizeof(int64_t) * m);
+      pe[d] = (int64_t *)malloc(sizeof(int64_t) * m);
+      par[d] = (int64_t *)malloc(sizeof(int64_t) * m);
+      act[d] = (char *)calloc(m, 1);
+      leaf[d] = (char *)calloc(m, 1);
+    }
+    cell_ranges(t, pb, pe, par);
+    adaptive_flags(t, pb, pe, par, aleaf, act, leaf);
+    int64_t o = 0;
+    for (int d = 0; d <= D; ++d)
+      for (int64_t i = 0; i < t->ncell[d]; ++i, ++o) flags[o] = (uint8_t)((act[d][i] ? 1 : 0) | (leaf[d][i] ? 2 : 0));
+    for (int d = 0; d <= D; ++d) { free(pb[d]); free(pe[d]); free(par[d]); free(act[d]); free(leaf[d]); }
+    free(pb); free(pe); free(par); free(act); free(leaf);
+  }
+  orc_tree_free(t);
+  return total;
 }

@@ -66,6 +66,11 @@ int orc_fmm_ex(int dim, int64_t n, const double *pos, const double *mass, unsign
 int orc_fmm_adaptive(int dim, int64_t n, const double *pos, const double *mass, unsigned p, unsigned threshold,
                      unsigned aleaf, double eps2, int64_t direct_max, int64_t w_direct_max, double *grad,
                      double *pot);
+/* orc_fmm_adaptive's flags of every cell, level by level in the order of
+ * orc_tree_level_keys: bit 0 active target, bit 1 adaptive leaf.  Returns
+ * the number of cells (nothing written if above cap), or -1. */
+int64_t orc_adaptive_flags(int dim, int64_t n, const double *pos, unsigned threshold, unsigned aleaf, int64_t cap,
+                           uint8_t *flags);
 
 /* Scaled solid harmonics used by the CUDA path, m >= 0 only, packed
  * idx(n,m) = n(n+1)/2 + m, complex as (re, im):

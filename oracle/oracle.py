@@ -59,6 +59,9 @@ class Oracle:
                                  ctypes.c_double, ctypes.c_int64, _d, _d]
         L.orc_fmm_adaptive.argtypes = [ctypes.c_int, ctypes.c_int64, _d, _d, ctypes.c_uint, ctypes.c_uint,
                                        ctypes.c_uint, ctypes.c_double, ctypes.c_int64, ctypes.c_int64, _d, _d]
+        L.orc_adaptive_flags.restype = ctypes.c_int64
+        L.orc_adaptive_flags.argtypes = [ctypes.c_int, ctypes.c_int64, _d, ctypes.c_uint, ctypes.c_uint, ctypes.c_int64,
+                                         ctypes.c_void_p]
         for f in ("orc_regular_scaled", "orc_irregular_scaled", "orc_regular_racah", "orc_irregular_racah"):
             getattr(L, f).argtypes = [ctypes.c_uint, _d, _d]
         L.orc_p2m_3d.argtypes = [ctypes.c_uint, ctypes.c_int64, _d, _d, _d, _d]
@@ -161,6 +164,20 @@ class Oracle:
         if rc != 0:
             raise ValueError("orc_fmm_adaptive failed")
         return (g, pot) if want_pot else g
+
+    def adaptive_flags(self, pos, threshold, aleaf):
+        """orc_fmm_adaptive's per-cell flags, one uint8 array per level in
+        the order of tree()['level_keys']: bit 0 active target, bit 1
+        adaptive leaf (orc_adaptive_flags)."""
+        pos = _f64(pos)
+        n, dim = pos.shape
+        total = self.L.orc_adaptive_flags(dim, n, _p(pos, _d), threshold, aleaf, 0, None)
+        if total < 0:
+            raise ValueError("orc_adaptive_flags rejected the input")
+        flags = np.zeros(total, np.uint8)
+        self.L.orc_adaptive_flags(dim, n, _p(pos, _d), threshold, aleaf, total, flags.ctypes.data_as(ctypes.c_void_p))
+        sizes = [len(k) for k in self.tree(pos, threshold)["level_keys"]]
+        return np.split(flags, np.cumsum(sizes)[:-1])
 
     # ---- harmonics
     def _harm(self, fn, p, r, size):

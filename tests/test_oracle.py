@@ -238,3 +238,34 @@ def test_adaptive_w_list_multipoles_converge(oracle, gen):
         assert rel_l2(gw, gd) > 0  # the multipoles were used
         assert errs[-1] < 5 * rel_l2(gd, d) + 1e-9, (p, errs[-1], rel_l2(gd, d))
     assert errs[0] > 10 * errs[1] > 100 * errs[2]
+
+
+@pytest.mark.parametrize("gen,n,T,A", [("plummer_mixture", 20000, 16, 32), ("plummer", 20000, 32, 64),
+                                       ("uniform3d", 5000, 8, 8), ("disk_clumps2d", 20000, 16, 32)])
+def test_adaptive_flags_have_a_closed_form(oracle, gen, n, T, A):
+    """The adaptive targets' top-down rule (orc_fmm_adaptive) equals a rule
+    a GPU can apply to every cell at once: a cell is an active target iff it
+    is the root or its parent holds more than A particles; an adaptive leaf
+    iff it is active and holds at most A particles or is at the leaf level.
+    (A cell's particles are a subset of its parent's.)  The adaptive leaves
+    partition the particles."""
+    pos, m = workloads.WORKLOADS[gen](n, seed=3)
+    dim = pos.shape[1]
+    t = oracle.tree(pos, T)
+    D, keys = t["depth"], t["level_keys"]
+    flags = oracle.adaptive_flags(pos, T, A)
+    leaf_cnt = np.diff(t["leaf_start"])
+    cnt = [np.bincount(np.searchsorted(keys[d], t["leaf_keys"] >> np.uint64(dim * (D - d))), weights=leaf_cnt,
+                       minlength=len(keys[d])).astype(np.int64) for d in range(D + 1)]
+    covered = 0
+    for d in range(D + 1):
+        if d == 0:
+            act = np.ones(len(keys[0]), bool)
+        else:
+            parent = np.searchsorted(keys[d - 1], keys[d] >> np.uint64(dim))
+            act = cnt[d - 1][parent] > A
+        leaf = act & ((cnt[d] <= A) | (d == D))
+        np.testing.assert_array_equal(flags[d] & 1, act.astype(np.uint8))
+        np.testing.assert_array_equal((flags[d] >> 1) & 1, leaf.astype(np.uint8))
+        covered += int(cnt[d][leaf].sum())
+    assert covered == n
