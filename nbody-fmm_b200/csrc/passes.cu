@@ -1353,7 +1353,6 @@ __global__ void k_order_table(int dim, int p, int margin, int n_slots, int per_l
 }
 
 // ------------------------------------------------------------ driver
-static inline float fmax3(float a, float b, float c) { return std::max(a, std::max(b, c)); }
 
 int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, const double *d_pos_g,
                    const double *d_mass_g, int p, double eps2, double G,
@@ -1956,7 +1955,6 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   ws.launches += 1;
   if (ev) cudaEventRecord(ev[5], st);
   stats.n_cells = ncell;
-  (void)fmax3;
   CUDA_TRY(cudaGetLastError());
   return FMM_OK;
 }
