@@ -119,6 +119,10 @@ typedef struct fmm_config {
   float judge_budget;   /* FMM_ORDER_LEARNED: relative L2 error above which the evaluation is redone at p */
   int32_t judge_every;  /* FMM_ORDER_LEARNED: check every judge_every-th learned evaluation of a system
                            (default 1: every one) */
+  int32_t adaptive_leaf;/* adaptive targets (3D trees of depth >= 3; elsewhere ignored): a cell whose parent
+                           holds at most this many particles is no target, and each particle sums the
+                           particles of the colleagues of its deepest target cell directly.  0 (default):
+                           every cell is a target, the reference's uniform tree.  Not yet run on a GPU. */
 } fmm_config;
 
 typedef struct fmm_stats {

@@ -78,6 +78,9 @@ struct ExpBuffers {
   DevBuf<float> cf;              // learned orders: per-cell features (ORD_CF floats per cell)
   DevBuf<double> frms;           // learned orders: [0] F_rms of the previous pass (G = 1), [1] scratch,
                                  // [2] total mass
+  DevBuf<uint8_t> aflag;         // adaptive targets, per cell: bit 0 target, bit 1 adaptive leaf
+  DevBuf<int> alist;             // adaptive targets: the adaptive leaves, then their count
+  DevBuf<double> xs;             // adaptive targets: FP64 positions in leaf order (dim per particle)
 };
 
 // Per-pass parameters.
@@ -108,6 +111,7 @@ void upload_class_tables();
 int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, const double *d_pos,
                    const double *d_mass, int p, double eps2, double G,
                    const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, int64_t direct_max,
-                   const OrderOpts &order, cudaStream_t st, fmm_stats &stats, cudaEvent_t *ev);
+                   const OrderOpts &order, cudaStream_t st, fmm_stats &stats, cudaEvent_t *ev,
+                   int adaptive_leaf = 0);
 
 }  // namespace fmm

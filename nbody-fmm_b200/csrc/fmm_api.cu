@@ -71,6 +71,7 @@ static int check_cfg(const fmm_config *c) {
   if (c->order_mode != FMM_ORDER_FIXED && c->m2l_mode != FMM_M2L_TC)
     return FMM_ERR_UNSUPPORTED;  // per-pair orders live in the tensor-core kernel; the plain FMM is fixed-p
   if (c->order_margin < 0 || c->order_margin > FMM_MAX_P) return FMM_ERR_INVALID_ARGUMENT;
+  if (c->adaptive_leaf < 0) return FMM_ERR_INVALID_ARGUMENT;
   return FMM_OK;
 }
 
@@ -178,6 +179,9 @@ int fmm_destroy(fmm_ctx *c) {
   c->eb.elev.release();
   c->eb.ukey.release();
   c->eb.p2m_list.release();
+  c->eb.aflag.release();
+  c->eb.alist.release();
+  c->eb.xs.release();
   c->eb.hbatches.release();
   c->eb.hbatches2.release();
   c->eb.uval.release();
@@ -239,7 +243,7 @@ static int pass(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass
   c->stats.judge_rel_l2 = jr;
   c->stats.order_fallbacks = fb;
   rc = run_fmm_passes(c->ws, c->tree, c->ops, c->eb, d_pos, d_mass, c->cfg.p, c->cfg.eps2, c->cfg.G, g, d_acc, d_pot,
-                      c->cfg.m2l_mode, direct_threshold(c->cfg), oo, st, c->stats, c->ev);
+                      c->cfg.m2l_mode, direct_threshold(c->cfg), oo, st, c->stats, c->ev, c->cfg.adaptive_leaf);
   c->stats.direct_max = direct_threshold(c->cfg);
   if (rc) return rc;
   if (!c->ws.ok) return FMM_ERR_OUT_OF_MEMORY;

@@ -693,6 +693,71 @@ __global__ void k_p2p(P2PArgs a) {
   if (lane == 0 && a.pair_count) atomicAdd(a.pair_count, (unsigned long long)npairs);
 }
 
+// Adaptive targets: one warp per adaptive leaf B (any level), listed in
+// alist[0 .. *acount), taken by the warps of a fixed grid in turn.  B's
+// particles sum the particles of B itself (j != i) and of its colleagues at
+// B's level, the pairs that the deeper levels' interaction lists and the leaf
+// level's near field would sum in the uniform tree.  Colleagues touch B, so
+// each difference x_i - x_j is formed in FP64 from the leaf-ordered FP64
+// positions xs and rounded once to FP32.  Writes the output as k_p2p does.
+template <int DIM, bool POT>
+__global__ void k_p2p_cells(P2PArgs a, const int *alist, const unsigned *acount, const double *xs) {
+  constexpr int NS = DIM == 3 ? 27 : 9;
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
+  const int ncells = (int)*acount;
+  bool bad = false;
+  long long npairs = 0;
+  for (int wl = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); wl < ncells; wl += nwarps) {
+    const int g = alist[wl];
+    const int tb = a.pbeg[g], nt = a.pend[g] - tb;
+    const int tp = nt < 32 ? nt : 32;
+    int Gl = 1;
+    while (Gl * 2 * tp <= 32) Gl *= 2;
+    const int tpp = 32 / Gl;
+    const int *cl = a.coll + (int64_t)g * NS;
+    for (int t0 = 0; t0 < nt; t0 += tpp) {
+      const int ti = t0 + lane / Gl, sub = lane % Gl;
+      const bool act = ti < nt;
+      const int me_i = tb + (act ? ti : 0);
+      const double xi = xs[DIM * (size_t)me_i], yi = xs[DIM * (size_t)me_i + 1],
+                   zi = DIM == 3 ? xs[DIM * (size_t)me_i + 2] : 0.0;
+      float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
+      for (int s = 0; s < NS; ++s) {
+        const int S = cl[s];
+        if (S < 0) continue;
+        const int se = a.pend[S];
+        if (t0 == 0 && lane == 0) npairs += (long long)nt * (se - a.pbeg[S]) - (S == g ? nt : 0);
+        for (int j = a.pbeg[S] + sub; j < se; j += Gl) {
+          if (j == me_i) continue;
+          const float rx = (float)(xi - xs[DIM * (size_t)j]);
+          const float ry = (float)(yi - xs[DIM * (size_t)j + 1]);
+          const float rz = DIM == 3 ? (float)(zi - xs[DIM * (size_t)j + 2]) : 0.f;
+          pair_acc<DIM, true, POT>(rx, ry, rz, a.part[j].w, a.eps2, ax, ay, az, ph);
+        }
+      }
+      for (int o = 1; o < Gl; o <<= 1) {
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+        ph += __shfl_xor_sync(0xffffffffu, ph, o);
+      }
+      if (act && sub == 0) {
+        const float4 f = a.far[me_i];
+        const uint32_t o = a.perm[me_i];
+        double vx = a.G * ((double)f.x + ax), vy = a.G * ((double)f.y + ay), vz = a.G * ((double)f.z + az);
+        a.acc[DIM * (size_t)o] = vx;
+        a.acc[DIM * (size_t)o + 1] = vy;
+        if (DIM == 3) a.acc[3 * (size_t)o + 2] = vz;
+        if (a.pot) a.pot[o] = a.G * ((double)f.w + ph);
+        bad |= !(isfinite(vx) && isfinite(vy) && isfinite(vz));
+      }
+    }
+  }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.err, FMM_DEV_ERR_NONFINITE_OUTPUT);
+  if (lane == 0 && a.pair_count && npairs) atomicAdd(a.pair_count, (unsigned long long)npairs);
+}
+
 // --------------------------------------------------------- direct far field
 // Offsets of every particle (leaf order) from the centre of its ancestor at
 // each level d in [d0, d1], FP32, with the mass: the frames in which pairs of
@@ -740,6 +805,8 @@ struct DirectArgs {
   int any_fdirect;
   float4 *far;
   unsigned long long *pair_count;
+  const uint8_t *aflag;    // adaptive targets (null: every cell is a target), indexed by cell - cell0
+  int cell0;
 };
 
 // One warp per level-d target cell T with n_T <= direct_max: the sources are
@@ -888,6 +955,7 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   int lv = a.nlev - 1;  // deep levels, which hold most of the warps, first
   while (wl < a.w0[lv]) --lv;
   const int T = a.first[lv] + (wl - a.w0[lv]);
+  if (a.aflag && !(a.aflag[T - a.cell0] & 1)) return;  // the whole warp: no target
   const int tb = a.pbeg[T], nt = a.pend[T] - tb;
   if ((long long)nt > a.direct_max && !a.any_fdirect) return;
   const float4 *off = a.off[lv];
@@ -996,10 +1064,12 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
 // cell), key_m2l for M2L with 255 for cells that cannot have an M2L pair under
 // the direct-pair rule (every child S of the parent's colleagues has
 // n_T * n_S <= direct_max; adjacency is ignored, so the test only errs
-// towards keeping a cell).
+// towards keeping a cell), and with adaptive targets (aflag set) for cells
+// that are no target.
 __global__ void k_class_keys(const uint64_t *ckey, const int *cpbeg, const int *cpend, const int *cparent,
                              const int *ccoll, const int *cchild, long long direct_max, int first, int count, int level,
-                             int dim, uint64_t *keys_all, uint64_t *keys_m2l, uint32_t *vals, int out_off) {
+                             int dim, uint64_t *keys_all, uint64_t *keys_m2l, uint32_t *vals, int out_off,
+                             const uint8_t *aflag, int cell0) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   int g = first + i;
@@ -1021,6 +1091,7 @@ __global__ void k_class_keys(const uint64_t *ckey, const int *cpbeg, const int *
       }
     }
   }
+  if (aflag && !(aflag[g - cell0] & 1)) m2l = false;
   keys_m2l[out_off + i] = m2l ? k : 255u;
 }
 
@@ -1352,12 +1423,43 @@ __global__ void k_order_table(int dim, int p, int margin, int n_slots, int per_l
   }
 }
 
+// Adaptive targets, per cell g (flag[g - cell0]): bit 0, a target: the root,
+// or a cell whose parent holds more than A particles (every ancestor then
+// does too, since a cell's particles are a subset of its parent's); bit 1,
+// an adaptive leaf: a target with at most A particles, or a leaf.  The
+// adaptive leaves are appended to alist, their count kept in *acount.
+__global__ void k_adaptive_flags(const int *pbeg, const int *pend, const int *parent, int cell0, int ncell,
+                                 int first1, int leaf_first, int A, uint8_t *flag, int *alist, unsigned *acount) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31;
+  const int g = cell0 + i;
+  bool is_leaf = false;
+  if (i < ncell) {
+    const bool tgt = g < first1 || pend[parent[g]] - pbeg[parent[g]] > A;
+    is_leaf = tgt && (pend[g] - pbeg[g] <= A || g >= leaf_first);
+    flag[i] = (uint8_t)((tgt ? 1 : 0) | (is_leaf ? 2 : 0));
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, is_leaf);
+  unsigned base = 0;
+  if (lane == 0 && m) base = atomicAdd(acount, (unsigned)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (is_leaf) alist[base + __popc(m & ((1u << lane) - 1u))] = g;
+}
+
+// FP64 positions in leaf order: xs[i] = pos[perm[i]].
+__global__ void k_gather_pos(const double *pos, const uint32_t *perm, int64_t n, int dim, double *xs) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const size_t o = (size_t)perm[i] * dim;
+  for (int k = 0; k < dim; ++k) xs[(size_t)i * dim + k] = pos[o + k];
+}
+
 // ------------------------------------------------------------ driver
 
 int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, const double *d_pos_g,
                    const double *d_mass_g, int p, double eps2, double G,
                    const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, int64_t direct_max,
-                   const OrderOpts &order, cudaStream_t st, fmm_stats &stats, cudaEvent_t *ev) {
+                   const OrderOpts &order, cudaStream_t st, fmm_stats &stats, cudaEvent_t *ev,
+                   int adaptive_leaf) {
   const int dim = t.dim, D = t.depth, KS = ops.KS;
   const int64_t n = t.n;
   const bool want_pot = d_pot != nullptr;  // the potential is summed only when it is asked for
@@ -1405,6 +1507,16 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   // pairs (for M2L) and, without the shortcuts (which build their own lists
   // below), every cell (for M2M and L2L) and consecutive M2M parents
   const bool shortcut = dim == 3 && D >= 3;
+  // adaptive targets (3D shortcut pass only): flags and the adaptive leaves
+  const bool adaptive = shortcut && adaptive_leaf > 0;
+  if (adaptive) {
+    if (!eb.aflag.reserve(ncell) || !eb.alist.reserve((size_t)ncell + 1)) return FMM_ERR_OUT_OF_MEMORY;
+    CUDA_TRY(cudaMemsetAsync(eb.alist.ptr + ncell, 0, sizeof(int), st));
+    k_adaptive_flags<<<cdiv(ncell, TPB), TPB, 0, st>>>(ws.cell_pbeg, ws.cell_pend, ws.cell_parent, cell0, ncell,
+                                                        t.level_off[1], t.level_off[D], adaptive_leaf, eb.aflag.ptr,
+                                                        eb.alist.ptr, (unsigned *)(eb.alist.ptr + ncell));
+    ws.launches += 1;
+  }
   std::vector<int> lvl_b0(D + 2, 0), lvl_b1(D + 2, 0), m2l_b0(D + 2, 0), m2l_b1(D + 2, 0);
   std::vector<int> m2m_b0(D + 1, 0), m2m_b1(D + 1, 0);
   int ntl = 0;
@@ -1420,7 +1532,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
       k_class_keys<<<cdiv(t.level_count[d], TPB), TPB, 0, st>>>(
           ws.cell_key, ws.cell_pbeg, ws.cell_pend, ws.cell_parent, ws.cell_coll, ws.cell_child, direct_max,
           t.level_off[d], t.level_count[d], d, dim, eb.ckey.ptr, eb.ckey_m2l.ptr, eb.cval.ptr,
-          t.level_off[d] - t.level_off[2]);
+          t.level_off[d] - t.level_off[2], adaptive ? eb.aflag.ptr : nullptr, cell0);
     ws.launches += D - 1;
     CUDA_TRY(cudaMemsetAsync(eb.cls_count.ptr, 0, 512 * sizeof(uint32_t), st));
     uint64_t *kk = eb.ckey.ptr, *kk2 = eb.ckey_alt.ptr;
@@ -1892,6 +2004,8 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     da.any_fdirect = any_fdirect;
     da.far = ws.far;
     da.pair_count = ws.counters + 3;
+    da.aflag = adaptive ? eb.aflag.ptr : nullptr;
+    da.cell0 = cell0;
     da.nlev = 0;
     int64_t nw = 0;
     for (int d = 2; d <= D; ++d) {
@@ -1945,7 +2059,15 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   pa.err = ws.dev_err;
   pa.pair_count = ws.counters + 1;
   const int pgrid = cdiv((int64_t)pa.nleaves * 32, TPB);
-  if (dim == 3) {
+  if (adaptive) {
+    // every particle lies in exactly one adaptive leaf, which writes its output
+    if (!eb.xs.reserve((size_t)n * 3)) return FMM_ERR_OUT_OF_MEMORY;
+    k_gather_pos<<<cdiv(n, TPB), TPB, 0, st>>>(d_pos_g, t.d_perm, n, dim, eb.xs.ptr);
+    ws.launches += 1;
+    const unsigned *acount = (const unsigned *)(eb.alist.ptr + ncell);
+    if (want_pot) k_p2p_cells<3, true><<<148 * 8, TPB, 0, st>>>(pa, eb.alist.ptr, acount, eb.xs.ptr);
+    else k_p2p_cells<3, false><<<148 * 8, TPB, 0, st>>>(pa, eb.alist.ptr, acount, eb.xs.ptr);
+  } else if (dim == 3) {
     if (want_pot) k_p2p<3, true><<<pgrid, TPB, 0, st>>>(pa);
     else k_p2p<3, false><<<pgrid, TPB, 0, st>>>(pa);
   } else {

@@ -64,7 +64,7 @@ class FmmConfig(ctypes.Structure):
         ("eps2", ctypes.c_double), ("G", ctypes.c_double), ("device", ctypes.c_int32),
         ("direct_max", ctypes.c_int32), ("order_mode", ctypes.c_int32), ("order_margin", ctypes.c_int32),
         ("order_tol", ctypes.c_float), ("judge_samples", ctypes.c_int32), ("judge_budget", ctypes.c_float),
-        ("judge_every", ctypes.c_int32),
+        ("judge_every", ctypes.c_int32), ("adaptive_leaf", ctypes.c_int32),
     ]
 
 
@@ -219,7 +219,7 @@ class Context:
 
     def __init__(self, dim=3, p=8, leaf_cap=64, m2l_mode=FMM_M2L_FP32, eps2=0.0, G=1.0, device=0, direct_max=-1,
                  order_mode=FMM_ORDER_FIXED, order_margin=1, order_tol=2e-6, judge_samples=0, judge_budget=1e-6,
-                 judge_every=1, order_model=None):
+                 judge_every=1, order_model=None, adaptive_leaf=0):
         L = load_library()
         cfg = FmmConfig()
         _check(L.fmm_config_default(ctypes.byref(cfg)))
@@ -228,6 +228,7 @@ class Context:
         cfg.order_mode, cfg.order_margin = order_mode, order_margin
         cfg.order_tol, cfg.judge_samples, cfg.judge_budget = order_tol, judge_samples, judge_budget
         cfg.judge_every = judge_every
+        cfg.adaptive_leaf = adaptive_leaf
         h = _vp()
         _check(L.fmm_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

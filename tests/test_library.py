@@ -47,6 +47,10 @@ def test_create_rejects_bad_config():
     cfg.dim = 3
     cfg.p = 99
     assert L.fmm_create(ctypes.byref(cfg), ctypes.byref(h)) == fmmgpu.FMM_ERR_INVALID_ARGUMENT
+    cfg.p = 8
+    assert cfg.adaptive_leaf == 0  # the default: the reference's uniform targets
+    cfg.adaptive_leaf = -1
+    assert L.fmm_create(ctypes.byref(cfg), ctypes.byref(h)) == fmmgpu.FMM_ERR_INVALID_ARGUMENT
 
 
 def test_no_cpu_fallback_without_gpu():
