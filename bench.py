@@ -272,7 +272,7 @@ def run_ours(args, world, rank, local):
     okw = dict(order_mode=fmmgpu.FMM_ORDER_LEARNED, judge_samples=args.judge, judge_budget=1e-6,
                judge_every=args.judge_every) if learned else {}
     ctx = fmmgpu.Context(dim=3, p=p, leaf_cap=leaf, m2l_mode=mode, G=1.0, device=local, direct_max=args.direct_max,
-                         **okw)
+                         adaptive_leaf=args.adaptive, **okw)
     tune = None
     if args.autotune and args.direct_max < 0:
         # the autotuner picks the direct-pair threshold on this input (setup, outside the timed steps)
@@ -354,7 +354,8 @@ def run_ours(args, world, rank, local):
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": f"synthetic (seeded {'Plummer mixture' if mixture else 'Plummer sphere'})",
         "impl": "fmmgpu",
-        "config": workload_desc(n, p, leaf, args.m2l, s_last.get("direct_max"), mixture),
+        "config": dict(workload_desc(n, p, leaf, args.m2l, s_last.get("direct_max"), mixture),
+                       adaptive_leaf=args.adaptive),
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(n * 3 * 8 + n * 8),
                 "d2h_bytes_per_step": int(n * 3 * 8)},
         "roofline": roof, "rooflines": roofs, "error": err, "phases_ms": ph,
@@ -379,7 +380,7 @@ def run_ours(args, world, rank, local):
     # FP32 GPU FMM (the method without tensor cores and learned orders)
     def compare(m2l_mode, label):
         pc = fmmgpu.Context(dim=3, p=p, leaf_cap=args.leaf, m2l_mode=m2l_mode, G=1.0, device=local,
-                            direct_max=args.direct_max)
+                            direct_max=args.direct_max, adaptive_leaf=args.adaptive)
         chosen = None
         if args.autotune and args.direct_max < 0:  # tuned the same way as the headline
             b = pc.autotune(n, d_pos.data_ptr(), d_mass.data_ptr(), tune_leaf=tune_leaf,
@@ -635,6 +636,9 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ensemble", action="store_true", help="the batched-ensemble configuration instead")
+    ap.add_argument("--adaptive", type=int, default=0,
+                    help="adaptive targets: cells under parents of at most this many particles are no targets "
+                         "(0: the uniform tree of the reference)")
     ap.add_argument("--frames-every", type=int, default=0,
                     help="measure frame output instead: a device frame every K steps of the pass loop")
     args = ap.parse_args()
