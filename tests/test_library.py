@@ -64,3 +64,33 @@ def test_no_cpu_fallback_without_gpu():
         pass
     with pytest.raises(fmmgpu.FmmError):
         fmmgpu.Context()
+
+
+def test_binding_structs_match_header(tmp_path):
+    """The ctypes mirrors of the header's structs have the C layout: the
+    same size and the same offset for every field, as the C compiler lays
+    them out from include/fmm_gpu.h."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    mirrors = {"fmm_config": fmmgpu.FmmConfig, "fmm_stats": fmmgpu.FmmStats,
+               "fmm_tune_result": fmmgpu.FmmTuneResult}
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "fmm_gpu.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'  printf("{cname}.{f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(ln.split() for ln in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                   check=True).stdout.splitlines())
+    for cname, py in mirrors.items():
+        assert int(got[cname]) == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert int(got[f"{cname}.{f}"]) == getattr(py, f).offset, f"{cname}.{f}"
