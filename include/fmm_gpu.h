@@ -192,15 +192,19 @@ FMM_API int fmm_evaluate_batched(fmm_ctx *ctx, int32_t nsys, const int64_t *offs
    capacity in {32, 64, 128, 256} (which changes the tree: the reference's
    algorithm at that threshold) at the threshold K^2/25, then the thresholds
    K^2/100, K^2/50 and K^2/12.5 at the best capacity (seven candidates).
-   Learned orders are tuned with them (every candidate is evaluated twice,
+   Every candidate keeps the configured adaptive_leaf; with FMM_TUNE_ADAPTIVE
+   the values 16, 32 and 64 are then tried at the best candidate's leaf
+   capacity and threshold.  Learned orders are tuned with them (every candidate is evaluated twice,
    the second timed).  result may be NULL.  Synchronous. */
 #define FMM_TUNE_LEAF 1
+#define FMM_TUNE_ADAPTIVE 2 /* then adaptive_leaf in {16, 32, 64} at the best of the above (experimental) */
 typedef struct fmm_tune_result {
   int32_t n_candidates;
   int32_t best;            /* index of the chosen candidate */
   int32_t leaf_cap[16];    /* candidates */
   int32_t direct_max[16];
   double ms[16];           /* device time of each candidate's timed evaluation */
+  int32_t adaptive_leaf[16];
 } fmm_tune_result;
 FMM_API int fmm_autotune(fmm_ctx *ctx, int64_t n, const double *d_pos, const double *d_mass, int32_t flags,
                          fmm_tune_result *result, void *stream);

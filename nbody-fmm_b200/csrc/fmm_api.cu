@@ -450,13 +450,16 @@ int fmm_autotune(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mas
   CUDA_TRY(cudaEventCreate(&e1));
   int rc = FMM_OK;
   double best = 1e300;
-  auto trial = [&](int lc, double f) {
+  auto threshold = [&](double f) { return (int32_t)std::max(8.0, base * f); };
+  auto trial = [&](int lc, int32_t dm, int32_t al) {
     if (rc || res.n_candidates >= 16) return;
     const int k = res.n_candidates++;
     c->cfg.leaf_cap = lc;
-    c->cfg.direct_max = (int32_t)std::max(8.0, base * f);
+    c->cfg.direct_max = dm;
+    c->cfg.adaptive_leaf = al;
     res.leaf_cap[k] = lc;
-    res.direct_max[k] = c->cfg.direct_max;
+    res.direct_max[k] = dm;
+    res.adaptive_leaf[k] = al;
     const bool twice = c->cfg.order_mode == FMM_ORDER_LEARNED;
     c->frms_n = -1;  // learned orders: start the system afresh
     for (int r = 0; r < (twice ? 2 : 1) && !rc; ++r) rc = evaluate_device(c, n, d_pos, d_mass, c->d_acc.ptr, nullptr, st);
@@ -476,12 +479,19 @@ int fmm_autotune(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mas
   };
   // coordinate search: the leaf capacity at the default threshold, then the
   // threshold at the best capacity
+  const int32_t al0 = saved.adaptive_leaf;
   if (flags & FMM_TUNE_LEAF) {
-    for (int lc : {32, 64, 128, 256}) trial(lc, 1.0);
+    for (int lc : {32, 64, 128, 256}) trial(lc, threshold(1.0), al0);
     const int lc = res.leaf_cap[res.best];
-    for (double f : {0.25, 0.5, 2.0}) trial(lc, f);
+    for (double f : {0.25, 0.5, 2.0}) trial(lc, threshold(f), al0);
   } else {
-    for (double f : {0.125, 0.25, 0.5, 1.0, 2.0}) trial(c->cfg.leaf_cap, f);
+    for (double f : {0.125, 0.25, 0.5, 1.0, 2.0}) trial(saved.leaf_cap, threshold(f), al0);
+  }
+  // then the adaptive-target threshold at the best leaf capacity and direct-pair threshold
+  if ((flags & FMM_TUNE_ADAPTIVE) && !rc) {
+    const int b = res.best;
+    for (int32_t al : {16, 32, 64})
+      if (al != al0) trial(res.leaf_cap[b], res.direct_max[b], al);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -489,6 +499,7 @@ int fmm_autotune(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mas
   if (rc) return rc;
   c->cfg.leaf_cap = res.leaf_cap[res.best];
   c->cfg.direct_max = res.direct_max[res.best];
+  c->cfg.adaptive_leaf = res.adaptive_leaf[res.best];
   c->frms_n = -1;
   if (result) *result = res;
   return FMM_OK;

@@ -82,10 +82,12 @@ class FmmStats(ctypes.Structure):
 
 class FmmTuneResult(ctypes.Structure):
     _fields_ = [("n_candidates", ctypes.c_int32), ("best", ctypes.c_int32), ("leaf_cap", ctypes.c_int32 * 16),
-                ("direct_max", ctypes.c_int32 * 16), ("ms", ctypes.c_double * 16)]
+                ("direct_max", ctypes.c_int32 * 16), ("ms", ctypes.c_double * 16),
+                ("adaptive_leaf", ctypes.c_int32 * 16)]
 
 
 FMM_TUNE_LEAF = 1
+FMM_TUNE_ADAPTIVE = 2
 
 
 class FmmError(RuntimeError):
@@ -358,17 +360,20 @@ class Context:
         _check(_lib.fmm_evaluate_batched(self._h, len(offsets) - 1, _p(offsets, _i64), pos_ptr, mass_ptr, acc_ptr,
                                          pot_ptr, workers))
 
-    def autotune(self, n, pos_ptr, mass_ptr, tune_leaf=False, stream=None):
-        """Times candidate direct-pair thresholds (and leaf capacities) on the
-        given system and keeps the fastest (fmm_autotune).  Returns the
-        candidates as a list of dicts and the chosen one."""
+    def autotune(self, n, pos_ptr, mass_ptr, tune_leaf=False, stream=None, tune_adaptive=False):
+        """Times candidate direct-pair thresholds (and leaf capacities, and
+        adaptive-target thresholds) on the given system and keeps the fastest
+        (fmm_autotune).  Returns the candidates as a list of dicts and the
+        chosen one."""
         r = FmmTuneResult()
-        _check(_lib.fmm_autotune(self._h, n, pos_ptr, mass_ptr, FMM_TUNE_LEAF if tune_leaf else 0, ctypes.byref(r),
-                                 stream))
-        cands = [{"leaf_cap": r.leaf_cap[i], "direct_max": r.direct_max[i], "ms": r.ms[i]}
-                 for i in range(r.n_candidates)]
-        self.cfg.leaf_cap, self.cfg.direct_max = cands[r.best]["leaf_cap"], cands[r.best]["direct_max"]
-        return cands, cands[r.best]
+        flags = (FMM_TUNE_LEAF if tune_leaf else 0) | (FMM_TUNE_ADAPTIVE if tune_adaptive else 0)
+        _check(_lib.fmm_autotune(self._h, n, pos_ptr, mass_ptr, flags, ctypes.byref(r), stream))
+        cands = [{"leaf_cap": r.leaf_cap[i], "direct_max": r.direct_max[i], "adaptive_leaf": r.adaptive_leaf[i],
+                  "ms": r.ms[i]} for i in range(r.n_candidates)]
+        best = cands[r.best]
+        self.cfg.leaf_cap, self.cfg.direct_max = best["leaf_cap"], best["direct_max"]
+        self.cfg.adaptive_leaf = best["adaptive_leaf"]
+        return cands, best
 
     # ---- learned pair orders
     def set_order_model(self, params):
