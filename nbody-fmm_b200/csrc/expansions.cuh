@@ -80,6 +80,7 @@ struct ExpBuffers {
                                  // [2] total mass
   DevBuf<uint8_t> aflag;         // adaptive targets, per cell: bit 0 target, bit 1 adaptive leaf
   DevBuf<int> alist;             // adaptive targets: the adaptive leaves, then their count
+  DevBuf<int> ftl;               // adaptive targets: the direct far field's targets per level, then counts
   DevBuf<double> xs;             // adaptive targets: FP64 positions in leaf order (dim per particle)
 };
 

@@ -181,6 +181,7 @@ int fmm_destroy(fmm_ctx *c) {
   c->eb.p2m_list.release();
   c->eb.aflag.release();
   c->eb.alist.release();
+  c->eb.ftl.release();
   c->eb.xs.release();
   c->eb.hbatches.release();
   c->eb.hbatches2.release();

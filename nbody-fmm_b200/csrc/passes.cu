@@ -792,7 +792,8 @@ static constexpr int DF_MAX_LEVELS = 33;
 
 struct DirectArgs {
   // levels of the launch, coarse first: warps [w0[k], w0[k+1]) take the
-  // cells first[k] + (warp - w0[k])
+  // cells first[k] + (warp - w0[k]), or with a target list (k_direct_far's
+  // LIST) the cells tlist[first[k] + (warp - w0[k])]
   int nlev;
   int first[DF_MAX_LEVELS], w0[DF_MAX_LEVELS + 1];
   const float4 *off[DF_MAX_LEVELS];  // particle offsets from their level-d ancestor's centre
@@ -805,8 +806,7 @@ struct DirectArgs {
   int any_fdirect;
   float4 *far;
   unsigned long long *pair_count;
-  const uint8_t *aflag;    // adaptive targets (null: every cell is a target), indexed by cell - cell0
-  int cell0;
+  const int *tlist;        // adaptive targets: each level's targets, from first[k]
 };
 
 // One warp per level-d target cell T with n_T <= direct_max: the sources are
@@ -942,7 +942,7 @@ __device__ inline void blocked_shape(int nt, int R, int &Gl, float &cost) {
   cost = (float)(rounds * R) / (float)Gl;
 }
 
-template <int DIM, bool POT>
+template <int DIM, bool POT, bool LIST = false>
 __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   constexpr int NS = DIM == 3 ? 27 : 9, NC = 1 << DIM, NCAND = NS * NC, NR = (NCAND + 31) / 32;
   __shared__ float4 s_cell_all[8][189];
@@ -954,8 +954,7 @@ __global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
   if (wl >= a.w0[a.nlev]) return;
   int lv = a.nlev - 1;  // deep levels, which hold most of the warps, first
   while (wl < a.w0[lv]) --lv;
-  const int T = a.first[lv] + (wl - a.w0[lv]);
-  if (a.aflag && !(a.aflag[T - a.cell0] & 1)) return;  // the whole warp: no target
+  const int T = LIST ? a.tlist[a.first[lv] + (wl - a.w0[lv])] : a.first[lv] + (wl - a.w0[lv]);
   const int tb = a.pbeg[T], nt = a.pend[T] - tb;
   if ((long long)nt > a.direct_max && !a.any_fdirect) return;
   const float4 *off = a.off[lv];
@@ -1443,6 +1442,22 @@ __global__ void k_adaptive_flags(const int *pbeg, const int *pend, const int *pa
   if (lane == 0 && m) base = atomicAdd(acount, (unsigned)__popc(m));
   base = __shfl_sync(0xffffffffu, base, 0);
   if (is_leaf) alist[base + __popc(m & ((1u << lane) - 1u))] = g;
+}
+
+// Adaptive targets of one level for the direct far field: the cells with
+// flag bit 0 that can have direct pairs, appended to seg (warp-aggregated;
+// their order within the level is free), their count in *cnt.
+__global__ void k_level_targets(const uint8_t *aflag, int cell0, int first, int count, const int *pbeg,
+                                const int *pend, long long direct_max, int any_fdirect, int *seg, unsigned *cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31;
+  const int g = first + i;
+  const bool tgt = i < count && (aflag[g - cell0] & 1) &&
+                   ((long long)(pend[g] - pbeg[g]) <= direct_max || any_fdirect);
+  const unsigned m = __ballot_sync(0xffffffffu, tgt);
+  unsigned base = 0;
+  if (lane == 0 && m) base = atomicAdd(cnt, (unsigned)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (tgt) seg[base + __popc(m & ((1u << lane) - 1u))] = g;
 }
 
 // FP64 positions in leaf order: xs[i] = pos[perm[i]].
@@ -2004,24 +2019,46 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     da.any_fdirect = any_fdirect;
     da.far = ws.far;
     da.pair_count = ws.counters + 3;
-    da.aflag = adaptive ? eb.aflag.ptr : nullptr;
-    da.cell0 = cell0;
+    da.tlist = nullptr;
+    // adaptive targets: each level's targets listed in its own segment of
+    // the list (the level's cells in order, gaps after the targets)
+    std::vector<unsigned> ntgt;
+    if (adaptive) {
+      const int ncl = t.level_off[D] + t.level_count[D] - t.level_off[2];
+      if (!eb.ftl.reserve((size_t)ncl + D + 1)) return FMM_ERR_OUT_OF_MEMORY;
+      unsigned *cnt = (unsigned *)(eb.ftl.ptr + ncl);
+      CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned) * (D + 1), st));
+      for (int d = 2; d <= D; ++d)
+        k_level_targets<<<cdiv(t.level_count[d], TPB), TPB, 0, st>>>(
+            eb.aflag.ptr, cell0, t.level_off[d], t.level_count[d], ws.cell_pbeg, ws.cell_pend, direct_max,
+            any_fdirect, eb.ftl.ptr + (t.level_off[d] - t.level_off[2]), cnt + d);
+      ws.launches += D - 1;
+      ntgt.assign(D + 1, 0u);
+      CUDA_TRY(cudaMemcpyAsync(ntgt.data(), cnt, sizeof(unsigned) * (D + 1), cudaMemcpyDeviceToHost, st));
+      CUDA_TRY(cudaStreamSynchronize(st));
+      da.tlist = eb.ftl.ptr;
+    }
     da.nlev = 0;
     int64_t nw = 0;
     for (int d = 2; d <= D; ++d) {
       const int k = da.nlev++;
       const double invd = std::ldexp(1.0, -d);
-      da.first[k] = t.level_off[d];
+      da.first[k] = adaptive ? t.level_off[d] - t.level_off[2] : t.level_off[d];
       da.w0[k] = (int)nw;
       da.off[k] = d == D ? ws.part : eb.lvl_off.ptr + (size_t)(d - 2) * n;
       da.h[k][0] = (float)(g.ext[0] * invd);
       da.h[k][1] = (float)(g.ext[1] * invd);
       da.h[k][2] = (float)(g.ext[2] * invd);
-      nw += t.level_count[d];
+      nw += adaptive ? (int64_t)ntgt[d] : (int64_t)t.level_count[d];
     }
     da.w0[da.nlev] = (int)nw;
     const int64_t grid = cdiv(nw * 32, TPB);
-    if (dim == 3) {
+    if (adaptive) {
+      if (grid > 0) {
+        if (want_pot) k_direct_far<3, true, true><<<grid, TPB, 0, st>>>(da);
+        else k_direct_far<3, false, true><<<grid, TPB, 0, st>>>(da);
+      }
+    } else if (dim == 3) {
       if (want_pot) k_direct_far<3, true><<<grid, TPB, 0, st>>>(da);
       else k_direct_far<3, false><<<grid, TPB, 0, st>>>(da);
     } else {
