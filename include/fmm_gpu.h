@@ -9,8 +9,8 @@
  *     QuadratureMethod::integrate(SystemUpdateMethod*, std::vector<Particle>&, const double&)
  *         (src/quadratures/quadrature_method.hpp:24).
  * A reference-side adapter packs the particles into plain arrays and calls
- * the entry points below (the adapter is shown in INTEGRATION.md and shipped
- * as nbody-fmm_b200/cpp/gpu_fmm.hpp).
+ * the entry points below (nbody-fmm_b200/cpp/gpu_fmm.hpp: GpuFMM and
+ * GpuNaiveUpdate as SystemUpdateMethod implementations).
  *
  * Conventions:
  *  - positions / velocities / accelerations are row-major n x dim FP64
@@ -172,6 +172,9 @@ FMM_API int fmm_evaluate(fmm_ctx *ctx, int64_t n, const double *pos, const doubl
  * of the device-side checks. */
 FMM_API int fmm_evaluate_device(fmm_ctx *ctx, int64_t n, const double *d_pos, const double *d_mass, double *d_acc,
                         double *d_pot, void *stream);
+/* Waits for the context's stream and for the stream of the last
+ * fmm_evaluate_device call (which must still exist), not for the whole
+ * device, then returns the status of the device-side checks. */
 FMM_API int fmm_synchronize(fmm_ctx *ctx);
 
 /* Batched ensemble: nsys independent systems stored one after another in
@@ -241,6 +244,16 @@ FMM_API int fmm_tree_leaves(fmm_ctx *ctx, uint64_t *keys, int64_t *start, int64_
  * NodeI::compute_interaction_list (node_i.cpp:23-99).  With tkey == NULL
  * only *count is set. */
 FMM_API int fmm_tree_pairs(fmm_ctx *ctx, int32_t level, int32_t kind, int64_t *count, uint64_t *tkey, uint64_t *skey);
+
+/* Adaptive-target flags (fmm_config.adaptive_leaf = A) of every cell of the
+ * tree kept by fmm_tree_build, level by level from the root, each level in
+ * ascending key order (the order of fmm_tree_level_keys): bit 0, a target
+ * (the root, or a cell whose parent holds more than A particles); bit 1, an
+ * adaptive leaf (a target with at most A particles, or a leaf).  flags holds
+ * the tree's cell count (the sum of fmm_tree_level_size over its levels).
+ * No counterpart in the reference, whose targets are every cell of its
+ * uniform-depth tree (tree.cpp:43-69, node_i.cpp:105-120). */
+FMM_API int fmm_tree_adaptive_flags(fmm_ctx *ctx, int32_t adaptive_leaf, uint8_t *flags);
 
 /* FP64 direct sum that allocates no device memory and needs no context.
  * It has no counterpart in the reference (whose NaiveUpdate allocates

@@ -30,11 +30,13 @@ static __device__ __align__(256) double4 g_noalloc_partials[FMM_NOALLOC_MAX_TARG
 
 static std::mutex g_noalloc_mutex;
 static double4 *g_noalloc_ptr[FMM_NOALLOC_MAX_DEVICES] = {};
+static int g_noalloc_sms[FMM_NOALLOC_MAX_DEVICES] = {};
 
-// Device address of the scratch array on the current device.  In host code
-// the array's name is only a stand-in, so the address must come from
+// Device address of the scratch array on the current device, and that
+// device's SM count (which sizes the source chunks).  In host code the
+// array's name is only a stand-in, so the address must come from
 // cudaGetSymbolAddress, once per device, with that device current.
-static int noalloc_scratch(double4 **out) {
+static int noalloc_scratch(double4 **out, int *sms) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return FMM_ERR_NO_DEVICE;
   if (dev < 0 || dev >= FMM_NOALLOC_MAX_DEVICES) return FMM_ERR_UNSUPPORTED;
@@ -46,9 +48,17 @@ static int noalloc_scratch(double4 **out) {
       set_cuda_error(e, "cudaGetSymbolAddress(g_noalloc_partials)", __FILE__, __LINE__);
       return FMM_ERR_CUDA;
     }
+    int nsm = 0;
+    e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess || nsm <= 0) {
+      set_cuda_error(e, "cudaDeviceGetAttribute(cudaDevAttrMultiProcessorCount)", __FILE__, __LINE__);
+      return FMM_ERR_CUDA;
+    }
+    g_noalloc_sms[dev] = nsm;
     g_noalloc_ptr[dev] = (double4 *)p;
   }
   *out = g_noalloc_ptr[dev];
+  *sms = g_noalloc_sms[dev];
   return FMM_OK;
 }
 
@@ -138,11 +148,12 @@ extern "C" int fmm_direct_noalloc(int32_t dim, int64_t n, const double *d_pos, c
   if (n == 0) return FMM_ERR_INVALID_ARGUMENT;  // targets given but no particles
   if (!d_pos || !d_mass || !d_acc) return FMM_ERR_INVALID_ARGUMENT;
   double4 *scratch = nullptr;
-  int rc = noalloc_scratch(&scratch);
+  int sms = 0;
+  int rc = noalloc_scratch(&scratch, &sms);
   if (rc) return rc;
   const int bx = (int)((nt + NA_THREADS - 1) / NA_THREADS);
   // about four blocks per SM, without exceeding the scratch or 4096 sources per chunk
-  int64_t by = std::max<int64_t>(1, std::min<int64_t>((148 * 4 + bx - 1) / bx, (n + 4095) / 4096));
+  int64_t by = std::max<int64_t>(1, std::min<int64_t>(((int64_t)sms * 4 + bx - 1) / bx, (n + 4095) / 4096));
   by = std::min<int64_t>(by, FMM_NOALLOC_MAX_TARGETS / nt);
   const int64_t chunk = (n + by - 1) / by;
   cudaStream_t st = (cudaStream_t)stream;

@@ -29,6 +29,7 @@ using namespace fmm;
 struct fmm_ctx {
   fmm_config cfg;
   cudaStream_t stream = nullptr;
+  cudaStream_t last_stream = nullptr;  // the stream of the last fmm_evaluate_device call (what fmm_synchronize waits on)
   Workspace ws;
   TreeState tree;
   OpTables ops;
@@ -362,6 +363,7 @@ int fmm_evaluate_device(fmm_ctx *c, int64_t n, const double *d_pos, const double
   if (!c) return FMM_ERR_INVALID_ARGUMENT;
   CUDA_TRY(cudaSetDevice(c->cfg.device));
   cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  c->last_stream = st;
   return evaluate_device(c, n, d_pos, d_mass, d_acc, d_pot, st);
 }
 
@@ -506,10 +508,13 @@ int fmm_autotune(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mas
   return FMM_OK;
 }
 
+// Waits for the context's own stream and the stream of the last
+// fmm_evaluate_device call, not for the whole device: other work of the host
+// process (other libraries' streams) is not waited for.
 int fmm_synchronize(fmm_ctx *c) {
   if (!c) return FMM_ERR_INVALID_ARGUMENT;
   CUDA_TRY(cudaSetDevice(c->cfg.device));
-  CUDA_TRY(cudaDeviceSynchronize());
+  if (c->last_stream && c->last_stream != c->stream) CUDA_TRY(cudaStreamSynchronize(c->last_stream));
   return finish(c, c->stream);
 }
 
@@ -738,6 +743,22 @@ int fmm_tree_pairs(fmm_ctx *c, int32_t level, int32_t kind, int64_t *count, uint
   }
   *count = k;
   return FMM_OK;
+}
+
+int fmm_tree_adaptive_flags(fmm_ctx *c, int32_t adaptive_leaf, uint8_t *flags) {
+  if (!c || !flags || !c->have_tree || adaptive_leaf < 1) return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaSetDevice(c->cfg.device));
+  const int m = c->tree.n_cells;
+  DevBuf<uint8_t> f;
+  DevBuf<int> l;
+  int rc = f.reserve((size_t)m) && l.reserve((size_t)m + 1) ? FMM_OK : FMM_ERR_OUT_OF_MEMORY;
+  if (!rc) rc = adaptive_flags_of_tree(c->ws, c->tree, adaptive_leaf, f.ptr, l.ptr, c->stream);
+  if (!rc && cudaMemcpyAsync(flags, f.ptr, (size_t)m, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess) rc = FMM_ERR_CUDA;
+  if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = FMM_ERR_CUDA;
+  c->ws.launches += 1;
+  f.release();
+  l.release();
+  return rc;
 }
 
 int fmm_last_stats(fmm_ctx *c, fmm_stats *out) {
