@@ -68,7 +68,7 @@ class Oracle:
         self.L = L
 
     # ---- tree
-    def tree(self, pos, threshold):
+    def tree(self, pos, threshold, with_pairs=True):
         pos = _f64(pos)
         n, dim = pos.shape
         h = self.L.orc_tree_build(dim, n, _p(pos, _d), threshold)
@@ -92,7 +92,7 @@ class Oracle:
                 self.L.orc_tree_level_keys(h, d, _p(k, _u64))
                 levels.append(k)
                 pl = []
-                for kind in (0, 1):
+                for kind in ((0, 1) if with_pairs else ()):
                     c = self.L.orc_tree_npairs(h, d, kind)
                     tk = np.zeros(max(c, 1), np.uint64)
                     sk = np.zeros(max(c, 1), np.uint64)

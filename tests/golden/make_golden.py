@@ -20,7 +20,20 @@ Fixtures (inputs stored beside outputs, so tests never regenerate inputs):
   ref_harm.npz    PowerSet<3> and Irregular values, and MultipoleSet<3> P2M moments.
   ref_naive.npz   NaiveUpdate accelerations/G (2D and 3D) and 10 SyplecticEuler
                   steps with NaiveUpdate.
+  ref_se.npz      SyplecticEuler trajectories with forces large enough to
+                  move the state: 10 steps with NaiveUpdate (3D, 300 particles
+                  of mass 1e8) and 10 steps with the 2D FMM (uniform disk,
+                  1000 particles of mass 1e7, p = 12, threshold 16, where the
+                  reference's 2D FMM is accurate).
+  ref_tree_c2.json  Tree::init_tree on the 2^20 Plummer sphere (seed 2,
+                  threshold 64; depth 10, the reference's 32-bit key limit):
+                  depth, level sizes and SHA-256 digests of the leaf keys,
+                  leaf starts and membership (the arrays are 17 MB; about a
+                  minute of the reference's CPU).
+
+    python tests/golden/make_golden.py [fixture ...]   (default: all)
 """
+import hashlib
 import json
 import os
 import sys
@@ -59,8 +72,57 @@ TREE_CASES = [
 ]
 
 
+def tree_digests(depth, leaf_keys, leaf_start, perm):
+    """SHA-256 of the leaf arrays as little-endian uint64 / int64."""
+    return {"leaf_keys": hashlib.sha256(np.asarray(leaf_keys, "<u8").tobytes()).hexdigest(),
+            "leaf_start": hashlib.sha256(np.asarray(leaf_start, "<i8").tobytes()).hexdigest(),
+            "perm": hashlib.sha256(np.asarray(perm, "<i8").tobytes()).hexdigest()}
+
+
+def tree_c2(R):
+    from oracle import _d, _i64, _p, _u64
+
+    pos, _ = workloads.plummer(1 << 20, seed=2)
+    R.L.ref_set_params(2, 64)
+    D = R.L.ref_tree_build(3, len(pos), _p(pos, _d), _p(np.ones(len(pos)), _d))
+    sizes = [int(R.L.ref_tree_level_size(d)) for d in range(D + 1)]
+    keys = np.zeros(sizes[D], np.uint64)
+    start = np.zeros(sizes[D] + 1, np.int64)
+    perm = np.zeros(len(pos), np.int64)
+    R.L.ref_tree_leaves(_p(keys, _u64), _p(start, _i64), _p(perm, _i64))
+    R.L.ref_tree_free()
+    out = {"workload": "plummer(1 << 20, seed=2)", "threshold": 64, "depth": int(D), "level_sizes": sizes,
+           "sha256": tree_digests(D, keys, start, perm)}
+    with open(os.path.join(HERE, "ref_tree_c2.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
+def se_trajectories(R):
+    out = {"G": np.array(R.G)}
+    pos, _ = workloads.uniform_cube(300, seed=40)
+    m = np.full(300, 1e8)
+    vel = np.random.default_rng(41).normal(size=pos.shape) * 0.01
+    x, v = R.se_steps(pos, vel, m, 1e-3, 10, use_fmm=False)
+    out.update({"naive3/pos": pos, "naive3/vel": vel, "naive3/mass": m, "naive3/x": x, "naive3/v": v})
+    pos, _ = workloads.uniform_disk_2d(1000, seed=42)
+    m = np.full(1000, 1e7)
+    vel = np.random.default_rng(43).normal(size=pos.shape) * 0.01
+    x, v = R.se_steps(pos, vel, m, 1e-3, 10, use_fmm=True, p=12, threshold=16)
+    out.update({"fmm2/pos": pos, "fmm2/vel": vel, "fmm2/mass": m, "fmm2/x": x, "fmm2/v": v,
+                "fmm2/p": np.array(12), "fmm2/T": np.array(16)})
+    np.savez_compressed(os.path.join(HERE, "ref_se.npz"), **out)
+
+
 def main():
     R = RefLib()
+    which = set(sys.argv[1:]) or {"base", "se", "tree_c2"}
+    if "se" in which:
+        se_trajectories(R)
+    if "tree_c2" in which:
+        tree_c2(R)
+    if "base" not in which:
+        print("fixtures written to", HERE)
+        return
     with open(os.path.join(HERE, "tree15.json"), "w") as f:
         json.dump(tree15(R), f, indent=1)
 

@@ -68,6 +68,26 @@ def test_tree_matches_reference_fixture(name):
                 assert tree_pairs_set(t, d, kind) == set(zip(z[key][0].tolist(), z[key][1].tolist())), (d, kind)
 
 
+def test_tree_matches_reference_at_2p20():
+    """The tree of the 2^20 Plummer sphere at threshold 64 (seed 2), depth
+    10, where the reference's 32-bit list keys (node_i.cpp:31,63) are at
+    their limit: depth, level sizes and the SHA-256 of the leaf keys, leaf
+    starts and membership equal the reference's Tree::init_tree
+    (ref_tree_c2.json, generated from the compiled reference)."""
+    import hashlib
+
+    g = json.load(open(os.path.join(GOLDEN, "ref_tree_c2.json")))
+    pos, _ = workloads.plummer(1 << 20, seed=2)
+    with fmmgpu.Context(dim=3, leaf_cap=g["threshold"]) as c:
+        t = c.tree(pos, with_pairs=False)
+    assert t["depth"] == g["depth"] == 10
+    assert [len(k) for k in t["level_keys"]] == g["level_sizes"]
+    got = {"leaf_keys": hashlib.sha256(np.asarray(t["leaf_keys"], "<u8").tobytes()).hexdigest(),
+           "leaf_start": hashlib.sha256(np.asarray(t["leaf_start"], "<i8").tobytes()).hexdigest(),
+           "perm": hashlib.sha256(np.asarray(t["perm"], "<i8").tobytes()).hexdigest()}
+    assert got == g["sha256"]
+
+
 @pytest.mark.parametrize("gen,n,T", [("uniform3d", 30000, 16), ("plummer", 50000, 64), ("plummer", 20000, 4)])
 def test_tree_matches_oracle(oracle, gen, n, T):
     pos, _ = workloads.WORKLOADS[gen](n, seed=3)

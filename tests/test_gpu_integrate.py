@@ -76,3 +76,47 @@ def test_two_bodies_approach():
             assert d < prev
             assert x[0, 0] > -10.0 and x[1, 0] < 10.0
             prev = d
+
+
+def test_se_naive_matches_reference_trajectory():
+    """The reference's own SyplecticEuler with NaiveUpdate (ref_naive.npz, 300
+    particles, masses 1/300, 10 steps of 1e-3) and with heavy particles whose
+    forces move the state (ref_se.npz, masses 1e8), replayed with the GPU's
+    FP64 direct sum in NaiveUpdate's form (FMM_SOFT_NAIVE_REF) as the update
+    method (symplectic_euler.cpp:8-15: v += dt a, then x += dt v)."""
+    from conftest import golden
+
+    for fx, pre, sfx in ((golden("ref_naive.npz"), "d3/", ("se_x", "se_v")),
+                         (golden("ref_se.npz"), "naive3/", ("x", "v"))):
+        G = float(fx["G"])
+        x, v, m = fx[pre + "pos"].copy(), fx[pre + "vel"].copy(), fx[pre + "mass"]
+        with fmmgpu.Context(dim=3, G=G) as c:
+            for _ in range(10):
+                v = v + 1e-3 * c.direct(x, m, soft_mode=fmmgpu.FMM_SOFT_NAIVE_REF)
+                x = x + 1e-3 * v
+        xr, vr = fx[pre + sfx[0]], fx[pre + sfx[1]]
+        v0 = fx[pre + "vel"]
+        np.testing.assert_allclose(x, xr, rtol=0, atol=1e-13)
+        # the velocity change is the forces' doing: compared relative to itself
+        dv, dvr = v - v0, vr - v0
+        if pre == "naive3/":
+            assert np.linalg.norm(dvr) > 1e-3 * np.linalg.norm(v0)  # the forces do move the state
+            assert np.linalg.norm(dv - dvr) / np.linalg.norm(dvr) < 1e-10
+
+
+def test_se_fmm_2d_matches_reference_trajectory():
+    """fmm_integrate (SyplecticEuler, 2D FMM at p = 12, threshold 16) against
+    the reference's SyplecticEuler driving its own 2D FMM::update on a
+    uniform disk (ref_se.npz), where the reference's 2D FMM is accurate: the
+    velocity changes agree within 1e-6 relative, the FP32 force bar."""
+    from conftest import golden
+
+    fx = golden("ref_se.npz")
+    x0, v0, m = fx["fmm2/pos"], fx["fmm2/vel"], fx["fmm2/mass"]
+    with fmmgpu.Context(dim=2, p=int(fx["fmm2/p"]), leaf_cap=int(fx["fmm2/T"]), G=float(fx["G"]), direct_max=0) as c:
+        x, v, _ = c.integrate(fmmgpu.FMM_INT_SYMPLECTIC_EULER, 1e-3, 10, x0, v0, m)
+    dv, dvr = v - v0, fx["fmm2/v"] - v0
+    assert np.linalg.norm(dvr) > 1e-3 * np.linalg.norm(v0)
+    assert np.linalg.norm(dv - dvr) / np.linalg.norm(dvr) < 1e-6
+    dx, dxr = x - x0, fx["fmm2/x"] - x0
+    assert np.linalg.norm(dx - dxr) / np.linalg.norm(dxr) < 1e-6

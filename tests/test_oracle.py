@@ -269,3 +269,47 @@ def test_adaptive_flags_have_a_closed_form(oracle, gen, n, T, A):
         np.testing.assert_array_equal((flags[d] >> 1) & 1, leaf.astype(np.uint8))
         covered += int(cnt[d][leaf].sum())
     assert covered == n
+
+
+def test_oracle_se_matches_reference_trajectories(oracle):
+    """The oracle's NaiveUpdate and 2D FMM (mass centres, as the reference
+    forms them) driving SyplecticEuler (symplectic_euler.cpp:8-15) reproduce
+    the reference's own trajectories in ref_se.npz."""
+    z = golden("ref_se.npz")
+    G = float(z["G"])
+
+    def se(force, x, v):
+        for _ in range(10):
+            v = v + 1e-3 * G * force(x)
+            x = x + 1e-3 * v
+        return x, v
+
+    m = z["naive3/mass"]
+    x, v = se(lambda y: oracle.naive_ref(y, m), z["naive3/pos"], z["naive3/vel"])
+    assert rel_l2(v - z["naive3/vel"], z["naive3/v"] - z["naive3/vel"]) < 1e-12
+    assert np.abs(x - z["naive3/x"]).max() < 1e-13
+    m = z["fmm2/mass"]
+    p, T = int(z["fmm2/p"]), int(z["fmm2/T"])
+    x, v = se(lambda y: oracle.fmm(y, m, p, T, centre_mode=1), z["fmm2/pos"], z["fmm2/vel"])
+    assert rel_l2(v - z["fmm2/vel"], z["fmm2/v"] - z["fmm2/vel"]) < 1e-10
+    assert rel_l2(x - z["fmm2/pos"], z["fmm2/x"] - z["fmm2/pos"]) < 1e-10
+
+
+def test_oracle_tree_matches_reference_at_2p20(oracle):
+    """The oracle's tree of the 2^20 Plummer sphere (seed 2, threshold 64,
+    depth 10) has the reference's depth, level sizes and leaf arrays
+    (SHA-256 digests in ref_tree_c2.json, from the compiled reference)."""
+    import hashlib
+    import json
+
+    from fmmgpu import workloads
+
+    g = json.load(open(os.path.join(GOLDEN, "ref_tree_c2.json")))
+    pos, _ = workloads.plummer(1 << 20, seed=2)
+    t = oracle.tree(pos, g["threshold"], with_pairs=False)
+    assert t["depth"] == g["depth"]
+    assert [len(k) for k in t["level_keys"]] == g["level_sizes"]
+    got = {"leaf_keys": hashlib.sha256(np.asarray(t["leaf_keys"], "<u8").tobytes()).hexdigest(),
+           "leaf_start": hashlib.sha256(np.asarray(t["leaf_start"], "<i8").tobytes()).hexdigest(),
+           "perm": hashlib.sha256(np.asarray(t["perm"], "<i8").tobytes()).hexdigest()}
+    assert got == g["sha256"]
