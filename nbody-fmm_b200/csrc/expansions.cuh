@@ -82,6 +82,8 @@ struct ExpBuffers {
   DevBuf<int> alist;             // adaptive targets: the adaptive leaves, then their count
   DevBuf<int> ftl;               // adaptive targets: the direct far field's targets per level, then counts
   DevBuf<double> xs;             // adaptive targets: FP64 positions in leaf order (dim per particle)
+  DevBuf<uint32_t> ccnt;         // adaptive targets: colleague-sum items per adaptive leaf, then their offsets
+  DevBuf<int2> citems;           // adaptive targets: colleague-sum items (adaptive leaf index, source chunk)
 };
 
 // Per-pass parameters.
@@ -108,6 +110,7 @@ struct OrderOpts {
   float *feat = nullptr, *labels = nullptr;
 };
 void upload_class_tables();
+int adaptive_flags_of_tree(const Workspace &ws, const TreeState &t, int A, uint8_t *flag, int *list, cudaStream_t st);
 
 int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, const double *d_pos,
                    const double *d_mass, int p, double eps2, double G,

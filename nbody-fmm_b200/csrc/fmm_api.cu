@@ -184,6 +184,8 @@ int fmm_destroy(fmm_ctx *c) {
   c->eb.alist.release();
   c->eb.ftl.release();
   c->eb.xs.release();
+  c->eb.ccnt.release();
+  c->eb.citems.release();
   c->eb.hbatches.release();
   c->eb.hbatches2.release();
   c->eb.uval.release();

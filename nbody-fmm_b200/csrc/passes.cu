@@ -600,6 +600,11 @@ __device__ inline void pair_acc(float rx, float ry, float rz, float w, float eps
   }
 }
 
+// Fire-and-forget vector reduction into a float4 in global memory.
+__device__ inline void red_add4(float4 *p, float x, float y, float z, float w) {
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(x), "f"(y), "f"(z), "f"(w) : "memory");
+}
+
 struct P2PArgs {
   int leaf_first, nleaves, depth;
   const int *pbeg, *pend, *coll, *parent, *child, *leaf_of;
@@ -693,69 +698,172 @@ __global__ void k_p2p(P2PArgs a) {
   if (lane == 0 && a.pair_count) atomicAdd(a.pair_count, (unsigned long long)npairs);
 }
 
-// Adaptive targets: one warp per adaptive leaf B (any level), listed in
-// alist[0 .. *acount), taken by the warps of a fixed grid in turn.  B's
-// particles sum the particles of B itself (j != i) and of its colleagues at
-// B's level, the pairs that the deeper levels' interaction lists and the leaf
-// level's near field would sum in the uniform tree.  Colleagues touch B, so
-// each difference x_i - x_j is formed in FP64 from the leaf-ordered FP64
-// positions xs and rounded once to FP32.  Writes the output as k_p2p does.
+// Adaptive targets: the colleague sums of the adaptive leaves.  An adaptive
+// leaf B (any level, listed in alist[0 .. acount)) sums the particles of B
+// itself (j != i) and of its colleagues at B's level: the pairs that the
+// deeper levels' interaction lists and the leaf level's near field would sum
+// in the uniform tree.  A colleague may hold millions of particles (a sparse
+// cell next to a dense clump), so the work is cut into items of at most
+// CL_CHUNK sources of B's concatenated colleague list, each one warp's job;
+// items of one B add into the far-field accumulator with vector reductions.
+//
+// Precision: colleagues touch B, so pairs can be far closer than the cell
+// size.  Positions are taken relative to an origin inside B (its first
+// particle) in FP64 and split into FP32 hi + lo parts; a difference
+// (t_hi - s_hi) + (t_lo - s_lo) is then rounded once relative to itself, as
+// in the uniform near field.
+static constexpr int CL_CHUNK = 256;
+
+// Number of items of each listed adaptive leaf (0 past the list's end), over
+// [0, ncell) so that the host needs no count.
+__global__ void k_colleague_count(const int *alist, const unsigned *acount, int ncell, const int *coll,
+                                  const int *pbeg, const int *pend, int ns, uint32_t *cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ncell) return;
+  uint32_t items = 0;
+  if (i < (int)*acount) {
+    const int B = alist[i];
+    long long S = 0;
+    for (int s = 0; s < ns; ++s) {
+      const int C = coll[(int64_t)B * ns + s];
+      if (C >= 0) S += pend[C] - pbeg[C];
+    }
+    items = pend[B] > pbeg[B] ? (uint32_t)((S + CL_CHUNK - 1) / CL_CHUNK) : 0u;
+  }
+  cnt[i] = items;
+}
+
+// items[off[i] + k] = (i, k) for the k-th chunk of listed leaf i.
+__global__ void k_colleague_fill(const unsigned *acount, int ncell, const uint32_t *cnt, const uint32_t *off,
+                                 int2 *items) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ncell || i >= (int)*acount) return;
+  const uint32_t o = off[i], c = cnt[i];
+  for (uint32_t k = 0; k < c; ++k) items[o + k] = make_int2(i, (int)k);
+}
+
+__device__ inline void split_hi_lo(double d, float &hi, float &lo) {
+  hi = (float)d;
+  lo = (float)(d - (double)hi);
+}
+
+// One warp per item (grid-stride): the targets of B in rounds of 32 / Gl
+// (Gl lanes per target share the sources), the item's sources staged 32 at
+// a time through shared memory.
 template <int DIM, bool POT>
-__global__ void k_p2p_cells(P2PArgs a, const int *alist, const unsigned *acount, const double *xs) {
+__global__ void __launch_bounds__(256) k_colleague_sum(P2PArgs a, const int *alist, const int2 *items,
+                                                       const uint32_t *nitems, const double *xs, float4 *far) {
   constexpr int NS = DIM == 3 ? 27 : 9;
-  const int lane = threadIdx.x & 31;
+  __shared__ float4 s_hi_all[8][32], s_lo_all[8][32];
+  __shared__ int s_pref_all[8][NS + 1], s_cell_all[8][NS];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  float4 *s_hi = s_hi_all[wib], *s_lo = s_lo_all[wib];
+  int *s_pref = s_pref_all[wib], *s_cell = s_cell_all[wib];
   const int nwarps = (int)((gridDim.x * blockDim.x) >> 5);
-  const int ncells = (int)*acount;
-  bool bad = false;
+  const int total = (int)*nitems;
   long long npairs = 0;
-  for (int wl = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); wl < ncells; wl += nwarps) {
-    const int g = alist[wl];
-    const int tb = a.pbeg[g], nt = a.pend[g] - tb;
+  for (int it = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5); it < total; it += nwarps) {
+    const int2 item = items[it];
+    const int B = alist[item.x];
+    const int tb = a.pbeg[B], nt = a.pend[B] - tb;
+    // B's colleagues (B itself included), compacted, with the prefix of their sizes
+    const int C = lane < NS ? a.coll[(int64_t)B * NS + lane] : -1;
+    const int nc = C >= 0 ? a.pend[C] - a.pbeg[C] : 0;
+    const unsigned m = __ballot_sync(0xffffffffu, C >= 0);
+    int x = nc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    const int ncoll = __popc(m);
+    if (C >= 0) {
+      const int at = __popc(m & ((1u << lane) - 1u));
+      s_cell[at] = C;
+      s_pref[at + 1] = x;  // inclusive prefix (zero-size colleagues repeat the previous value)
+    }
+    if (lane == 0) s_pref[0] = 0;
+    __syncwarp();
+    const int S = s_pref[ncoll];
+    const int f0 = item.y * CL_CHUNK, f1 = min(S, f0 + CL_CHUNK);
+    // B's own particles in the concatenation (the pairs j == i are skipped)
+    const int bl = __ffs(__ballot_sync(0xffffffffu, C == B)) - 1;
+    const int bend = __shfl_sync(0xffffffffu, x, bl), bbeg = bend - __shfl_sync(0xffffffffu, nc, bl);
+    const double ox = xs[DIM * (size_t)tb], oy = xs[DIM * (size_t)tb + 1], oz = DIM == 3 ? xs[DIM * (size_t)tb + 2] : 0.0;
     const int tp = nt < 32 ? nt : 32;
     int Gl = 1;
     while (Gl * 2 * tp <= 32) Gl *= 2;
     const int tpp = 32 / Gl;
-    const int *cl = a.coll + (int64_t)g * NS;
     for (int t0 = 0; t0 < nt; t0 += tpp) {
       const int ti = t0 + lane / Gl, sub = lane % Gl;
       const bool act = ti < nt;
       const int me_i = tb + (act ? ti : 0);
-      const double xi = xs[DIM * (size_t)me_i], yi = xs[DIM * (size_t)me_i + 1],
-                   zi = DIM == 3 ? xs[DIM * (size_t)me_i + 2] : 0.0;
+      float thx, tlx, thy, tly, thz = 0.f, tlz = 0.f;
+      split_hi_lo(xs[DIM * (size_t)me_i] - ox, thx, tlx);
+      split_hi_lo(xs[DIM * (size_t)me_i + 1] - oy, thy, tly);
+      if (DIM == 3) split_hi_lo(xs[DIM * (size_t)me_i + 2] - oz, thz, tlz);
       float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
-      for (int s = 0; s < NS; ++s) {
-        const int S = cl[s];
-        if (S < 0) continue;
-        const int se = a.pend[S];
-        if (t0 == 0 && lane == 0) npairs += (long long)nt * (se - a.pbeg[S]) - (S == g ? nt : 0);
-        for (int j = a.pbeg[S] + sub; j < se; j += Gl) {
-          if (j == me_i) continue;
-          const float rx = (float)(xi - xs[DIM * (size_t)j]);
-          const float ry = (float)(yi - xs[DIM * (size_t)j + 1]);
-          const float rz = DIM == 3 ? (float)(zi - xs[DIM * (size_t)j + 2]) : 0.f;
-          pair_acc<DIM, true, POT>(rx, ry, rz, a.part[j].w, a.eps2, ax, ay, az, ph);
+      for (int fb = f0; fb < f1; fb += 32) {
+        const int f = fb + lane;
+        if (f < f1) {
+          // colleague holding concatenated position f: the last k with s_pref[k] <= f
+          int lo = 0, hi = ncoll - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (s_pref[mid] <= f) lo = mid;
+            else hi = mid - 1;
+          }
+          const int j = a.pbeg[s_cell[lo]] + (f - s_pref[lo]);
+          float hx, lx, hy, ly, hz = 0.f, lz = 0.f;
+          split_hi_lo(xs[DIM * (size_t)j] - ox, hx, lx);
+          split_hi_lo(xs[DIM * (size_t)j + 1] - oy, hy, ly);
+          if (DIM == 3) split_hi_lo(xs[DIM * (size_t)j + 2] - oz, hz, lz);
+          s_hi[lane] = make_float4(hx, hy, hz, a.part[j].w);
+          s_lo[lane] = make_float4(lx, ly, lz, __int_as_float(j));
         }
+        __syncwarp();
+        const int cnt = min(32, f1 - fb);
+        for (int k = sub; k < cnt; k += Gl) {
+          const float4 q = s_hi[k], ql = s_lo[k];
+          if (__float_as_int(ql.w) == me_i) continue;
+          const float rx = (thx - q.x) + (tlx - ql.x);
+          const float ry = (thy - q.y) + (tly - ql.y);
+          const float rz = (thz - q.z) + (tlz - ql.z);
+          pair_acc<DIM, true, POT>(rx, ry, rz, q.w, a.eps2, ax, ay, az, ph);
+        }
+        __syncwarp();
       }
       for (int o = 1; o < Gl; o <<= 1) {
         ax += __shfl_xor_sync(0xffffffffu, ax, o);
         ay += __shfl_xor_sync(0xffffffffu, ay, o);
         az += __shfl_xor_sync(0xffffffffu, az, o);
-        ph += __shfl_xor_sync(0xffffffffu, ph, o);
+        if (POT) ph += __shfl_xor_sync(0xffffffffu, ph, o);
       }
-      if (act && sub == 0) {
-        const float4 f = a.far[me_i];
-        const uint32_t o = a.perm[me_i];
-        double vx = a.G * ((double)f.x + ax), vy = a.G * ((double)f.y + ay), vz = a.G * ((double)f.z + az);
-        a.acc[DIM * (size_t)o] = vx;
-        a.acc[DIM * (size_t)o + 1] = vy;
-        if (DIM == 3) a.acc[3 * (size_t)o + 2] = vz;
-        if (a.pot) a.pot[o] = a.G * ((double)f.w + ph);
-        bad |= !(isfinite(vx) && isfinite(vy) && isfinite(vz));
-      }
+      if (act && sub == 0) red_add4(far + me_i, ax, ay, az, ph);
     }
+    if (lane == 0) npairs += (long long)nt * (f1 - f0) - max(0, min(f1, bend) - max(f0, bbeg));
   }
-  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.err, FMM_DEV_ERR_NONFINITE_OUTPUT);
   if (lane == 0 && a.pair_count && npairs) atomicAdd(a.pair_count, (unsigned long long)npairs);
+}
+
+// The output: acc[perm[i]] = G * far[i] (and the potential), with the
+// finiteness check, after every contribution was added into far.
+template <int DIM>
+__global__ void k_far_output(const float4 *far, const uint32_t *perm, int64_t n, double G, double *acc, double *pot,
+                             unsigned int *err) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  bool bad = false;
+  if (i < n) {
+    const float4 f = far[i];
+    const uint32_t o = perm[i];
+    const double vx = G * (double)f.x, vy = G * (double)f.y, vz = G * (double)f.z;
+    acc[DIM * (size_t)o] = vx;
+    acc[DIM * (size_t)o + 1] = vy;
+    if (DIM == 3) acc[3 * (size_t)o + 2] = vz;
+    if (pot) pot[o] = G * (double)f.w;
+    bad = !(isfinite(vx) && isfinite(vy) && isfinite(vz));
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(err, FMM_DEV_ERR_NONFINITE_OUTPUT);
 }
 
 // --------------------------------------------------------- direct far field
@@ -782,10 +890,6 @@ __global__ void k_level_offsets(const double *pos, const double *mass, const uin
     out[(size_t)(d - d0) * n + i] =
         make_float4((float)(px - cx), (float)(py - cy), DIM == 3 ? (float)(pz - cz) : 0.f, w);
   }
-}
-
-__device__ inline void red_add4(float4 *p, float x, float y, float z, float w) {
-  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(p), "f"(x), "f"(y), "f"(z), "f"(w) : "memory");
 }
 
 static constexpr int DF_MAX_LEVELS = 33;
@@ -1460,6 +1564,20 @@ __global__ void k_level_targets(const uint8_t *aflag, int cell0, int first, int 
   if (tgt) seg[base + __popc(m & ((1u << lane) - 1u))] = g;
 }
 
+// The adaptive-target flags of every cell of a built tree, root first
+// (fmm_tree_adaptive_flags): the kernel the force pass runs, into flag[],
+// with its list of adaptive leaves in list[0 .. ncell) and their count at
+// list[ncell].
+int adaptive_flags_of_tree(const Workspace &ws, const TreeState &t, int A, uint8_t *flag, int *list, cudaStream_t st) {
+  if (t.depth < 1 || t.n_cells <= 0) return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaMemsetAsync(list + t.n_cells, 0, sizeof(int), st));
+  k_adaptive_flags<<<cdiv(t.n_cells, 256), 256, 0, st>>>(ws.cell_pbeg, ws.cell_pend, ws.cell_parent, t.cell0,
+                                                          t.n_cells, t.level_off[1], t.level_off[t.depth], A, flag,
+                                                          list, (unsigned *)(list + t.n_cells));
+  CUDA_TRY(cudaGetLastError());
+  return FMM_OK;
+}
+
 // FP64 positions in leaf order: xs[i] = pos[perm[i]].
 __global__ void k_gather_pos(const double *pos, const uint32_t *perm, int64_t n, int dim, double *xs) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -2002,6 +2120,33 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     k_l2p2d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far);
   ws.launches += 1;
   if (ev) cudaEventRecord(ev[4], st);
+  // adaptive targets: the direct far field's targets per level and the
+  // colleague-sum items, counted on the device and read back together
+  std::vector<unsigned> ntgt;
+  uint32_t n_items = 0;
+  if (adaptive) {
+    const int ncl = t.level_off[D] + t.level_count[D] - t.level_off[2];
+    if (!eb.ftl.reserve((size_t)ncl + D + 2) || !eb.ccnt.reserve(2 * (size_t)ncell)) return FMM_ERR_OUT_OF_MEMORY;
+    unsigned *cnt = (unsigned *)(eb.ftl.ptr + ncl);
+    CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned) * (D + 2), st));
+    for (int d = 2; d <= D; ++d)
+      k_level_targets<<<cdiv(t.level_count[d], TPB), TPB, 0, st>>>(
+          eb.aflag.ptr, cell0, t.level_off[d], t.level_count[d], ws.cell_pbeg, ws.cell_pend, direct_max,
+          any_fdirect, eb.ftl.ptr + (t.level_off[d] - t.level_off[2]), cnt + d);
+    const unsigned *acount = (const unsigned *)(eb.alist.ptr + ncell);
+    uint32_t *ccnt = eb.ccnt.ptr, *coff = eb.ccnt.ptr + ncell;
+    k_colleague_count<<<cdiv(ncell, TPB), TPB, 0, st>>>(eb.alist.ptr, acount, ncell, ws.cell_coll, ws.cell_pbeg,
+                                                         ws.cell_pend, dim == 3 ? 27 : 9, ccnt);
+    exclusive_scan(ws, ccnt, coff, ncell, cnt + D + 1, st);
+    ws.launches += D;
+    ntgt.assign(D + 2, 0u);
+    CUDA_TRY(cudaMemcpyAsync(ntgt.data(), cnt, sizeof(unsigned) * (D + 2), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    n_items = ntgt[D + 1];
+    if (!eb.citems.reserve((size_t)n_items + 1)) return FMM_ERR_OUT_OF_MEMORY;
+    k_colleague_fill<<<cdiv(ncell, TPB), TPB, 0, st>>>(acount, ncell, ccnt, coff, eb.citems.ptr);
+    ws.launches += 1;
+  }
   // direct far field, all levels >= 2 (they have interaction lists) in one
   // launch, coarse levels first so that their long warps start early
   if ((direct_max > 0 || any_fdirect) && D >= 2) {
@@ -2019,25 +2164,9 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     da.any_fdirect = any_fdirect;
     da.far = ws.far;
     da.pair_count = ws.counters + 3;
-    da.tlist = nullptr;
     // adaptive targets: each level's targets listed in its own segment of
     // the list (the level's cells in order, gaps after the targets)
-    std::vector<unsigned> ntgt;
-    if (adaptive) {
-      const int ncl = t.level_off[D] + t.level_count[D] - t.level_off[2];
-      if (!eb.ftl.reserve((size_t)ncl + D + 1)) return FMM_ERR_OUT_OF_MEMORY;
-      unsigned *cnt = (unsigned *)(eb.ftl.ptr + ncl);
-      CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned) * (D + 1), st));
-      for (int d = 2; d <= D; ++d)
-        k_level_targets<<<cdiv(t.level_count[d], TPB), TPB, 0, st>>>(
-            eb.aflag.ptr, cell0, t.level_off[d], t.level_count[d], ws.cell_pbeg, ws.cell_pend, direct_max,
-            any_fdirect, eb.ftl.ptr + (t.level_off[d] - t.level_off[2]), cnt + d);
-      ws.launches += D - 1;
-      ntgt.assign(D + 1, 0u);
-      CUDA_TRY(cudaMemcpyAsync(ntgt.data(), cnt, sizeof(unsigned) * (D + 1), cudaMemcpyDeviceToHost, st));
-      CUDA_TRY(cudaStreamSynchronize(st));
-      da.tlist = eb.ftl.ptr;
-    }
+    da.tlist = adaptive ? eb.ftl.ptr : nullptr;
     da.nlev = 0;
     int64_t nw = 0;
     for (int d = 2; d <= D; ++d) {
@@ -2097,13 +2226,18 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   pa.pair_count = ws.counters + 1;
   const int pgrid = cdiv((int64_t)pa.nleaves * 32, TPB);
   if (adaptive) {
-    // every particle lies in exactly one adaptive leaf, which writes its output
+    // every particle lies in exactly one adaptive leaf: its colleague sums
+    // add into far, then every particle's output is written
     if (!eb.xs.reserve((size_t)n * 3)) return FMM_ERR_OUT_OF_MEMORY;
     k_gather_pos<<<cdiv(n, TPB), TPB, 0, st>>>(d_pos_g, t.d_perm, n, dim, eb.xs.ptr);
-    ws.launches += 1;
-    const unsigned *acount = (const unsigned *)(eb.alist.ptr + ncell);
-    if (want_pot) k_p2p_cells<3, true><<<148 * 8, TPB, 0, st>>>(pa, eb.alist.ptr, acount, eb.xs.ptr);
-    else k_p2p_cells<3, false><<<148 * 8, TPB, 0, st>>>(pa, eb.alist.ptr, acount, eb.xs.ptr);
+    const uint32_t *nit = (const uint32_t *)(eb.ftl.ptr + (t.level_off[D] + t.level_count[D] - t.level_off[2])) + D + 1;
+    if (n_items > 0) {
+      const int cgrid = (int)std::min<int64_t>(cdiv((int64_t)n_items * 32, TPB), 148 * 16);
+      if (want_pot) k_colleague_sum<3, true><<<cgrid, TPB, 0, st>>>(pa, eb.alist.ptr, eb.citems.ptr, nit, eb.xs.ptr, ws.far);
+      else k_colleague_sum<3, false><<<cgrid, TPB, 0, st>>>(pa, eb.alist.ptr, eb.citems.ptr, nit, eb.xs.ptr, ws.far);
+    }
+    k_far_output<3><<<cdiv(n, TPB), TPB, 0, st>>>(ws.far, t.d_perm, n, G, d_acc, d_pot, ws.dev_err);
+    ws.launches += 3;
   } else if (dim == 3) {
     if (want_pot) k_p2p<3, true><<<pgrid, TPB, 0, st>>>(pa);
     else k_p2p<3, false><<<pgrid, TPB, 0, st>>>(pa);

@@ -51,7 +51,8 @@ EXPORTED = (
     "fmm_strerror", "fmm_version", "fmm_config_default", "fmm_create", "fmm_destroy", "fmm_evaluate",
     "fmm_evaluate_device", "fmm_synchronize", "fmm_direct", "fmm_direct_device", "fmm_integrate",
     "fmm_tree_build", "fmm_tree_depth", "fmm_tree_level_size", "fmm_tree_level_keys", "fmm_tree_leaves",
-    "fmm_tree_pairs", "fmm_last_stats", "fmm_launch_count", "fmm_direct_noalloc", "fmm_order_set_model",
+    "fmm_tree_pairs", "fmm_tree_adaptive_flags", "fmm_last_stats", "fmm_launch_count", "fmm_direct_noalloc",
+    "fmm_order_set_model",
     "fmm_order_get_model", "fmm_order_collect", "fmm_order_train", "fmm_order_forward_grad", "fmm_autotune",
     "fmm_evaluate_batched", "fmm_frames_open", "fmm_frames_write", "fmm_frames_write_device", "fmm_frames_flush",
     "fmm_frames_close", "fmm_integrate_frames",
@@ -129,6 +130,7 @@ def load_library(path=LIB_PATH):
     L.fmm_tree_level_keys.argtypes = [_vp, ctypes.c_int32, _u64]
     L.fmm_tree_leaves.argtypes = [_vp, _u64, _i64, _i64]
     L.fmm_tree_pairs.argtypes = [_vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64), _u64, _u64]
+    L.fmm_tree_adaptive_flags.argtypes = [_vp, ctypes.c_int32, ctypes.c_void_p]
     L.fmm_last_stats.argtypes = [_vp, ctypes.POINTER(FmmStats)]
     L.fmm_launch_count.restype = ctypes.c_int64
     L.fmm_launch_count.argtypes = [_vp]
@@ -344,6 +346,21 @@ class Context:
                     pl.append((tk[: c.value], sk[: c.value]))
             pairs.append(pl)
         return dict(depth=D, leaf_keys=keys, leaf_start=start, perm=perm, level_keys=levels, pairs=pairs)
+
+    def adaptive_flags(self, adaptive_leaf):
+        """The adaptive-target flags of the tree last built by tree(), one
+        uint8 array per level in the order of its level_keys (bit 0 target,
+        bit 1 adaptive leaf; fmm_tree_adaptive_flags)."""
+        sizes = []
+        cnt = ctypes.c_int64()
+        D = ctypes.c_int32()
+        _check(_lib.fmm_tree_depth(self._h, ctypes.byref(D)))
+        for d in range(D.value + 1):
+            _check(_lib.fmm_tree_level_size(self._h, d, ctypes.byref(cnt)))
+            sizes.append(cnt.value)
+        flags = np.zeros(sum(sizes), np.uint8)
+        _check(_lib.fmm_tree_adaptive_flags(self._h, adaptive_leaf, flags.ctypes.data_as(ctypes.c_void_p)))
+        return np.split(flags, np.cumsum(sizes)[:-1])
 
     def stats(self):
         s = FmmStats()

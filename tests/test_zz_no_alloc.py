@@ -66,3 +66,37 @@ def test_direct_noalloc_rejects_oversize():
         fmmgpu.direct_noalloc(3, 4, _ptr(d), _ptr(d), _ptr(d), None, ntargets=fmmgpu.FMM_NOALLOC_MAX_TARGETS + 1,
                               targets_ptr=_ptr(d))
     assert e.value.code == fmmgpu.FMM_ERR_TOO_LARGE
+
+
+def test_direct_noalloc_full_scratch_and_two_d():
+    """A call with the largest target count the scratch holds (one source
+    chunk per target) and a 2D call with NaiveUpdate's softening, each
+    against fmm_direct."""
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    nmax = fmmgpu.FMM_NOALLOC_MAX_TARGETS
+    n = 20000
+    pos, m = workloads.plummer(n, seed=22)
+    targets = np.random.default_rng(4).integers(0, n, nmax).astype(np.int64)  # repeats allowed
+    pos2 = np.random.default_rng(5).random((n, 2))
+    m2 = np.full(n, 1.0 / n)
+    with fmmgpu.Context(dim=3, G=1.0) as c:
+        ref_full = c.direct(pos, m, targets=targets)
+    with fmmgpu.Context(dim=2, G=1.0) as c:
+        ref_2d = c.direct(pos2, m2, soft_mode=fmmgpu.FMM_SOFT_NAIVE_REF)
+    d_pos, d_mass = torch.from_numpy(pos).to(dev), torch.from_numpy(m).to(dev)
+    d_tg = torch.from_numpy(targets).to(dev)
+    d_acc = torch.full((nmax, 3), float("nan"), dtype=torch.float64, device=dev)
+    d_pos2, d_m2 = torch.from_numpy(pos2).to(dev), torch.from_numpy(m2).to(dev)
+    d_acc2 = torch.full((n, 2), float("nan"), dtype=torch.float64, device=dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.synchronize(dev)
+    fmmgpu.direct_noalloc(3, n, _ptr(d_pos), _ptr(d_mass), _ptr(d_acc), None, ntargets=nmax, targets_ptr=_ptr(d_tg),
+                          stream=stream.cuda_stream)
+    stream.synchronize()
+    assert rel_l2(d_acc.cpu().numpy(), ref_full) < 1e-12
+    fmmgpu.direct_noalloc(2, n, _ptr(d_pos2), _ptr(d_m2), _ptr(d_acc2), None, soft_mode=fmmgpu.FMM_SOFT_NAIVE_REF,
+                          stream=stream.cuda_stream)
+    stream.synchronize()
+    assert rel_l2(d_acc2.cpu().numpy(), ref_2d) < 1e-12
