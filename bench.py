@@ -1,47 +1,64 @@
 #!/usr/bin/env python
 """Throughput of the FMM force pass on B200 at 1e-6 relative force error
-(particles per second), tensor-core translations against the plain FP32 GPU
-FMM.
+(particles per second): learned M2L orders on the tensor cores against the
+plain FP32 GPU FMM.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload mixture|plummer|disk2d]
 
 A step is one force evaluation of the whole system: tree build (the
 reference's Tree::init_tree) and every FMM pass, the work of the
-reference's FMM::update (src/system_updaters/FMM.cpp:9-12).  Workload: a 3D
-Plummer sphere of N = 2^20 particles (scale radius 1, truncated at 20, seed
-2, equal masses summing to 1), leaf capacity 64, forces in FP32 from FP64
-positions, G = 1, at expansion order p = 12: the lowest order whose relative
-L2 force error against the FP64 direct sum is <= 1e-6 on this input
-(p = 11 gives 1.06e-6, p = 12 8.6e-7).  M2L, M2M and L2L run on the tensor
-cores (tcgen05, 3xBF16 split, FP32 accumulation); interaction-list pairs with
-n_T * n_S <= direct_max are summed directly.
+reference's FMM::update (src/system_updaters/FMM.cpp:9-12).
+
+Workloads (seeded synthetic inputs; the reference measures on no dataset):
+  mixture (default): 3D, N = 2^24 particles in 32 Plummer spheres (scale
+       radii log-uniform in [0.01, 0.1], centres uniform in [0,1]^3, equal
+       mass per sphere, seed 5), maximum order p = 12, leaf capacity tuned
+       with the direct-pair threshold (the configuration leaves it open),
+       error judged against the FP64 direct sum on 8192 sampled targets.
+  plummer: 3D Plummer sphere N = 2^20 (scale radius 1, truncated at 20, seed
+       2), leaf capacity 64, p = 12, 4096 judge targets.
+  disk2d: 2D, N = 2^22: half uniform in the unit disk, half in 64 Gaussian
+       clumps (sigma 0.005), log-normal(0, 0.5) masses normalised to 1 (seed
+       3), p = 16, leaf capacity 32, tensor-core M2L at fixed p (learned
+       orders are 3D only), 4096 judge targets.
+Forces in FP32 from FP64 positions, G = 1.  M2L, M2M and L2L run on the
+tensor cores (tcgen05, 3xBF16 split, FP32 accumulation); interaction-list
+pairs with n_T * n_S <= direct_max are summed directly.  In 3D the targets
+are adaptive (fmm_config.adaptive_leaf, default 32, tuned over {0, 16, 32,
+64} with the other settings; 0 is the reference's uniform targets): cells
+whose parent holds at most that many particles are no targets, and the
+particles of the deepest target cells sum their colleagues directly.
 
 value: N * K / (sum of the K per-step device times), inputs resident in HBM,
        timed with CUDA events on the launching stream; a 256 MiB buffer is
        written between steps (outside the event pair) to flush L2.  With N
        GPUs each rank runs its own replica (the single-system pass does not
        shard), value sums the particles of all ranks over the slowest rank.
-order: the tensor-core tiles take the orders the learned MLP picks
+order: (3D) the tensor-core tiles take the orders the learned MLP picks
        (FMM_ORDER_LEARNED); the judge (512 targets against the FP64 direct
        sum, budget 1e-6, fixed-order fallback) checks the first and then every
-       8th evaluation, inside the timed steps.  The first evaluation runs at
-       p (warm-up).
+       8th evaluation, inside the timed steps, so value includes its cost.
+       The first evaluation runs at p (warm-up).
 tc_fixed_order, plain: the same workload and maximum order through the
        tensor cores at fixed p, and through the plain FP32 GPU FMM (SIMT
-       contractions, FMM_M2L_FP32), timed the same way; speedup_vs_plain is
-       the headline against the latter at equal error.
+       contractions, FMM_M2L_FP32), timed the same way and autotuned the same
+       way; speedup_vs_plain is the headline against the latter at equal
+       error.
 e2e:   the headline configuration through the public C ABI with pinned host
        buffers (fmm_evaluate: host-to-device copy of positions and masses,
        the pass, device-to-host copy of accelerations), wall clock per call.
-autotune: before timing, fmm_autotune times the candidate direct-pair
-       thresholds on this input and keeps the fastest (setup, not timed).
+autotune: before timing, fmm_autotune times candidate settings on this input
+       and keeps the fastest (setup, not timed).
 roofline: the dominant kernel by live-measured time, and both of the two
        largest: the tensor-core M2L (algorithmic FLOPs 2 K^2 per
-       interaction-list pair, K = (p+1)^2, against the measured sustained
-       BF16 peak) and the direct far field (20 FLOPs per particle pair,
-       against the FP32 peak derived from the SM count and clock).
+       interaction-list pair, K = (p+1)^2 in 3D and 2p+1 in 2D, against the
+       measured sustained BF16 peak) and the direct far field (20 FLOPs per
+       particle pair, against the FP32 peak derived from the SM count and
+       clock).
 cpu_baseline: the reference itself (compiled from its sources into
-       oracle/_ref) timing FMM::update on a bounded Plummer sample, 1 thread.
+       oracle/_ref) timing FMM::update on a bounded sample of the workload,
+       1 thread, with the reference's own force error on that sample.
 --impl reference: the reference's CPU FMM on all host cores (one process per
        core, each a bounded sample of the same workload), rank 0 only.
 """
@@ -62,13 +79,35 @@ sys.path.insert(0, os.path.join(ROOT, "nbody-fmm_b200"))
 METRIC = "3D FMM particles/s at 1e-6 rel force err: learned+TC vs plain GPU FMM"
 UNIT = "particles/s"
 REF_SAMPLE_N = 512           # particles per reference process per step (about 2 s at p = 12)
-CPU_SAMPLE_N = 2048     # single-thread CPU baseline sample (about 20 s at p = 12)
+# single-thread CPU baseline sample: about 20 s at p = 12.  The 65,536
+# particles a CPU comparison would ideally use take about 8 minutes of one
+# core at the reference's ~130 particles/s, longer than the whole bench run.
+CPU_SAMPLE_N = 2048
+JUDGE_TARGETS = {"mixture": 8192, "plummer": 4096, "disk2d": 4096}
 
 
-def workload_desc(n, p, leaf, m2l, direct_max=None, mixture=False):
-    inputs = (f"3D clustered mixture N={n} (32 Plummer spheres, scale radii log-uniform in [0.01, 0.1], "
-              f"centres uniform in [0,1]^3, equal mass per sphere, seed 5)" if mixture
-              else f"3D Plummer sphere N={n} (a=1, r<=20, seed 2)")
+def workload_inputs(workload, n):
+    if workload == "mixture":
+        return (f"3D clustered mixture N={n} (32 Plummer spheres, scale radii log-uniform in [0.01, 0.1], "
+                f"centres uniform in [0,1]^3, equal mass per sphere, seed 5)")
+    if workload == "disk2d":
+        return (f"2D disk N={n} (half uniform in the unit disk, half in 64 Gaussian clumps sigma 0.005, "
+                f"log-normal(0, 0.5) masses normalised to 1, seed 3)")
+    return f"3D Plummer sphere N={n} (a=1, r<=20, seed 2)"
+
+
+def make_workload(workload, n):
+    from fmmgpu import workloads
+
+    if workload == "mixture":
+        return workloads.plummer_mixture(n, seed=5)
+    if workload == "disk2d":
+        return workloads.disk_clumps_2d(n, seed=3)
+    return workloads.plummer(n, seed=2)
+
+
+def workload_desc(n, p, leaf, m2l, direct_max=None, workload="mixture"):
+    inputs = workload_inputs(workload, n)
     return {
         "workload": f"{inputs}, p={p}, leaf capacity {leaf}, "
                     f"one force evaluation (tree build + all FMM passes) per step",
@@ -237,12 +276,13 @@ def run_ours(args, world, rank, local):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     n, p, leaf = args.n, args.p, args.leaf
     mixture = args.workload == "mixture"
+    dim = 2 if args.workload == "disk2d" else 3
     tune_leaf = mixture  # the mixture's configuration leaves the leaf capacity open
     mode = fmmgpu.FMM_M2L_TC if args.m2l == "tc" else fmmgpu.FMM_M2L_FP32
-    pos, mass = workloads.plummer_mixture(n, seed=5) if mixture else workloads.plummer(n, seed=2)
+    pos, mass = make_workload(args.workload, n)
     d_pos = torch.from_numpy(pos).to(dev)
     d_mass = torch.from_numpy(mass).to(dev)
-    d_acc = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    d_acc = torch.empty((n, dim), dtype=torch.float64, device=dev)
     d_pot = torch.empty((n,), dtype=torch.float64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     # a stream of our own (torch's default stream has handle 0, which the C
@@ -255,34 +295,42 @@ def run_ours(args, world, rank, local):
             torch.distributed.barrier()
         torch.cuda.synchronize(dev)
 
-    # the judge: FP64 direct sum on 4096 sampled targets (8192 on the mixture)
+    # the judge: FP64 direct sum on 8192 sampled targets (mixture) or 4096
     rng = np.random.default_rng(7)
-    tg = np.sort(rng.choice(n, size=min(8192 if mixture else 4096, n), replace=False)).astype(np.int64)
+    tg = np.sort(rng.choice(n, size=min(JUDGE_TARGETS[args.workload], n), replace=False)).astype(np.int64)
     d_tg = torch.from_numpy(tg).to(dev)
-    r_acc = torch.empty((len(tg), 3), dtype=torch.float64, device=dev)
+    r_acc = torch.empty((len(tg), dim), dtype=torch.float64, device=dev)
     r_pot = torch.empty((len(tg),), dtype=torch.float64, device=dev)
-    with fmmgpu.Context(dim=3, G=1.0, device=local) as jc:
+    with fmmgpu.Context(dim=dim, G=1.0, device=local) as jc:
         jc.direct_device(n, d_pos.data_ptr(), d_mass.data_ptr(), len(tg), d_tg.data_ptr(), r_acc.data_ptr(),
                          r_pot.data_ptr(), stream=stream.cuda_stream)
     torch.cuda.synchronize(dev)
     judge = (d_tg, r_acc.cpu().numpy(), r_pot.cpu().numpy())
 
     # headline: the chosen M2L mode
-    learned = args.order == "learned" and mode == fmmgpu.FMM_M2L_TC
+    learned = args.order == "learned" and mode == fmmgpu.FMM_M2L_TC and dim == 3
     okw = dict(order_mode=fmmgpu.FMM_ORDER_LEARNED, judge_samples=args.judge, judge_budget=1e-6,
                judge_every=args.judge_every) if learned else {}
-    ctx = fmmgpu.Context(dim=3, p=p, leaf_cap=leaf, m2l_mode=mode, G=1.0, device=local, direct_max=args.direct_max,
-                         adaptive_leaf=args.adaptive, **okw)
+    # adaptive targets (3D): a fixed threshold, or by default 32 with the
+    # autotuner trying 0 (the reference's uniform targets), 16 and 64 too
+    tune_adaptive = dim == 3 and args.adaptive is None
+    adaptive = (32 if tune_adaptive else args.adaptive) if dim == 3 else 0
+    ctx = fmmgpu.Context(dim=dim, p=p, leaf_cap=leaf, m2l_mode=mode, G=1.0, device=local, direct_max=args.direct_max,
+                         adaptive_leaf=adaptive, **okw)
     tune = None
     if args.autotune and args.direct_max < 0:
-        # the autotuner picks the direct-pair threshold on this input (setup, outside the timed steps)
+        # the autotuner picks the direct-pair threshold (and on the mixture the
+        # leaf capacity, on 3D inputs the adaptive-target threshold) on this
+        # input: setup, outside the timed steps
         t0 = time.perf_counter()
         cands, best = ctx.autotune(n, d_pos.data_ptr(), d_mass.data_ptr(), tune_leaf=tune_leaf,
-                                   stream=stream.cuda_stream)
+                                   tune_adaptive=tune_adaptive, stream=stream.cuda_stream)
         tune = {"seconds": time.perf_counter() - t0, "chosen_direct_max": best["direct_max"],
-                "chosen_leaf_cap": best["leaf_cap"],
-                "candidates": [[x["leaf_cap"], x["direct_max"], round(x["ms"], 3)] for x in cands]}
+                "chosen_leaf_cap": best["leaf_cap"], "chosen_adaptive_leaf": best["adaptive_leaf"],
+                "candidates (leaf_cap, direct_max, adaptive_leaf, ms)":
+                    [[x["leaf_cap"], x["direct_max"], x["adaptive_leaf"], round(x["ms"], 3)] for x in cands]}
         leaf = best["leaf_cap"]
+        adaptive = best["adaptive_leaf"]
     sampler = ClockSampler(local)
     sampler.start()
     time.sleep(0.3)
@@ -295,7 +343,7 @@ def run_ours(args, world, rank, local):
     # end to end through the C ABI with pinned host buffers
     h_pos = torch.from_numpy(pos).pin_memory()
     h_mass = torch.from_numpy(mass).pin_memory()
-    h_acc = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    h_acc = torch.empty((n, dim), dtype=torch.float64).pin_memory()
     hp, hm, ha = h_pos.numpy(), h_mass.numpy(), h_acc.numpy()
     ctx.evaluate(hp, hm, out=ha)
     e2e_steps = max(3, args.steps // 2)
@@ -317,11 +365,13 @@ def run_ours(args, world, rank, local):
     tc_src = "MEASURED_PEAKS.json bf16_tflops_sustained (cuBLAS bf16, seconds-long loop)"
     if tc_peak is None:
         tc_peak, tc_src = 1400.0, "fallback sustained bf16 figure (MEASURED_PEAKS.json absent)"
-    K = (p + 1) ** 2
+    K = (p + 1) ** 2 if dim == 3 else 2 * p + 1
     ph = _phases(stats)
     s_last = stats[-1]
     m2l_flops = 2.0 * K * K * s_last["m2l_pairs"]
     far_flops = 20.0 * s_last["far_direct_pairs"]
+    near_pairs = s_last["p2p_pairs"] - s_last["far_direct_pairs"]
+    near_ms = ph["ms_p2p"] - ph["ms_far_direct"]
     traffic = load_traffic()
     roofs = {
         "m2l_tc" if mode == fmmgpu.FMM_M2L_TC else "m2l_fp32": {
@@ -343,6 +393,14 @@ def run_ours(args, world, rank, local):
             "flops_per_launch": far_flops, "pairs": int(s_last["far_direct_pairs"]),
             "ms_per_launch": ph["ms_far_direct"], "traffic": traffic.get("far_direct"),
         },
+        "near_field": {
+            "kernel": ("k_colleague_sum (adaptive leaves and their colleagues, FP32) + output" if adaptive
+                       else "k_p2p (leaf near field, FP32) + output"), "bound": "fp32", "unit": "TFLOP/s",
+            "achieved": 20.0 * near_pairs / (near_ms / 1e3) / 1e12 if near_ms > 0 else None,
+            "peak": fp32_peak, "peak_source": f"derived: 148 SM x 128 FP32 lanes x 2 x {sm_max:.0f} MHz",
+            "flops_per_launch": 20.0 * near_pairs, "pairs": int(near_pairs), "ms_per_launch": near_ms,
+            "traffic": traffic.get("near_field"),
+        },
     }
     for r in roofs.values():
         r["frac"] = r["achieved"] / r["peak"] if r["achieved"] else None
@@ -352,12 +410,15 @@ def run_ours(args, world, rank, local):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": f"synthetic (seeded {'Plummer mixture' if mixture else 'Plummer sphere'})",
+        "dtype": "f32", "data": f"synthetic ({workload_inputs(args.workload, n)})",
         "impl": "fmmgpu",
-        "config": dict(workload_desc(n, p, leaf, args.m2l, s_last.get("direct_max"), mixture),
-                       adaptive_leaf=args.adaptive),
-        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(n * 3 * 8 + n * 8),
-                "d2h_bytes_per_step": int(n * 3 * 8)},
+        "config": dict(workload_desc(n, p, leaf, args.m2l, s_last.get("direct_max"), args.workload),
+                       adaptive_leaf=adaptive,
+                       judge_in_timed_steps=(f"learned-order judge: {args.judge} targets against the FP64 direct "
+                                             f"sum every {args.judge_every}th evaluation, inside the timed steps"
+                                             if learned else "none")),
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(n * dim * 8 + n * 8),
+                "d2h_bytes_per_step": int(n * dim * 8)},
         "roofline": roof, "rooflines": roofs, "error": err, "phases_ms": ph,
         "tree": {"depth": s_last["depth"], "leaves": s_last["n_leaves"], "cells": s_last["n_cells"],
                  "p2p_pairs": s_last["p2p_pairs"], "far_direct_pairs": s_last["far_direct_pairs"],
@@ -379,13 +440,14 @@ def run_ours(args, world, rank, local):
     # comparisons at the same order: tensor cores at fixed p, and the plain
     # FP32 GPU FMM (the method without tensor cores and learned orders)
     def compare(m2l_mode, label):
-        pc = fmmgpu.Context(dim=3, p=p, leaf_cap=args.leaf, m2l_mode=m2l_mode, G=1.0, device=local,
-                            direct_max=args.direct_max, adaptive_leaf=args.adaptive)
+        a0 = (32 if tune_adaptive else args.adaptive) if dim == 3 else 0
+        pc = fmmgpu.Context(dim=dim, p=p, leaf_cap=args.leaf, m2l_mode=m2l_mode, G=1.0, device=local,
+                            direct_max=args.direct_max, adaptive_leaf=a0)
         chosen = None
         if args.autotune and args.direct_max < 0:  # tuned the same way as the headline
             b = pc.autotune(n, d_pos.data_ptr(), d_mass.data_ptr(), tune_leaf=tune_leaf,
-                            stream=stream.cuda_stream)[1]
-            chosen = {"direct_max": b["direct_max"], "leaf_cap": b["leaf_cap"]}
+                            tune_adaptive=tune_adaptive, stream=stream.cuda_stream)[1]
+            chosen = {"direct_max": b["direct_max"], "leaf_cap": b["leaf_cap"], "adaptive_leaf": b["adaptive_leaf"]}
         psteps = max(3, args.steps // 2)
         pms, pst, _ = _timed(pc, n, d_pos, d_mass, d_acc, stream, flush, psteps, max(1, args.warmup), barrier)
         ptot = max_over_ranks(float(sum(pms)), world, dev)
@@ -400,7 +462,7 @@ def run_ours(args, world, rank, local):
         line["plain"] = compare(fmmgpu.FMM_M2L_FP32, "fp32 SIMT, fixed p")
         line["speedup_vs_plain"] = value / line["plain"]["value"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(p, leaf, mixture)
+        line["cpu_baseline"] = cpu_baseline(p, leaf, args.workload)
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:
@@ -470,60 +532,92 @@ def run_frames(args, world, rank, local):
 
 def run_ensemble(args, world, rank, local):
     """The batched-ensemble configuration: 256 independent Plummer spheres,
-    N per system log-uniform in [1024, 65536] (seed 4), p = 8, leaf 64, all
-    evaluated by one fmm_evaluate_batched call (concurrent worker streams);
-    aggregate particles/s over the wall clock of the call, per-system error
-    against the FP64 direct sum on up to 64 sampled targets per system."""
+    N per system log-uniform in [1024, 65536] (seed 4), p = 8, leaf 64.  With
+    N GPUs the systems are split between the ranks by cost (fmmgpu.ensemble:
+    longest processing time first, no exchange between GPUs) and each rank
+    evaluates its share with one fmm_evaluate_batched call per step
+    (concurrent worker streams).  value: all particles over the slowest
+    rank's wall clock per step (host timer around the synchronous call, max
+    over ranks); per-system error against the FP64 direct sum on up to 64
+    sampled targets per system, gathered to rank 0."""
     import torch
 
     import fmmgpu
-    from fmmgpu import workloads
+    from fmmgpu import ensemble, workloads
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
     sizes = workloads.ensemble_sizes(256, 1024, 65536, seed=4)
-    pos, mass = [], []
-    for k, n in enumerate(sizes):
-        p_, m_ = workloads.plummer(int(n), seed=1000 + k)
-        pos.append(p_)
-        mass.append(m_)
-    pos, mass = np.concatenate(pos), np.concatenate(mass)
-    off = np.r_[0, np.cumsum(sizes)].astype(np.int64)
-    ntot = int(off[-1])
+    shares = ensemble.partition_systems(sizes, world)
+    mine = shares[rank]
+    pos_l, mass_l = [], []
+    for k in mine:
+        p_, m_ = workloads.plummer(int(sizes[k]), seed=1000 + k)
+        pos_l.append(p_)
+        mass_l.append(m_)
+    pos = np.concatenate(pos_l) if pos_l else np.zeros((0, 3))
+    mass = np.concatenate(mass_l) if mass_l else np.zeros(0)
+    off = np.r_[0, np.cumsum([int(sizes[k]) for k in mine])].astype(np.int64)
+    nloc = int(off[-1])
+    ntot = int(np.sum(sizes))
     d_pos, d_m = torch.from_numpy(pos).to(dev), torch.from_numpy(mass).to(dev)
-    d_acc = torch.empty((ntot, 3), dtype=torch.float64, device=dev)
+    d_acc = torch.empty((max(nloc, 1), 3), dtype=torch.float64, device=dev)
     torch.cuda.synchronize(dev)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(dev)
+
     res = {}
+    errs = []
     with fmmgpu.Context(dim=3, p=8, leaf_cap=64, G=1.0, m2l_mode=fmmgpu.FMM_M2L_TC, device=local) as c:
         for label, workers in (("concurrent", 0), ("one_stream", 1)):
             for _ in range(max(1, args.warmup)):
                 c.evaluate_batched(off, d_pos.data_ptr(), d_m.data_ptr(), d_acc.data_ptr(), None, workers)
             steps = max(2, args.steps // 4)
+            barrier()
             t0 = time.perf_counter()
             for _ in range(steps):
                 c.evaluate_batched(off, d_pos.data_ptr(), d_m.data_ptr(), d_acc.data_ptr(), None, workers)
             torch.cuda.synchronize(dev)
-            dt = (time.perf_counter() - t0) / steps
-            res[label] = {"value": ntot / dt, "ms_per_step": dt * 1e3, "workers": workers or min(8, len(sizes))}
+            dt = max_over_ranks((time.perf_counter() - t0) / steps, world, dev)
+            res[label] = {"value": ntot / dt, "ms_per_step": dt * 1e3, "workers": workers or min(8, len(mine))}
         acc = d_acc.cpu().numpy()
-        rng = np.random.default_rng(9)
-        errs = []
-        for s in range(len(sizes)):
+        rng = np.random.default_rng(9 + rank)
+        for s in range(len(mine)):
             a, b = int(off[s]), int(off[s + 1])
             tg = np.sort(rng.choice(b - a, min(64, b - a), replace=False)).astype(np.int64)
             ref = c.direct(pos[a:b], mass[a:b], targets=tg)
             errs.append(float(np.linalg.norm(acc[a:b][tg] - ref) / np.linalg.norm(ref)))
+    loads = ensemble.rank_loads(sizes, shares)
+    if world > 1:
+        gathered = [None] * world
+        torch.distributed.all_gather_object(gathered, errs)
+        errs = [e for g in gathered for e in g]
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
     line = {
         "metric": "batched ensemble particles/s (256 Plummer systems, p=8)", "value": res["concurrent"]["value"],
-        "unit": UNIT, "n_gpus": 1, "steps": max(2, args.steps // 4), "warmup": max(1, args.warmup),
-        "ms_per_step": res["concurrent"]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "unit": UNIT, "n_gpus": world, "steps": max(2, args.steps // 4), "warmup": max(1, args.warmup),
+        "ms_per_step": res["concurrent"]["ms_per_step"], "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Plummer spheres)", "impl": "fmmgpu",
         "config": {"workload": f"256 independent Plummer spheres, N log-uniform in [1024, 65536] (seed 4), "
-                               f"{ntot} particles, p=8, leaf capacity 64, one fmm_evaluate_batched call per step",
-                   "timing": "wall clock of the call (host threads feeding worker streams)"},
+                               f"{ntot} particles, p=8, leaf capacity 64, one fmm_evaluate_batched call per rank "
+                               f"per step",
+                   "timing": "wall clock of the call (host threads feeding worker streams), max over ranks",
+                   "parallelism": f"systems split over {world} rank(s) by cost, longest processing time first; "
+                                  f"no collective on the data path",
+                   "rank_systems": [len(x) for x in shares],
+                   "rank_load_max_over_mean": max(loads) / (sum(loads) / len(loads))},
         "one_stream": res["one_stream"], "speedup_concurrent": res["concurrent"]["value"] / res["one_stream"]["value"],
         "error_per_system": {"vs": "FP64 direct sum, up to 64 targets per system", "median": float(np.median(errs)),
-                             "max": float(np.max(errs))},
+                             "max": float(np.max(errs)), "systems": len(errs)},
     }
     print(json.dumps(line), flush=True)
 
@@ -552,32 +646,55 @@ def load_traffic():
 
 
 # ------------------------------------------------------------- reference
+def sample_workload(workload, n, seed):
+    """A bounded sample of the workload's distribution (own seed)."""
+    from fmmgpu import workloads
+
+    if workload == "mixture":
+        return workloads.plummer_mixture(n, seed=seed)
+    if workload == "disk2d":
+        return workloads.disk_clumps_2d(n, seed=seed)
+    return workloads.plummer(n, seed=seed)
+
+
 def _ref_worker(args):
-    n, p, leaf, seed = args[:4]
-    mixture = len(args) > 4 and args[4]
+    """Times the reference's FMM::update on one sample; with check, also its
+    relative L2 force error against the FP64 direct sum (the oracle's)."""
+    n, p, leaf, seed, workload = args[:5]
+    check = len(args) > 5 and args[5]
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     sys.path.insert(0, os.path.join(ROOT, "nbody-fmm_b200"))
     from oracle import RefLib
-    from fmmgpu import workloads
 
     R = RefLib()
-    pos, m = workloads.plummer_mixture(n, seed=seed) if mixture else workloads.plummer(n, seed=seed)
+    pos, m = sample_workload(workload, n, seed)
     t0 = time.perf_counter()
-    R.fmm(pos, m, p, leaf)
-    return time.perf_counter() - t0
+    g = R.fmm(pos, m, p, leaf)
+    dt = time.perf_counter() - t0
+    if not check:
+        return dt
+    from oracle import Oracle
+
+    ref = Oracle().direct(pos, m)
+    return dt, float(np.linalg.norm(g - ref) / np.linalg.norm(ref))
 
 
-def cpu_baseline(p, leaf, mixture=False):
-    """The reference FMM::update, single thread, on a bounded sample."""
-    seed = 5 if mixture else 2
+def cpu_baseline(p, leaf, workload="mixture"):
+    """The reference FMM::update, single thread, on a bounded sample, with
+    its own force error there."""
+    seed = {"mixture": 5, "disk2d": 3}.get(workload, 2)
     try:
-        dt = _ref_worker((CPU_SAMPLE_N, p, leaf, seed, mixture))
+        dt, err = _ref_worker((CPU_SAMPLE_N, p, leaf, seed, workload, True))
     except Exception as e:  # reference build missing
         return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": f"unavailable: {e}"}
-    inputs = "Plummer mixture" if mixture else "Plummer"
     return {"value": CPU_SAMPLE_N / dt, "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": f"reference FMM::update (oracle/_ref, g++ -O2), {inputs} N={CPU_SAMPLE_N} seed {seed}, "
-                      f"p={p}, leaf capacity {leaf}, 1 thread, {dt:.1f} s"}
+            "sample": f"reference FMM::update (oracle/_ref, g++ -O2), {workload_inputs(workload, CPU_SAMPLE_N)} "
+                      f"(sample seed {seed}), p={p}, leaf capacity {leaf}, 1 thread, {dt:.1f} s; N bounded so the "
+                      f"bench stays within minutes (65,536 particles would take ~8 min of one core)",
+            "reference_force_rel_l2": err,
+            "reference_error_note": "the reference's own force error on this sample against the FP64 direct sum: its "
+                                    "3D M2M/M2L/L2L (multipole_set3D.cpp:45-118, local_set3D.cpp:51-81) do not "
+                                    "converge, so its 3D result is about 1e-1 off at every p"}
 
 
 def run_reference(args, world, rank):
@@ -588,26 +705,31 @@ def run_reference(args, world, rank):
     cores = os.cpu_count() or 1
     ctx = mp.get_context("spawn")
     n, p, leaf = REF_SAMPLE_N, args.p, args.leaf
-    mixture = args.workload == "mixture"
+    wl = args.workload
     with ctx.Pool(cores) as pool:
         for _ in range(args.warmup):
-            pool.map(_ref_worker, [(n, p, leaf, 2 + i, mixture) for i in range(cores)])
+            pool.map(_ref_worker, [(n, p, leaf, 2 + i, wl) for i in range(cores)])
         step_s = []
         for _ in range(args.steps):
-            ts = pool.map(_ref_worker, [(n, p, leaf, 2 + i, mixture) for i in range(cores)])
+            ts = pool.map(_ref_worker, [(n, p, leaf, 2 + i, wl) for i in range(cores)])
             step_s.append(max(ts))
+        _, err = pool.apply(_ref_worker, ((n, p, leaf, 2, wl, True),))
     total = sum(step_s)
     value = n * cores * args.steps / total
-    inputs = "Plummer mixture" if mixture else "Plummer"
-    sample = (f"reference FMM::update (oracle/_ref, g++ -O2) on {cores} processes x {inputs} N={n} (seeds 2..), "
-              f"p={p}, leaf capacity {leaf}, one process per host core; step = slowest process")
+    sample = (f"reference FMM::update (oracle/_ref, g++ -O2) on {cores} processes x samples of "
+              f"{workload_inputs(wl, n)} (seeds 2..), p={p}, leaf capacity {leaf}, one process per host core; "
+              f"step = slowest process")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64",
-        "data": f"synthetic (seeded {'Plummer mixture' if mixture else 'Plummer sphere'})", "impl": "reference",
-        "config": workload_desc(args.n, p, leaf, "reference (CPU)", mixture=mixture),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+        "data": f"synthetic ({workload_inputs(wl, args.n)}, bounded samples)", "impl": "reference",
+        "config": dict(workload_desc(args.n, p, leaf, "reference (CPU)", workload=wl),
+                       same_config=False, sample_n=n,
+                       why_sample="the reference's CPU FMM runs ~130 particles/s per core at p = 12; the full "
+                                  "workload would take days"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample,
+                         "reference_force_rel_l2": err},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -619,12 +741,13 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="plummer", choices=["plummer", "mixture"],
-                    help="plummer: the 2^20 Plummer sphere (default); mixture: the 16M clustered mixture of the "
-                         "learned-order configuration, leaf capacity tuned with the threshold")
-    ap.add_argument("--n", type=int, default=None, help="particles (default 2^20, mixture 2^24)")
-    ap.add_argument("--p", type=int, default=12)
-    ap.add_argument("--leaf", type=int, default=64)
+    ap.add_argument("--workload", default="mixture", choices=["mixture", "plummer", "disk2d"],
+                    help="mixture (default): the 16M clustered Plummer mixture of the learned-order configuration, "
+                         "leaf capacity tuned with the threshold; plummer: the 2^20 Plummer sphere; disk2d: the 2D "
+                         "4M clumped disk at p = 16")
+    ap.add_argument("--n", type=int, default=None, help="particles (default: mixture 2^24, plummer 2^20, disk2d 2^22)")
+    ap.add_argument("--p", type=int, default=None, help="expansion order (default 12; disk2d 16)")
+    ap.add_argument("--leaf", type=int, default=None, help="leaf capacity (default 64; disk2d 32)")
     ap.add_argument("--m2l", default="tc", choices=["fp32", "tc"])
     ap.add_argument("--direct-max", type=int, default=-1, help="-1: the library's automatic threshold")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
@@ -636,15 +759,22 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ensemble", action="store_true", help="the batched-ensemble configuration instead")
-    ap.add_argument("--adaptive", type=int, default=0,
-                    help="adaptive targets: cells under parents of at most this many particles are no targets "
-                         "(0: the uniform tree of the reference)")
+    ap.add_argument("--adaptive", type=int, default=None,
+                    help="adaptive targets (3D): cells under parents of at most this many particles are no targets "
+                         "(0: the uniform targets of the reference); default: 32, tuned over {0, 16, 32, 64} with "
+                         "the other settings")
     ap.add_argument("--frames-every", type=int, default=0,
                     help="measure frame output instead: a device frame every K steps of the pass loop")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 0)
+    if args.frames_every > 0:
+        args.workload = "plummer"  # frame output is measured on the 2^20 Plummer sphere
     if args.n is None:
-        args.n = 1 << 24 if args.workload == "mixture" else 1 << 20
+        args.n = {"mixture": 1 << 24, "plummer": 1 << 20, "disk2d": 1 << 22}[args.workload]
+    if args.p is None:
+        args.p = 16 if args.workload == "disk2d" else 12
+    if args.leaf is None:
+        args.leaf = 32 if args.workload == "disk2d" else 64
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, world, rank)

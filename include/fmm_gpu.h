@@ -122,7 +122,7 @@ typedef struct fmm_config {
   int32_t adaptive_leaf;/* adaptive targets (3D trees of depth >= 3; elsewhere ignored): a cell whose parent
                            holds at most this many particles is no target, and each particle sums the
                            particles of the colleagues of its deepest target cell directly.  0 (default):
-                           every cell is a target, the reference's uniform tree.  Not yet run on a GPU. */
+                           every cell is a target, the reference's uniform tree. */
 } fmm_config;
 
 typedef struct fmm_stats {
@@ -196,11 +196,13 @@ FMM_API int fmm_evaluate_batched(fmm_ctx *ctx, int32_t nsys, const int64_t *offs
    algorithm at that threshold) at the threshold K^2/25, then the thresholds
    K^2/100, K^2/50 and K^2/12.5 at the best capacity (seven candidates).
    Every candidate keeps the configured adaptive_leaf; with FMM_TUNE_ADAPTIVE
-   the values 16, 32 and 64 are then tried at the best candidate's leaf
-   capacity and threshold.  Learned orders are tuned with them (every candidate is evaluated twice,
+   the values 0 (the uniform targets), 16, 32 and 64 are then tried at the
+   best candidate's leaf capacity and threshold.  Adaptive targets change
+   only which pairs are summed directly (exactly), not the expansions, so
+   the candidates differ in time, not in truncation error.  Learned orders are tuned with them (every candidate is evaluated twice,
    the second timed).  result may be NULL.  Synchronous. */
 #define FMM_TUNE_LEAF 1
-#define FMM_TUNE_ADAPTIVE 2 /* then adaptive_leaf in {16, 32, 64} at the best of the above (experimental) */
+#define FMM_TUNE_ADAPTIVE 2 /* then adaptive_leaf in {0, 16, 32, 64} at the best of the above */
 typedef struct fmm_tune_result {
   int32_t n_candidates;
   int32_t best;            /* index of the chosen candidate */

@@ -495,7 +495,7 @@ int fmm_autotune(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mas
   // then the adaptive-target threshold at the best leaf capacity and direct-pair threshold
   if ((flags & FMM_TUNE_ADAPTIVE) && !rc) {
     const int b = res.best;
-    for (int32_t al : {16, 32, 64})
+    for (int32_t al : {0, 16, 32, 64})
       if (al != al0) trial(res.leaf_cap[b], res.direct_max[b], al);
   }
   cudaEventDestroy(e0);

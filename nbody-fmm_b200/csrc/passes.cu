@@ -2111,17 +2111,9 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     int rc = launch_contract(c2, l2_b1[d] - l2_b0[d], st, ws.launches);
     if (rc) return rc;
   }
-  // L2P
-  if (dim == 3)
-    (want_pot ? k_l2p3d<true> : k_l2p3d<false>)<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far,
-                                          shortcut ? eb.esrc.ptr : nullptr, shortcut ? eb.elev.ptr : nullptr,
-                                          t.level_off[D], D, eb.lvl_off.ptr, (float)(1.0 / emax));
-  else
-    k_l2p2d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far);
-  ws.launches += 1;
-  if (ev) cudaEventRecord(ev[4], st);
   // adaptive targets: the direct far field's targets per level and the
   // colleague-sum items, counted on the device and read back together
+  // (timed with the downward pass)
   std::vector<unsigned> ntgt;
   uint32_t n_items = 0;
   if (adaptive) {
@@ -2147,6 +2139,15 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     k_colleague_fill<<<cdiv(ncell, TPB), TPB, 0, st>>>(acount, ncell, ccnt, coff, eb.citems.ptr);
     ws.launches += 1;
   }
+  // L2P
+  if (dim == 3)
+    (want_pot ? k_l2p3d<true> : k_l2p3d<false>)<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far,
+                                          shortcut ? eb.esrc.ptr : nullptr, shortcut ? eb.elev.ptr : nullptr,
+                                          t.level_off[D], D, eb.lvl_off.ptr, (float)(1.0 / emax));
+  else
+    k_l2p2d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far);
+  ws.launches += 1;
+  if (ev) cudaEventRecord(ev[4], st);
   // direct far field, all levels >= 2 (they have interaction lists) in one
   // launch, coarse levels first so that their long warps start early
   if ((direct_max > 0 || any_fdirect) && D >= 2) {

@@ -1,6 +1,6 @@
 """The bench's reference arm (CPU only, `bench.py --impl reference`): it
 times the reference's own FMM::update on the host cores and prints exactly
-one JSON line with the keys the driver reads, for both workloads."""
+one JSON line with the keys the driver reads, for every workload."""
 import json
 import os
 import subprocess
@@ -13,7 +13,7 @@ KEYS = ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "
         "vs_baseline", "dtype", "data", "config", "impl", "cpu_baseline", "e2e")
 
 
-@pytest.mark.parametrize("workload", ["plummer", "mixture"])
+@pytest.mark.parametrize("workload", ["plummer", "mixture", "disk2d"])
 def test_reference_arm_prints_one_contract_line(workload):
     if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref.so")):
         pytest.skip("the reference is not built here (oracle/_ref)")
@@ -33,3 +33,6 @@ def test_reference_arm_prints_one_contract_line(workload):
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == line["value"]
     assert ("mixture" in line["config"]["workload"]) == (workload == "mixture")
     assert ("mixture" in cb["sample"]) == (workload == "mixture")
+    assert ("2D" in line["config"]["workload"]) == (workload == "disk2d")
+    # the reference's own force error on its sample is stated beside its speed
+    assert cb["reference_force_rel_l2"] > 0
