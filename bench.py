@@ -324,11 +324,13 @@ def run_ours(args, world, rank, local):
         # input: setup, outside the timed steps
         t0 = time.perf_counter()
         cands, best = ctx.autotune(n, d_pos.data_ptr(), d_mass.data_ptr(), tune_leaf=tune_leaf,
-                                   tune_adaptive=tune_adaptive, stream=stream.cuda_stream)
+                                   tune_adaptive=tune_adaptive, tune_kernels=True, stream=stream.cuda_stream)
         tune = {"seconds": time.perf_counter() - t0, "chosen_direct_max": best["direct_max"],
                 "chosen_leaf_cap": best["leaf_cap"], "chosen_adaptive_leaf": best["adaptive_leaf"],
-                "candidates (leaf_cap, direct_max, adaptive_leaf, ms)":
-                    [[x["leaf_cap"], x["direct_max"], x["adaptive_leaf"], round(x["ms"], 3)] for x in cands]}
+                "chosen_p2p_chunk": best["p2p_chunk"], "chosen_m2l_run": best["m2l_run"],
+                "candidates (leaf_cap, direct_max, adaptive_leaf, p2p_chunk, m2l_run, ms)":
+                    [[x["leaf_cap"], x["direct_max"], x["adaptive_leaf"], x["p2p_chunk"], x["m2l_run"],
+                      round(x["ms"], 3)] for x in cands]}
         leaf = best["leaf_cap"]
         adaptive = best["adaptive_leaf"]
     sampler = ClockSampler(local)
@@ -446,8 +448,8 @@ def run_ours(args, world, rank, local):
         chosen = None
         if args.autotune and args.direct_max < 0:  # tuned the same way as the headline
             b = pc.autotune(n, d_pos.data_ptr(), d_mass.data_ptr(), tune_leaf=tune_leaf,
-                            tune_adaptive=tune_adaptive, stream=stream.cuda_stream)[1]
-            chosen = {"direct_max": b["direct_max"], "leaf_cap": b["leaf_cap"], "adaptive_leaf": b["adaptive_leaf"]}
+                            tune_adaptive=tune_adaptive, tune_kernels=True, stream=stream.cuda_stream)[1]
+            chosen = {k: b[k] for k in ("direct_max", "leaf_cap", "adaptive_leaf", "p2p_chunk", "m2l_run")}
         psteps = max(3, args.steps // 2)
         pms, pst, _ = _timed(pc, n, d_pos, d_mass, d_acc, stream, flush, psteps, max(1, args.warmup), barrier)
         ptot = max_over_ranks(float(sum(pms)), world, dev)

@@ -123,6 +123,11 @@ typedef struct fmm_config {
                            holds at most this many particles is no target, and each particle sums the
                            particles of the colleagues of its deepest target cell directly.  0 (default):
                            every cell is a target, the reference's uniform tree. */
+  int32_t p2p_chunk;    /* adaptive targets: sources per work item of the colleague sums (a multiple of 32 in
+                           [32, 4096]; 0: automatic, 256) */
+  int32_t m2l_run;      /* FMM_M2L_TC: interaction offsets (slots) per work item of the tensor-core M2L, the
+                           batch shape (in [8, 189]; 0: automatic: 24 when there are fewer than four target
+                           batches per CTA, else a whole batch) */
 } fmm_config;
 
 typedef struct fmm_stats {
@@ -197,12 +202,15 @@ FMM_API int fmm_evaluate_batched(fmm_ctx *ctx, int32_t nsys, const int64_t *offs
    K^2/100, K^2/50 and K^2/12.5 at the best capacity (seven candidates).
    Every candidate keeps the configured adaptive_leaf; with FMM_TUNE_ADAPTIVE
    the values 0 (the uniform targets), 16, 32 and 64 are then tried at the
-   best candidate's leaf capacity and threshold.  Adaptive targets change
+   best candidate's leaf capacity and threshold; with FMM_TUNE_KERNELS the
+   kernel shapes last.  Adaptive targets change
    only which pairs are summed directly (exactly), not the expansions, so
    the candidates differ in time, not in truncation error.  Learned orders are tuned with them (every candidate is evaluated twice,
    the second timed).  result may be NULL.  Synchronous. */
 #define FMM_TUNE_LEAF 1
 #define FMM_TUNE_ADAPTIVE 2 /* then adaptive_leaf in {0, 16, 32, 64} at the best of the above */
+#define FMM_TUNE_KERNELS 4  /* then the kernel shapes at the best of the above: p2p_chunk in {128, 512}
+                               (with adaptive targets) and m2l_run in {24, 189} (tensor-core M2L) */
 typedef struct fmm_tune_result {
   int32_t n_candidates;
   int32_t best;            /* index of the chosen candidate */
@@ -210,6 +218,8 @@ typedef struct fmm_tune_result {
   int32_t direct_max[16];
   double ms[16];           /* device time of each candidate's timed evaluation */
   int32_t adaptive_leaf[16];
+  int32_t p2p_chunk[16];
+  int32_t m2l_run[16];
 } fmm_tune_result;
 FMM_API int fmm_autotune(fmm_ctx *ctx, int64_t n, const double *d_pos, const double *d_mass, int32_t flags,
                          fmm_tune_result *result, void *stream);
@@ -244,7 +254,9 @@ FMM_API int fmm_tree_leaves(fmm_ctx *ctx, uint64_t *keys, int64_t *start, int64_
 /* Neighbour (kind 0, |delta| <= 1, self excluded) or interaction (kind 1)
  * list pairs of level d as (target key, source key): the lists of
  * NodeI::compute_interaction_list (node_i.cpp:23-99).  With tkey == NULL
- * only *count is set. */
+ * only *count is set.  The tree must come from fmm_tree_build (a force pass
+ * with adaptive targets keeps colleague rows of its target cells only, and
+ * then this returns FMM_ERR_INVALID_ARGUMENT). */
 FMM_API int fmm_tree_pairs(fmm_ctx *ctx, int32_t level, int32_t kind, int64_t *count, uint64_t *tkey, uint64_t *skey);
 
 /* Adaptive-target flags (fmm_config.adaptive_leaf = A) of every cell of the

@@ -78,8 +78,6 @@ struct ExpBuffers {
   DevBuf<float> cf;              // learned orders: per-cell features (ORD_CF floats per cell)
   DevBuf<double> frms;           // learned orders: [0] F_rms of the previous pass (G = 1), [1] scratch,
                                  // [2] total mass
-  DevBuf<uint8_t> aflag;         // adaptive targets, per cell: bit 0 target, bit 1 adaptive leaf
-  DevBuf<int> alist;             // adaptive targets: the adaptive leaves, then their count
   DevBuf<int> ftl;               // adaptive targets: the direct far field's targets per level, then counts
   DevBuf<double> xs;             // adaptive targets: FP64 positions in leaf order (dim per particle)
   DevBuf<uint32_t> ccnt;         // adaptive targets: colleague-sum items per adaptive leaf, then their offsets
@@ -110,12 +108,11 @@ struct OrderOpts {
   float *feat = nullptr, *labels = nullptr;
 };
 void upload_class_tables();
-int adaptive_flags_of_tree(const Workspace &ws, const TreeState &t, int A, uint8_t *flag, int *list, cudaStream_t st);
 
 int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, const double *d_pos,
                    const double *d_mass, int p, double eps2, double G,
                    const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, int64_t direct_max,
                    const OrderOpts &order, cudaStream_t st, fmm_stats &stats, cudaEvent_t *ev,
-                   int adaptive_leaf = 0);
+                   int adaptive_leaf = 0, int p2p_chunk = 0, int m2l_run = 0);
 
 }  // namespace fmm

@@ -73,6 +73,8 @@ static int check_cfg(const fmm_config *c) {
     return FMM_ERR_UNSUPPORTED;  // per-pair orders live in the tensor-core kernel; the plain FMM is fixed-p
   if (c->order_margin < 0 || c->order_margin > FMM_MAX_P) return FMM_ERR_INVALID_ARGUMENT;
   if (c->adaptive_leaf < 0) return FMM_ERR_INVALID_ARGUMENT;
+  if (c->p2p_chunk != 0 && (c->p2p_chunk < 32 || c->p2p_chunk > 4096 || c->p2p_chunk % 32)) return FMM_ERR_INVALID_ARGUMENT;
+  if (c->m2l_run != 0 && (c->m2l_run < 8 || c->m2l_run > 189)) return FMM_ERR_INVALID_ARGUMENT;
   return FMM_OK;
 }
 
@@ -180,8 +182,6 @@ int fmm_destroy(fmm_ctx *c) {
   c->eb.elev.release();
   c->eb.ukey.release();
   c->eb.p2m_list.release();
-  c->eb.aflag.release();
-  c->eb.alist.release();
   c->eb.ftl.release();
   c->eb.xs.release();
   c->eb.ccnt.release();
@@ -228,7 +228,7 @@ static int pass(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass
                 cudaStream_t st, const OrderOpts &oo, bool want64) {
   const int dim = c->cfg.dim;
   CUDA_TRY(cudaEventRecord(c->ev[0], st));
-  int rc = build_tree(c->ws, c->tree, d_pos, d_mass, n, dim, c->cfg.leaf_cap, st);
+  int rc = build_tree(c->ws, c->tree, d_pos, d_mass, n, dim, c->cfg.leaf_cap, st, c->cfg.adaptive_leaf);
   if (rc) return rc;
   if (!c->ws.ok) return FMM_ERR_OUT_OF_MEMORY;
   c->have_tree = true;
@@ -247,7 +247,8 @@ static int pass(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mass
   c->stats.judge_rel_l2 = jr;
   c->stats.order_fallbacks = fb;
   rc = run_fmm_passes(c->ws, c->tree, c->ops, c->eb, d_pos, d_mass, c->cfg.p, c->cfg.eps2, c->cfg.G, g, d_acc, d_pot,
-                      c->cfg.m2l_mode, direct_threshold(c->cfg), oo, st, c->stats, c->ev, c->cfg.adaptive_leaf);
+                      c->cfg.m2l_mode, direct_threshold(c->cfg), oo, st, c->stats, c->ev, c->cfg.adaptive_leaf,
+                      c->cfg.p2p_chunk, c->cfg.m2l_run);
   c->stats.direct_max = direct_threshold(c->cfg);
   if (rc) return rc;
   if (!c->ws.ok) return FMM_ERR_OUT_OF_MEMORY;
@@ -456,15 +457,19 @@ int fmm_autotune(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mas
   int rc = FMM_OK;
   double best = 1e300;
   auto threshold = [&](double f) { return (int32_t)std::max(8.0, base * f); };
-  auto trial = [&](int lc, int32_t dm, int32_t al) {
+  auto trial = [&](int lc, int32_t dm, int32_t al, int32_t pc, int32_t mr) {
     if (rc || res.n_candidates >= 16) return;
     const int k = res.n_candidates++;
     c->cfg.leaf_cap = lc;
     c->cfg.direct_max = dm;
     c->cfg.adaptive_leaf = al;
+    c->cfg.p2p_chunk = pc;
+    c->cfg.m2l_run = mr;
     res.leaf_cap[k] = lc;
     res.direct_max[k] = dm;
     res.adaptive_leaf[k] = al;
+    res.p2p_chunk[k] = pc;
+    res.m2l_run[k] = mr;
     const bool twice = c->cfg.order_mode == FMM_ORDER_LEARNED;
     c->frms_n = -1;  // learned orders: start the system afresh
     for (int r = 0; r < (twice ? 2 : 1) && !rc; ++r) rc = evaluate_device(c, n, d_pos, d_mass, c->d_acc.ptr, nullptr, st);
@@ -484,19 +489,30 @@ int fmm_autotune(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mas
   };
   // coordinate search: the leaf capacity at the default threshold, then the
   // threshold at the best capacity
-  const int32_t al0 = saved.adaptive_leaf;
+  const int32_t al0 = saved.adaptive_leaf, pc0 = saved.p2p_chunk, mr0 = saved.m2l_run;
   if (flags & FMM_TUNE_LEAF) {
-    for (int lc : {32, 64, 128, 256}) trial(lc, threshold(1.0), al0);
+    for (int lc : {32, 64, 128, 256}) trial(lc, threshold(1.0), al0, pc0, mr0);
     const int lc = res.leaf_cap[res.best];
-    for (double f : {0.25, 0.5, 2.0}) trial(lc, threshold(f), al0);
+    for (double f : {0.25, 0.5, 2.0}) trial(lc, threshold(f), al0, pc0, mr0);
   } else {
-    for (double f : {0.125, 0.25, 0.5, 1.0, 2.0}) trial(saved.leaf_cap, threshold(f), al0);
+    for (double f : {0.125, 0.25, 0.5, 1.0, 2.0}) trial(saved.leaf_cap, threshold(f), al0, pc0, mr0);
   }
   // then the adaptive-target threshold at the best leaf capacity and direct-pair threshold
   if ((flags & FMM_TUNE_ADAPTIVE) && !rc) {
     const int b = res.best;
     for (int32_t al : {0, 16, 32, 64})
-      if (al != al0) trial(res.leaf_cap[b], res.direct_max[b], al);
+      if (al != al0) trial(res.leaf_cap[b], res.direct_max[b], al, pc0, mr0);
+  }
+  // then the kernel shapes: the colleague-sum chunk (adaptive targets) and
+  // the tensor-core M2L work-item length (the batch shape)
+  if ((flags & FMM_TUNE_KERNELS) && !rc) {
+    int b = res.best;
+    if (res.adaptive_leaf[b] > 0 && c->cfg.dim == 3)
+      for (int32_t pc : {128, 512}) trial(res.leaf_cap[b], res.direct_max[b], res.adaptive_leaf[b], pc, mr0);
+    b = res.best;
+    if (c->cfg.m2l_mode == FMM_M2L_TC)
+      for (int32_t mr : {24, 189})
+        trial(res.leaf_cap[b], res.direct_max[b], res.adaptive_leaf[b], res.p2p_chunk[b], mr);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -505,6 +521,8 @@ int fmm_autotune(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mas
   c->cfg.leaf_cap = res.leaf_cap[res.best];
   c->cfg.direct_max = res.direct_max[res.best];
   c->cfg.adaptive_leaf = res.adaptive_leaf[res.best];
+  c->cfg.p2p_chunk = res.p2p_chunk[res.best];
+  c->cfg.m2l_run = res.m2l_run[res.best];
   c->frms_n = -1;
   if (result) *result = res;
   return FMM_OK;
@@ -699,6 +717,9 @@ int fmm_tree_leaves(fmm_ctx *c, uint64_t *keys, int64_t *start, int64_t *perm) {
 int fmm_tree_pairs(fmm_ctx *c, int32_t level, int32_t kind, int64_t *count, uint64_t *tkey, uint64_t *skey) {
   if (!c || !count || !c->have_tree || level < 0 || level > c->tree.depth || (kind != 0 && kind != 1))
     return FMM_ERR_INVALID_ARGUMENT;
+  // a force pass with adaptive targets keeps colleague rows for its target cells only: the lists need a tree
+  // from fmm_tree_build
+  if (c->tree.adaptive_leaf > 0) return FMM_ERR_INVALID_ARGUMENT;
   CUDA_TRY(cudaSetDevice(c->cfg.device));
   const TreeState &t = c->tree;
   const int dim = t.dim, nc = 1 << dim, ns = dim == 3 ? 27 : 9;
@@ -754,7 +775,7 @@ int fmm_tree_adaptive_flags(fmm_ctx *c, int32_t adaptive_leaf, uint8_t *flags) {
   DevBuf<uint8_t> f;
   DevBuf<int> l;
   int rc = f.reserve((size_t)m) && l.reserve((size_t)m + 1) ? FMM_OK : FMM_ERR_OUT_OF_MEMORY;
-  if (!rc) rc = adaptive_flags_of_tree(c->ws, c->tree, adaptive_leaf, f.ptr, l.ptr, c->stream);
+  if (!rc) rc = launch_adaptive_flags(c->ws, c->tree, adaptive_leaf, f.ptr, l.ptr, c->stream);
   if (!rc && cudaMemcpyAsync(flags, f.ptr, (size_t)m, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess) rc = FMM_ERR_CUDA;
   if (!rc && cudaStreamSynchronize(c->stream) != cudaSuccess) rc = FMM_ERR_CUDA;
   c->ws.launches += 1;

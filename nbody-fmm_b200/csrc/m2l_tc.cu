@@ -570,6 +570,7 @@ static int tc_launch_p(const TcArgs &a, int nb, unsigned int *work, cudaStream_t
   TcArgs b = a;
   b.chunk_slots = TC_MAX_SLOTS;
   if (a.mode == TC_M2L && nb < 4 * per_sm * nsm) b.chunk_slots = 24;
+  if (a.mode == TC_M2L && a.run_slots > 0) b.chunk_slots = std::min(a.run_slots, TC_MAX_SLOTS);
   const int chunks = a.mode == TC_M2L ? (TC_MAX_SLOTS + b.chunk_slots - 1) / b.chunk_slots : 1;
   const int grid = std::min(nb * chunks, per_sm * nsm);
   k_tc_translate<P16><<<grid, TC_M, sh, st>>>(b, nb, work);

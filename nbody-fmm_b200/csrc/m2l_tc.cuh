@@ -33,6 +33,7 @@ struct TcArgs {
   unsigned int *err;
   unsigned long long *tiles;  // M2L: number of (batch, slot) tiles contracted (nullable)
   unsigned long long *widths; // M2L: sum of the tiles' padded widths (nullable)
+  int run_slots;            // M2L: slots per work item requested (fmm_config.m2l_run; 0: the launcher's rule)
   int chunk_slots;          // M2L: slots per work item (set by the launcher; a batch of more slots is
                             // split into items whose sums all add into the targets)
 };

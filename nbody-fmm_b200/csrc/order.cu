@@ -64,10 +64,13 @@ __device__ inline unsigned long long splitmix(unsigned long long x) {
   return x ^ (x >> 31);
 }
 
+// Warp-wide maximum of a non-NaN float in one redux.sync: the float's bits
+// mapped to an int of the same order (negative values have their magnitude
+// bits flipped).
 __device__ inline float warp_max(float v) {
-#pragma unroll
-  for (int o = 16; o; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
+  const int i = __float_as_int(v);
+  const int m = __reduce_max_sync(0xffffffffu, i >= 0 ? i : i ^ 0x7fffffff);
+  return __int_as_float(m >= 0 ? m : m ^ 0x7fffffff);
 }
 
 // Features of tile (batch b, present slot i), computed by one warp (lanes
@@ -104,8 +107,7 @@ __device__ void tile_features(const TileArgs &a, int b, int i, int lane, float *
   sp2 = warp_max(sp2);
 #pragma unroll
   for (int n = 0; n < 13; ++n) mA[n] = warp_max(mA[n]);
-#pragma unroll
-  for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  cnt = __reduce_add_sync(0xffffffffu, cnt);
   const float lmt = log10f((float)fmax(*a.mtot, 1e-300));
   f[0] = level * (1.f / 16.f);
   f[1] = mT * 0.125f;
@@ -531,86 +533,168 @@ static size_t mlp_grad_smem() {
 }
 
 // ---------------------------------------------------------------- inference
-// One block per M2L batch; each warp takes present slots (tiles) in turn:
-// tile features, the MLP with the lanes over the hidden units (weights
-// transposed in shared memory), then the lowest order within the budget.
+// Persistent blocks, each loading the weights into shared memory once (as
+// BF16): a block takes M2L batches in turn and each warp takes groups of 16
+// of the batch's present slots (tiles).  The warp computes the features of
+// its 16 tiles (lanes over each tile's rows), then runs the MLP on all 16 at
+// once with warp-level BF16 tensor-core products (mma.sync m16n8k16, FP32
+// accumulation; rows = tiles, the layer outputs of one product are the
+// inputs of the next in registers), then sets each tile's order: the lowest
+// within the budget of its offset.
 static constexpr int INF_WARPS = 8;
+static constexpr int INF_T = 16;  // tiles per warp group (the product's M)
 
-__global__ void __launch_bounds__(32 * INF_WARPS) k_order_infer(InferArgs a) {
-  __shared__ float w1t[ORD_NF * ORD_NH], w2t[ORD_NH * ORD_NH], w3t[ORD_NH * 16], bias[2 * ORD_NH + 16];
-  __shared__ float hs[INF_WARPS][2][ORD_NH];
+__device__ inline uint32_t bf2(float lo, float hi) {
+  const __nv_bfloat162 t = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const uint32_t *>(&t);
+}
+
+__device__ inline void mma16816(float *c, const uint32_t *a, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// One dense layer of the 16-tile group: out[16 x 8 NT] = in[16 x 16 KT] W^T
+// + bias, ReLU (relu) and rounding to BF16 for the next layer's A fragments.
+// W is [out][in] BF16 in shared memory with row stride ws (in 16-bit
+// units); A fragments of k-step k are afrag[k][4].
+template <int KT, int NT>
+__device__ inline void mlp_layer(const uint32_t (*afrag)[4], const uint16_t *W, int ws, const float *bias, int lane,
+                                 float (*c)[4]) {
+  const int g = lane >> 2, t4 = lane & 3;
+#pragma unroll
+  for (int nt = 0; nt < NT; ++nt) {
+    const float b0 = bias[nt * 8 + t4 * 2], b1 = bias[nt * 8 + t4 * 2 + 1];
+    c[nt][0] = b0;
+    c[nt][1] = b1;
+    c[nt][2] = b0;
+    c[nt][3] = b1;
+    const uint16_t *wr = W + (size_t)(nt * 8 + g) * ws + t4 * 2;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+      const uint32_t w0 = *reinterpret_cast<const uint32_t *>(wr + kt * 16);
+      const uint32_t w1 = *reinterpret_cast<const uint32_t *>(wr + kt * 16 + 8);
+      mma16816(c[nt], afrag[kt], w0, w1);
+    }
+  }
+}
+
+// C fragments of n-tiles 2k and 2k+1 (ReLU, BF16) are the A fragment of k-step k.
+template <int NT>
+__device__ inline void relu_to_a(const float (*c)[4], uint32_t (*afrag)[4]) {
+#pragma unroll
+  for (int k = 0; k < NT / 2; ++k) {
+    afrag[k][0] = bf2(fmaxf(c[2 * k][0], 0.f), fmaxf(c[2 * k][1], 0.f));
+    afrag[k][1] = bf2(fmaxf(c[2 * k][2], 0.f), fmaxf(c[2 * k][3], 0.f));
+    afrag[k][2] = bf2(fmaxf(c[2 * k + 1][0], 0.f), fmaxf(c[2 * k + 1][1], 0.f));
+    afrag[k][3] = bf2(fmaxf(c[2 * k + 1][2], 0.f), fmaxf(c[2 * k + 1][3], 0.f));
+  }
+}
+
+static constexpr int INF_W1S = ORD_NF + 8, INF_W2S = ORD_NH + 8;  // padded row strides (16-bit units)
+
+__global__ void __launch_bounds__(32 * INF_WARPS) k_order_infer(InferArgs a, int nbm) {
+  __shared__ __align__(16) uint16_t w1s[ORD_NH * INF_W1S], w2s[ORD_NH * INF_W2S], w3s[16 * INF_W2S];
+  __shared__ float bias[2 * ORD_NH + 16];
+  __shared__ __align__(16) uint16_t xs[INF_WARPS][INF_T][ORD_NF + 8];  // features, BF16, one row per tile
+  __shared__ float ys[INF_WARPS][INF_T][17];                          // outputs
+  __shared__ float thr_s[INF_WARPS][INF_T];
+  __shared__ uint8_t empty_s[INF_WARPS][INF_T];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  if ((int)blockIdx.y * INF_WARPS >= a.t.nslots[blockIdx.x]) return;  // nothing for this block
-  for (int e = tid; e < ORD_NH * ORD_NF; e += blockDim.x) {
-    const int j = e / ORD_NF, i = e % ORD_NF;
-    w1t[i * ORD_NH + j] = bf16r(a.params[ORD_W1 + e]);
-  }
-  for (int e = tid; e < ORD_NH * ORD_NH; e += blockDim.x) {
-    const int j = e / ORD_NH, i = e % ORD_NH;
-    w2t[i * ORD_NH + j] = bf16r(a.params[ORD_W2 + e]);
-  }
-  for (int e = tid; e < 16 * ORD_NH; e += blockDim.x) {
-    const int o = e / ORD_NH, i = e % ORD_NH;
-    w3t[i * 16 + o] = bf16r(a.params[ORD_W3 + e]);
-  }
+  for (int e = tid; e < ORD_NH * ORD_NF; e += blockDim.x)
+    w1s[(e / ORD_NF) * INF_W1S + e % ORD_NF] = __bfloat16_as_ushort(__float2bfloat16_rn(a.params[ORD_W1 + e]));
+  for (int e = tid; e < ORD_NH * ORD_NH; e += blockDim.x)
+    w2s[(e / ORD_NH) * INF_W2S + e % ORD_NH] = __bfloat16_as_ushort(__float2bfloat16_rn(a.params[ORD_W2 + e]));
+  for (int e = tid; e < 16 * ORD_NH; e += blockDim.x)
+    w3s[(e / ORD_NH) * INF_W2S + e % ORD_NH] = __bfloat16_as_ushort(__float2bfloat16_rn(a.params[ORD_W3 + e]));
   for (int e = tid; e < ORD_NH; e += blockDim.x) {
     bias[e] = a.params[ORD_B1 + e];
     bias[ORD_NH + e] = a.params[ORD_B2 + e];
   }
   if (tid < 16) bias[2 * ORD_NH + tid] = a.params[ORD_B3 + tid];
   __syncthreads();
-  const int b = blockIdx.x;
-  const int ns = a.t.nslots[b];
-  const size_t base = (size_t)b * 189;
   const double frms = *a.frms;
   const double pbar = a.n > 0 ? (double)(*a.nt_sum) / (double)a.n : 1.0;
   const float lmt = log10f((float)fmax(*a.t.mtot, 1e-300));
-  const float sd = (float)(a.emax * ldexp(1.0, -a.t.batches[b].z));
-  for (int i = blockIdx.y * INF_WARPS + warp; i < ns; i += INF_WARPS * gridDim.y) {
-    int q = a.p;
-    if (frms > 0.0) {
-      float f[ORD_NF];
-      int off, level;
-      tile_features(a.t, b, i, lane, f, off, level);
-      // layer 1: units lane and lane + 32
-      float h0 = bias[lane], h1 = bias[lane + 32];
+  const int g = lane >> 2, t4 = lane & 3;
+  for (int b = blockIdx.x; b < nbm; b += gridDim.x) {
+    const int ns = a.t.nslots[b];
+    const size_t base = (size_t)b * 189;
+    const float sd = (float)(a.emax * ldexp(1.0, -a.t.batches[b].z));
+    for (int i0 = warp * INF_T; i0 < ns; i0 += INF_WARPS * INF_T) {
+      const int nt = min(INF_T, ns - i0);
+      if (frms <= 0.0) {  // no budget yet (the system's first evaluation): every tile at p
+        if (lane < nt) {
+          const int K = (a.p + 1) * (a.p + 1);
+          a.slot_p16[base + i0 + lane] = (uint8_t)((K + 15) & ~15);
+        }
+        continue;
+      }
+      // features of the group's tiles, one row each (zero rows past the end)
+      for (int tt = 0; tt < INF_T; ++tt) {
+        float f[ORD_NF];
+        int off = 0, level = 0;
+        if (tt < nt) {
+          tile_features(a.t, b, i0 + tt, lane, f, off, level);
+        } else {
 #pragma unroll
-      for (int k = 0; k < ORD_NF; ++k) {
-        const float x = bf16r(f[k]);
-        h0 = fmaf(w1t[k * ORD_NH + lane], x, h0);
-        h1 = fmaf(w1t[k * ORD_NH + lane + 32], x, h1);
-      }
-      hs[warp][0][lane] = bf16r(fmaxf(h0, 0.f));
-      hs[warp][0][lane + 32] = bf16r(fmaxf(h1, 0.f));
-      __syncwarp();
-      float g0 = bias[ORD_NH + lane], g1 = bias[ORD_NH + lane + 32];
-#pragma unroll 8
-      for (int k = 0; k < ORD_NH; ++k) {
-        const float x = hs[warp][0][k];
-        g0 = fmaf(w2t[k * ORD_NH + lane], x, g0);
-        g1 = fmaf(w2t[k * ORD_NH + lane + 32], x, g1);
-      }
-      hs[warp][1][lane] = bf16r(fmaxf(g0, 0.f));
-      hs[warp][1][lane + 32] = bf16r(fmaxf(g1, 0.f));
-      __syncwarp();
-      float y = 0.f;
-      if (lane < ORD_NQ) {
-        y = bias[2 * ORD_NH + lane];
-        for (int k = 0; k < ORD_NH; ++k) y = fmaf(w3t[k * 16 + lane], hs[warp][1][k], y);
+          for (int k = 0; k < ORD_NF; ++k) f[k] = 0.f;
+        }
+        if (lane == 0) {
+#pragma unroll
+          for (int k = 0; k < ORD_NF; k += 2)
+            *reinterpret_cast<uint32_t *>(&xs[warp][tt][k]) = bf2(f[k], f[k + 1]);
+          const int dx = off % 7 - 3, dy = (off / 7) % 7 - 3, dz = off / 49 - 3;
+          const float ex = dx * a.t.ax * sd, ey = dy * a.t.ay * sd, ez = dz * a.t.az * sd;
+          const float R2 = ex * ex + ey * ey + ez * ez;
+          thr_s[warp][tt] = log10f(a.tol * (float)frms * R2 / (float)sqrt(pbar)) - lmt;
+          empty_s[warp][tt] = f[18] == 0.f;
+        }
       }
       __syncwarp();
-      // budget of this tile's offset
-      const int dx = off % 7 - 3, dy = (off / 7) % 7 - 3, dz = off / 49 - 3;
-      const float ex = dx * a.t.ax * sd, ey = dy * a.t.ay * sd, ez = dz * a.t.az * sd;
-      const float R2 = ex * ex + ey * ey + ez * ez;
-      const float thr = log10f(a.tol * (float)frms * R2 / (float)sqrt(pbar)) - lmt;
-      const unsigned ok = __ballot_sync(0xffffffffu, lane < ORD_NQ && ORD_QMIN + lane < a.p && y <= thr);
-      q = ok ? ORD_QMIN + __ffs(ok) - 1 : a.p;
-      if (f[18] == 0.f) q = ORD_QMIN;  // no pair in the tile
-    }
-    if (lane == 0) {
-      const int K = (q + 1) * (q + 1);
-      a.slot_p16[base + i] = (uint8_t)((K + 15) & ~15);
+      // the MLP on the 16 tiles
+      uint32_t a1[2][4];
+#pragma unroll
+      for (int kt = 0; kt < 2; ++kt) {
+        a1[kt][0] = *reinterpret_cast<const uint32_t *>(&xs[warp][g][kt * 16 + t4 * 2]);
+        a1[kt][1] = *reinterpret_cast<const uint32_t *>(&xs[warp][g + 8][kt * 16 + t4 * 2]);
+        a1[kt][2] = *reinterpret_cast<const uint32_t *>(&xs[warp][g][kt * 16 + t4 * 2 + 8]);
+        a1[kt][3] = *reinterpret_cast<const uint32_t *>(&xs[warp][g + 8][kt * 16 + t4 * 2 + 8]);
+      }
+      float c1[8][4];
+      mlp_layer<2, 8>(a1, w1s, INF_W1S, bias, lane, c1);
+      uint32_t a2[4][4];
+      relu_to_a<8>(c1, a2);
+      float c2[8][4];
+      mlp_layer<4, 8>(a2, w2s, INF_W2S, bias + ORD_NH, lane, c2);
+      uint32_t a3[4][4];
+      relu_to_a<8>(c2, a3);
+      float c3[2][4];
+      mlp_layer<4, 2>(a3, w3s, INF_W2S, bias + 2 * ORD_NH, lane, c3);
+#pragma unroll
+      for (int nt2 = 0; nt2 < 2; ++nt2) {
+        ys[warp][g][nt2 * 8 + t4 * 2] = c3[nt2][0];
+        ys[warp][g][nt2 * 8 + t4 * 2 + 1] = c3[nt2][1];
+        ys[warp][g + 8][nt2 * 8 + t4 * 2] = c3[nt2][2];
+        ys[warp][g + 8][nt2 * 8 + t4 * 2 + 1] = c3[nt2][3];
+      }
+      __syncwarp();
+      // each tile's order: the lowest q in 4..p-1 whose predicted error is within its budget, else p
+      if (lane < nt) {
+        int q = a.p;
+        for (int k = 0; k < ORD_NQ; ++k)
+          if (ORD_QMIN + k < a.p && ys[warp][lane][k] <= thr_s[warp][lane]) {
+            q = ORD_QMIN + k;
+            break;
+          }
+        if (empty_s[warp][lane]) q = ORD_QMIN;  // no pair in the tile
+        const int K = (q + 1) * (q + 1);
+        a.slot_p16[base + i0 + lane] = (uint8_t)((K + 15) & ~15);
+      }
+      __syncwarp();
     }
   }
 }
@@ -707,8 +791,8 @@ int order_probe_errors(const ProbeArgs &a, cudaStream_t st, int64_t &launches) {
 
 int order_infer(const InferArgs &a, int nbm, cudaStream_t st, int64_t &launches) {
   if (nbm <= 0) return FMM_OK;
-  // blocks (batch, y) take every gridDim.y-th group of INF_WARPS slots
-  k_order_infer<<<dim3(nbm, 8), 32 * INF_WARPS, 0, st>>>(a);
+  // persistent blocks: the weights are staged once per block
+  k_order_infer<<<std::min(nbm, 148 * 4), 32 * INF_WARPS, 0, st>>>(a, nbm);
   launches += 1;
   return cudaGetLastError() == cudaSuccess ? FMM_OK : FMM_ERR_CUDA;
 }

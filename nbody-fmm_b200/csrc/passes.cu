@@ -704,20 +704,21 @@ __global__ void k_p2p(P2PArgs a) {
 // deeper levels' interaction lists and the leaf level's near field would sum
 // in the uniform tree.  A colleague may hold millions of particles (a sparse
 // cell next to a dense clump), so the work is cut into items of at most
-// CL_CHUNK sources of B's concatenated colleague list, each one warp's job;
+// p2p_chunk sources of B's concatenated colleague list, each one warp's job;
 // items of one B add into the far-field accumulator with vector reductions.
 //
 // Precision: colleagues touch B, so pairs can be far closer than the cell
 // size.  Positions are taken relative to an origin inside B (its first
 // particle) in FP64 and split into FP32 hi + lo parts; a difference
 // (t_hi - s_hi) + (t_lo - s_lo) is then rounded once relative to itself, as
-// in the uniform near field.
-static constexpr int CL_CHUNK = 256;
+// in the uniform near field.  The chunk (sources per item) is a setting,
+// fmm_config.p2p_chunk, 256 by default.
+static constexpr int CL_CHUNK_DEFAULT = 256;
 
 // Number of items of each listed adaptive leaf (0 past the list's end), over
 // [0, ncell) so that the host needs no count.
 __global__ void k_colleague_count(const int *alist, const unsigned *acount, int ncell, const int *coll,
-                                  const int *pbeg, const int *pend, int ns, uint32_t *cnt) {
+                                  const int *pbeg, const int *pend, int ns, int chunk, uint32_t *cnt) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ncell) return;
   uint32_t items = 0;
@@ -728,7 +729,7 @@ __global__ void k_colleague_count(const int *alist, const unsigned *acount, int 
       const int C = coll[(int64_t)B * ns + s];
       if (C >= 0) S += pend[C] - pbeg[C];
     }
-    items = pend[B] > pbeg[B] ? (uint32_t)((S + CL_CHUNK - 1) / CL_CHUNK) : 0u;
+    items = pend[B] > pbeg[B] ? (uint32_t)((S + chunk - 1) / chunk) : 0u;
   }
   cnt[i] = items;
 }
@@ -752,7 +753,8 @@ __device__ inline void split_hi_lo(double d, float &hi, float &lo) {
 // a time through shared memory.
 template <int DIM, bool POT>
 __global__ void __launch_bounds__(256) k_colleague_sum(P2PArgs a, const int *alist, const int2 *items,
-                                                       const uint32_t *nitems, const double *xs, float4 *far) {
+                                                       const uint32_t *nitems, const double *xs, float4 *far,
+                                                       int chunk) {
   constexpr int NS = DIM == 3 ? 27 : 9;
   __shared__ float4 s_hi_all[8][32], s_lo_all[8][32];
   __shared__ int s_pref_all[8][NS + 1], s_cell_all[8][NS];
@@ -785,7 +787,7 @@ __global__ void __launch_bounds__(256) k_colleague_sum(P2PArgs a, const int *ali
     if (lane == 0) s_pref[0] = 0;
     __syncwarp();
     const int S = s_pref[ncoll];
-    const int f0 = item.y * CL_CHUNK, f1 = min(S, f0 + CL_CHUNK);
+    const int f0 = item.y * chunk, f1 = min(S, f0 + chunk);
     // B's own particles in the concatenation (the pairs j == i are skipped)
     const int bl = __ffs(__ballot_sync(0xffffffffu, C == B)) - 1;
     const int bend = __shfl_sync(0xffffffffu, x, bl), bbeg = bend - __shfl_sync(0xffffffffu, nc, bl);
@@ -1179,8 +1181,8 @@ __global__ void k_class_keys(const uint64_t *ckey, const int *cpbeg, const int *
   const uint64_t k = ((uint64_t)level << dim) | (ckey[g] & ((1u << dim) - 1));
   keys_all[out_off + i] = k;
   vals[out_off + i] = (uint32_t)g;
-  bool m2l = true;
-  if (direct_max > 0) {
+  bool m2l = !aflag || (aflag[g - cell0] & 1);  // with adaptive targets only targets (and their rows) count
+  if (m2l && direct_max > 0) {
     const int nc = 1 << dim, ns = dim == 3 ? 27 : 9;
     const long long nt = cpend[g] - cpbeg[g];
     const int *pc = ccoll + (int64_t)cparent[g] * ns;
@@ -1194,7 +1196,6 @@ __global__ void k_class_keys(const uint64_t *ckey, const int *cpbeg, const int *
       }
     }
   }
-  if (aflag && !(aflag[g - cell0] & 1)) m2l = false;
   keys_m2l[out_off + i] = m2l ? k : 255u;
 }
 
@@ -1526,28 +1527,6 @@ __global__ void k_order_table(int dim, int p, int margin, int n_slots, int per_l
   }
 }
 
-// Adaptive targets, per cell g (flag[g - cell0]): bit 0, a target: the root,
-// or a cell whose parent holds more than A particles (every ancestor then
-// does too, since a cell's particles are a subset of its parent's); bit 1,
-// an adaptive leaf: a target with at most A particles, or a leaf.  The
-// adaptive leaves are appended to alist, their count kept in *acount.
-__global__ void k_adaptive_flags(const int *pbeg, const int *pend, const int *parent, int cell0, int ncell,
-                                 int first1, int leaf_first, int A, uint8_t *flag, int *alist, unsigned *acount) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31;
-  const int g = cell0 + i;
-  bool is_leaf = false;
-  if (i < ncell) {
-    const bool tgt = g < first1 || pend[parent[g]] - pbeg[parent[g]] > A;
-    is_leaf = tgt && (pend[g] - pbeg[g] <= A || g >= leaf_first);
-    flag[i] = (uint8_t)((tgt ? 1 : 0) | (is_leaf ? 2 : 0));
-  }
-  const unsigned m = __ballot_sync(0xffffffffu, is_leaf);
-  unsigned base = 0;
-  if (lane == 0 && m) base = atomicAdd(acount, (unsigned)__popc(m));
-  base = __shfl_sync(0xffffffffu, base, 0);
-  if (is_leaf) alist[base + __popc(m & ((1u << lane) - 1u))] = g;
-}
-
 // Adaptive targets of one level for the direct far field: the cells with
 // flag bit 0 that can have direct pairs, appended to seg (warp-aggregated;
 // their order within the level is free), their count in *cnt.
@@ -1564,20 +1543,6 @@ __global__ void k_level_targets(const uint8_t *aflag, int cell0, int first, int 
   if (tgt) seg[base + __popc(m & ((1u << lane) - 1u))] = g;
 }
 
-// The adaptive-target flags of every cell of a built tree, root first
-// (fmm_tree_adaptive_flags): the kernel the force pass runs, into flag[],
-// with its list of adaptive leaves in list[0 .. ncell) and their count at
-// list[ncell].
-int adaptive_flags_of_tree(const Workspace &ws, const TreeState &t, int A, uint8_t *flag, int *list, cudaStream_t st) {
-  if (t.depth < 1 || t.n_cells <= 0) return FMM_ERR_INVALID_ARGUMENT;
-  CUDA_TRY(cudaMemsetAsync(list + t.n_cells, 0, sizeof(int), st));
-  k_adaptive_flags<<<cdiv(t.n_cells, 256), 256, 0, st>>>(ws.cell_pbeg, ws.cell_pend, ws.cell_parent, t.cell0,
-                                                          t.n_cells, t.level_off[1], t.level_off[t.depth], A, flag,
-                                                          list, (unsigned *)(list + t.n_cells));
-  CUDA_TRY(cudaGetLastError());
-  return FMM_OK;
-}
-
 // FP64 positions in leaf order: xs[i] = pos[perm[i]].
 __global__ void k_gather_pos(const double *pos, const uint32_t *perm, int64_t n, int dim, double *xs) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1592,7 +1557,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
                    const double *d_mass_g, int p, double eps2, double G,
                    const PassGeom &g, double *d_acc, double *d_pot, int m2l_mode, int64_t direct_max,
                    const OrderOpts &order, cudaStream_t st, fmm_stats &stats, cudaEvent_t *ev,
-                   int adaptive_leaf) {
+                   int adaptive_leaf, int p2p_chunk, int m2l_run) {
   const int dim = t.dim, D = t.depth, KS = ops.KS;
   const int64_t n = t.n;
   const bool want_pot = d_pot != nullptr;  // the potential is summed only when it is asked for
@@ -1642,12 +1607,10 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   const bool shortcut = dim == 3 && D >= 3;
   // adaptive targets (3D shortcut pass only): flags and the adaptive leaves
   const bool adaptive = shortcut && adaptive_leaf > 0;
-  if (adaptive) {
-    if (!eb.aflag.reserve(ncell) || !eb.alist.reserve((size_t)ncell + 1)) return FMM_ERR_OUT_OF_MEMORY;
-    CUDA_TRY(cudaMemsetAsync(eb.alist.ptr + ncell, 0, sizeof(int), st));
-    k_adaptive_flags<<<cdiv(ncell, TPB), TPB, 0, st>>>(ws.cell_pbeg, ws.cell_pend, ws.cell_parent, cell0, ncell,
-                                                        t.level_off[1], t.level_off[D], adaptive_leaf, eb.aflag.ptr,
-                                                        eb.alist.ptr, (unsigned *)(eb.alist.ptr + ncell));
+  if (adaptive && t.adaptive_leaf != adaptive_leaf) {  // not computed with the tree
+    if (!ws.reserve_adaptive(ncell)) return FMM_ERR_OUT_OF_MEMORY;
+    int rc = launch_adaptive_flags(ws, t, adaptive_leaf, ws.aflag, ws.alist, st);
+    if (rc) return rc;
     ws.launches += 1;
   }
   std::vector<int> lvl_b0(D + 2, 0), lvl_b1(D + 2, 0), m2l_b0(D + 2, 0), m2l_b1(D + 2, 0);
@@ -1665,7 +1628,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
       k_class_keys<<<cdiv(t.level_count[d], TPB), TPB, 0, st>>>(
           ws.cell_key, ws.cell_pbeg, ws.cell_pend, ws.cell_parent, ws.cell_coll, ws.cell_child, direct_max,
           t.level_off[d], t.level_count[d], d, dim, eb.ckey.ptr, eb.ckey_m2l.ptr, eb.cval.ptr,
-          t.level_off[d] - t.level_off[2], adaptive ? eb.aflag.ptr : nullptr, cell0);
+          t.level_off[d] - t.level_off[2], adaptive ? ws.aflag : nullptr, cell0);
     ws.launches += D - 1;
     CUDA_TRY(cudaMemsetAsync(eb.cls_count.ptr, 0, 512 * sizeof(uint32_t), st));
     uint64_t *kk = eb.ckey.ptr, *kk2 = eb.ckey_alt.ptr;
@@ -1754,6 +1717,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   ta.KS = KS;
   ta.P16 = P16;
   ta.err = ws.dev_err;
+  ta.run_slots = m2l_run;
 
   uint8_t *lact = nullptr, *needs = nullptr, *msrc = nullptr, *mmode = nullptr;
   if (shortcut) {
@@ -2116,6 +2080,7 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   // (timed with the downward pass)
   std::vector<unsigned> ntgt;
   uint32_t n_items = 0;
+  const int cl_chunk = p2p_chunk > 0 ? p2p_chunk : CL_CHUNK_DEFAULT;
   if (adaptive) {
     const int ncl = t.level_off[D] + t.level_count[D] - t.level_off[2];
     if (!eb.ftl.reserve((size_t)ncl + D + 2) || !eb.ccnt.reserve(2 * (size_t)ncell)) return FMM_ERR_OUT_OF_MEMORY;
@@ -2123,12 +2088,12 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     CUDA_TRY(cudaMemsetAsync(cnt, 0, sizeof(unsigned) * (D + 2), st));
     for (int d = 2; d <= D; ++d)
       k_level_targets<<<cdiv(t.level_count[d], TPB), TPB, 0, st>>>(
-          eb.aflag.ptr, cell0, t.level_off[d], t.level_count[d], ws.cell_pbeg, ws.cell_pend, direct_max,
+          ws.aflag, cell0, t.level_off[d], t.level_count[d], ws.cell_pbeg, ws.cell_pend, direct_max,
           any_fdirect, eb.ftl.ptr + (t.level_off[d] - t.level_off[2]), cnt + d);
-    const unsigned *acount = (const unsigned *)(eb.alist.ptr + ncell);
+    const unsigned *acount = (const unsigned *)(ws.alist + ncell);
     uint32_t *ccnt = eb.ccnt.ptr, *coff = eb.ccnt.ptr + ncell;
-    k_colleague_count<<<cdiv(ncell, TPB), TPB, 0, st>>>(eb.alist.ptr, acount, ncell, ws.cell_coll, ws.cell_pbeg,
-                                                         ws.cell_pend, dim == 3 ? 27 : 9, ccnt);
+    k_colleague_count<<<cdiv(ncell, TPB), TPB, 0, st>>>(ws.alist, acount, ncell, ws.cell_coll, ws.cell_pbeg,
+                                                         ws.cell_pend, dim == 3 ? 27 : 9, cl_chunk, ccnt);
     exclusive_scan(ws, ccnt, coff, ncell, cnt + D + 1, st);
     ws.launches += D;
     ntgt.assign(D + 2, 0u);
@@ -2234,8 +2199,10 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     const uint32_t *nit = (const uint32_t *)(eb.ftl.ptr + (t.level_off[D] + t.level_count[D] - t.level_off[2])) + D + 1;
     if (n_items > 0) {
       const int cgrid = (int)std::min<int64_t>(cdiv((int64_t)n_items * 32, TPB), 148 * 16);
-      if (want_pot) k_colleague_sum<3, true><<<cgrid, TPB, 0, st>>>(pa, eb.alist.ptr, eb.citems.ptr, nit, eb.xs.ptr, ws.far);
-      else k_colleague_sum<3, false><<<cgrid, TPB, 0, st>>>(pa, eb.alist.ptr, eb.citems.ptr, nit, eb.xs.ptr, ws.far);
+      if (want_pot) k_colleague_sum<3, true><<<cgrid, TPB, 0, st>>>(pa, ws.alist, eb.citems.ptr, nit, eb.xs.ptr, ws.far,
+                                                                  cl_chunk);
+      else k_colleague_sum<3, false><<<cgrid, TPB, 0, st>>>(pa, ws.alist, eb.citems.ptr, nit, eb.xs.ptr, ws.far,
+                                                                   cl_chunk);
     }
     k_far_output<3><<<cdiv(n, TPB), TPB, 0, st>>>(ws.far, t.d_perm, n, G, d_acc, d_pot, ws.dev_err);
     ws.launches += 3;

@@ -329,19 +329,46 @@ __global__ void k_make_parents(uint64_t *ckey, int *cpbeg, int *cpend, int *cpar
   if (j == nchild - 1 || flags[j + 1]) cpend[pi] = cpend[cbase + j];
 }
 
+// Adaptive targets, per cell g (flag[g - cell0]): bit 0, a target: the root,
+// or a cell whose parent holds more than A particles (every ancestor then
+// does too, since a cell's particles are a subset of its parent's); bit 1,
+// an adaptive leaf: a target with at most A particles, or a leaf.  The
+// adaptive leaves are appended to alist, their count kept in *acount.
+__global__ void k_adaptive_flags(const int *pbeg, const int *pend, const int *parent, int cell0, int ncell,
+                                 int first1, int leaf_first, int A, uint8_t *flag, int *alist, unsigned *acount) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31;
+  const int g = cell0 + i;
+  bool is_leaf = false;
+  if (i < ncell) {
+    const bool tgt = g < first1 || pend[parent[g]] - pbeg[parent[g]] > A;
+    is_leaf = tgt && (pend[g] - pbeg[g] <= A || g >= leaf_first);
+    flag[i] = (uint8_t)((tgt ? 1 : 0) | (is_leaf ? 2 : 0));
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, is_leaf);
+  unsigned base = 0;
+  if (lane == 0 && m) base = atomicAdd(acount, (unsigned)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (is_leaf) alist[base + __popc(m & ((1u << lane) - 1u))] = g;
+}
+
 // Colleagues (|delta| <= 1 on every axis, same level, self included) of the
 // cells of one level.  With c = 2P + b per axis (b the cell's child bit),
 // the neighbour at offset delta is child ((b + delta) mod 2) of the parent's
 // colleague at offset floor((b + delta) / 2), so each of the 3^dim slots is
 // two dependent loads and no key decoding.
+//
+// With adaptive targets (aflag set) only target cells get a row: nothing
+// reads the row of a cell that is no target (their parents' rows serve the
+// targets, and a target's parent is a target).
 __global__ void k_colleagues(const uint64_t *ckey, const int *cparent, const int *cchild, int *ccoll, int base,
-                             int count, int dim) {
+                             int count, int dim, const uint8_t *aflag, int cell0) {
   // blocks of 8 cells x ns slots, one thread per (cell, slot): consecutive
   // threads write consecutive slots
   const int nc = 1 << dim, ns = dim == 3 ? 27 : 9;
   const int ci = blockIdx.x * 8 + (int)threadIdx.x / ns, s = (int)threadIdx.x % ns;
   if (ci >= count) return;
   const int c = base + ci;
+  if (aflag && !(aflag[c - cell0] & 1)) return;
   const int b = (int)(ckey[c] & (uint64_t)(nc - 1));
   int pslot = 0, child = 0, mul = 1;
   for (int a = 0; a < dim; ++a) {
@@ -403,10 +430,21 @@ static int bit_width_u64(uint64_t v) {
   return w;
 }
 
+int launch_adaptive_flags(const Workspace &ws, const TreeState &t, int A, uint8_t *flag, int *list, cudaStream_t st) {
+  if (t.depth < 1 || t.n_cells <= 0) return FMM_ERR_INVALID_ARGUMENT;
+  CUDA_TRY(cudaMemsetAsync(list + t.n_cells, 0, sizeof(int), st));
+  k_adaptive_flags<<<cdiv(t.n_cells, 256), 256, 0, st>>>(ws.cell_pbeg, ws.cell_pend, ws.cell_parent, t.cell0,
+                                                          t.n_cells, t.level_off[1], t.level_off[t.depth], A, flag,
+                                                          list, (unsigned *)(list + t.n_cells));
+  CUDA_TRY(cudaGetLastError());
+  return FMM_OK;
+}
+
 int build_tree(Workspace &ws, TreeState &t, const double *d_pos, const double *d_mass, int64_t n, int dim,
-               int threshold, cudaStream_t st) {
+               int threshold, cudaStream_t st, int adaptive_leaf) {
   t.dim = dim;
   t.n = n;
+  t.adaptive_leaf = 0;
   const int Dmax = ((64 / dim) >> dim) << dim;  // tree.cpp:38
   const int TPB = 256;
   const int nbN = cdiv(n, TPB);
@@ -507,12 +545,24 @@ int build_tree(Workspace &ws, TreeState &t, const double *d_pos, const double *d
   // leaf children are -1
   k_fill_i32<<<cdiv((int64_t)nleaves * nc, TPB), TPB, 0, st>>>(ws.cell_child + (int64_t)lbase[D] * nc,
                                                                 (int64_t)nleaves * nc, -1);
+  // adaptive targets (3D trees of depth >= 3, as the force pass runs them):
+  // the flags now, so that only target cells get colleague rows
+  const uint8_t *aflag = nullptr;
+  if (adaptive_leaf > 0 && dim == 3 && D >= 3) {
+    if (!ws.reserve_adaptive(t.n_cells)) return FMM_ERR_OUT_OF_MEMORY;
+    int rc = launch_adaptive_flags(ws, t, adaptive_leaf, ws.aflag, ws.alist, st);
+    if (rc) return rc;
+    ws.launches += 1;
+    t.adaptive_leaf = adaptive_leaf;
+    aflag = ws.aflag;
+  }
   // colleagues, top-down
   k_root_colleague<<<1, 32, 0, st>>>(ws.cell_coll, lbase[0], dim);
   ws.launches += 2;
   for (int d = 1; d <= D; ++d) {
     k_colleagues<<<cdiv(t.level_count[d], 8), 8 * ns, 0, st>>>(ws.cell_key, ws.cell_parent, ws.cell_child,
-                                                                ws.cell_coll, lbase[d], t.level_count[d], dim);
+                                                                ws.cell_coll, lbase[d], t.level_count[d], dim, aflag,
+                                                                t.cell0);
     ws.launches += 1;
   }
   // particles in leaf order

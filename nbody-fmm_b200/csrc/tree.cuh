@@ -57,6 +57,8 @@ struct Workspace {
   // per cell
   DevBuf<uint64_t> bcell_key;
   DevBuf<int> bcell_pbeg, bcell_pend, bcell_parent, bcell_child, bcell_coll;
+  DevBuf<uint8_t> baflag;    // adaptive targets, per cell: bit 0 target, bit 1 adaptive leaf
+  DevBuf<int> balist;        // adaptive targets: the adaptive leaves, then their count
   // misc
   DevBuf<uint32_t> bscan, bhist;
   DevBuf<unsigned long long> bbox;
@@ -72,6 +74,8 @@ struct Workspace {
   float4 *part = nullptr, *part_lo = nullptr, *far = nullptr;
   uint64_t *cell_key = nullptr;
   int *cell_pbeg = nullptr, *cell_pend = nullptr, *cell_parent = nullptr, *cell_child = nullptr, *cell_coll = nullptr;
+  uint8_t *aflag = nullptr;
+  int *alist = nullptr;
   unsigned long long *box_u64 = nullptr;
   double *geom = nullptr;
   uint32_t *scalars = nullptr;
@@ -115,6 +119,12 @@ struct Workspace {
     cell_coll = bcell_coll.ptr;
     return ok;
   }
+  bool reserve_adaptive(int64_t ncell) {
+    ok &= baflag.reserve((size_t)ncell) && balist.reserve((size_t)ncell + 1);
+    aflag = baflag.ptr;
+    alist = balist.ptr;
+    return ok;
+  }
   uint32_t *scan_tmp(int nb) {
     ok &= bscan.reserve((size_t)nb);
     return bscan.ptr;
@@ -129,7 +139,7 @@ struct Workspace {
     bu32A.release(); bu32B.release(); bu32C.release();
     bleaf_of.release(); bpart.release(); bpart_lo.release(); bfar.release();
     bcell_key.release(); bcell_pbeg.release(); bcell_pend.release(); bcell_parent.release();
-    bcell_child.release(); bcell_coll.release();
+    bcell_child.release(); bcell_coll.release(); baflag.release(); balist.release();
     bscan.release(); bhist.release(); bbox.release(); bgeom.release(); bscalars.release(); berr.release(); bcount.release();
   }
 };
@@ -147,6 +157,8 @@ struct TreeState {
   std::vector<int> level_count, level_off;
   int cell0 = 0;      // index of the root
   int n_cells = 0;
+  int adaptive_leaf = 0;  // adaptive targets: the threshold ws.aflag / ws.alist were computed for (0: none, and
+                          // every cell has its colleague row; else only the target cells have one)
   uint64_t *d_leafkey_sorted = nullptr;
   uint32_t *d_perm = nullptr;  // leaf order -> input index
 };
@@ -156,6 +168,9 @@ void exclusive_scan(Workspace &ws, const uint32_t *in, uint32_t *out, int64_t n,
 void radix_sort(Workspace &ws, uint64_t *&keys, uint32_t *&vals, uint64_t *&keys_alt, uint32_t *&vals_alt, int64_t n,
                 int bits, cudaStream_t st);
 int build_tree(Workspace &ws, TreeState &t, const double *d_pos, const double *d_mass, int64_t n, int dim,
-               int threshold, cudaStream_t st);
+               int threshold, cudaStream_t st, int adaptive_leaf = 0);
+// Adaptive-target flags of every cell of a built tree into flag[0 .. n_cells)
+// and the adaptive leaves into list[0 .. count), count at list[n_cells].
+int launch_adaptive_flags(const Workspace &ws, const TreeState &t, int A, uint8_t *flag, int *list, cudaStream_t st);
 
 }  // namespace fmm

@@ -65,7 +65,8 @@ class FmmConfig(ctypes.Structure):
         ("eps2", ctypes.c_double), ("G", ctypes.c_double), ("device", ctypes.c_int32),
         ("direct_max", ctypes.c_int32), ("order_mode", ctypes.c_int32), ("order_margin", ctypes.c_int32),
         ("order_tol", ctypes.c_float), ("judge_samples", ctypes.c_int32), ("judge_budget", ctypes.c_float),
-        ("judge_every", ctypes.c_int32), ("adaptive_leaf", ctypes.c_int32),
+        ("judge_every", ctypes.c_int32), ("adaptive_leaf", ctypes.c_int32), ("p2p_chunk", ctypes.c_int32),
+        ("m2l_run", ctypes.c_int32),
     ]
 
 
@@ -84,11 +85,13 @@ class FmmStats(ctypes.Structure):
 class FmmTuneResult(ctypes.Structure):
     _fields_ = [("n_candidates", ctypes.c_int32), ("best", ctypes.c_int32), ("leaf_cap", ctypes.c_int32 * 16),
                 ("direct_max", ctypes.c_int32 * 16), ("ms", ctypes.c_double * 16),
-                ("adaptive_leaf", ctypes.c_int32 * 16)]
+                ("adaptive_leaf", ctypes.c_int32 * 16), ("p2p_chunk", ctypes.c_int32 * 16),
+                ("m2l_run", ctypes.c_int32 * 16)]
 
 
 FMM_TUNE_LEAF = 1
 FMM_TUNE_ADAPTIVE = 2
+FMM_TUNE_KERNELS = 4
 
 
 class FmmError(RuntimeError):
@@ -223,7 +226,7 @@ class Context:
 
     def __init__(self, dim=3, p=8, leaf_cap=64, m2l_mode=FMM_M2L_FP32, eps2=0.0, G=1.0, device=0, direct_max=-1,
                  order_mode=FMM_ORDER_FIXED, order_margin=1, order_tol=2e-6, judge_samples=0, judge_budget=1e-6,
-                 judge_every=1, order_model=None, adaptive_leaf=0):
+                 judge_every=1, order_model=None, adaptive_leaf=0, p2p_chunk=0, m2l_run=0):
         L = load_library()
         cfg = FmmConfig()
         _check(L.fmm_config_default(ctypes.byref(cfg)))
@@ -233,6 +236,7 @@ class Context:
         cfg.order_tol, cfg.judge_samples, cfg.judge_budget = order_tol, judge_samples, judge_budget
         cfg.judge_every = judge_every
         cfg.adaptive_leaf = adaptive_leaf
+        cfg.p2p_chunk, cfg.m2l_run = p2p_chunk, m2l_run
         h = _vp()
         _check(L.fmm_create(ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
@@ -377,19 +381,23 @@ class Context:
         _check(_lib.fmm_evaluate_batched(self._h, len(offsets) - 1, _p(offsets, _i64), pos_ptr, mass_ptr, acc_ptr,
                                          pot_ptr, workers))
 
-    def autotune(self, n, pos_ptr, mass_ptr, tune_leaf=False, stream=None, tune_adaptive=False):
-        """Times candidate direct-pair thresholds (and leaf capacities, and
-        adaptive-target thresholds) on the given system and keeps the fastest
-        (fmm_autotune).  Returns the candidates as a list of dicts and the
-        chosen one."""
+    def autotune(self, n, pos_ptr, mass_ptr, tune_leaf=False, stream=None, tune_adaptive=False,
+                 tune_kernels=False):
+        """Times candidate direct-pair thresholds (and leaf capacities,
+        adaptive-target thresholds and kernel shapes) on the given system and
+        keeps the fastest (fmm_autotune).  Returns the candidates as a list of
+        dicts and the chosen one."""
         r = FmmTuneResult()
-        flags = (FMM_TUNE_LEAF if tune_leaf else 0) | (FMM_TUNE_ADAPTIVE if tune_adaptive else 0)
+        flags = ((FMM_TUNE_LEAF if tune_leaf else 0) | (FMM_TUNE_ADAPTIVE if tune_adaptive else 0) |
+                 (FMM_TUNE_KERNELS if tune_kernels else 0))
         _check(_lib.fmm_autotune(self._h, n, pos_ptr, mass_ptr, flags, ctypes.byref(r), stream))
         cands = [{"leaf_cap": r.leaf_cap[i], "direct_max": r.direct_max[i], "adaptive_leaf": r.adaptive_leaf[i],
-                  "ms": r.ms[i]} for i in range(r.n_candidates)]
+                  "p2p_chunk": r.p2p_chunk[i], "m2l_run": r.m2l_run[i], "ms": r.ms[i]}
+                 for i in range(r.n_candidates)]
         best = cands[r.best]
         self.cfg.leaf_cap, self.cfg.direct_max = best["leaf_cap"], best["direct_max"]
         self.cfg.adaptive_leaf = best["adaptive_leaf"]
+        self.cfg.p2p_chunk, self.cfg.m2l_run = best["p2p_chunk"], best["m2l_run"]
         return cands, best
 
     # ---- learned pair orders

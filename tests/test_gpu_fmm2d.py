@@ -83,3 +83,32 @@ def test_two_d_edge_cases():
         a = c.evaluate(pos, m)
         d = c.direct(pos, m)
         assert rel_l2(a, d) < 1e-3
+
+
+def test_c3_full_size_error_vs_direct():
+    """The 2D configuration at its own size: N = 2^22 (half uniform in the
+    unit disk, half in 64 Gaussian clumps of sigma 0.005, log-normal masses,
+    seed 3), p = 16, leaf capacity 32, M2L on the tensor cores (3xBF16,
+    FP32 accumulation), with the automatic direct-pair rule.  Against the
+    FP64 direct sum on the GPU on 4096 sampled targets: relative L2 force
+    error <= 1e-6 (the reference's own 2D FMM on this clumped input is
+    1.5e-3 to 7.7e-3 off, so the direct sum is the judge)."""
+    torch = pytest.importorskip("torch")
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    n = 1 << 22
+    pos, m = workloads.disk_clumps_2d(n, seed=3)
+    tg = np.sort(np.random.default_rng(7).choice(n, 4096, replace=False)).astype(np.int64)
+    d_pos, d_m = torch.from_numpy(pos).to(dev), torch.from_numpy(m).to(dev)
+    d_tg = torch.from_numpy(tg).to(dev)
+    d_acc = torch.empty((n, 2), dtype=torch.float64, device=dev)
+    d_ref = torch.empty((len(tg), 2), dtype=torch.float64, device=dev)
+    with fmmgpu.Context(dim=2, p=16, leaf_cap=32, G=1.0, m2l_mode=fmmgpu.FMM_M2L_TC) as c:
+        c.direct_device(n, d_pos.data_ptr(), d_m.data_ptr(), len(tg), d_tg.data_ptr(), d_ref.data_ptr())
+        c.evaluate_device(n, d_pos.data_ptr(), d_m.data_ptr(), d_acc.data_ptr())
+        c.synchronize()
+        st = c.stats()
+    a = d_acc[d_tg].cpu().numpy()
+    ref = d_ref.cpu().numpy()
+    assert st["m2l_tiles"] > 0  # the tensor-core M2L ran
+    assert rel_l2(a, ref) < 1e-6
