@@ -4,7 +4,8 @@ direct sums.
     python -m fmmgpu.train_order [--out fmmgpu/order_model.npy] [--tiles 4096]
 
 For each training system (seeded Plummer spheres, Plummer mixtures and
-uniform cubes, none of them the benchmark's input) one fixed-order force
+uniform cubes, and 16M clustered mixtures of the benchmark's distribution
+with other seeds than its input's) one fixed-order force
 evaluation at p = 12 samples M2L tiles and measures, in FP64, the truncation
 error of every pair of every sampled tile at orders 4..12 against the pair's
 own direct sum (fmm_order_collect); a tile's label is the largest over its
@@ -27,31 +28,61 @@ sys.path.insert(0, os.path.dirname(HERE))
 import fmmgpu  # noqa: E402
 from fmmgpu import workloads  # noqa: E402
 
-SYSTEMS = [  # (generator, N, seed)
-    ("plummer", 1 << 20, 101), ("plummer", 1 << 19, 102), ("plummer", 1 << 18, 103), ("plummer", 1 << 20, 108),
-    ("plummer_mixture", 1 << 20, 104), ("plummer_mixture", 1 << 19, 105), ("plummer_mixture", 1 << 21, 109),
-    ("uniform3d", 1 << 19, 106), ("uniform3d", 1 << 18, 107), ("uniform3d", 1 << 20, 110),
+# (generator, N, seed, settings): smaller Plummer spheres, mixtures and
+# uniform cubes at leaf capacity 64, and the 16M clustered mixture's own
+# distribution (other seeds than the benchmark input's 5) at the settings the
+# autotuner keeps for it: leaf capacity 128, adaptive targets 32, direct-pair
+# threshold 1142.  The 16M systems take about ten minutes each: their
+# sampled pairs include large cells whose FP64 probe is long.
+C5 = dict(leaf_cap=128, adaptive_leaf=32, direct_max=1142)
+SYSTEMS = [
+    ("plummer", 1 << 20, 101, {}), ("plummer", 1 << 19, 102, {}), ("plummer", 1 << 18, 103, {}),
+    ("plummer", 1 << 20, 108, {}), ("plummer_mixture", 1 << 20, 104, {}), ("plummer_mixture", 1 << 19, 105, {}),
+    ("plummer_mixture", 1 << 21, 109, {}), ("uniform3d", 1 << 19, 106, {}), ("uniform3d", 1 << 18, 107, {}),
+    ("uniform3d", 1 << 20, 110, {}),
+    ("plummer_mixture", 1 << 24, 201, C5), ("plummer_mixture", 1 << 24, 202, C5),
 ]
+C5_TILES = 16384  # sampled tiles per 16M mixture
 
 
-def collect(torch, dev, p, tiles_per_system, seed0=1):
-    feats, labels = [], []
-    for gi, (gen, n, seed) in enumerate(SYSTEMS):
-        pos, m = workloads.WORKLOADS[gen](n, seed=seed)
-        d_pos = torch.from_numpy(pos).to(dev)
-        d_m = torch.from_numpy(m).to(dev)
-        d_f = torch.zeros((tiles_per_system, fmmgpu.FMM_ORDER_NFEAT), dtype=torch.float32, device=dev)
-        d_l = torch.zeros((tiles_per_system, fmmgpu.FMM_ORDER_NOUT), dtype=torch.float32, device=dev)
-        torch.cuda.synchronize()
-        with fmmgpu.Context(dim=3, p=p, leaf_cap=64, m2l_mode=fmmgpu.FMM_M2L_TC, G=1.0) as c:
-            c.order_collect(n, d_pos.data_ptr(), d_m.data_ptr(), tiles_per_system, seed0 + gi, d_f.data_ptr(),
-                            d_l.data_ptr())
-        f, l = d_f.cpu().numpy(), d_l.cpu().numpy()
+def collect(torch, dev, p, tiles_per_system, seed0=1, systems=None, save_dir=None):
+    """Samples tiles of every system; with save_dir, each system's tiles are
+    saved there as soon as they are collected (tiles_<index>.npz) and a
+    system whose file exists is loaded instead of collected again."""
+    feats, labels, c5 = [], [], []
+    pairs = 0
+    for gi, (gen, n, seed, kw) in enumerate(SYSTEMS):
+        if systems is not None and gi not in systems:
+            continue
+        path = os.path.join(save_dir, f"tiles_{gi}.npz") if save_dir else None
+        if path and os.path.exists(path):
+            z = np.load(path)
+            f, l = z["feat"], z["labels"]
+        else:
+            pos, m = workloads.WORKLOADS[gen](n, seed=seed)
+            d_pos = torch.from_numpy(pos).to(dev)
+            d_m = torch.from_numpy(m).to(dev)
+            nt = C5_TILES if kw else tiles_per_system
+            d_f = torch.zeros((nt, fmmgpu.FMM_ORDER_NFEAT), dtype=torch.float32, device=dev)
+            d_l = torch.zeros((nt, fmmgpu.FMM_ORDER_NOUT), dtype=torch.float32, device=dev)
+            torch.cuda.synchronize()
+            cfg = dict(leaf_cap=64)
+            cfg.update(kw)
+            with fmmgpu.Context(dim=3, p=p, m2l_mode=fmmgpu.FMM_M2L_TC, G=1.0, **cfg) as c:
+                c.order_collect(n, d_pos.data_ptr(), d_m.data_ptr(), nt, seed0 + gi, d_f.data_ptr(),
+                                d_l.data_ptr())
+            f, l = d_f.cpu().numpy(), d_l.cpu().numpy()
+            del d_pos, d_m
+            if path:
+                np.savez_compressed(path, feat=f, labels=l)
         ok = f[:, 18] > 0  # rows where the draw found a tile with pairs
         feats.append(f[ok])
         labels.append(l[ok])
-        print(f"  {gen} N={n}: {ok.sum()} tiles", flush=True)
-    return np.concatenate(feats), np.concatenate(labels)
+        c5.append(np.full(int(ok.sum()), bool(kw)))
+        npairs = int(np.rint(f[ok, 18] * 128).sum())  # feature 18: the tile's pair count / 128
+        pairs += npairs
+        print(f"  {gen} N={n} seed {seed} {kw or ''}: {ok.sum()} tiles, {npairs} pairs", flush=True)
+    return np.concatenate(feats), np.concatenate(labels), pairs, np.concatenate(c5)
 
 
 def main():
@@ -63,19 +94,28 @@ def main():
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--data", default=None, help="save the collected tiles (.npz) here")
+    ap.add_argument("--tiles-dir", default=None,
+                    help="keep each system's sampled tiles here as they are collected, and reuse them")
+    ap.add_argument("--systems", default=None, help="comma-separated indices into SYSTEMS (default: all)")
+    ap.add_argument("--collect-only", action="store_true", help="collect (into --tiles-dir) and stop")
     args = ap.parse_args()
     import torch
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     t0 = time.time()
-    feat, lab = collect(torch, dev, 12, args.tiles)
+    systems = None if args.systems is None else {int(x) for x in args.systems.split(",")}
+    if args.tiles_dir:
+        os.makedirs(args.tiles_dir, exist_ok=True)
+    feat, lab, npairs, is_c5 = collect(torch, dev, 12, args.tiles, systems=systems, save_dir=args.tiles_dir)
     t_col = time.time() - t0
+    if args.collect_only:
+        return
     if args.data:
         np.savez_compressed(args.data, feat=feat, labels=lab)
     rng = np.random.default_rng(args.seed)
     idx = rng.permutation(len(feat))
-    feat, lab = feat[idx], lab[idx]
+    feat, lab, is_c5 = feat[idx], lab[idx], is_c5[idx]
     nval = len(feat) // 10
     vf, vl, tf, tl = feat[:nval], lab[:nval], feat[nval:], lab[nval:]
     d_tf = torch.from_numpy(np.ascontiguousarray(tf)).to(dev)
@@ -102,18 +142,26 @@ def main():
     # order choice on held-out tiles at thresholds spanning the labels: the
     # fraction of tiles given at least the order their measured errors need,
     # and the mean order chosen against the mean order needed
-    suff = {}
-    for pct in (25, 50, 75):
-        thr = float(np.percentile(vl[:, 4], pct))
-        need = np.argmax(np.c_[vl <= thr, np.ones(n, bool)], axis=1)
-        pick = np.argmax(np.c_[pred <= thr, np.ones(n, bool)], axis=1)
-        suff[f"label(q=8) p{pct} = {thr:.2f}"] = {"sufficient": float(np.mean(pick >= need)),
-                                                  "mean_q_needed": float(need.mean() + 4),
-                                                  "mean_q_chosen": float(pick.mean() + 4)}
+    def sufficiency(rows):
+        out = {}
+        for pct in (25, 50, 75):
+            thr = float(np.percentile(vl[:, 4], pct))
+            need = np.argmax(np.c_[vl[rows] <= thr, np.ones(rows.sum(), bool)], axis=1)
+            pick = np.argmax(np.c_[pred[rows] <= thr, np.ones(rows.sum(), bool)], axis=1)
+            out[f"label(q=8) p{pct} = {thr:.2f}"] = {"sufficient": float(np.mean(pick >= need)),
+                                                     "mean_q_needed": float(need.mean() + 4),
+                                                     "mean_q_chosen": float(pick.mean() + 4)}
+        return out
+
+    suff = sufficiency(np.ones(n, bool))
+    vc5 = is_c5[:nval]
+    suff_c5 = sufficiency(vc5) if vc5.any() else {}
     np.save(args.out, params)
-    report = {"tiles": int(len(feat)), "train": int(len(tf)), "held_out": int(n),
+    report = {"tiles": int(len(feat)), "pairs": npairs, "pairs_16M_mixture": int(np.rint(feat[is_c5, 18] * 128).sum()),
+              "train": int(len(tf)), "held_out": int(n),
               "epochs": args.epochs, "loss_first": float(loss[0]), "loss_last": float(loss[-1]),
               "held_out_loss": float(d_loss.item()), "order_sufficient_fraction": suff,
+              "order_sufficient_fraction_16M_mixture": suff_c5, "held_out_16M_mixture": int(vc5.sum()),
               "collect_s": t_col, "train_s": t_train, "systems": SYSTEMS}
     with open(os.path.splitext(args.out)[0] + "_report.json", "w") as fh:
         json.dump(report, fh, indent=1)
