@@ -792,14 +792,13 @@ __global__ void __launch_bounds__(256) k_colleague_sum(P2PArgs a, const int *ali
     const int bl = __ffs(__ballot_sync(0xffffffffu, C == B)) - 1;
     const int bend = __shfl_sync(0xffffffffu, x, bl), bbeg = bend - __shfl_sync(0xffffffffu, nc, bl);
     const double ox = xs[DIM * (size_t)tb], oy = xs[DIM * (size_t)tb + 1], oz = DIM == 3 ? xs[DIM * (size_t)tb + 2] : 0.0;
-    // Gl lanes per target (any count, not only powers of two, so that up
-    // to 32 - Gl + 1 lanes are busy), 32 / Gl targets per round
     const int tp = nt < 32 ? nt : 32;
-    const int Gl = 32 / tp;
+    int Gl = 1;
+    while (Gl * 2 * tp <= 32) Gl *= 2;
     const int tpp = 32 / Gl;
     for (int t0 = 0; t0 < nt; t0 += tpp) {
       const int ti = t0 + lane / Gl, sub = lane % Gl;
-      const bool act = ti < nt && lane < tpp * Gl;
+      const bool act = ti < nt;
       const int me_i = tb + (act ? ti : 0);
       float thx, tlx, thy, tly, thz = 0.f, tlz = 0.f;
       split_hi_lo(xs[DIM * (size_t)me_i] - ox, thx, tlx);
@@ -836,17 +835,11 @@ __global__ void __launch_bounds__(256) k_colleague_sum(P2PArgs a, const int *ali
         }
         __syncwarp();
       }
-      // the group's sum into its first lane (shift-down tree within groups of Gl)
       for (int o = 1; o < Gl; o <<= 1) {
-        const float tx = __shfl_down_sync(0xffffffffu, ax, o), ty = __shfl_down_sync(0xffffffffu, ay, o);
-        const float tz = __shfl_down_sync(0xffffffffu, az, o);
-        const float tw = POT ? __shfl_down_sync(0xffffffffu, ph, o) : 0.f;
-        if (sub + o < Gl) {
-          ax += tx;
-          ay += ty;
-          az += tz;
-          if (POT) ph += tw;
-        }
+        ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        az += __shfl_xor_sync(0xffffffffu, az, o);
+        if (POT) ph += __shfl_xor_sync(0xffffffffu, ph, o);
       }
       if (act && sub == 0) red_add4(far + me_i, ax, ay, az, ph);
     }
