@@ -310,7 +310,7 @@ def run_ours(args, world, rank, local):
     # headline: the chosen M2L mode
     learned = args.order == "learned" and mode == fmmgpu.FMM_M2L_TC and dim == 3
     okw = dict(order_mode=fmmgpu.FMM_ORDER_LEARNED, judge_samples=args.judge, judge_budget=1e-6,
-               judge_every=args.judge_every) if learned else {}
+               judge_every=args.judge_every, order_tol=args.order_tol) if learned else {}
     # adaptive targets (3D): a fixed threshold, or by default 32 with the
     # autotuner trying 0 (the reference's uniform targets), 16 and 64 too
     tune_adaptive = dim == 3 and args.adaptive is None
@@ -433,6 +433,7 @@ def run_ours(args, world, rank, local):
 
     if learned:
         line["order"] = {"mode": "learned (M2L tile orders from the MLP in fmmgpu/order_model.npy)",
+                         "order_tol": args.order_tol,
                          "judge_samples": args.judge, "judge_budget": 1e-6, "judge_every": args.judge_every,
                          "fallbacks_in_timed_steps": int(sum(s["order_fallbacks"] for s in stats)),
                          "judged_in_timed_steps": int(sum(1 for s in stats if s["judge_rel_l2"] > 0)),
@@ -758,6 +759,8 @@ def main():
                     help="M2L tile orders (tensor-core mode): learned by the MLP, or fixed p")
     ap.add_argument("--judge", type=int, default=512, help="learned orders: targets checked against FP64 direct")
     ap.add_argument("--judge-every", type=int, default=8, help="learned orders: check every k-th evaluation")
+    ap.add_argument("--order-tol", type=float, default=2e-6,
+                    help="learned orders: relative L2 force budget of the reduced orders (fmm_config.order_tol)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ensemble", action="store_true", help="the batched-ensemble configuration instead")
