@@ -75,7 +75,7 @@ struct ExpBuffers {
   DevBuf<uint8_t> m2l_w;         // per M2L batch and present slot: padded width of its order
   DevBuf<int> m2l_split;         // variable orders: [4][batch][189] (lo slot, lo op, hi slot, hi op) + counts
   DevBuf<uint8_t> m2l_split_w;   // [2][batch][189] widths of the lo / hi lists
-  DevBuf<float> cf;              // learned orders: per-cell features (ORD_CF floats per cell)
+  DevBuf<uint16_t> cf;           // learned orders: per-cell features (ORD_CF BF16 values per cell)
   DevBuf<double> frms;           // learned orders: [0] F_rms of the previous pass (G = 1), [1] scratch,
                                  // [2] total mass
   DevBuf<int> ftl;               // adaptive targets: the direct far field's targets per level, then counts

@@ -18,14 +18,17 @@ namespace fmm {
 __device__ inline float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
 // ---------------------------------------------------------------- features
+// Cell features, ORD_CF values per cell stored as BF16 (32 bytes: one memory
+// sector, so the per-pair gathers of the tile features read one sector per
+// cell; the MLP rounds its inputs to BF16 in any case).
 __global__ void k_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int cell0,
-                                int p, int KS, const uint8_t *mode, float *cf) {
+                                int p, int KS, const uint8_t *mode, uint16_t *cf) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const int c = first + i;
   if (mode && !mode[c - cell0]) return;
   const float *m = M + (size_t)(c - cell0) * KS;
-  float *o = cf + (size_t)(c - cell0) * ORD_CF;
+  float o[ORD_CF];
   const float m0 = fabsf(m[0]);
   o[0] = log2f(1.f + (float)(pend[c] - pbeg[c]));
   for (int n = 1; n <= 12; ++n) {
@@ -39,6 +42,27 @@ __global__ void k_cell_features(const float *M, const int *pbeg, const int *pend
   }
   o[13] = m0 > 0.f ? log10f(m0) : -30.f;
   o[14] = o[15] = 0.f;
+  uint32_t w[ORD_CF / 2];
+#pragma unroll
+  for (int k = 0; k < ORD_CF / 2; ++k) {
+    const __nv_bfloat162 t = __floats2bfloat162_rn(o[2 * k], o[2 * k + 1]);
+    w[k] = *reinterpret_cast<const uint32_t *>(&t);
+  }
+  uint4 *dst = reinterpret_cast<uint4 *>(cf + (size_t)(c - cell0) * ORD_CF);
+  dst[0] = make_uint4(w[0], w[1], w[2], w[3]);
+  dst[1] = make_uint4(w[4], w[5], w[6], w[7]);
+}
+
+// The 16 BF16 features of a cell, as floats.
+__device__ inline void load_cf(const uint16_t *cf, float *f) {
+  const uint4 *src = reinterpret_cast<const uint4 *>(cf);
+  const uint4 a = src[0], b = src[1];
+  const uint32_t w[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    f[2 * k] = __uint_as_float(w[k] << 16);
+    f[2 * k + 1] = __uint_as_float(w[k] & 0xffff0000u);
+  }
 }
 
 __global__ void k_mass_total(const float4 *part, int64_t n, double *mtot) {
@@ -90,7 +114,9 @@ __device__ void tile_features(const TileArgs &a, int b, int i, int lane, float *
     const int S = a.src_tab[(base + sl) * 128 + r];
     if (S < 0) continue;
     const int T = a.tlist[bt.x + r];
-    const float *cT = a.cf + (size_t)(T - a.cell0) * ORD_CF, *cS = a.cf + (size_t)(S - a.cell0) * ORD_CF;
+    float cT[ORD_CF], cS[ORD_CF];
+    load_cf(a.cf + (size_t)(T - a.cell0) * ORD_CF, cT);
+    load_cf(a.cf + (size_t)(S - a.cell0) * ORD_CF, cS);
     mT = fmaxf(mT, cT[0]);
     mS = fmaxf(mS, cS[0]);
     sp1 = fmaxf(sp1, cT[1]);
@@ -748,7 +774,7 @@ int order_judge_compare(const double *acc, const double *ref, const int64_t *tar
 }
 
 int order_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int cell0, int p,
-                        int KS, const uint8_t *mode, float *cf, const float4 *part, int64_t n, double *mtot,
+                        int KS, const uint8_t *mode, uint16_t *cf, const float4 *part, int64_t n, double *mtot,
                         cudaStream_t st, int64_t &launches) {
   CUDA_TRY(cudaMemsetAsync(mtot, 0, sizeof(double), st));
   if (n > 0) {

@@ -45,7 +45,7 @@ struct OrderGeom {
 // formed (mode != 0), the others are left as they are.  Also the total mass
 // of the n particles `part` (mass in w) into *mtot.
 int order_cell_features(const float *M, const int *pbeg, const int *pend, int first, int count, int cell0, int p,
-                        int KS, const uint8_t *mode, float *cf, const float4 *part, int64_t n, double *mtot,
+                        int KS, const uint8_t *mode, uint16_t *cf, const float4 *part, int64_t n, double *mtot,
                         cudaStream_t st, int64_t &launches);
 
 // The resolved M2L tables and what the tile features read.
@@ -53,7 +53,7 @@ struct TileArgs {
   const int4 *batches;
   const int *tlist, *src_tab, *slot_list, *tslot_list, *nslots;
   const int *pbeg, *pend;
-  const float *cf;      // cell features
+  const uint16_t *cf;   // cell features (ORD_CF BF16 values per cell)
   const double *mtot;   // device: total mass
   int cell0;
   float ax, ay, az;     // cell aspect (extent / largest extent)

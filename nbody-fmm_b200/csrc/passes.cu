@@ -1049,7 +1049,7 @@ __device__ inline void blocked_shape(int nt, int R, int &Gl, float &cost) {
 }
 
 template <int DIM, bool POT, bool LIST = false>
-__global__ void __launch_bounds__(256, 3) k_direct_far(DirectArgs a) {
+__global__ void __launch_bounds__(256, 4) k_direct_far(DirectArgs a) {
   constexpr int NS = DIM == 3 ? 27 : 9, NC = 1 << DIM, NCAND = NS * NC, NR = (NCAND + 31) / 32;
   __shared__ float4 s_cell_all[8][189];
   __shared__ int s_pref_all[8][190];
