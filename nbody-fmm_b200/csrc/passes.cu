@@ -751,11 +751,114 @@ __device__ inline void split_hi_lo(double d, float &hi, float &lo) {
   lo = (float)(d - (double)hi);
 }
 
-// One warp per item (grid-stride): the targets of B in rounds of 32 / Gl
-// (Gl lanes per target share the sources), the item's sources staged 32 at
-// a time through shared memory.
+// One item's concatenated source range [f0, f1), B's own particles at
+// [bbeg, bend) in it, and the FP64 origin of the hi + lo offsets.
+struct CollChunk {
+  int f0, f1, bbeg, bend, ncoll;
+  double ox, oy, oz;
+};
+
+// Lanes per target group for R targets per lane (largest power of two with
+// ceil(nt / R) * Gl <= 32) and the work of the busiest lane per source:
+// rounds x (R pairs of about 19 instructions with the hi + lo differences,
+// and 4 for the two staged loads and the loop) / Gl.
+__device__ inline void colleague_shape(int nt, int R, int &Gl, float &cost) {
+  const int groups = (nt + R - 1) / R;
+  Gl = 1;
+  while (Gl * 2 * groups <= 32) Gl *= 2;
+  const int rounds = (groups + 32 / Gl - 1) / (32 / Gl);
+  cost = (float)rounds * (float)(19 * R + 4) / (float)Gl;
+}
+
+// The targets of B, R to a lane, in target groups of Gl lanes that share the
+// sources (every Gl-th of each chunk of 32 staged through shared memory).
+// Only chunks that hold some of B's own particles test for j == i.
+template <int R, int DIM, bool POT>
+__device__ void colleague_targets(const P2PArgs &a, const double *xs, float4 *far, int tb, int nt, int Gl,
+                                  const CollChunk &cc, const int *s_pref, const int *s_cell, float4 *s_hi,
+                                  float4 *s_lo, int lane) {
+  const int groups = (nt + R - 1) / R, gpr = 32 / Gl;
+  for (int g0 = 0; g0 < groups; g0 += gpr) {
+    const int gi = g0 + lane / Gl, sub = lane % Gl;
+    const bool live = gi < groups;
+    float thx[R], tlx[R], thy[R], tly[R], thz[R], tlz[R], ax[R], ay[R], az[R], ph[R];
+    int me[R];  // the target's particle index (target 0's for the lanes' padding)
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int ti = gi * R + r;
+      me[r] = tb + (live && ti < nt ? ti : 0);
+      split_hi_lo(xs[DIM * (size_t)me[r]] - cc.ox, thx[r], tlx[r]);
+      split_hi_lo(xs[DIM * (size_t)me[r] + 1] - cc.oy, thy[r], tly[r]);
+      thz[r] = tlz[r] = 0.f;
+      if (DIM == 3) split_hi_lo(xs[DIM * (size_t)me[r] + 2] - cc.oz, thz[r], tlz[r]);
+      ax[r] = ay[r] = az[r] = ph[r] = 0.f;
+    }
+    for (int fb = cc.f0; fb < cc.f1; fb += 32) {
+      const int f = fb + lane;
+      if (f < cc.f1) {
+        // colleague holding concatenated position f: the last k with s_pref[k] <= f
+        int lo = 0, hi = cc.ncoll - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (s_pref[mid] <= f) lo = mid;
+          else hi = mid - 1;
+        }
+        const int j = a.pbeg[s_cell[lo]] + (f - s_pref[lo]);
+        float hx, lx, hy, ly, hz = 0.f, lz = 0.f;
+        split_hi_lo(xs[DIM * (size_t)j] - cc.ox, hx, lx);
+        split_hi_lo(xs[DIM * (size_t)j + 1] - cc.oy, hy, ly);
+        if (DIM == 3) split_hi_lo(xs[DIM * (size_t)j + 2] - cc.oz, hz, lz);
+        s_hi[lane] = make_float4(hx, hy, hz, a.part[j].w);
+        s_lo[lane] = make_float4(lx, ly, lz, __int_as_float(j));
+      }
+      __syncwarp();
+      const int cnt = min(32, cc.f1 - fb);
+      if (fb < cc.bend && fb + cnt > cc.bbeg) {
+        for (int k = sub; k < cnt; k += Gl) {
+          const float4 q = s_hi[k], ql = s_lo[k];
+          const int j = __float_as_int(ql.w);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            if (j == me[r]) continue;
+            const float rx = (thx[r] - q.x) + (tlx[r] - ql.x);
+            const float ry = (thy[r] - q.y) + (tly[r] - ql.y);
+            const float rz = (thz[r] - q.z) + (tlz[r] - ql.z);
+            pair_acc<DIM, false, POT>(rx, ry, rz, q.w, a.eps2, ax[r], ay[r], az[r], ph[r]);
+          }
+        }
+      } else {
+        for (int k = sub; k < cnt; k += Gl) {
+          const float4 q = s_hi[k], ql = s_lo[k];
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            const float rx = (thx[r] - q.x) + (tlx[r] - ql.x);
+            const float ry = (thy[r] - q.y) + (tly[r] - ql.y);
+            const float rz = (thz[r] - q.z) + (tlz[r] - ql.z);
+            pair_acc<DIM, false, POT>(rx, ry, rz, q.w, a.eps2, ax[r], ay[r], az[r], ph[r]);
+          }
+        }
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      for (int o = 1; o < Gl; o <<= 1) {
+        ax[r] += __shfl_xor_sync(0xffffffffu, ax[r], o);
+        ay[r] += __shfl_xor_sync(0xffffffffu, ay[r], o);
+        az[r] += __shfl_xor_sync(0xffffffffu, az[r], o);
+        if (POT) ph[r] += __shfl_xor_sync(0xffffffffu, ph[r], o);
+      }
+      const int ti = gi * R + r;
+      if (sub == 0 && live && ti < nt) red_add4(far + tb + ti, ax[r], ay[r], az[r], ph[r]);
+    }
+  }
+}
+
+// One warp per item (grid-stride): B's targets R to a lane in groups of Gl
+// lanes (colleague_targets), the item's sources staged 32 at a time through
+// shared memory.
 template <int DIM, bool POT>
-__global__ void __launch_bounds__(256) k_colleague_sum(P2PArgs a, const int *alist, const int2 *items,
+__global__ void __launch_bounds__(256, 4) k_colleague_sum(P2PArgs a, const int *alist, const int2 *items,
                                                        const uint32_t *nitems, const double *xs, float4 *far,
                                                        int chunk) {
   constexpr int NS = DIM == 3 ? 27 : 9;
@@ -795,56 +898,26 @@ __global__ void __launch_bounds__(256) k_colleague_sum(P2PArgs a, const int *ali
     const int bl = __ffs(__ballot_sync(0xffffffffu, C == B)) - 1;
     const int bend = __shfl_sync(0xffffffffu, x, bl), bbeg = bend - __shfl_sync(0xffffffffu, nc, bl);
     const double ox = xs[DIM * (size_t)tb], oy = xs[DIM * (size_t)tb + 1], oz = DIM == 3 ? xs[DIM * (size_t)tb + 2] : 0.0;
-    const int tp = nt < 32 ? nt : 32;
-    int Gl = 1;
-    while (Gl * 2 * tp <= 32) Gl *= 2;
-    const int tpp = 32 / Gl;
-    for (int t0 = 0; t0 < nt; t0 += tpp) {
-      const int ti = t0 + lane / Gl, sub = lane % Gl;
-      const bool act = ti < nt;
-      const int me_i = tb + (act ? ti : 0);
-      float thx, tlx, thy, tly, thz = 0.f, tlz = 0.f;
-      split_hi_lo(xs[DIM * (size_t)me_i] - ox, thx, tlx);
-      split_hi_lo(xs[DIM * (size_t)me_i + 1] - oy, thy, tly);
-      if (DIM == 3) split_hi_lo(xs[DIM * (size_t)me_i + 2] - oz, thz, tlz);
-      float ax = 0.f, ay = 0.f, az = 0.f, ph = 0.f;
-      for (int fb = f0; fb < f1; fb += 32) {
-        const int f = fb + lane;
-        if (f < f1) {
-          // colleague holding concatenated position f: the last k with s_pref[k] <= f
-          int lo = 0, hi = ncoll - 1;
-          while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (s_pref[mid] <= f) lo = mid;
-            else hi = mid - 1;
-          }
-          const int j = a.pbeg[s_cell[lo]] + (f - s_pref[lo]);
-          float hx, lx, hy, ly, hz = 0.f, lz = 0.f;
-          split_hi_lo(xs[DIM * (size_t)j] - ox, hx, lx);
-          split_hi_lo(xs[DIM * (size_t)j + 1] - oy, hy, ly);
-          if (DIM == 3) split_hi_lo(xs[DIM * (size_t)j + 2] - oz, hz, lz);
-          s_hi[lane] = make_float4(hx, hy, hz, a.part[j].w);
-          s_lo[lane] = make_float4(lx, ly, lz, __int_as_float(j));
-        }
-        __syncwarp();
-        const int cnt = min(32, f1 - fb);
-        for (int k = sub; k < cnt; k += Gl) {
-          const float4 q = s_hi[k], ql = s_lo[k];
-          if (__float_as_int(ql.w) == me_i) continue;
-          const float rx = (thx - q.x) + (tlx - ql.x);
-          const float ry = (thy - q.y) + (tly - ql.y);
-          const float rz = (thz - q.z) + (tlz - ql.z);
-          pair_acc<DIM, false, POT>(rx, ry, rz, q.w, a.eps2, ax, ay, az, ph);
-        }
-        __syncwarp();
+    // the register blocking R in 1..4 with the least work on the busiest lane (larger R on ties)
+    int bestR = 1, bestG = 1;
+    float best = 1e30f;
+#pragma unroll
+    for (int R = 1; R <= 4; ++R) {
+      int G;
+      float c;
+      colleague_shape(nt, R, G, c);
+      if (c <= best) {
+        best = c;
+        bestR = R;
+        bestG = G;
       }
-      for (int o = 1; o < Gl; o <<= 1) {
-        ax += __shfl_xor_sync(0xffffffffu, ax, o);
-        ay += __shfl_xor_sync(0xffffffffu, ay, o);
-        az += __shfl_xor_sync(0xffffffffu, az, o);
-        if (POT) ph += __shfl_xor_sync(0xffffffffu, ph, o);
-      }
-      if (act && sub == 0) red_add4(far + me_i, ax, ay, az, ph);
+    }
+    const CollChunk cc{f0, f1, bbeg, bend, ncoll, ox, oy, oz};
+    switch (bestR) {
+      case 1: colleague_targets<1, DIM, POT>(a, xs, far, tb, nt, bestG, cc, s_pref, s_cell, s_hi, s_lo, lane); break;
+      case 2: colleague_targets<2, DIM, POT>(a, xs, far, tb, nt, bestG, cc, s_pref, s_cell, s_hi, s_lo, lane); break;
+      case 3: colleague_targets<3, DIM, POT>(a, xs, far, tb, nt, bestG, cc, s_pref, s_cell, s_hi, s_lo, lane); break;
+      default: colleague_targets<4, DIM, POT>(a, xs, far, tb, nt, bestG, cc, s_pref, s_cell, s_hi, s_lo, lane); break;
     }
     if (lane == 0) npairs += (long long)nt * (f1 - f0) - max(0, min(f1, bend) - max(f0, bbeg));
   }
