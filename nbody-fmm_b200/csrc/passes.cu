@@ -437,10 +437,15 @@ __device__ inline float2 lget(const float *Lr, int n, int m) {
 // evaluating it there gives the same field without the L2L chain.  Offsets
 // of the particles from level-d centres: `part` at the leaf level,
 // lvl_off[(d - 2) n + i] above.
-template <bool POT>
+//
+// P > 0: the order as a compile-time constant (P == p), so that the loops over
+// (l, m) unroll completely and every coefficient index and recurrence factor
+// is an immediate; P = 0 takes any p at run time.
+template <int P, bool POT>
 __global__ void k_l2p3d(const float4 *part, const int *leaf_of, int64_t n, int cell0, float inv_s, int p, int KS,
                         const float *L, float4 *far, const int *esrc, const uint8_t *elev, int leaf_first, int D,
                         const float4 *lvl_off, float inv_s0) {
+  if (P) p = P;
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float4 q = part[i];
@@ -460,6 +465,7 @@ __global__ void k_l2p3d(const float4 *part, const int *leaf_of, int64_t n, int c
   const float x = q.x * inv_s, y = q.y * inv_s, z = q.z * inv_s, r2 = x * x + y * y + z * z;
   float gx = 0.f, gy = 0.f, gz = 0.f, ph = 0.f;
   float dre = 1.f, dim_ = 0.f;
+#pragma unroll
   for (int m = 0; m <= p; ++m) {
     if (m > 0) {
       float h = -0.5f / m;
@@ -469,6 +475,7 @@ __global__ void k_l2p3d(const float4 *part, const int *leaf_of, int64_t n, int c
     }
     const float wm = m ? 2.f : 1.f;
     float p1re = dre, p1im = dim_, p2re = 0.f, p2im = 0.f;
+#pragma unroll
     for (int l = m; l <= p; ++l) {
       float cre, cim;
       if (l == m) {
@@ -498,6 +505,19 @@ __global__ void k_l2p3d(const float4 *part, const int *leaf_of, int64_t n, int c
     }
   }
   far[i] = make_float4(gx * inv_s * inv_s, gy * inv_s * inv_s, gz * inv_s * inv_s, ph * inv_s);
+}
+
+using L2P3dFn = void (*)(const float4 *, const int *, int64_t, int, float, int, int, const float *, float4 *, const int *,
+                         const uint8_t *, int, int, const float4 *, float);
+
+// The L2P instantiation for order p: unrolled for the orders the passes use
+// most (8: batched ensembles, 12: a 1e-6 force error), the generic one else.
+static L2P3dFn l2p3d_kernel(int p, bool pot) {
+  switch (p) {
+    case 8: return pot ? k_l2p3d<8, true> : k_l2p3d<8, false>;
+    case 12: return pot ? k_l2p3d<12, true> : k_l2p3d<12, false>;
+    default: return pot ? k_l2p3d<0, true> : k_l2p3d<0, false>;
+  }
 }
 
 // ------------------------------------------------------------------ 2D
@@ -1379,9 +1399,12 @@ static constexpr int P2M_WARPS = 4, P2M_KC = (FMM_MAX_P * FMM_MAX_P + 2 * FMM_MA
 
 // One particle's contributions w R~_l^m (real parts, then -imaginary parts
 // as the layout stores them) into a shared-memory row.
+template <int P>
 __device__ inline void p2m_row(float x, float y, float z, float w, int p, float *row) {
+  if (P) p = P;
   const float r2 = x * x + y * y + z * z;
   float dre = 1.f, dim_ = 0.f;
+#pragma unroll
   for (int m = 0; m <= p; ++m) {
     if (m > 0) {
       const float h = -0.5f / m;
@@ -1390,6 +1413,7 @@ __device__ inline void p2m_row(float x, float y, float z, float w, int p, float 
       dim_ = nim;
     }
     float p1re = dre, p1im = dim_, p2re = 0.f, p2im = 0.f;
+#pragma unroll
     for (int l = m; l <= p; ++l) {
       float cre, cim;
       if (l == m) {
@@ -1412,15 +1436,19 @@ __device__ inline void p2m_row(float x, float y, float z, float w, int p, float 
 
 // P2M of the mode-1 cells (their own particles at their own level, no M2M).
 // Persistent warps take the list 32 (8 or 16 for short lists) cells at a
-// time.  Consecutive cells of
-// at most 32 particles share 32-particle chunks; a larger cell takes chunks
-// of its own with a running sum.  In a chunk each lane writes the
-// contributions of one particle as a row of a shared-memory tile (odd
-// stride: conflict-free), then the lanes sum each cell's rows column by
-// column, in particle order, and store the cell's row once, padding
-// columns zero (no atomics, no reductions across lanes).
+// time.  Consecutive cells of at most 32 particles share 32-particle chunks;
+// a larger cell takes chunks of its own with a running sum.  In a chunk each
+// lane writes the contributions of one particle as a row of a shared-memory
+// tile (odd stride: conflict-free), then the lanes sum each cell's rows
+// column by column, in particle order, and store the cell's row once,
+// padding columns zero (no atomics, no reductions across lanes).  PO > 0:
+// the order as a compile-time constant (PO == a.p, the row loops unrolled);
+// PO = 0: any order.
+template <int PO>
 __global__ void __launch_bounds__(32 * P2M_WARPS) k_p2m_list(P2MListArgs a) {
   extern __shared__ float s_tile[];
+  // locals, not writes into a (which would copy the parameter block to local memory)
+  const int ord = PO ? PO : a.p, K = PO ? (PO + 1) * (PO + 1) : a.K;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   float *S = s_tile + (size_t)wib * 32 * a.rs;
   const unsigned total = *a.count;
@@ -1460,12 +1488,12 @@ __global__ void __launch_bounds__(32 * P2M_WARPS) k_p2m_list(P2MListArgs a) {
         for (int e0 = 0; e0 < nj; e0 += 32) {
           const int cnt = min(32, nj - e0);
           const float4 q = lane < cnt ? off[pbj + e0 + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
-          p2m_row(q.x * inv_s, q.y * inv_s, q.z * inv_s, q.w, a.p, S + lane * a.rs);
+          p2m_row<PO>(q.x * inv_s, q.y * inv_s, q.z * inv_s, q.w, ord, S + lane * a.rs);
           __syncwarp();
 #pragma unroll
           for (int t = 0; t < P2M_KC; ++t) {
             const int col = lane + 32 * t;
-            if (col < a.K)
+            if (col < K)
               for (int r = 0; r < cnt; ++r) acc[t] += S[r * a.rs + col];
           }
           __syncwarp();
@@ -1474,7 +1502,7 @@ __global__ void __launch_bounds__(32 * P2M_WARPS) k_p2m_list(P2MListArgs a) {
 #pragma unroll
         for (int t = 0; t < P2M_KC; ++t) {
           const int col = lane + 32 * t;
-          if (col < a.KS) mrow[col] = col < a.K ? acc[t] : 0.f;
+          if (col < a.KS) mrow[col] = col < K ? acc[t] : 0.f;
         }
         ++j;
         continue;
@@ -1493,7 +1521,7 @@ __global__ void __launch_bounds__(32 * P2M_WARPS) k_p2m_list(P2MListArgs a) {
       const int mpb = __shfl_sync(0xffffffffu, pb, myk), mlv = __shfl_sync(0xffffffffu, lv, myk);
       const float4 q = lane < used ? a.off[mlv][mpb + lane - s0] : make_float4(0.f, 0.f, 0.f, 0.f);
       const float inv_s = a.inv_s[mlv];
-      p2m_row(q.x * inv_s, q.y * inv_s, q.z * inv_s, q.w, a.p, S + lane * a.rs);
+      p2m_row<PO>(q.x * inv_s, q.y * inv_s, q.z * inv_s, q.w, ord, S + lane * a.rs);
       __syncwarp();
       for (int k = j; k <= j1; ++k) {
         const int r0 = __shfl_sync(0xffffffffu, P - n, k) - start, nk = __shfl_sync(0xffffffffu, n, k);
@@ -1501,7 +1529,7 @@ __global__ void __launch_bounds__(32 * P2M_WARPS) k_p2m_list(P2MListArgs a) {
         float *mrow = a.M + (size_t)(ck - a.cell0) * a.KS;
         for (int col = lane; col < a.KS; col += 32) {
           float v = 0.f;
-          if (col < a.K)
+          if (col < K)
             for (int r = r0; r < r0 + nk; ++r) v += S[r * a.rs + col];
           mrow[col] = v;
         }
@@ -1510,6 +1538,28 @@ __global__ void __launch_bounds__(32 * P2M_WARPS) k_p2m_list(P2MListArgs a) {
       j = j1 + 1;
     }
   }
+}
+
+// Launches k_p2m_list<P> with its dynamic shared memory (32 rows of rs
+// floats per warp), raising the instantiation's limit once per device.
+template <int P>
+static int launch_p2m_list(const P2MListArgs &pm, cudaStream_t st) {
+  const size_t psh = sizeof(float) * (size_t)P2M_WARPS * 32 * pm.rs;
+  {
+    static std::mutex mu;
+    static size_t attr[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return FMM_ERR_CUDA;
+    std::lock_guard<std::mutex> lk(mu);
+    if (attr[dev] < psh) {
+      CUDA_TRY(cudaFuncSetAttribute(k_p2m_list<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psh));
+      CUDA_TRY(cudaFuncSetAttribute(k_p2m_list<P>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                    cudaSharedmemCarveoutMaxShared));
+      attr[dev] = psh;
+    }
+  }
+  k_p2m_list<P><<<148 * 2, 32 * P2M_WARPS, psh, st>>>(pm);
+  return FMM_OK;
 }
 
 // ------------------------------------------------------------ L2L shortcut
@@ -1958,21 +2008,9 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
     pm.KS = KS;
     pm.rs = ops.K | 1;
     pm.M = eb.M.ptr;
-    const size_t psh = sizeof(float) * (size_t)P2M_WARPS * 32 * pm.rs;
-    {
-      static std::mutex mu;
-      static size_t attr[64] = {};
-      int dev = 0;
-      if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return FMM_ERR_CUDA;
-      std::lock_guard<std::mutex> lk(mu);
-      if (attr[dev] < psh) {
-        CUDA_TRY(cudaFuncSetAttribute(k_p2m_list, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psh));
-        CUDA_TRY(cudaFuncSetAttribute(k_p2m_list, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                      cudaSharedmemCarveoutMaxShared));
-        attr[dev] = psh;
-      }
-    }
-    k_p2m_list<<<148 * 2, 32 * P2M_WARPS, psh, st>>>(pm);
+    const int ps = p == 8 ? launch_p2m_list<8>(pm, st) : p == 12 ? launch_p2m_list<12>(pm, st)
+                                                                 : launch_p2m_list<0>(pm, st);
+    if (ps != FMM_OK) return ps;
   } else if (dim == 3) {
     k_p2m3d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.M.ptr);
   } else {
@@ -2182,9 +2220,10 @@ int run_fmm_passes(Workspace &ws, TreeState &t, OpTables &ops, ExpBuffers &eb, c
   }
   // L2P
   if (dim == 3)
-    (want_pot ? k_l2p3d<true> : k_l2p3d<false>)<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far,
-                                          shortcut ? eb.esrc.ptr : nullptr, shortcut ? eb.elev.ptr : nullptr,
-                                          t.level_off[D], D, eb.lvl_off.ptr, (float)(1.0 / emax));
+    l2p3d_kernel(p, want_pot)<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr,
+                                                           ws.far, shortcut ? eb.esrc.ptr : nullptr,
+                                                           shortcut ? eb.elev.ptr : nullptr, t.level_off[D], D,
+                                                           eb.lvl_off.ptr, (float)(1.0 / emax));
   else
     k_l2p2d<<<cdiv(n, TPB), TPB, 0, st>>>(ws.part, ws.leaf_of, n, cell0, inv_sD, p, KS, eb.L.ptr, ws.far);
   ws.launches += 1;
