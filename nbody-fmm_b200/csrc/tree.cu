@@ -7,9 +7,11 @@
 // floor(2^d * q) with q = (x - a) / (b - a) in FP64, because dividing by a
 // power of two commutes with IEEE rounding; so the key at depth d is the key
 // at D shifted right by dim*(D-d).  One radix sort of the D-keys then gives
-// the maximum leaf occupancy of any depth as a maximum run length, and a
-// second stable sort of the depth-d keys in input order reproduces the
-// reference's leaves with their particles in input order (tree.cpp:62-66).
+// the maximum leaf occupancy of any depth as a maximum run length.  The
+// reference's leaves with their particles in input order (tree.cpp:62-66)
+// are the runs of that order with each run put back in input order (a rank
+// count inside the leaf), or for leaves of more than 512 particles a second
+// stable sort of the depth-d keys in input order.
 #include <algorithm>
 #include <vector>
 
@@ -108,8 +110,11 @@ void exclusive_scan(Workspace &ws, const uint32_t *in, uint32_t *out, int64_t n,
 
 // ------------------------------------------------------------ radix sort
 static constexpr int RS_BLOCK = 256;
-static constexpr int RS_ROUNDS = 16;
+static constexpr int RS_ROUNDS = 8;
 static constexpr int RS_TILE = RS_BLOCK * RS_ROUNDS;
+// Largest leaf whose order k_leaf_order redoes in place (each particle counts
+// the smaller input indices of its leaf); larger leaves take the full sort.
+static constexpr int LEAF_ORDER_MAX = 512;
 
 __global__ void k_radix_hist(const uint64_t *keys, int64_t n, int shift, uint32_t *hist, int nb) {
   __shared__ uint32_t h[256];
@@ -124,42 +129,73 @@ __global__ void k_radix_hist(const uint64_t *keys, int64_t n, int shift, uint32_
   hist[(int64_t)threadIdx.x * nb + blockIdx.x] = h[threadIdx.x];
 }
 
-// Stable scatter: items are ranked in (round, warp, lane) order, which is
-// their input order inside the tile.
-__global__ void k_radix_scatter(const uint64_t *kin, const uint32_t *vin, uint64_t *kout, uint32_t *vout,
-                                int64_t n, int shift, const uint32_t *offs, int nb) {
-  __shared__ uint32_t s_off[256];
+// Stable scatter of one tile of RS_TILE items: items are ranked in (round,
+// warp, lane) order, which is their input order inside the tile, and placed
+// in shared memory in digit order; then consecutive threads write each
+// digit's run to its consecutive places in the output (coalesced stores).
+__global__ void __launch_bounds__(RS_BLOCK) k_radix_scatter(const uint64_t *kin, const uint32_t *vin, uint64_t *kout,
+                                                            uint32_t *vout, int64_t n, int shift, const uint32_t *offs,
+                                                            int nb) {
+  __shared__ uint64_t s_key[RS_TILE];
+  __shared__ uint32_t s_val[RS_TILE];
+  __shared__ uint32_t s_goff[256], s_tstart[256], s_run[256], s_warp[RS_BLOCK / 32];
   __shared__ uint32_t s_cnt[RS_BLOCK / 32][256];
   __shared__ uint32_t s_pre[RS_BLOCK / 32][256];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  s_off[tid] = offs[(int64_t)tid * nb + blockIdx.x];
-  int64_t base = (int64_t)blockIdx.x * RS_TILE;
+  const int64_t base = (int64_t)blockIdx.x * RS_TILE;
+  const int tile_n = (int)min((int64_t)RS_TILE, n - base);
+  s_goff[tid] = offs[(int64_t)tid * nb + blockIdx.x];  // the digit's first place in the output
+  s_run[tid] = 0;
+  s_tstart[tid] = 0;  // the tile's digit histogram first
+  __syncthreads();
+  uint64_t key[RS_ROUNDS];
+  uint32_t val[RS_ROUNDS], dig[RS_ROUNDS];
+#pragma unroll
+  for (int r = 0; r < RS_ROUNDS; ++r) {
+    const int k = r * RS_BLOCK + tid;
+    const bool valid = k < tile_n;
+    key[r] = valid ? kin[base + k] : 0ull;
+    val[r] = valid ? vin[base + k] : 0u;
+    dig[r] = valid ? (uint32_t)((key[r] >> shift) & 255u) : 256u + lane;  // invalid lanes: distinct, unused
+    if (valid) atomicAdd(&s_tstart[dig[r]], 1u);
+  }
+  __syncthreads();
+  uint32_t total;
+  const uint32_t ex = block_excl_scan(s_tstart[tid], s_warp, total);  // syncs after every thread read its count
+  s_tstart[tid] = ex;  // the digit's first place in the tile's digit order
   const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
   for (int r = 0; r < RS_ROUNDS; ++r) {
     for (int w = 0; w < RS_BLOCK / 32; ++w) s_cnt[w][tid] = 0;
     __syncthreads();
-    int64_t i = base + (int64_t)r * RS_BLOCK + tid;
-    bool valid = i < n;
-    uint64_t key = valid ? kin[i] : 0;
-    uint32_t d = valid ? (uint32_t)((key >> shift) & 255u) : 256u + lane;
-    uint32_t peers = __match_any_sync(0xffffffffu, d);
-    uint32_t rank = __popc(peers & lt);
+    const uint32_t d = dig[r];
+    const bool valid = d < 256u;
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t rank = __popc(peers & lt);
     if (valid && rank == 0) s_cnt[warp][d] = __popc(peers);
     __syncthreads();
     uint32_t run = 0;
     for (int w = 0; w < RS_BLOCK / 32; ++w) {
-      uint32_t c = s_cnt[w][tid];
+      const uint32_t c = s_cnt[w][tid];
       s_pre[w][tid] = run;
       run += c;
     }
     __syncthreads();
     if (valid) {
-      uint32_t pos = s_off[d] + s_pre[warp][d] + rank;
-      kout[pos] = key;
-      vout[pos] = vin[i];
+      const uint32_t lp = s_tstart[d] + s_run[d] + s_pre[warp][d] + rank;
+      s_key[lp] = key[r];
+      s_val[lp] = val[r];
     }
     __syncthreads();
-    s_off[tid] += run;
+    s_run[tid] += run;
+  }
+  __syncthreads();
+  for (int k = tid; k < tile_n; k += RS_BLOCK) {
+    const uint64_t kk = s_key[k];
+    const uint32_t d = (uint32_t)((kk >> shift) & 255u);
+    const uint32_t pos = s_goff[d] + ((uint32_t)k - s_tstart[d]);
+    kout[pos] = kk;
+    vout[pos] = s_val[k];
   }
 }
 
@@ -291,6 +327,27 @@ __global__ void k_run_max(const uint32_t *starts, const uint32_t *nruns, int64_t
     m = y > m ? y : m;
   }
   if ((threadIdx.x & 31) == 0) atomicMax(maxlen, m);
+}
+
+// The final particle order from the Dmax order.  A leaf is a run of equal
+// depth-D keys (the Dmax key shifted right by `shift`); inside it the final
+// order is the input order, i.e. the particles sorted by their input index
+// (vals), so each particle's place is its rank among its leaf's indices.
+// Runs come from the depth loop's last pass: exclusive scan idx of the run
+// flags, run starts, nruns runs.  The result equals the stable sort of the
+// depth-D keys from input order.
+__global__ void k_leaf_order(const uint64_t *keys, const uint32_t *vals, const uint32_t *flags, const uint32_t *idx,
+                             const uint32_t *starts, uint32_t nruns, int64_t n, int shift, uint64_t *lk,
+                             uint32_t *pv) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t L = idx[i] + flags[i] - 1u;  // this particle's run
+  const int64_t s = starts[L], e = L + 1u < nruns ? (int64_t)starts[L + 1u] : n;
+  const uint32_t v = vals[i];
+  int64_t r = 0;
+  for (int64_t j = s; j < e; ++j) r += vals[j] < v ? 1 : 0;
+  pv[s + r] = v;
+  lk[s + r] = shift >= 64 ? 0ull : keys[i] >> shift;
 }
 
 // Leaves: one per run of equal leaf keys in the sorted order.
@@ -470,7 +527,7 @@ int build_tree(Workspace &ws, TreeState &t, const double *d_pos, const double *d
 
   // depth loop, tree.cpp:43-69
   unsigned int max_n = (unsigned int)n;
-  unsigned int depth = 0;
+  unsigned int depth = 0, nruns = 0;
   uint32_t *flags = ws.u32A, *idx = ws.u32B, *starts = ws.u32C;
   do {
     uint64_t n_leafs = (uint64_t)(max_n - 1) / (unsigned)threshold + 1;
@@ -487,17 +544,27 @@ int build_tree(Workspace &ws, TreeState &t, const double *d_pos, const double *d
     CUDA_TRY(cudaMemcpyAsync(h, ws.scalars, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     max_n = h[1];
+    nruns = h[0];
   } while (depth < (unsigned)Dmax && max_n > (unsigned)threshold);
   t.depth = (int)depth;
   const int D = t.depth;
 
   // final order: stable sort of the depth-D leaf keys, starting from input
-  // order, so each leaf keeps its particles in input order (tree.cpp:62-66)
-  k_leafkeys_input<<<nbN, TPB, 0, st>>>(d_pos, n, dim, Dmax, D, ws.geom, ws.keyC, ws.valC);
-  ws.launches += 1;
+  // order, so each leaf keeps its particles in input order (tree.cpp:62-66).
+  // The depth-D key is the Dmax key shifted right, so the Dmax order already
+  // groups the leaves; with leaves of at most LEAF_ORDER_MAX particles only
+  // the order inside each leaf is redone (k_leaf_order), else the leaf keys
+  // are sorted afresh from input order.
   uint64_t *lk = ws.keyC, *lkAlt = ws.keyA;
   uint32_t *pv = ws.valC, *pvAlt = ws.valA;
-  radix_sort(ws, lk, pv, lkAlt, pvAlt, n, dim * D, st);
+  if (max_n <= (unsigned)LEAF_ORDER_MAX) {
+    k_leaf_order<<<nbN, TPB, 0, st>>>(kA, vA, flags, idx, starts, nruns, n, dim * (Dmax - D), lk, pv);
+    ws.launches += 1;
+  } else {
+    k_leafkeys_input<<<nbN, TPB, 0, st>>>(d_pos, n, dim, Dmax, D, ws.geom, ws.keyC, ws.valC);
+    ws.launches += 1;
+    radix_sort(ws, lk, pv, lkAlt, pvAlt, n, dim * D, st);
+  }
   t.d_leafkey_sorted = lk;
   t.d_perm = pv;
 
