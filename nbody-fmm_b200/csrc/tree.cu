@@ -440,6 +440,37 @@ __global__ void k_colleagues(const uint64_t *ckey, const int *cparent, const int
   ccoll[(int64_t)c * ns + s] = Q >= 0 ? cchild[(int64_t)Q * nc + child] : -1;
 }
 
+// The same rows with adaptive targets, one thread per cell: most cells of the
+// deep levels are no target and leave after one flag load, instead of 3^dim
+// threads each; a target's thread writes its 3^dim slots.
+template <int DIM>
+__global__ void k_colleagues_targets(const uint64_t *ckey, const int *cparent, const int *cchild, int *ccoll,
+                                     int base, int count, const uint8_t *aflag, int cell0) {
+  constexpr int NC = 1 << DIM, NS = DIM == 3 ? 27 : 9;
+  const int ci = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ci >= count) return;
+  const int c = base + ci;
+  if (!(aflag[c - cell0] & 1)) return;
+  const int b = (int)(ckey[c] & (uint64_t)(NC - 1));
+  const int *prow = ccoll + (int64_t)cparent[c] * NS;
+  int *row = ccoll + (int64_t)c * NS;
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    int pslot = 0, child = 0, mul = 1;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a) {
+      const int delta = (s / mul) % 3 - 1;
+      const int v = ((b >> a) & 1) + delta;  // in [-1, 2]
+      const int f = (v + 2) / 2 - 1;        // floor(v / 2)
+      pslot += (f + 1) * mul;
+      child |= (v - 2 * f) << a;
+      mul *= 3;
+    }
+    const int Q = prow[pslot];
+    row[s] = Q >= 0 ? cchild[(int64_t)Q * NC + child] : -1;
+  }
+}
+
 __global__ void k_root_colleague(int *ccoll, int root, int dim) {
   if (threadIdx.x == 0) {
     int ns = dim == 3 ? 27 : 9;
@@ -627,9 +658,13 @@ int build_tree(Workspace &ws, TreeState &t, const double *d_pos, const double *d
   k_root_colleague<<<1, 32, 0, st>>>(ws.cell_coll, lbase[0], dim);
   ws.launches += 2;
   for (int d = 1; d <= D; ++d) {
-    k_colleagues<<<cdiv(t.level_count[d], 8), 8 * ns, 0, st>>>(ws.cell_key, ws.cell_parent, ws.cell_child,
-                                                                ws.cell_coll, lbase[d], t.level_count[d], dim, aflag,
-                                                                t.cell0);
+    if (aflag)  // adaptive targets are 3D only
+      k_colleagues_targets<3><<<cdiv(t.level_count[d], TPB), TPB, 0, st>>>(
+          ws.cell_key, ws.cell_parent, ws.cell_child, ws.cell_coll, lbase[d], t.level_count[d], aflag, t.cell0);
+    else
+      k_colleagues<<<cdiv(t.level_count[d], 8), 8 * ns, 0, st>>>(ws.cell_key, ws.cell_parent, ws.cell_child,
+                                                                  ws.cell_coll, lbase[d], t.level_count[d], dim,
+                                                                  nullptr, t.cell0);
     ws.launches += 1;
   }
   // particles in leaf order
