@@ -316,7 +316,7 @@ def run_ours(args, world, rank, local):
     tune_adaptive = dim == 3 and args.adaptive is None
     adaptive = (32 if tune_adaptive else args.adaptive) if dim == 3 else 0
     ctx = fmmgpu.Context(dim=dim, p=p, leaf_cap=leaf, m2l_mode=mode, G=1.0, device=local, direct_max=args.direct_max,
-                         adaptive_leaf=adaptive, **okw)
+                         adaptive_leaf=adaptive, p2p_chunk=args.p2p_chunk, m2l_run=args.m2l_run, **okw)
     tune = None
     if args.autotune and args.direct_max < 0:
         # the autotuner picks the direct-pair threshold (and on the mixture the
@@ -769,6 +769,12 @@ def main():
                     help="adaptive targets (3D): cells under parents of at most this many particles are no targets "
                          "(0: the uniform targets of the reference); default: 32, tuned over {0, 16, 32, 64} with "
                          "the other settings")
+    ap.add_argument("--p2p-chunk", type=int, default=0,
+                    help="sources per colleague-sum work item (0: the library default; the autotuner's choice "
+                         "when it runs)")
+    ap.add_argument("--m2l-run", type=int, default=0,
+                    help="M2L offsets per tensor-core work item (0: the library default; the autotuner's choice "
+                         "when it runs)")
     ap.add_argument("--frames-every", type=int, default=0,
                     help="measure frame output instead: a device frame every K steps of the pass loop")
     args = ap.parse_args()
