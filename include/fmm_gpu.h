@@ -202,13 +202,15 @@ FMM_API int fmm_evaluate_batched(fmm_ctx *ctx, int32_t nsys, const int64_t *offs
    K^2/100, K^2/50 and K^2/12.5 at the best capacity (seven candidates).
    Every candidate keeps the configured adaptive_leaf; with FMM_TUNE_ADAPTIVE
    the values 0 (the uniform targets), 16, 32 and 64 are then tried at the
-   best candidate's leaf capacity and threshold; with FMM_TUNE_KERNELS the
-   kernel shapes last.  Adaptive targets change
+   best candidate's leaf capacity and threshold, then the best threshold
+   times 1/sqrt(2) and sqrt(2); with FMM_TUNE_KERNELS the kernel shapes last
+   (at most 16 candidates in all).  Adaptive targets change
    only which pairs are summed directly (exactly), not the expansions, so
    the candidates differ in time, not in truncation error.  Learned orders are tuned with them (every candidate is evaluated twice,
    the second timed).  result may be NULL.  Synchronous. */
 #define FMM_TUNE_LEAF 1
-#define FMM_TUNE_ADAPTIVE 2 /* then adaptive_leaf in {0, 16, 32, 64} at the best of the above */
+#define FMM_TUNE_ADAPTIVE 2 /* then adaptive_leaf in {0, 16, 32, 64} at the best of the above, and the
+                               threshold times 1/sqrt(2) and sqrt(2) at the best of those */
 #define FMM_TUNE_KERNELS 4  /* then the kernel shapes at the best of the above: p2p_chunk in {128, 512}
                                (with adaptive targets) and m2l_run in {24, 189} (tensor-core M2L) */
 typedef struct fmm_tune_result {

@@ -497,11 +497,18 @@ int fmm_autotune(fmm_ctx *c, int64_t n, const double *d_pos, const double *d_mas
   } else {
     for (double f : {0.125, 0.25, 0.5, 1.0, 2.0}) trial(saved.leaf_cap, threshold(f), al0, pc0, mr0);
   }
-  // then the adaptive-target threshold at the best leaf capacity and direct-pair threshold
+  // then the adaptive-target threshold at the best leaf capacity and
+  // direct-pair threshold, and the direct-pair threshold once more, a factor
+  // sqrt(2) either side of the best: the adaptive targets move the balance
+  // between direct pairs and M2L
   if ((flags & FMM_TUNE_ADAPTIVE) && !rc) {
-    const int b = res.best;
+    int b = res.best;
     for (int32_t al : {0, 16, 32, 64})
       if (al != al0) trial(res.leaf_cap[b], res.direct_max[b], al, pc0, mr0);
+    b = res.best;
+    const double dm = (double)res.direct_max[b];
+    for (double f : {0.70710678118654752, 1.41421356237309505})
+      trial(res.leaf_cap[b], (int32_t)std::max(8.0, dm * f), res.adaptive_leaf[b], pc0, mr0);
   }
   // then the kernel shapes: the colleague-sum chunk (adaptive targets) and
   // the tensor-core M2L work-item length (the batch shape)

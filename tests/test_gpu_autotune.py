@@ -72,6 +72,12 @@ def test_autotune_adaptive_and_kernel_shapes():
         a0 = c.evaluate(pos, m)
         cands, best = c.autotune(n, d_pos.data_ptr(), d_m.data_ptr(), tune_adaptive=True, tune_kernels=True)
         assert {0, 16, 64} <= {x["adaptive_leaf"] for x in cands}
+        # five thresholds, three more adaptive thresholds, then the best
+        # threshold of those times 1/sqrt(2) and sqrt(2)
+        b8 = cands[int(np.argmin([x["ms"] for x in cands[:8]]))]
+        assert [x["direct_max"] for x in cands[8:10]] == [
+            max(8, int(b8["direct_max"] * f)) for f in (0.70710678118654752, 1.41421356237309505)]
+        assert all(x["adaptive_leaf"] == b8["adaptive_leaf"] for x in cands[8:10])
         assert {128, 512} <= {x["p2p_chunk"] for x in cands} or best["adaptive_leaf"] == 0
         assert {24, 189} <= {x["m2l_run"] for x in cands}
         assert best["ms"] == min(x["ms"] for x in cands)
