@@ -1395,7 +1395,7 @@ struct P2MListArgs {
   int rs;                            // shared-memory row stride: K rounded up to odd
   float *M;
 };
-static constexpr int P2M_WARPS = 4, P2M_KC = (FMM_MAX_P * FMM_MAX_P + 2 * FMM_MAX_P + 4 + 31) / 32;
+static constexpr int P2M_WARPS = 5, P2M_KC = (FMM_MAX_P * FMM_MAX_P + 2 * FMM_MAX_P + 4 + 31) / 32;
 
 // One particle's contributions w R~_l^m (real parts, then -imaginary parts
 // as the layout stores them) into a shared-memory row.

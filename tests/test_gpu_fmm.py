@@ -101,6 +101,26 @@ def test_tree_matches_oracle(oracle, gen, n, T):
             assert tree_pairs_set(t, d, kind) == tree_pairs_set(o, d, kind), (d, kind)
 
 
+@pytest.mark.parametrize("nclump", [400, 700])
+def test_tree_dense_clump_matches_oracle(oracle, nclump):
+    """A clump of nclump particles inside one cell of the maximum depth: the
+    depth loop runs to depth 16 and that leaf holds all of them.  Up to 512
+    particles per leaf the Dmax order is put back in input order inside each
+    leaf; above that the leaf keys are sorted afresh from input order.  Both
+    paths must give the oracle's tree bit for bit."""
+    rng = np.random.default_rng(11)
+    pos = rng.random((3000, 3))
+    clump = 0.4 + 1e-7 * rng.random((nclump, 3))
+    pos = np.concatenate([pos, clump])[rng.permutation(3000 + nclump)]  # the clump spread over the input order
+    with fmmgpu.Context(dim=3, leaf_cap=16) as c:
+        t = c.tree(pos)
+    o = oracle.tree(pos, 16)
+    assert o["depth"] == 16 and int(np.diff(o["leaf_start"]).max()) == nclump
+    _assert_same_tree(t, o["depth"], o["leaf_keys"], o["leaf_start"], o["perm"])
+    for d in range(o["depth"] + 1):
+        np.testing.assert_array_equal(t["level_keys"][d], o["level_keys"][d])
+
+
 def test_direct_matches_oracle(oracle):
     pos, m = workloads.plummer(3000, seed=4)
     with fmmgpu.Context(dim=3, G=1.0) as c:
